@@ -1,0 +1,184 @@
+"""Python host layer over libwinoconv.so (the B200 Winograd conv2d library).
+
+Import with ``importlib.import_module("2024pra_conv_b200")`` (the directory
+name starts with a digit).  Everything here is a thin ctypes veneer over the
+C-ABI declared in include/conv2d.h and include/winoconv.h; device memory and
+streams come from torch.  There is no CPU path: if the compiled library is
+missing, import-time loading raises.
+
+Mirrors of the reference interface (reference include/conv2d.h:8-70):
+``Problem`` (problem_t), ``KernelInfo`` (kernelInfo_t), ``get_param_size``
+(getParamsize) and ``get_kernel_info`` (getkernelInfo) take the same fields
+and return the same codes as the C entry points.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libwinoconv.so")
+
+# Error codes of include/winoconv.h.
+WINO_OK, WINO_EINVAL, WINO_EUNSUPPORTED, WINO_ECUDA, WINO_EDEVICE = 0, 1, 2, 3, 4
+VAR_F16, VAR_BF16, VAR_F8, VAR_F16_HILO = 0, 1, 2, 3
+
+
+class WinoError(RuntimeError):
+    def __init__(self, code, what):
+        super().__init__(f"{what} failed with code {code}")
+        self.code = code
+
+
+class Problem(ctypes.Structure):
+    """problem_t (reference include/conv2d.h:8-27)."""
+    _fields_ = [("in_", ctypes.c_void_p), ("weight", ctypes.c_void_p), ("out", ctypes.c_void_p),
+                ("transform_pin", ctypes.c_void_p), ("transform_filter", ctypes.c_void_p),
+                ("mid_result", ctypes.c_void_p)] + [
+        (f, ctypes.c_uint) for f in ("n", "c", "h", "w", "k", "r", "s", "u", "v", "p", "q")]
+
+
+def _kernel_info_fields():
+    out = []
+    for i in range(1, 5):
+        out += [(f"{f}{i}", ctypes.c_uint) for f in
+                ("blockx", "blocky", "blockz", "threadx", "thready", "threadz", "dynmicLdsSize")]
+        out.append((f"kernelPtr{i}", ctypes.c_void_p))
+    return out
+
+
+class KernelInfo(ctypes.Structure):
+    """kernelInfo_t (reference include/conv2d.h:29-66)."""
+    _fields_ = _kernel_info_fields()
+
+    def slot(self, i):
+        g = lambda f: getattr(self, f"{f}{i}")
+        return dict(grid=(g("blockx"), g("blocky"), g("blockz")),
+                    block=(g("threadx"), g("thready"), g("threadz")),
+                    lds=g("dynmicLdsSize"), kernel=g("kernelPtr"))
+
+
+_lib = None
+
+
+def lib():
+    """The loaded library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(
+                f"{LIB_PATH} not built: run `python 2024pra_conv_b200/build.py` "
+                "(there is no fallback path)")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, i, sz = ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t
+        sigs = {
+            "wino_getParamsize": ([ctypes.POINTER(Problem), ctypes.POINTER(i)], i),
+            "wino_getkernelInfo": ([ctypes.POINTER(Problem), ctypes.POINTER(KernelInfo), vp], i),
+            "wino_check_shape": ([i, i, i, i, i], i),
+            "wino_ucache_bytes": ([i, i, i], sz),
+            "wino_filter_transform": ([vp, vp, i, i, vp], i),
+            "wino_conv2d_fused": ([vp, vp, vp, i, i, i, i, i, vp], i),
+            "wino_launch_kernelinfo": ([vp, vp, vp], i),
+            "wino_error_read_clear": ([ctypes.POINTER(ctypes.c_uint32)], i),
+        }
+        for name, (args, res) in sigs.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+def _check(code, what):
+    if code != WINO_OK:
+        raise WinoError(code, what)
+
+
+def _stream(stream=None):
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+# ------------------------------------------------------------ drop-in ABI ---
+def get_param_size(problem: Problem) -> int:
+    n = ctypes.c_int(0)
+    _check(lib().wino_getParamsize(ctypes.byref(problem), ctypes.byref(n)), "getParamsize")
+    return n.value
+
+
+def get_kernel_info(problem: Problem, param: ctypes.Array):
+    """Returns (code, KernelInfo); the code is returned, not raised, so tests
+    can check the rejection paths exactly as a C caller sees them."""
+    ki = KernelInfo()
+    code = lib().wino_getkernelInfo(ctypes.byref(problem), ctypes.byref(ki),
+                                    ctypes.cast(param, ctypes.c_void_p))
+    return code, ki
+
+
+def launch_kernel_info(ki: KernelInfo, param: ctypes.Array, stream=None):
+    _check(lib().wino_launch_kernelinfo(ctypes.byref(ki), ctypes.cast(param, ctypes.c_void_p),
+                                        _stream(stream)), "launch_kernelinfo")
+
+
+def make_problem(x, w, y, transform_pin=None, transform_filter=None, mid_result=None,
+                 r=3, s=3, u=1, v=1, p=1, q=1) -> Problem:
+    n, c, h, wd = x.shape
+    k = w.shape[0]
+    ptr = lambda t: 0 if t is None else t.data_ptr()
+    return Problem(ptr(x), ptr(w), ptr(y), ptr(transform_pin), ptr(transform_filter),
+                   ptr(mid_result), n, c, h, wd, k, r, s, u, v, p, q)
+
+
+def dropin_conv2d(x, w, stream=None):
+    """Run the drop-in path the way the reference harness does
+    (src/main.cpp:33-108): caller-allocated output and workspaces sized as
+    there, getParamsize, getkernelInfo, then the four launch slots."""
+    import torch
+    n, c, h, wd = x.shape
+    k = w.shape[0]
+    y = torch.empty((n, k, h, wd), dtype=torch.float16, device=x.device)
+    tf = torch.empty(16 * k * c, dtype=torch.float16, device=x.device)
+    pr = make_problem(x, w, y, None, tf, None)
+    size = get_param_size(pr)
+    param = (ctypes.c_char * size)()
+    code, ki = get_kernel_info(pr, param)
+    _check(code, "getkernelInfo")
+    launch_kernel_info(ki, param, stream)
+    return y
+
+
+# ------------------------------------------------------------ extension API -
+def ucache_bytes(k, c, variant=VAR_F16) -> int:
+    return int(lib().wino_ucache_bytes(k, c, variant))
+
+
+def filter_transform(w, stream=None):
+    """fp16 KCRS weights -> fp16 U cache (flat tensor, tile-major layout)."""
+    import torch
+    k, c = w.shape[:2]
+    u = torch.empty(16 * k * c, dtype=torch.float16, device=w.device)
+    _check(lib().wino_filter_transform(ctypes.c_void_p(w.data_ptr()), ctypes.c_void_p(u.data_ptr()),
+                                       k, c, _stream(stream)), "filter_transform")
+    return u
+
+
+def conv2d_fused(x, ucache, k, out=None, stream=None):
+    import torch
+    n, c, h, wd = x.shape
+    y = out if out is not None else torch.empty((n, k, h, wd), dtype=torch.float16, device=x.device)
+    _check(lib().wino_conv2d_fused(ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(ucache.data_ptr()),
+                                   ctypes.c_void_p(y.data_ptr()), n, c, h, wd, k, _stream(stream)),
+           "conv2d_fused")
+    return y
+
+
+def conv2d(x, w, stream=None):
+    """Filter transform followed by the fused conv (fp16 variant)."""
+    return conv2d_fused(x, filter_transform(w, stream), w.shape[0], stream=stream)
+
+
+def error_read_clear() -> int:
+    code = ctypes.c_uint32(0)
+    _check(lib().wino_error_read_clear(ctypes.byref(code)), "error_read_clear")
+    return code.value

@@ -1,0 +1,451 @@
+// Fused Winograd F(2x2,3x3) conv2d for sm_100a: input transform, the 16
+// per-tap channel GEMMs on tcgen05 tensor cores, and the output transform in
+// one persistent kernel.  Only the NCHW input, the cached U and the NKPQ
+// output touch global memory.
+//
+// Reference path replaced (reference files):
+//   input transform  B^T d B    src/preprocessing.cuh:273-424 (BTdB1/2/3)
+//   16 tap GEMMs                src/matrixmul.cuh:139-556 (matrixMul1/3/4/5/6)
+//   output transform A^T m A    src/conv2d.cpp:17-250 (store, store1..5)
+// which there run as three kernels with V and M round-tripping through HBM.
+//
+// Work unit ("block"): 128 consecutive Winograd tiles x 32 output channels.
+// The tensor core computes, per tap t,
+//     M_t[tile][k] = sum_c V_t[tile][c] * U_t[k][c]
+// as a 128 x 32 x 16 MMA per 16-channel step, accumulating in TMEM: lane =
+// tile, columns t*32 .. t*32+31 = output channels (16 taps x 32 = 512 cols).
+//
+// Warp roles (18 warps):
+//   warp 0       TMEM allocation; one thread issues the MMAs
+//   warp 1       one thread bulk-copies the U piece of each 16-channel step
+//   warps 2-9    V producers: B^T d B in packed fp16 straight into the
+//                MN-major shared-memory operand (8 tiles x 8 channels per
+//                core matrix), two stages deep
+//   warps 10-17  epilogue: drain TMEM tap by tap (each drained tap is handed
+//                back to the MMA thread at once, so the next block's MMAs
+//                overlap the drain), A^T m A in fp32, fp16 NKPQ stores.
+#include <cuda_runtime.h>
+#include "tc_sm100.cuh"
+#include "wino_common.cuh"
+
+namespace wino {
+
+static __device__ uint32_t g_fused_err;
+
+namespace fused {
+
+constexpr int TILES = 128;             // MMA M: tiles per block
+constexpr int NTAP = 16;
+constexpr int V_TAP_BYTES = TILES * 16 * 2;          // 4 KB per tap per step
+constexpr int V_STAGE_BYTES = NTAP * V_TAP_BYTES;    // 64 KB
+constexpr int U_STAGE_BYTES = NTAP * KB * 16 * 2;    // 16 KB (full k-block)
+constexpr int STAGE_BYTES = V_STAGE_BYTES + U_STAGE_BYTES;
+constexpr int NSTAGE = 2;
+constexpr int NWARP = 18;
+constexpr int NTHREAD = NWARP * 32;
+constexpr int WARP_MMA = 0, WARP_U = 1, WARP_V0 = 2, NWARP_V = 8, WARP_E0 = 10, NWARP_E = 8;
+constexpr int SMEM_BYTES = NSTAGE * STAGE_BYTES + 1024;
+
+struct Shared {
+  uint64_t full[NSTAGE];
+  uint64_t empty[NSTAGE];
+  uint64_t accf;
+  uint64_t tapfree[NTAP];
+  uint32_t tmem_base;
+  int abort_flag;
+};
+
+struct Geometry {
+  int N, C, H, W, K, P, Q, TP, TQ;
+  long long NT;         // tiles in the batch
+  int nTB, nKB, CS;     // tile blocks, k blocks, 16-channel steps
+  long long nblocks;
+};
+
+__device__ __forceinline__ Geometry make_geometry(const KernelParam& p) {
+  Geometry g;
+  g.N = p.n; g.C = p.c; g.H = p.h; g.W = p.w; g.K = p.k;
+  g.P = p.Oh; g.Q = p.Ow;
+  g.TP = (g.P + 1) >> 1; g.TQ = (g.Q + 1) >> 1;
+  g.NT = (long long)g.N * g.TP * g.TQ;
+  g.nTB = (int)((g.NT + TILES - 1) / TILES);
+  g.nKB = (g.K + KB - 1) / KB;
+  g.CS = g.C >> 4;
+  g.nblocks = (long long)g.nTB * g.nKB;
+  return g;
+}
+
+// ---- input words ------------------------------------------------------------
+// A "word" is two horizontally adjacent fp16 inputs (cols 2m, 2m+1) of one row,
+// zero outside the image.  `row` points at column 0 of the row (or is null
+// for a row outside the image).
+__device__ __forceinline__ uint32_t load_word(const __half* row, int m, int W, bool w_even) {
+  if (!row) return 0u;
+  const int c0 = 2 * m;
+  if (w_even) {
+    if (m < 0 || c0 >= W) return 0u;
+    return __ldg(reinterpret_cast<const unsigned int*>(row) + m);
+  }
+  const unsigned short* r16 = reinterpret_cast<const unsigned short*>(row);
+  uint32_t lo = (c0 >= 0 && c0 < W) ? (uint32_t)__ldg(r16 + c0) : 0u;
+  uint32_t hi = (c0 + 1 >= 0 && c0 + 1 < W) ? (uint32_t)__ldg(r16 + c0 + 1) : 0u;
+  return lo | (hi << 16);
+}
+
+__device__ __forceinline__ uint32_t hadd2(uint32_t a, uint32_t b) {
+  __half2 r = __hadd2(*reinterpret_cast<__half2*>(&a), *reinterpret_cast<__half2*>(&b));
+  return *reinterpret_cast<uint32_t*>(&r);
+}
+__device__ __forceinline__ uint32_t hsub2(uint32_t a, uint32_t b) {
+  __half2 r = __hsub2(*reinterpret_cast<__half2*>(&a), *reinterpret_cast<__half2*>(&b));
+  return *reinterpret_cast<uint32_t*>(&r);
+}
+// (hi(x), hi(y)) and (lo(x), lo(y)) packed as (low half, high half).
+__device__ __forceinline__ uint32_t pk_hi(uint32_t x, uint32_t y) { return __byte_perm(x, y, 0x7632); }
+__device__ __forceinline__ uint32_t pk_lo(uint32_t x, uint32_t y) { return __byte_perm(x, y, 0x5410); }
+
+// B^T rows as word operations: e_a = sum_i Bt[a][i] d_i.
+__device__ __forceinline__ uint32_t bt_row(int a, uint32_t d0, uint32_t d1, uint32_t d2, uint32_t d3) {
+  switch (a) {
+    case 0: return hsub2(d0, d2);
+    case 1: return hadd2(d1, d2);
+    case 2: return hsub2(d2, d1);
+    default: return hsub2(d1, d3);
+  }
+}
+
+// Column half of the transform for one e-row and a pair of tiles whose window
+// columns (a0..a3) are given as lane pairs: V[a][b] for b = 0..3.
+__device__ __forceinline__ void bt_cols(uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                        uint32_t v[4]) {
+  v[0] = hsub2(a0, a2);
+  v[1] = hadd2(a1, a2);
+  v[2] = hsub2(a2, a1);
+  v[3] = hsub2(a1, a3);
+}
+
+// Produce V for 8 consecutive tiles (tile0 .. tile0+7) of channel c, all 16
+// taps, into shared memory: for tap t the 16 bytes at dst + t*V_TAP_BYTES.
+// Each e-row a (taps 4a..4a+3) is stored as soon as it is formed.
+// Fast path: all 8 tiles in one tile row and W even (word loads).
+__device__ __forceinline__ void produce_v8(const __half* __restrict__ X, const Geometry& g,
+                                           long long tile0, int c, uint32_t dst) {
+  const bool w_even = (g.W & 1) == 0;
+  const long long per_img = (long long)g.TP * g.TQ;
+  bool fast = false;
+  int n0 = 0, ty0 = 0, tx0 = 0;
+  if (tile0 + 7 < g.NT) {
+    n0 = (int)(tile0 / per_img);
+    const int r = (int)(tile0 - (long long)n0 * per_img);
+    ty0 = r / g.TQ;
+    tx0 = r - ty0 * g.TQ;
+    fast = w_even && (tx0 + 7 < g.TQ);
+  }
+  if (fast) {
+    const __half* plane = X + ((size_t)n0 * g.C + c) * (size_t)g.H * g.W;
+    uint32_t d[4][10];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int y = 2 * ty0 - 1 + i;
+      const __half* row = (y >= 0 && y < g.H) ? plane + (size_t)y * g.W : nullptr;
+#pragma unroll
+      for (int j = 0; j < 10; ++j) d[i][j] = load_word(row, tx0 - 1 + j, g.W, true);
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      uint32_t e[10];
+#pragma unroll
+      for (int j = 0; j < 10; ++j) e[j] = bt_row(a, d[0][j], d[1][j], d[2][j], d[3][j]);
+      uint32_t out[4][4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int u = 2 * q;
+        uint32_t v[4];
+        bt_cols(pk_hi(e[u], e[u + 1]), pk_lo(e[u + 1], e[u + 2]), pk_hi(e[u + 1], e[u + 2]),
+                pk_lo(e[u + 2], e[u + 3]), v);
+#pragma unroll
+        for (int b = 0; b < 4; ++b) out[b][q] = v[b];
+      }
+#pragma unroll
+      for (int b = 0; b < 4; ++b)
+        st_shared_v4(dst + (4 * a + b) * V_TAP_BYTES, out[b][0], out[b][1], out[b][2], out[b][3]);
+    }
+  } else {
+    // General path: each tile locates its own window (row or image changes
+    // inside the group, odd widths, tiles past the end of the batch).  Per
+    // e-row only the two input rows that B^T combines are read.
+    const __half* plane[8];
+    int tyv[8], txv[8];
+#pragma unroll
+    for (int s = 0; s < 8; ++s) {
+      const long long tile = tile0 + s;
+      if (tile < g.NT) {
+        const int n = (int)(tile / per_img);
+        const int r = (int)(tile - (long long)n * per_img);
+        tyv[s] = r / g.TQ;
+        txv[s] = r - tyv[s] * g.TQ;
+        plane[s] = X + ((size_t)n * g.C + c) * (size_t)g.H * g.W;
+      } else {
+        plane[s] = nullptr;
+        tyv[s] = 0;
+        txv[s] = 0;
+      }
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      // rows combined by Bt[a]: (0,2), (1,2), (2,1), (1,3) as (plus, minus / plus)
+      const int ra = (a == 0) ? 0 : (a == 2 ? 2 : 1);
+      const int rb = (a == 0) ? 2 : (a == 3 ? 3 : (a == 1 ? 2 : 1));
+      uint32_t ew[8][3];
+#pragma unroll
+      for (int s = 0; s < 8; ++s) {
+        const int ya = 2 * tyv[s] - 1 + ra, yb = 2 * tyv[s] - 1 + rb;
+        const __half* rowa = (plane[s] && ya >= 0 && ya < g.H) ? plane[s] + (size_t)ya * g.W : nullptr;
+        const __half* rowb = (plane[s] && yb >= 0 && yb < g.H) ? plane[s] + (size_t)yb * g.W : nullptr;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          const uint32_t wa = load_word(rowa, txv[s] - 1 + j, g.W, w_even);
+          const uint32_t wb = load_word(rowb, txv[s] - 1 + j, g.W, w_even);
+          ew[s][j] = (a == 1) ? hadd2(wa, wb) : hsub2(wa, wb);
+        }
+      }
+      uint32_t out[4][4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int s0 = 2 * q, s1 = 2 * q + 1;
+        uint32_t v[4];
+        bt_cols(pk_hi(ew[s0][0], ew[s1][0]), pk_lo(ew[s0][1], ew[s1][1]), pk_hi(ew[s0][1], ew[s1][1]),
+                pk_lo(ew[s0][2], ew[s1][2]), v);
+#pragma unroll
+        for (int b = 0; b < 4; ++b) out[b][q] = v[b];
+      }
+#pragma unroll
+      for (int b = 0; b < 4; ++b)
+        st_shared_v4(dst + (4 * a + b) * V_TAP_BYTES, out[b][0], out[b][1], out[b][2], out[b][3]);
+    }
+  }
+}
+
+// Output-transform coefficient of tap t = 4a+b for output (i, j):
+// At[i][a] * At[j][b] with At = [[1,1,1,0],[0,1,-1,-1]].
+__host__ __device__ constexpr int at_coef(int i, int a) {
+  return i == 0 ? (a == 3 ? 0 : 1) : (a == 0 ? 0 : (a == 1 ? 1 : -1));
+}
+
+}  // namespace fused
+
+using namespace fused;
+
+__global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam p) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  __shared__ Shared sh;
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const Geometry g = make_geometry(p);
+  const int warp = warp_id();
+  const int lane = lane_id();
+  uint32_t* err = &g_fused_err;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < NSTAGE; ++s) {
+      mbar_init(&sh.full[s], NWARP_V + 1);
+      mbar_init(&sh.empty[s], 1);
+    }
+    mbar_init(&sh.accf, 1);
+    for (int t = 0; t < NTAP; ++t) mbar_init(&sh.tapfree[t], NWARP_E);
+    sh.abort_flag = 0;
+    fence_barrier_init();
+  }
+  if (warp == WARP_MMA) {
+    tmem_alloc(&sh.tmem_base, 512);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = sh.tmem_base;
+  volatile int* abort_flag = &sh.abort_flag;
+  const uint32_t smem_base = smem_u32(smem);
+  auto v_stage = [&](int s) { return smem_base + s * STAGE_BYTES; };
+  auto u_stage = [&](int s) { return smem_base + s * STAGE_BYTES + V_STAGE_BYTES; };
+
+  if (warp == WARP_MMA) {
+    if (lane == 0) {
+      uint32_t it = 0, bi = 0;
+      for (long long b = blockIdx.x; b < g.nblocks && !*abort_flag; b += gridDim.x, ++bi) {
+        const int kb = (int)(b % g.nKB);
+        const int kbs = kblock_rows(kb, g.K);
+        const uint32_t idesc = instr_desc(128, kbs, 0, 0, 1, 0);
+        for (int s = 0; s < g.CS; ++s, ++it) {
+          const int st = it & 1;
+          if (!mbar_wait(&sh.full[st], (it >> 1) & 1, abort_flag, err, ERR_WAIT_FULL)) break;
+          tc_fence_after();
+#pragma unroll 1
+          for (int t = 0; t < NTAP; ++t) {
+            if (s == 0 && bi > 0) {
+              if (!mbar_wait(&sh.tapfree[t], (bi - 1) & 1, abort_flag, err, ERR_WAIT_DRAIN)) break;
+              tc_fence_after();
+            }
+            const uint64_t ad = smem_desc(v_stage(st) + t * V_TAP_BYTES, 128, 256);
+            const uint64_t bd = smem_desc(u_stage(st) + t * kbs * 32, 128, 256);
+            mma_f16(tmem + t * KB, ad, bd, idesc, s > 0 ? 1u : 0u);
+          }
+          mma_commit(&sh.empty[st]);
+        }
+        mma_commit(&sh.accf);
+      }
+    }
+    __syncwarp();
+  } else if (warp == WARP_U) {
+    if (lane == 0) {
+      const __half* ucache = static_cast<const __half*>(p.transform_filter);
+      uint32_t it = 0;
+      for (long long b = blockIdx.x; b < g.nblocks && !*abort_flag; b += gridDim.x) {
+        const int kb = (int)(b % g.nKB);
+        const uint32_t bytes = NTAP * kblock_rows(kb, g.K) * 16 * 2;
+        for (int s = 0; s < g.CS; ++s, ++it) {
+          const int st = it & 1;
+          if (it >= NSTAGE &&
+              !mbar_wait(&sh.empty[st], ((it >> 1) - 1) & 1, abort_flag, err, ERR_WAIT_EMPTY))
+            break;
+          mbar_arrive_expect_tx(&sh.full[st], bytes);
+          bulk_g2s(smem + st * STAGE_BYTES + V_STAGE_BYTES, ucache + u_piece(kb, s, g.K, g.C), bytes,
+                   &sh.full[st]);
+        }
+      }
+      if (*abort_flag) __nanosleep(20000);  // let copies already issued land
+    }
+    __syncwarp();
+  } else if (warp >= WARP_V0 && warp < WARP_V0 + NWARP_V) {
+    const int vw = warp - WARP_V0;
+    const int grp = 2 * vw + (lane >> 4);  // tile group (8 tiles) 0..15
+    const int cl = lane & 15;              // channel inside the step
+    const __half* X = static_cast<const __half*>(p.pin);
+    uint32_t it = 0;
+    for (long long b = blockIdx.x; b < g.nblocks && !*abort_flag; b += gridDim.x) {
+      const long long tb = b / g.nKB;
+      const long long tile0 = tb * TILES + grp * 8;
+      bool ok = true;
+      for (int s = 0; s < g.CS; ++s, ++it) {
+        const int st = it & 1;
+        if (it >= NSTAGE &&
+            !mbar_wait(&sh.empty[st], ((it >> 1) - 1) & 1, abort_flag, err, ERR_WAIT_EMPTY)) {
+          ok = false;
+          break;
+        }
+        const uint32_t dst = v_stage(st) + grp * 256 + (cl >> 3) * 128 + (cl & 7) * 16;
+        produce_v8(X, g, tile0, s * 16 + cl, dst);
+        fence_proxy_async_shared();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&sh.full[st]);
+      }
+      if (!ok) break;
+    }
+  } else if (warp >= WARP_E0) {
+    const int quarter = warp & 3;            // TMEM lanes 32*quarter .. +31
+    const int half = (warp - WARP_E0) >> 2;  // output channels 16*half .. +15 of the block
+    __half* Y = static_cast<__half*>(p.pout);
+    const long long per_img = (long long)g.TP * g.TQ;
+    uint32_t bi = 0;
+    for (long long b = blockIdx.x; b < g.nblocks; b += gridDim.x, ++bi) {
+      if (!mbar_wait(&sh.accf, bi & 1, abort_flag, err, ERR_WAIT_ACCUM)) break;
+      tc_fence_after();
+      const long long tb = b / g.nKB;
+      const int kb = (int)(b % g.nKB);
+      const int kbs = kblock_rows(kb, g.K);
+      const bool active = half * 16 < kbs;
+      float y[16][4];
+#pragma unroll
+      for (int kk = 0; kk < 16; ++kk)
+#pragma unroll
+        for (int o = 0; o < 4; ++o) y[kk][o] = 0.f;
+      const uint32_t tbase = tmem + ((uint32_t)(quarter * 32) << 16) + half * 16;
+#pragma unroll
+      for (int t = 0; t < NTAP; ++t) {
+        float m[16];
+        if (active) {
+          tmem_ld16(tbase + t * KB, m);
+          tmem_ld_wait();
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&sh.tapfree[t]);
+        if (active) {
+          const int a = t >> 2, bcol = t & 3;
+          const int c00 = at_coef(0, a) * at_coef(0, bcol), c01 = at_coef(0, a) * at_coef(1, bcol);
+          const int c10 = at_coef(1, a) * at_coef(0, bcol), c11 = at_coef(1, a) * at_coef(1, bcol);
+#pragma unroll
+          for (int kk = 0; kk < 16; ++kk) {
+            y[kk][0] += (float)c00 * m[kk];
+            y[kk][1] += (float)c01 * m[kk];
+            y[kk][2] += (float)c10 * m[kk];
+            y[kk][3] += (float)c11 * m[kk];
+          }
+        }
+      }
+      const long long tile = tb * TILES + quarter * 32 + lane;
+      if (active && tile < g.NT) {
+        const int n = (int)(tile / per_img);
+        const int r = (int)(tile - (long long)n * per_img);
+        const int ty = r / g.TQ, tx = r - (r / g.TQ) * g.TQ;
+        const int oy = 2 * ty, ox = 2 * tx;
+        const bool two_cols = ox + 1 < g.Q;
+        const bool two_rows = oy + 1 < g.P;
+        const bool q_even = (g.Q & 1) == 0;
+#pragma unroll
+        for (int kk = 0; kk < 16; ++kk) {
+          const int k = kb * KB + half * 16 + kk;
+          if (k >= g.K) break;
+          __half* o = Y + (((size_t)n * g.K + k) * g.P + oy) * (size_t)g.Q + ox;
+          if (two_cols && q_even) {
+            *reinterpret_cast<__half2*>(o) = __floats2half2_rn(y[kk][0], y[kk][1]);
+            if (two_rows) *reinterpret_cast<__half2*>(o + g.Q) = __floats2half2_rn(y[kk][2], y[kk][3]);
+          } else {
+            o[0] = __float2half_rn(y[kk][0]);
+            if (two_cols) o[1] = __float2half_rn(y[kk][1]);
+            if (two_rows) {
+              o[g.Q] = __float2half_rn(y[kk][2]);
+              if (two_cols) o[g.Q + 1] = __float2half_rn(y[kk][3]);
+            }
+          }
+        }
+      }
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == WARP_MMA) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 512);
+  }
+}
+
+}  // namespace wino
+
+using namespace wino;
+
+extern "C" {
+
+void* wino_fused_kernel_ptr() { return (void*)fused_wino_f16_kernel; }
+int wino_fused_smem_bytes() { return fused::SMEM_BYTES; }
+int wino_fused_threads() { return fused::NTHREAD; }
+
+int wino_fused_prepare() {
+  return (int)cudaFuncSetAttribute(fused_wino_f16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   fused::SMEM_BYTES);
+}
+
+// Work blocks of a problem (tile blocks x output-channel blocks).
+long long wino_fused_nblocks(int n, int h, int w, int k) {
+  const long long nt = (long long)n * ((h + 1) / 2) * ((w + 1) / 2);
+  return ((nt + fused::TILES - 1) / fused::TILES) * ((k + KB - 1) / KB);
+}
+
+uint32_t wino_fused_error_read_clear() {
+  uint32_t v = 0, z = 0;
+  cudaMemcpyFromSymbol(&v, g_fused_err, sizeof(v));
+  cudaMemcpyToSymbol(g_fused_err, &z, sizeof(z));
+  return v;
+}
+
+}  // extern "C"

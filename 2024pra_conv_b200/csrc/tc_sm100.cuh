@@ -2,9 +2,10 @@
 // mbarriers with bounded waits, bulk copies global->shared, tcgen05 tensor
 // memory (alloc / mma / commit / ld / st) and cluster shared-memory access.
 //
-// Every wait is bounded: after WAIT_LIMIT polls the waiter records an error
-// code in the library's device error word and returns false, so a protocol
-// bug ends the kernel with a status the host reads instead of a hung GPU.
+// Every wait is bounded: after WINO_WAIT_NS nanoseconds the waiter records an
+// error code in the kernel's device error word and returns false, so a
+// protocol bug ends the kernel with a status the host reads instead of a hung
+// GPU.
 #pragma once
 #include <cstdint>
 #include <cuda_fp16.h>
@@ -25,9 +26,16 @@ enum : uint32_t {
   ERR_BAD_SHAPE = 16,     // kernel launched with a shape it cannot run
 };
 
-#ifndef WINO_WAIT_LIMIT
-#define WINO_WAIT_LIMIT (1u << 26)
+// Longest any single wait may take before it is declared failed (ns).
+#ifndef WINO_WAIT_NS
+#define WINO_WAIT_NS 1000000000ull
 #endif
+
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -66,7 +74,7 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, 1000;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
       "selp.u32 %0, 1, 0, p;\n\t}"
       : "=r"(ok)
       : "r"(smem_u32(bar)), "r"(parity)
@@ -79,7 +87,7 @@ __device__ __forceinline__ bool mbar_try_wait_cluster(uint64_t* bar, uint32_t pa
   uint32_t ok;
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2, 1000;\n\t"
+      "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
       "selp.u32 %0, 1, 0, p;\n\t}"
       : "=r"(ok)
       : "r"(smem_u32(bar)), "r"(parity)
@@ -89,27 +97,31 @@ __device__ __forceinline__ bool mbar_try_wait_cluster(uint64_t* bar, uint32_t pa
 
 // Bounded wait.  `abort` is a shared flag that any failing waiter raises so
 // that the other roles of the CTA stop waiting as well.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort,
-                                          uint32_t* err, uint32_t code) {
-  for (uint32_t i = 0; i < WINO_WAIT_LIMIT; ++i) {
-    if (mbar_try_wait(bar, parity)) return true;
+template <bool kCluster>
+__device__ __forceinline__ bool mbar_wait_impl(uint64_t* bar, uint32_t parity, volatile int* abort,
+                                               uint32_t* err, uint32_t code) {
+  auto poll = [&]() { return kCluster ? mbar_try_wait_cluster(bar, parity) : mbar_try_wait(bar, parity); };
+  if (poll()) return true;
+  const uint64_t t0 = globaltimer_ns();
+  for (uint32_t i = 1;; ++i) {
+    if (poll()) return true;
     if (abort && *abort) return false;
+    if ((i & 63) == 0 && globaltimer_ns() - t0 > WINO_WAIT_NS) break;
   }
   record_error(err, code);
   if (abort) *abort = 1;
   return false;
 }
 
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort,
+                                          uint32_t* err, uint32_t code) {
+  return mbar_wait_impl<false>(bar, parity, abort, err, code);
+}
+
 __device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, uint32_t parity,
                                                   volatile int* abort, uint32_t* err,
                                                   uint32_t code) {
-  for (uint32_t i = 0; i < WINO_WAIT_LIMIT; ++i) {
-    if (mbar_try_wait_cluster(bar, parity)) return true;
-    if (abort && *abort) return false;
-  }
-  record_error(err, code);
-  if (abort) *abort = 1;
-  return false;
+  return mbar_wait_impl<true>(bar, parity, abort, err, code);
 }
 
 // ------------------------------------------------------------ bulk copies ---

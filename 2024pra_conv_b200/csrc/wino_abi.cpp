@@ -1,0 +1,228 @@
+// Host side of the drop-in plugin ABI (include/conv2d.h) and of the
+// extension C-ABI (include/winoconv.h).  Plain C++ (compiled by the host
+// compiler, so the `_Float16` declarations of the reference-compatible
+// headers compile); kernels are reached through their entry pointers.
+//
+// getParamsize / getkernelInfo replace the reference's src/conv2d.cpp:9-14 and
+// :254-517.  The reference picks one of six hard-wired kernel quadruples by
+// (n, c) and returns 0 for every input; here any shape inside the contract
+// gets the same two real kernels (filter transform, fused conv) and anything
+// else is rejected with an error code before a kernel is chosen.
+#include <cstddef>
+#include <cstdint>
+#include <cstring>
+#include <mutex>
+#include <cuda_runtime.h>
+
+#include "conv2d.h"
+#include "mykernelParamType.cuh"
+#include "winoconv.h"
+#include "wino_param.h"
+
+// The kernel argument the device sees must be bit-for-bit the host struct.
+static_assert(sizeof(mykernelParamType) == sizeof(wino::KernelParam), "param size");
+#define WINO_SAME_OFFSET(f) \
+  static_assert(offsetof(mykernelParamType, f) == offsetof(wino::KernelParam, f), #f)
+WINO_SAME_OFFSET(pin);
+WINO_SAME_OFFSET(pweight);
+WINO_SAME_OFFSET(pout);
+WINO_SAME_OFFSET(transform_pin);
+WINO_SAME_OFFSET(transform_filter);
+WINO_SAME_OFFSET(mid_result);
+WINO_SAME_OFFSET(n);
+WINO_SAME_OFFSET(c);
+WINO_SAME_OFFSET(h);
+WINO_SAME_OFFSET(w);
+WINO_SAME_OFFSET(k);
+WINO_SAME_OFFSET(r);
+WINO_SAME_OFFSET(s);
+WINO_SAME_OFFSET(u);
+WINO_SAME_OFFSET(v);
+WINO_SAME_OFFSET(p);
+WINO_SAME_OFFSET(q);
+WINO_SAME_OFFSET(Oh);
+WINO_SAME_OFFSET(Ow);
+#undef WINO_SAME_OFFSET
+static_assert(sizeof(problem_t) == 96, "problem_t layout");
+static_assert(sizeof(kernelInfo_t) == 160, "kernelInfo_t layout");
+
+extern "C" {
+void* wino_dropin_filter_kernel_ptr();
+void* wino_fused_kernel_ptr();
+void* wino_noop_kernel_ptr();
+int wino_fused_prepare();
+int wino_fused_smem_bytes();
+int wino_fused_threads();
+long long wino_fused_nblocks(int n, int h, int w, int k);
+uint32_t wino_fused_error_read_clear();
+int wino_launch_filter_transform(const void* weight, void* ucache, void* ucache_lo, int K, int C,
+                                 int bf16, cudaStream_t stream);
+}
+
+namespace {
+
+constexpr int kMaxDim = 32767;  // dims are `short` in mykernelParamType
+
+int sm_count() {
+  int dev = 0, n = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+  if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+    return 148;
+  return n;
+}
+
+void set_slot(kernelInfo_t* ki, int slot, unsigned gx, unsigned gy, unsigned gz, unsigned tx,
+              unsigned ty, unsigned tz, unsigned lds, void* fn) {
+  unsigned* base = nullptr;
+  void** ptr = nullptr;
+  switch (slot) {
+    case 1: base = &ki->blockx1; ptr = &ki->kernelPtr1; break;
+    case 2: base = &ki->blockx2; ptr = &ki->kernelPtr2; break;
+    case 3: base = &ki->blockx3; ptr = &ki->kernelPtr3; break;
+    default: base = &ki->blockx4; ptr = &ki->kernelPtr4; break;
+  }
+  base[0] = gx; base[1] = gy; base[2] = gz;
+  base[3] = tx; base[4] = ty; base[5] = tz;
+  base[6] = lds;
+  *ptr = fn;
+}
+
+wino::KernelParam make_param(const void* x, const void* w, void* y, void* vws, void* ucache,
+                             void* mws, int n, int c, int h, int wd, int k) {
+  wino::KernelParam p;
+  p.pin = const_cast<void*>(x);
+  p.pweight = const_cast<void*>(w);
+  p.pout = y;
+  p.transform_pin = vws;
+  p.transform_filter = ucache;
+  p.mid_result = mws;
+  p.n = (short)n; p.c = (short)c; p.h = (short)h; p.w = (short)wd; p.k = (short)k;
+  p.r = 3; p.s = 3; p.u = 1; p.v = 1; p.p = 1; p.q = 1;
+  p.Oh = (short)h; p.Ow = (short)wd;
+  return p;
+}
+
+unsigned fused_grid(int n, int h, int w, int k) {
+  const long long nb = wino_fused_nblocks(n, h, w, k);
+  const long long sms = sm_count();
+  return (unsigned)(nb < sms ? nb : sms);
+}
+
+}  // namespace
+
+extern "C" int wino_check_shape(int n, int c, int h, int w, int k) {
+  if (n < 1 || c < 1 || h < 1 || w < 1 || k < 1) return WINO_EINVAL;
+  if (n > kMaxDim || c > kMaxDim || h > kMaxDim || w > kMaxDim || k > kMaxDim)
+    return WINO_EUNSUPPORTED;
+  if (c % 16 != 0 || k % 16 != 0) return WINO_EUNSUPPORTED;
+  return WINO_OK;
+}
+
+extern "C" size_t wino_ucache_bytes(int k, int c, int variant) {
+  const size_t elems = (size_t)16 * (size_t)k * (size_t)c;
+  switch (variant) {
+    case WINO_VAR_F8: return elems + (size_t)16 * k * sizeof(float);
+    case WINO_VAR_F16_HILO: return 2 * elems * 2;
+    default: return elems * 2;
+  }
+}
+
+// --------------------------------------------------------- drop-in ABI ----
+int getParamsize(problem_t* problem, int* paramSize) {
+  (void)problem;
+  if (!paramSize) return WINO_EINVAL;
+  *paramSize = (int)sizeof(mykernelParamType);
+  return WINO_OK;
+}
+
+int getkernelInfo(problem_t* problem, kernelInfo_t* kernelInfo, void* param) {
+  if (!problem || !kernelInfo || !param) return WINO_EINVAL;
+  const problem_t& pr = *problem;
+  if (pr.r != 3 || pr.s != 3 || pr.u != 1 || pr.v != 1 || pr.p != 1 || pr.q != 1)
+    return WINO_EUNSUPPORTED;
+  const int st = wino_check_shape((int)pr.n, (int)pr.c, (int)pr.h, (int)pr.w, (int)pr.k);
+  if (st != WINO_OK) return st;
+  if (!pr.in || !pr.weight || !pr.out || !pr.transform_filter) return WINO_EINVAL;
+  const int oh = ((int)pr.h - (int)pr.r + 2 * (int)pr.p) / (int)pr.u + 1;
+  const int ow = ((int)pr.w - (int)pr.s + 2 * (int)pr.q) / (int)pr.v + 1;
+
+  if (wino_fused_prepare() != 0) return WINO_ECUDA;
+
+  std::memset(kernelInfo, 0, sizeof(*kernelInfo));
+  const long long kc = (long long)pr.k * pr.c;
+  set_slot(kernelInfo, 1, (unsigned)((kc + 255) / 256), 1, 1, 256, 1, 1, 0,
+           wino_dropin_filter_kernel_ptr());
+  set_slot(kernelInfo, 2, fused_grid((int)pr.n, (int)pr.h, (int)pr.w, (int)pr.k), 1, 1,
+           (unsigned)wino_fused_threads(), 1, 1, (unsigned)wino_fused_smem_bytes(),
+           wino_fused_kernel_ptr());
+  set_slot(kernelInfo, 3, 1, 1, 1, 32, 1, 1, 0, wino_noop_kernel_ptr());
+  set_slot(kernelInfo, 4, 1, 1, 1, 32, 1, 1, 0, wino_noop_kernel_ptr());
+
+  mykernelParamType* a = static_cast<mykernelParamType*>(param);
+  a->pin = pr.in;
+  a->pweight = pr.weight;
+  a->pout = pr.out;
+  a->transform_pin = pr.transform_pin;
+  a->transform_filter = pr.transform_filter;
+  a->mid_result = pr.mid_result;
+  a->n = (short)pr.n; a->c = (short)pr.c; a->h = (short)pr.h; a->w = (short)pr.w;
+  a->k = (short)pr.k; a->r = (short)pr.r; a->s = (short)pr.s; a->u = (short)pr.u;
+  a->v = (short)pr.v; a->p = (short)pr.p; a->q = (short)pr.q;
+  a->Oh = (short)oh; a->Ow = (short)ow;
+  return WINO_OK;
+}
+
+extern "C" int wino_getParamsize(problem_t* problem, int* paramSize) {
+  return getParamsize(problem, paramSize);
+}
+extern "C" int wino_getkernelInfo(problem_t* problem, kernelInfo_t* kernelInfo, void* param) {
+  return getkernelInfo(problem, kernelInfo, param);
+}
+
+// ------------------------------------------------------- extension API ----
+extern "C" int wino_filter_transform(const void* weight, void* ucache, int k, int c, void* stream) {
+  if (!weight || !ucache) return WINO_EINVAL;
+  const int st = wino_check_shape(1, c, 1, 1, k);
+  if (st != WINO_OK) return st;
+  return wino_launch_filter_transform(weight, ucache, nullptr, k, c, 0, (cudaStream_t)stream) == 0
+             ? WINO_OK
+             : WINO_ECUDA;
+}
+
+extern "C" int wino_conv2d_fused(const void* x, const void* ucache, void* y, int n, int c, int h,
+                                 int w, int k, void* stream) {
+  if (!x || !ucache || !y) return WINO_EINVAL;
+  const int st = wino_check_shape(n, c, h, w, k);
+  if (st != WINO_OK) return st;
+  if (wino_fused_prepare() != 0) return WINO_ECUDA;
+  wino::KernelParam p = make_param(x, nullptr, y, nullptr, const_cast<void*>(ucache), nullptr, n, c,
+                                   h, w, k);
+  void* args[] = {&p};
+  const cudaError_t e = cudaLaunchKernel(wino_fused_kernel_ptr(), dim3(fused_grid(n, h, w, k)),
+                                         dim3(wino_fused_threads()), args,
+                                         (size_t)wino_fused_smem_bytes(), (cudaStream_t)stream);
+  return e == cudaSuccess ? WINO_OK : WINO_ECUDA;
+}
+
+// Launch the four slots of a filled kernelInfo_t in order on one stream, each
+// with args[0] = param, exactly as the reference harness does
+// (reference src/main.cpp:105-108, 121-124, hipExtLaunchKernel).
+extern "C" int wino_launch_kernelinfo(const void* kiv, void* param, void* stream) {
+  const kernelInfo_t* ki = static_cast<const kernelInfo_t*>(kiv);
+  if (!ki || !param) return WINO_EINVAL;
+  const unsigned* slots[4] = {&ki->blockx1, &ki->blockx2, &ki->blockx3, &ki->blockx4};
+  void* const fns[4] = {ki->kernelPtr1, ki->kernelPtr2, ki->kernelPtr3, ki->kernelPtr4};
+  for (int i = 0; i < 4; ++i) {
+    const unsigned* b = slots[i];
+    const cudaError_t e = cudaLaunchKernel(fns[i], dim3(b[0], b[1], b[2]), dim3(b[3], b[4], b[5]),
+                                           (void**)&param, (size_t)b[6], (cudaStream_t)stream);
+    if (e != cudaSuccess) return WINO_ECUDA;
+  }
+  return WINO_OK;
+}
+
+extern "C" int wino_error_read_clear(uint32_t* code) {
+  if (!code) return WINO_EINVAL;
+  *code = wino_fused_error_read_clear();
+  return WINO_OK;
+}

@@ -15,31 +15,52 @@
 #include <cstdint>
 #include <cuda_fp16.h>
 #include <cuda_bf16.h>
+#include <cuda_fp8.h>
 #include "wino_param.h"
 
 namespace wino {
 
 // ------------------------------------------------------------ U cache -------
 // The transformed filter U[t][k][c] is stored pre-tiled in the canonical
-// K-major no-swizzle layout the tensor core reads from shared memory, so a
-// CTA fetches the slice it needs with one bulk copy per tap and stage:
+// K-major no-swizzle layout the tensor core reads from shared memory, grouped
+// so that one K-step (16 input channels) of one output-channel block is a
+// single contiguous piece that a CTA fetches with one bulk copy:
 //
-//   block(cs, t) = U[t][0..K)[16*cs .. 16*cs+16)      (cs = c / 16)
-//   blocks ordered (cs, t); inside a block, 8-row groups of k (256 bytes
-//   each) hold two 8x8 core matrices (c 0-7, c 8-15) of 8 k-rows x 16 bytes.
+//   k-blocks of KB = 32 output channels (the last one may hold 16),
+//   inside a k-block: K-steps cs = c / 16, inside a K-step: taps t = 0..15,
+//   inside a tap: 8-row groups of k (256 bytes) each holding two 8 x 8 core
+//   matrices (channels 0-7 and 8-15 of the step), 8 k-rows x 16 bytes.
 //
-// fp16/bf16 element offset of (t, k, c) for K output channels:
-__host__ __device__ __forceinline__ size_t u_offset(int t, int k, int c, int K) {
-  const int cs = c >> 4, cc = c & 15;
-  return ((size_t)cs * 16 + t) * (size_t)K * 16 + (size_t)(k >> 3) * 128 + (cc >> 3) * 64 +
-         (k & 7) * 8 + (cc & 7);
+// A (k-block, K-step) piece holds 16 * kbs * 16 elements (kbs = rows of the
+// k-block), taps at a stride of kbs * 16 elements.  Total size 16*K*C.
+constexpr int KB = 32;
+
+__host__ __device__ __forceinline__ int kblock_rows(int kb, int K) {
+  const int r = K - kb * KB;
+  return r < KB ? r : KB;
 }
 
-// 8-bit element offset for the fp8 cache: K-steps of 32 channels.
-__host__ __device__ __forceinline__ size_t u8_offset(int t, int k, int c, int K) {
+// fp16/bf16 element offset of (t, k, c); C channels, K output channels.
+__host__ __device__ __forceinline__ size_t u_offset(int t, int k, int c, int K, int C) {
+  const int kb = k / KB, kr = k % KB;
+  const int kbs = kblock_rows(kb, K);
+  const int cs = c >> 4, cc = c & 15;
+  return (size_t)kb * KB * 16 * C + ((size_t)cs * 16 + t) * (size_t)(kbs * 16) + (kr >> 3) * 128 +
+         (cc >> 3) * 64 + (kr & 7) * 8 + (cc & 7);
+}
+
+// Start (elements) of the (k-block, K-step) piece.
+__host__ __device__ __forceinline__ size_t u_piece(int kb, int cs, int K, int C) {
+  return (size_t)kb * KB * 16 * C + (size_t)cs * 16 * (size_t)(kblock_rows(kb, K) * 16);
+}
+
+// 8-bit cache: K-steps of 32 channels, 8 k-rows x 16 bytes per core matrix.
+__host__ __device__ __forceinline__ size_t u8_offset(int t, int k, int c, int K, int C) {
+  const int kb = k / KB, kr = k % KB;
+  const int kbs = kblock_rows(kb, K);
   const int cs = c >> 5, cc = c & 31;
-  return ((size_t)cs * 16 + t) * (size_t)K * 32 + (size_t)(k >> 3) * 256 + (cc >> 4) * 128 +
-         (k & 7) * 16 + (cc & 15);
+  return (size_t)kb * KB * 16 * C + ((size_t)cs * 16 + t) * (size_t)(kbs * 32) + (kr >> 3) * 256 +
+         (cc >> 4) * 128 + (kr & 7) * 16 + (cc & 15);
 }
 
 // G g G^T of one 3x3 filter, in fp32 (16 outputs, row-major over the tap).

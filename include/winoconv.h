@@ -1,0 +1,75 @@
+/*
+ * Extension C-ABI of the B200 Winograd F(2x2,3x3) conv2d library
+ * (libwinoconv.so).  Plain C types only; every pointer is device memory unless
+ * stated otherwise; `stream` is a cudaStream_t (NULL = legacy default stream).
+ *
+ * The reference has no counterpart for these entry points beyond the plugin
+ * ABI in conv2d.h (reference include/conv2d.h:69-70): they expose the pieces
+ * that ABI hides (a one-shot filter transform whose result is reused across
+ * calls, the fused conv on a cached U, the unfused comparator path) so that a
+ * caller can keep U resident and so that tests and benchmarks can reach each
+ * stage.  Each function cites the reference stage it implements.
+ *
+ * Shape contract (all entry points): 3x3 filter, stride 1, pad 1,
+ * c % 16 == 0, k % 16 == 0, n, c, h, w, k in [1, 32767].
+ * Return: 0 on success or one of the WINO_E* codes below.
+ */
+#ifndef WINO_WINOCONV_H
+#define WINO_WINOCONV_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  WINO_OK = 0,
+  WINO_EINVAL = 1,        /* null pointer or invalid argument            */
+  WINO_EUNSUPPORTED = 2,  /* shape outside the contract above            */
+  WINO_ECUDA = 3,         /* a CUDA runtime call failed                  */
+  WINO_EDEVICE = 4        /* a kernel reported an error (see error word) */
+};
+
+/* Precision variants of the GEMM stage. */
+enum {
+  WINO_VAR_F16 = 0,       /* fp16 operands, fp32 accumulate              */
+  WINO_VAR_BF16 = 1,      /* bf16 operands, fp32 accumulate              */
+  WINO_VAR_F8 = 2,        /* fp8 e4m3 operands with per-channel scales   */
+  WINO_VAR_F16_HILO = 3   /* fp16 with the U residual as a second GEMM   */
+};
+
+/* Validate a problem against the shape contract (no CUDA calls). */
+int wino_check_shape(int n, int c, int h, int w, int k);
+
+/* Bytes of the U cache for a variant (fp16: 16*k*c*2). */
+size_t wino_ucache_bytes(int k, int c, int variant);
+
+/* Filter transform U = G g G^T of fp16 KCRS weights into the tile-major
+ * fp16 U cache (reference src/preprocessing.cuh:75-270, GgGT*).  One-shot:
+ * the result stays valid for as long as the weights do. */
+int wino_filter_transform(const void* weight, void* ucache, int k, int c, void* stream);
+
+/* Fused conv on a prepared fp16 U cache: input transform, tensor-core tap
+ * GEMMs and output transform in one persistent kernel (reference
+ * src/preprocessing.cuh:273-424, src/matrixmul.cuh:139-556,
+ * src/conv2d.cpp:17-250).  x: NCHW fp16, y: N K H W fp16. */
+int wino_conv2d_fused(const void* x, const void* ucache, void* y, int n, int c, int h, int w,
+                      int k, void* stream);
+
+/* Launch the four slots of a kernelInfo_t filled by getkernelInfo, in order,
+ * on `stream`, each with args[0] = param: the launch sequence of the
+ * reference harness (reference src/main.cpp:105-108).  `ki` is `const
+ * kernelInfo_t*` from conv2d.h, passed untyped so this header stands alone. */
+int wino_launch_kernelinfo(const void* ki, void* param, void* stream);
+
+/* Reads and clears the device error word of the conv kernels (0 = none;
+ * otherwise the first wait that ran out or the first bad-shape launch). */
+int wino_error_read_clear(uint32_t* code);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WINO_WINOCONV_H */

@@ -1,0 +1,102 @@
+"""CPU tests of the drop-in boundary: the library loads, exports every entry
+point declared in include/*.h, and rejects unsupported problems before any
+CUDA call (reference include/conv2d.h:69-70; the reference itself returns 0
+for every shape, src/conv2d.cpp:516)."""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+from conftest import ROOT
+
+
+def _declared_functions():
+    names = set()
+    for h in ("conv2d.h", "winoconv.h"):
+        src = open(os.path.join(ROOT, "include", h)).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        for m in re.finditer(r"^\s*(?:int|size_t|void\s*\*?)\s+(\w+)\s*\(", src, flags=re.M):
+            names.add(m.group(1))
+    return sorted(names)
+
+
+def test_headers_declare_the_reference_entry_points():
+    names = _declared_functions()
+    assert "getParamsize" in names and "getkernelInfo" in names
+    assert "wino_conv2d_fused" in names
+
+
+def test_library_exports_every_declared_symbol(wino):
+    lib = wino.LIB_PATH
+    out = subprocess.run(["nm", "-D", "--defined-only", lib], capture_output=True, text=True,
+                         check=True).stdout
+    exported = {l.split()[-1] for l in out.splitlines() if l.strip()}
+    missing = []
+    for name in _declared_functions():
+        if name in ("getParamsize", "getkernelInfo"):
+            # C++ linkage, as the reference header declares them
+            if not any(e.startswith(f"_Z{len(name)}{name}") for e in exported):
+                missing.append(name)
+        elif name not in exported:
+            missing.append(name)
+    assert not missing, missing
+    # The mangled names a reference caller links against.
+    assert "_Z12getParamsizeP9problem_tPi" in exported
+    assert "_Z13getkernelInfoP9problem_tP12kernelInfo_tPv" in exported
+
+
+def test_param_size_is_reference_layout(wino):
+    pr = wino.Problem()
+    assert wino.get_param_size(pr) == 80  # 6 pointers + 13 shorts on x86-64
+    assert ctypes.sizeof(wino.Problem) == 96
+    assert ctypes.sizeof(wino.KernelInfo) == 160
+
+
+def _problem(wino, **kw):
+    f = dict(in_=0x1000, weight=0x2000, out=0x3000, transform_pin=0, transform_filter=0x4000,
+             mid_result=0, n=2, c=64, h=14, w=14, k=64, r=3, s=3, u=1, v=1, p=1, q=1)
+    f.update(kw)
+    pr = wino.Problem()
+    for k_, v_ in f.items():
+        setattr(pr, k_, v_)
+    return pr
+
+
+@pytest.mark.parametrize("field,value,code", [
+    ("r", 5, 2), ("s", 1, 2), ("u", 2, 2), ("v", 2, 2), ("p", 0, 2), ("q", 2, 2),
+    ("c", 8, 2), ("k", 27, 2), ("c", 3, 2), ("h", 40000, 2), ("n", 0, 1), ("w", 0, 1),
+    ("in_", 0, 1), ("weight", 0, 1), ("out", 0, 1), ("transform_filter", 0, 1),
+])
+def test_getkernelinfo_rejects_unsupported(wino, field, value, code):
+    pr = _problem(wino, **{field: value})
+    param = (ctypes.c_char * 80)()
+    rc, _ = wino.get_kernel_info(pr, param)
+    assert rc == code
+
+
+def test_check_shape(wino):
+    L = wino.lib()
+    assert L.wino_check_shape(128, 256, 28, 28, 256) == 0
+    assert L.wino_check_shape(1, 48, 7, 7, 48) == 0
+    assert L.wino_check_shape(1, 24, 7, 7, 48) == 2
+    assert L.wino_ucache_bytes(256, 256, 0) == 16 * 256 * 256 * 2
+
+
+def test_host_u_cache_layout_is_a_bijection():
+    """The tile-major U offset formula visits every element exactly once."""
+    import numpy as np
+    for K, C in [(32, 16), (48, 32), (16, 48), (80, 64)]:
+        seen = np.zeros(16 * K * C, np.int32)
+        KB = 32
+        for t in range(16):
+            for k in range(K):
+                for c in range(C):
+                    kb, kr = divmod(k, KB)
+                    kbs = min(KB, K - kb * KB)
+                    cs, cc = divmod(c, 16)
+                    off = (kb * KB * 16 * C + (cs * 16 + t) * kbs * 16 + (kr >> 3) * 128 +
+                           (cc >> 3) * 64 + (kr & 7) * 8 + (cc & 7))
+                    seen[off] += 1
+        assert (seen == 1).all()

@@ -1,0 +1,61 @@
+"""CPU tests of the oracle: pinned against the reference's own conv2dcpu
+outputs (tests/golden), cross-checked against torch fp64, and the NumPy
+Winograd restatement checked against the direct convolution."""
+import numpy as np
+import pytest
+
+from conftest import golden_cases, load_golden
+
+
+@pytest.mark.parametrize("path", golden_cases(), ids=lambda p: p.rsplit("/", 1)[-1])
+def test_oracle_matches_reference_golden_bit_exact(oracle_mod, path):
+    x, w, y_ref = load_golden(path)
+    y64 = oracle_mod.conv2d_f64(x, w)
+    # The reference stores (_Float16)sum of the same double sum: bit-exact.
+    assert np.array_equal(y64.astype(np.float16), y_ref)
+
+
+def test_oracle_agrees_with_torch_float64(oracle_mod):
+    import torch
+    x, w = oracle_mod.make_inputs(2, 32, 9, 11, 48, seed=11, x_dist="normal")
+    y64 = oracle_mod.conv2d_f64(x, w)
+    yt = torch.nn.functional.conv2d(torch.from_numpy(x.astype(np.float64)),
+                                    torch.from_numpy(w.astype(np.float64)), padding=1).numpy()
+    assert np.max(np.abs(yt - y64)) <= 1e-12 * max(1.0, np.max(np.abs(y64)))
+
+
+@pytest.mark.parametrize("shape", [(1, 16, 7, 7, 16), (2, 32, 8, 6, 16), (1, 16, 1, 3, 32)])
+def test_winograd_restatement_is_exact(oracle_mod, shape):
+    from oracle import winograd as W
+    n, c, h, w, k = shape
+    x, wt = oracle_mod.make_inputs(n, c, h, w, k, seed=3)
+    y64 = oracle_mod.conv2d_f64(x, wt)
+    yw = W.conv2d_winograd_f64(x, wt)
+    assert np.max(np.abs(yw - y64)) <= 1e-12 * np.max(np.abs(y64))
+
+
+@pytest.mark.parametrize("dist", ["uniform", "normal", "student_t3", "relu_normal"])
+def test_fp16_winograd_error_budget(oracle_mod, dist):
+    """The rounding points of the fp16 kernel (U, V rounded once to fp16, fp32
+    accumulation, fp16 output) stay inside the rel-L2 <= 2e-3 target."""
+    from oracle import winograd as W
+    x, w = oracle_mod.make_inputs(2, 64, 14, 14, 32, seed=5, x_dist=dist)
+    y64 = oracle_mod.conv2d_f64(x, w)
+    ye = W.conv2d_winograd_emulated(x, w, "f16").astype(np.float16)
+    assert oracle_mod.rel_l2(ye, y64) < 2e-3
+
+
+def test_reference_check_rule_detects_planted_error(oracle_mod):
+    x, w = oracle_mod.make_reference_style_inputs(1, 16, 6, 6, 16, seed=2)
+    y = oracle_mod.conv2d_f64(x, w).astype(np.float16)
+    assert oracle_mod.reference_check(y, y) == 0
+    bad = y.copy()
+    bad.flat[17] = np.float16(float(bad.flat[17]) * 1.05)  # planted 5% error
+    assert oracle_mod.reference_check(bad, y) == 1
+
+
+def test_reference_cpu_multithreaded_matches_single(oracle_mod):
+    x, w = oracle_mod.make_inputs(4, 16, 6, 6, 16, seed=9)
+    a = oracle_mod.ref_conv2dcpu(x, w, threads=1)
+    b = oracle_mod.ref_conv2dcpu(x, w, threads=4)
+    assert np.array_equal(a, b)
