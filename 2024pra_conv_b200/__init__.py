@@ -79,6 +79,9 @@ def lib():
             "wino_filter_transform": ([vp, vp, i, i, vp], i),
             "wino_conv2d_fused": ([vp, vp, vp, i, i, i, i, i, vp], i),
             "wino_launch_kernelinfo": ([vp, vp, vp], i),
+            "wino_filter_transform_unfused": ([vp, vp, i, i, vp], i),
+            "wino_unfused_workspace_bytes": ([i, i, i, i, i, ctypes.POINTER(sz), ctypes.POINTER(sz)], i),
+            "wino_conv2d_unfused": ([vp, vp, vp, vp, vp, i, i, i, i, i, vp], i),
             "wino_error_read_clear": ([ctypes.POINTER(ctypes.c_uint32)], i),
         }
         for name, (args, res) in sigs.items():
@@ -176,6 +179,41 @@ def conv2d_fused(x, ucache, k, out=None, stream=None):
 def conv2d(x, w, stream=None):
     """Filter transform followed by the fused conv (fp16 variant)."""
     return conv2d_fused(x, filter_transform(w, stream), w.shape[0], stream=stream)
+
+
+def filter_transform_unfused(w, stream=None):
+    """fp16 KCRS weights -> fp16 U in the unfused GEMM's layout."""
+    import torch
+    k, c = w.shape[:2]
+    u = torch.empty(16 * k * c, dtype=torch.float16, device=w.device)
+    _check(lib().wino_filter_transform_unfused(ctypes.c_void_p(w.data_ptr()),
+                                               ctypes.c_void_p(u.data_ptr()), k, c, _stream(stream)),
+           "filter_transform_unfused")
+    return u
+
+
+class UnfusedWorkspace:
+    """Caller-owned V and M buffers of the unfused path for one shape."""
+
+    def __init__(self, n, c, h, w, k, device):
+        import torch
+        vb, mb = ctypes.c_size_t(0), ctypes.c_size_t(0)
+        _check(lib().wino_unfused_workspace_bytes(n, c, h, w, k, ctypes.byref(vb), ctypes.byref(mb)),
+               "unfused_workspace_bytes")
+        self.v = torch.empty(vb.value, dtype=torch.uint8, device=device)
+        self.m = torch.empty(mb.value, dtype=torch.uint8, device=device)
+
+
+def conv2d_unfused(x, ucache2, k, ws=None, out=None, stream=None):
+    import torch
+    n, c, h, wd = x.shape
+    ws = ws or UnfusedWorkspace(n, c, h, wd, k, x.device)
+    y = out if out is not None else torch.empty((n, k, h, wd), dtype=torch.float16, device=x.device)
+    _check(lib().wino_conv2d_unfused(ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(ucache2.data_ptr()),
+                                     ctypes.c_void_p(y.data_ptr()), ctypes.c_void_p(ws.v.data_ptr()),
+                                     ctypes.c_void_p(ws.m.data_ptr()), n, c, h, wd, k, _stream(stream)),
+           "conv2d_unfused")
+    return y
 
 
 def error_read_clear() -> int:

@@ -44,10 +44,11 @@ __device__ __forceinline__ void load_filter(const __half* w, int k, int c, int C
 
 // U (fp16 or bf16) for all K x C filters; hi-lo variant writes the residual
 // U - round(U) into a second cache when `lo` is non-null.
+// layout 0: fused-kernel U cache (u_offset); layout 1: unfused GEMM (u2_offset).
 template <typename T>
 __global__ void __launch_bounds__(256) filter_transform_kernel(const __half* __restrict__ w,
                                                                T* __restrict__ u, T* __restrict__ lo,
-                                                               int K, int C) {
+                                                               int K, int C, int layout) {
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (size_t)K * C) return;
   int k, c;
@@ -57,13 +58,14 @@ __global__ void __launch_bounds__(256) filter_transform_kernel(const __half* __r
   filter_tile(g, t16);
 #pragma unroll
   for (int t = 0; t < 16; ++t) {
+    const size_t off = layout ? u2_offset(t, k, c, K, C) : u_offset(t, k, c, K, C);
     const T hi = from_f32<T>(t16[t]);
-    u[u_offset(t, k, c, K, C)] = hi;
+    u[off] = hi;
     if (lo) {
       float r;
-      if constexpr (sizeof(T) == 2 && std::is_same<T, __half>::value) r = t16[t] - __half2float(hi);
+      if constexpr (std::is_same<T, __half>::value) r = t16[t] - __half2float(hi);
       else r = t16[t] - __bfloat162float(hi);
-      lo[u_offset(t, k, c, K, C)] = from_f32<T>(r);
+      lo[off] = from_f32<T>(r);
     }
   }
 }
@@ -127,15 +129,15 @@ extern "C" {
 void* wino_dropin_filter_kernel_ptr() { return (void*)dropin_filter_kernel; }
 
 int wino_launch_filter_transform(const void* weight, void* ucache, void* ucache_lo, int K, int C,
-                                 int bf16, cudaStream_t stream) {
+                                 int bf16, int layout, cudaStream_t stream) {
   const size_t n = (size_t)K * C;
   const unsigned blocks = (unsigned)((n + 255) / 256);
   if (bf16)
     filter_transform_kernel<__nv_bfloat16><<<blocks, 256, 0, stream>>>(
-        (const __half*)weight, (__nv_bfloat16*)ucache, (__nv_bfloat16*)ucache_lo, K, C);
+        (const __half*)weight, (__nv_bfloat16*)ucache, (__nv_bfloat16*)ucache_lo, K, C, layout);
   else
     filter_transform_kernel<__half><<<blocks, 256, 0, stream>>>(
-        (const __half*)weight, (__half*)ucache, (__half*)ucache_lo, K, C);
+        (const __half*)weight, (__half*)ucache, (__half*)ucache_lo, K, C, layout);
   return (int)cudaGetLastError();
 }
 

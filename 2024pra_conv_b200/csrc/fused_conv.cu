@@ -27,6 +27,7 @@
 #include <cuda_runtime.h>
 #include "tc_sm100.cuh"
 #include "wino_common.cuh"
+#include "vgen.cuh"
 
 namespace wino {
 
@@ -55,177 +56,6 @@ struct Shared {
   int abort_flag;
 };
 
-struct Geometry {
-  int N, C, H, W, K, P, Q, TP, TQ;
-  long long NT;         // tiles in the batch
-  int nTB, nKB, CS;     // tile blocks, k blocks, 16-channel steps
-  long long nblocks;
-};
-
-__device__ __forceinline__ Geometry make_geometry(const KernelParam& p) {
-  Geometry g;
-  g.N = p.n; g.C = p.c; g.H = p.h; g.W = p.w; g.K = p.k;
-  g.P = p.Oh; g.Q = p.Ow;
-  g.TP = (g.P + 1) >> 1; g.TQ = (g.Q + 1) >> 1;
-  g.NT = (long long)g.N * g.TP * g.TQ;
-  g.nTB = (int)((g.NT + TILES - 1) / TILES);
-  g.nKB = (g.K + KB - 1) / KB;
-  g.CS = g.C >> 4;
-  g.nblocks = (long long)g.nTB * g.nKB;
-  return g;
-}
-
-// ---- input words ------------------------------------------------------------
-// A "word" is two horizontally adjacent fp16 inputs (cols 2m, 2m+1) of one row,
-// zero outside the image.  `row` points at column 0 of the row (or is null
-// for a row outside the image).
-__device__ __forceinline__ uint32_t load_word(const __half* row, int m, int W, bool w_even) {
-  if (!row) return 0u;
-  const int c0 = 2 * m;
-  if (w_even) {
-    if (m < 0 || c0 >= W) return 0u;
-    return __ldg(reinterpret_cast<const unsigned int*>(row) + m);
-  }
-  const unsigned short* r16 = reinterpret_cast<const unsigned short*>(row);
-  uint32_t lo = (c0 >= 0 && c0 < W) ? (uint32_t)__ldg(r16 + c0) : 0u;
-  uint32_t hi = (c0 + 1 >= 0 && c0 + 1 < W) ? (uint32_t)__ldg(r16 + c0 + 1) : 0u;
-  return lo | (hi << 16);
-}
-
-__device__ __forceinline__ uint32_t hadd2(uint32_t a, uint32_t b) {
-  __half2 r = __hadd2(*reinterpret_cast<__half2*>(&a), *reinterpret_cast<__half2*>(&b));
-  return *reinterpret_cast<uint32_t*>(&r);
-}
-__device__ __forceinline__ uint32_t hsub2(uint32_t a, uint32_t b) {
-  __half2 r = __hsub2(*reinterpret_cast<__half2*>(&a), *reinterpret_cast<__half2*>(&b));
-  return *reinterpret_cast<uint32_t*>(&r);
-}
-// (hi(x), hi(y)) and (lo(x), lo(y)) packed as (low half, high half).
-__device__ __forceinline__ uint32_t pk_hi(uint32_t x, uint32_t y) { return __byte_perm(x, y, 0x7632); }
-__device__ __forceinline__ uint32_t pk_lo(uint32_t x, uint32_t y) { return __byte_perm(x, y, 0x5410); }
-
-// B^T rows as word operations: e_a = sum_i Bt[a][i] d_i.
-__device__ __forceinline__ uint32_t bt_row(int a, uint32_t d0, uint32_t d1, uint32_t d2, uint32_t d3) {
-  switch (a) {
-    case 0: return hsub2(d0, d2);
-    case 1: return hadd2(d1, d2);
-    case 2: return hsub2(d2, d1);
-    default: return hsub2(d1, d3);
-  }
-}
-
-// Column half of the transform for one e-row and a pair of tiles whose window
-// columns (a0..a3) are given as lane pairs: V[a][b] for b = 0..3.
-__device__ __forceinline__ void bt_cols(uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
-                                        uint32_t v[4]) {
-  v[0] = hsub2(a0, a2);
-  v[1] = hadd2(a1, a2);
-  v[2] = hsub2(a2, a1);
-  v[3] = hsub2(a1, a3);
-}
-
-// Produce V for 8 consecutive tiles (tile0 .. tile0+7) of channel c, all 16
-// taps, into shared memory: for tap t the 16 bytes at dst + t*V_TAP_BYTES.
-// Each e-row a (taps 4a..4a+3) is stored as soon as it is formed.
-// Fast path: all 8 tiles in one tile row and W even (word loads).
-__device__ __forceinline__ void produce_v8(const __half* __restrict__ X, const Geometry& g,
-                                           long long tile0, int c, uint32_t dst) {
-  const bool w_even = (g.W & 1) == 0;
-  const long long per_img = (long long)g.TP * g.TQ;
-  bool fast = false;
-  int n0 = 0, ty0 = 0, tx0 = 0;
-  if (tile0 + 7 < g.NT) {
-    n0 = (int)(tile0 / per_img);
-    const int r = (int)(tile0 - (long long)n0 * per_img);
-    ty0 = r / g.TQ;
-    tx0 = r - ty0 * g.TQ;
-    fast = w_even && (tx0 + 7 < g.TQ);
-  }
-  if (fast) {
-    const __half* plane = X + ((size_t)n0 * g.C + c) * (size_t)g.H * g.W;
-    uint32_t d[4][10];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int y = 2 * ty0 - 1 + i;
-      const __half* row = (y >= 0 && y < g.H) ? plane + (size_t)y * g.W : nullptr;
-#pragma unroll
-      for (int j = 0; j < 10; ++j) d[i][j] = load_word(row, tx0 - 1 + j, g.W, true);
-    }
-#pragma unroll
-    for (int a = 0; a < 4; ++a) {
-      uint32_t e[10];
-#pragma unroll
-      for (int j = 0; j < 10; ++j) e[j] = bt_row(a, d[0][j], d[1][j], d[2][j], d[3][j]);
-      uint32_t out[4][4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int u = 2 * q;
-        uint32_t v[4];
-        bt_cols(pk_hi(e[u], e[u + 1]), pk_lo(e[u + 1], e[u + 2]), pk_hi(e[u + 1], e[u + 2]),
-                pk_lo(e[u + 2], e[u + 3]), v);
-#pragma unroll
-        for (int b = 0; b < 4; ++b) out[b][q] = v[b];
-      }
-#pragma unroll
-      for (int b = 0; b < 4; ++b)
-        st_shared_v4(dst + (4 * a + b) * V_TAP_BYTES, out[b][0], out[b][1], out[b][2], out[b][3]);
-    }
-  } else {
-    // General path: each tile locates its own window (row or image changes
-    // inside the group, odd widths, tiles past the end of the batch).  Per
-    // e-row only the two input rows that B^T combines are read.
-    const __half* plane[8];
-    int tyv[8], txv[8];
-#pragma unroll
-    for (int s = 0; s < 8; ++s) {
-      const long long tile = tile0 + s;
-      if (tile < g.NT) {
-        const int n = (int)(tile / per_img);
-        const int r = (int)(tile - (long long)n * per_img);
-        tyv[s] = r / g.TQ;
-        txv[s] = r - tyv[s] * g.TQ;
-        plane[s] = X + ((size_t)n * g.C + c) * (size_t)g.H * g.W;
-      } else {
-        plane[s] = nullptr;
-        tyv[s] = 0;
-        txv[s] = 0;
-      }
-    }
-#pragma unroll
-    for (int a = 0; a < 4; ++a) {
-      // rows combined by Bt[a]: (0,2), (1,2), (2,1), (1,3) as (plus, minus / plus)
-      const int ra = (a == 0) ? 0 : (a == 2 ? 2 : 1);
-      const int rb = (a == 0) ? 2 : (a == 3 ? 3 : (a == 1 ? 2 : 1));
-      uint32_t ew[8][3];
-#pragma unroll
-      for (int s = 0; s < 8; ++s) {
-        const int ya = 2 * tyv[s] - 1 + ra, yb = 2 * tyv[s] - 1 + rb;
-        const __half* rowa = (plane[s] && ya >= 0 && ya < g.H) ? plane[s] + (size_t)ya * g.W : nullptr;
-        const __half* rowb = (plane[s] && yb >= 0 && yb < g.H) ? plane[s] + (size_t)yb * g.W : nullptr;
-#pragma unroll
-        for (int j = 0; j < 3; ++j) {
-          const uint32_t wa = load_word(rowa, txv[s] - 1 + j, g.W, w_even);
-          const uint32_t wb = load_word(rowb, txv[s] - 1 + j, g.W, w_even);
-          ew[s][j] = (a == 1) ? hadd2(wa, wb) : hsub2(wa, wb);
-        }
-      }
-      uint32_t out[4][4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int s0 = 2 * q, s1 = 2 * q + 1;
-        uint32_t v[4];
-        bt_cols(pk_hi(ew[s0][0], ew[s1][0]), pk_lo(ew[s0][1], ew[s1][1]), pk_hi(ew[s0][1], ew[s1][1]),
-                pk_lo(ew[s0][2], ew[s1][2]), v);
-#pragma unroll
-        for (int b = 0; b < 4; ++b) out[b][q] = v[b];
-      }
-#pragma unroll
-      for (int b = 0; b < 4; ++b)
-        st_shared_v4(dst + (4 * a + b) * V_TAP_BYTES, out[b][0], out[b][1], out[b][2], out[b][3]);
-    }
-  }
-}
-
 // Output-transform coefficient of tap t = 4a+b for output (i, j):
 // At[i][a] * At[j][b] with At = [[1,1,1,0],[0,1,-1,-1]].
 __host__ __device__ constexpr int at_coef(int i, int a) {
@@ -240,7 +70,7 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   __shared__ Shared sh;
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  const Geometry g = make_geometry(p);
+  const Geometry g = make_geometry(p, TILES);
   const int warp = warp_id();
   const int lane = lane_id();
   uint32_t* err = &g_fused_err;
@@ -333,7 +163,10 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
           break;
         }
         const uint32_t dst = v_stage(st) + grp * 256 + (cl >> 3) * 128 + (cl & 7) * 16;
-        produce_v8(X, g, tile0, s * 16 + cl, dst);
+        produce_v8(X, g, tile0, s * 16 + cl,
+                   [&](int t, uint32_t a, uint32_t b2, uint32_t c2, uint32_t d2) {
+                     st_shared_v4(dst + t * V_TAP_BYTES, a, b2, c2, d2);
+                   });
         fence_proxy_async_shared();
         __syncwarp();
         if (lane == 0) mbar_arrive(&sh.full[st]);

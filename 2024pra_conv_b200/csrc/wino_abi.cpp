@@ -55,8 +55,13 @@ int wino_fused_smem_bytes();
 int wino_fused_threads();
 long long wino_fused_nblocks(int n, int h, int w, int k);
 uint32_t wino_fused_error_read_clear();
+size_t wino_unfused_v_bytes(int n, int c, int h, int w);
+size_t wino_unfused_m_bytes(int n, int k, int h, int w);
+int wino_unfused_prepare();
+int wino_unfused_launch(const wino::KernelParam* p, int sms, cudaStream_t stream);
+uint32_t wino_unfused_error_read_clear();
 int wino_launch_filter_transform(const void* weight, void* ucache, void* ucache_lo, int K, int C,
-                                 int bf16, cudaStream_t stream);
+                                 int bf16, int layout, cudaStream_t stream);
 }
 
 namespace {
@@ -184,9 +189,40 @@ extern "C" int wino_filter_transform(const void* weight, void* ucache, int k, in
   if (!weight || !ucache) return WINO_EINVAL;
   const int st = wino_check_shape(1, c, 1, 1, k);
   if (st != WINO_OK) return st;
-  return wino_launch_filter_transform(weight, ucache, nullptr, k, c, 0, (cudaStream_t)stream) == 0
+  return wino_launch_filter_transform(weight, ucache, nullptr, k, c, 0, 0, (cudaStream_t)stream) == 0
              ? WINO_OK
              : WINO_ECUDA;
+}
+
+extern "C" int wino_filter_transform_unfused(const void* weight, void* ucache2, int k, int c,
+                                             void* stream) {
+  if (!weight || !ucache2) return WINO_EINVAL;
+  const int st = wino_check_shape(1, c, 1, 1, k);
+  if (st != WINO_OK) return st;
+  return wino_launch_filter_transform(weight, ucache2, nullptr, k, c, 0, 1, (cudaStream_t)stream) == 0
+             ? WINO_OK
+             : WINO_ECUDA;
+}
+
+extern "C" int wino_unfused_workspace_bytes(int n, int c, int h, int w, int k, size_t* v_bytes,
+                                            size_t* m_bytes) {
+  if (!v_bytes || !m_bytes) return WINO_EINVAL;
+  const int st = wino_check_shape(n, c, h, w, k);
+  if (st != WINO_OK) return st;
+  *v_bytes = wino_unfused_v_bytes(n, c, h, w);
+  *m_bytes = wino_unfused_m_bytes(n, k, h, w);
+  return WINO_OK;
+}
+
+extern "C" int wino_conv2d_unfused(const void* x, const void* ucache2, void* y, void* v_ws,
+                                   void* m_ws, int n, int c, int h, int w, int k, void* stream) {
+  if (!x || !ucache2 || !y || !v_ws || !m_ws) return WINO_EINVAL;
+  const int st = wino_check_shape(n, c, h, w, k);
+  if (st != WINO_OK) return st;
+  if (wino_unfused_prepare() != 0) return WINO_ECUDA;
+  wino::KernelParam p = make_param(x, nullptr, y, v_ws, const_cast<void*>(ucache2), m_ws, n, c, h,
+                                   w, k);
+  return wino_unfused_launch(&p, sm_count(), (cudaStream_t)stream) == 0 ? WINO_OK : WINO_ECUDA;
 }
 
 extern "C" int wino_conv2d_fused(const void* x, const void* ucache, void* y, int n, int c, int h,
@@ -223,6 +259,8 @@ extern "C" int wino_launch_kernelinfo(const void* kiv, void* param, void* stream
 
 extern "C" int wino_error_read_clear(uint32_t* code) {
   if (!code) return WINO_EINVAL;
-  *code = wino_fused_error_read_clear();
+  const uint32_t a = wino_fused_error_read_clear();
+  const uint32_t b = wino_unfused_error_read_clear();
+  *code = a ? a : b;
   return WINO_OK;
 }

@@ -63,6 +63,37 @@ __host__ __device__ __forceinline__ size_t u8_offset(int t, int k, int c, int K,
          (cc >> 4) * 128 + (kr & 7) * 16 + (cc & 15);
 }
 
+// ---------------------------------------------- unfused-path layouts -------
+// The unfused comparator runs the 16 tap GEMMs as one batched GEMM with
+// 128 x 128 output tiles; its operands are laid out so that one pipeline
+// stage (up to four 16-channel K-steps) is a single contiguous copy.
+//   U2: per tap, k-blocks of KB2 = 128 rows (the last may be shorter), per
+//       k-block the K-steps in order, each K-step the canonical K-major
+//       layout of wino_common's U cache (8-row groups of two core matrices).
+//   V2: per tap, per 128-tile block, per K-step: 16 tile groups of two 8x8
+//       MN-major core matrices (8 channels x 8 tiles) = 4 KB.
+//   M16: M[t][k][tile] fp16, tiles padded to whole 128-tile blocks.
+constexpr int KB2 = 128;
+constexpr int TB2 = 128;
+
+__host__ __device__ __forceinline__ int kblock2_rows(int kb, int K) {
+  const int r = K - kb * KB2;
+  return r < KB2 ? r : KB2;
+}
+
+__host__ __device__ __forceinline__ size_t u2_piece(int t, int kb, int cs, int K, int C) {
+  return (size_t)t * K * C + (size_t)kb * KB2 * C + (size_t)cs * kblock2_rows(kb, K) * 16;
+}
+
+__host__ __device__ __forceinline__ size_t u2_offset(int t, int k, int c, int K, int C) {
+  const int kb = k / KB2, kr = k % KB2, cs = c >> 4, cc = c & 15;
+  return u2_piece(t, kb, cs, K, C) + (kr >> 3) * 128 + (cc >> 3) * 64 + (kr & 7) * 8 + (cc & 7);
+}
+
+__host__ __device__ __forceinline__ size_t v2_piece(int t, int tb, int cs, int nTB, int CS) {
+  return (((size_t)t * nTB + tb) * CS + cs) * (size_t)(TB2 * 16);
+}
+
 // G g G^T of one 3x3 filter, in fp32 (16 outputs, row-major over the tap).
 __host__ __device__ __forceinline__ void filter_tile(const float g[9], float u[16]) {
   float tmp[4][3];

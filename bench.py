@@ -1,0 +1,422 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 Winograd F(2x2,3x3) fp16 conv2d.
+
+One step = one forward conv of the single-large-layer workload
+(N=128, C=K=256, H=W=28, 3x3, stride 1, pad 1; x = ReLU(N(0,1)),
+w ~ N(0, 2/(9C)), seed 0), run through the drop-in ABI exactly as the
+reference harness runs it: getkernelInfo once, then per step the four launch
+slots (filter transform, fused conv, two empty slots).
+
+Printed (rank 0, one JSON line):
+  value      direct-conv-equivalent TFLOP/s (2*N*K*C*P*Q*9 / time), whole job,
+             inputs resident in HBM, L2 flushed between steps
+  e2e        the same metric through the C-ABI with host buffers: each step
+             copies x host->device, runs the four slots, copies y back
+  roofline   the fused conv kernel against the tensor-pipe roofline: Winograd
+             GEMM FLOPs (2*16*K*C*N*ceil(P/2)*ceil(Q/2)) per launch over its
+             CUDA-event time, peak from MEASURED_PEAKS.json
+  cpu_baseline  the reference's own conv2dcpu (oracle/_ref) on this host's
+             cores over a bounded sample of images
+plus the fused-vs-unfused comparison and the error against FP64.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Multi-GPU (torchrun): every rank runs an independent replica (the operator
+does not shard); value = all ranks' FLOPs / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import importlib
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(n=128, c=256, h=28, w=28, k=256)
+WORKLOAD_NAME = "conv2d N128 C256 H28 W28 K256 3x3 s1 p1 fp16 (single large layer)"
+METRIC = "direct-conv-equiv TFLOP/s"
+L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
+
+
+def direct_flops(n, c, h, w, k):
+    return 2.0 * n * k * c * h * w * 9
+
+
+def wino_flops(n, c, h, w, k):
+    return 2.0 * 16 * k * c * n * ((h + 1) // 2) * ((w + 1) // 2)
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return dict(hbm_gbs=d["hbm_gbs"], tflops=d["bf16_tflops"],
+                    tflops_sustained=d.get("bf16_tflops_sustained"), source="measured")
+    except (OSError, KeyError, ValueError):
+        return dict(hbm_gbs=6650.0, tflops=1590.0, tflops_sustained=1400.0, source="fallback")
+
+
+def committed_traffic():
+    """DRAM bytes per fused launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "fused_conv_n128_c256_h28.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get("dram_bytes_per_launch")
+    except (OSError, ValueError):
+        return None
+
+
+# ------------------------------------------------------------------ clocks --
+class ClockSampler:
+    """Samples SM clock, power and throttle reasons through NVML."""
+
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown",
+               0x4: "sw_power_cap", 0x80: "hw_power_brake_slowdown", 0x1: "gpu_idle"}
+
+    def __init__(self, index, period_s=0.005):
+        self.samples = []
+        self.period = period_s
+        self._stop = threading.Event()
+        self._thread = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_sm = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        except Exception:  # noqa: BLE001 - NVML absent: report no clocks
+            self.nvml = None
+            self.max_sm = None
+
+    def _run(self):
+        nv = self.nvml
+        while not self._stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                pw = nv.nvmlDeviceGetPowerUsage(self.h) / 1000.0
+                self.samples.append((sm, rs, pw))
+            except Exception:  # noqa: BLE001
+                pass
+            time.sleep(self.period)
+
+    def __enter__(self):
+        if self.nvml:
+            self._thread = threading.Thread(target=self._run, daemon=True)
+            self._thread.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._thread:
+            self._thread.join()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_sm, "reasons": [], "samples": 0}
+        busy = [s for s in self.samples if not (s[1] & 0x1)] or self.samples
+        reasons = set()
+        for _, rs, _ in busy:
+            for bit, name in self.REASONS.items():
+                if rs & bit and name != "gpu_idle":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(s[0] for s in busy), "sm_max_mhz": self.max_sm,
+                "reasons": sorted(reasons), "samples": len(busy),
+                "power_w_max": max(s[2] for s in busy)}
+
+
+# ------------------------------------------------------------- CPU legs -----
+def cpu_reference_sample(seed=0, images=None, threads=None):
+    """Time the reference's conv2dcpu (oracle/_ref, unmodified verfiy.h) on
+    `images` images of the workload with all host threads."""
+    import numpy as np
+    import oracle
+    variants = oracle.ref_variants()
+    variant = "avx512fp16" if "avx512fp16" in variants else "portable"
+    threads = threads or oracle.ref_max_threads(variant)
+    images = images or max(2, threads)
+    W = WORKLOAD
+    x, w = oracle.make_inputs(images, W["c"], W["h"], W["w"], W["k"], seed=seed,
+                              x_dist="relu_normal", w_std=np.sqrt(2.0 / (9 * W["c"])))
+    t0 = time.perf_counter()
+    oracle.ref_conv2dcpu(x, w, threads=threads, variant=variant)
+    dt = time.perf_counter() - t0
+    flops = direct_flops(images, W["c"], W["h"], W["w"], W["k"])
+    return dict(tflops=flops / dt / 1e12, seconds=dt, images=images, threads=threads,
+                variant=variant)
+
+
+def run_reference_arm(args, rank):
+    if rank != 0:
+        return 0
+    samples = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_reference_sample(seed=i)
+        if i >= args.warmup:
+            samples.append(r)
+    secs = sum(s["seconds"] for s in samples)
+    flops = sum(direct_flops(s["images"], WORKLOAD["c"], WORKLOAD["h"], WORKLOAD["w"],
+                             WORKLOAD["k"]) for s in samples)
+    value = flops / secs / 1e12
+    s0 = samples[0]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "TFLOP/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": secs / len(samples) * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f16", "data": "synthetic (seeded)",
+        "config": {"workload": WORKLOAD_NAME, **WORKLOAD,
+                   "step": f"{s0['images']} images of the workload on the host CPU"},
+        "cpu_baseline": {"value": value, "unit": "TFLOP/s", "cores": s0["threads"],
+                         "kind": "reference",
+                         "sample": f"{s0['images']} of {WORKLOAD['n']} images per step, "
+                                   f"conv2dcpu build '{s0['variant']}', OpenMP over images"},
+        "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------- GPU arm ------
+def run_ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+    import oracle
+    wino = importlib.import_module("2024pra_conv_b200")
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    W = WORKLOAD
+    n, c, h, w, k = W["n"], W["c"], W["h"], W["w"], W["k"]
+    x16, w16 = oracle.make_inputs(n, c, h, w, k, seed=rank, x_dist="relu_normal",
+                                  w_std=np.sqrt(2.0 / (9 * c)))
+    x = torch.from_numpy(x16).to(dev)
+    wt = torch.from_numpy(w16).to(dev)
+    y = torch.empty((n, k, h, w), dtype=torch.float16, device=dev)
+    tf = torch.empty(16 * k * c, dtype=torch.float16, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+
+    # drop-in ABI: problem, getParamsize, getkernelInfo (once, as the harness)
+    pr = wino.make_problem(x, wt, y, None, tf, None)
+    param = (ctypes.c_char * wino.get_param_size(pr))()
+    code, ki = wino.get_kernel_info(pr, param)
+    if code != 0:
+        raise SystemExit(f"getkernelInfo failed: {code}")
+
+    def step():
+        wino.launch_kernel_info(ki, param, stream)
+
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+
+    def timed(fn, iters, flush_between=True):
+        """Sum of per-iteration CUDA-event times (ms) on the current stream."""
+        total = 0.0
+        times = []
+        for _ in range(iters):
+            if flush_between:
+                flush.zero_()
+            a, b = ev(), ev()
+            a.record(stream)
+            fn()
+            b.record(stream)
+            b.synchronize()
+            dt = a.elapsed_time(b)
+            times.append(dt)
+            total += dt
+        return total, times
+
+    sampler = ClockSampler(local_rank)
+    with sampler:
+        for _ in range(max(args.warmup, 3)):
+            step()
+        torch.cuda.synchronize()
+        # soak so the clocks under load are steady before the timed steps
+        t_end = time.time() + args.soak
+        while time.time() < t_end:
+            step()
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        total_ms, step_ms = timed(step, args.steps)
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+    clocks = sampler.summary()
+
+    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    max_ms = float(t.item())
+    dflops = direct_flops(n, c, h, w, k)
+    value = dflops * args.steps * world / (max_ms * 1e-3) / 1e12
+
+    # --- parity of the timed path (outside the timed region)
+    y64 = torch.nn.functional.conv2d(x.double(), wt.double(), padding=1)
+    yd = y.double()
+    rel_l2 = float(torch.linalg.vector_norm(yd - y64) / torch.linalg.vector_norm(y64))
+    max_norm = float((yd - y64).abs().max() / y64.abs().max())
+    del y64, yd
+
+    # --- per-kernel pieces: filter transform, fused conv on cached U, unfused path
+    ucache = wino.filter_transform(wt)
+    torch.cuda.synchronize()
+    iters = max(args.steps, 10)
+    ft_ms, _ = timed(lambda: wino.filter_transform(wt, stream), iters)
+    yf = torch.empty_like(y)
+    fused_ms, fused_times = timed(lambda: wino.conv2d_fused(x, ucache, k, out=yf, stream=stream), iters)
+    u2 = wino.filter_transform_unfused(wt)
+    ws = wino.UnfusedWorkspace(n, c, h, w, k, dev)
+    yu = torch.empty_like(y)
+    unf_ms, _ = timed(lambda: wino.conv2d_unfused(x, u2, k, ws=ws, out=yu, stream=stream), iters)
+    torch.cuda.synchronize()
+    unf_rel = float(torch.linalg.vector_norm(yu.double() - y.double()) /
+                    torch.linalg.vector_norm(y.double()))
+    del ws
+    fused_us = fused_ms / iters * 1e3
+    unfused_us = unf_ms / iters * 1e3
+    ft_us = ft_ms / iters * 1e3
+
+    # --- end to end through the C-ABI with host buffers
+    xh = torch.empty_like(x, device="cpu").pin_memory()
+    xh.copy_(x)
+    yh = torch.empty_like(y, device="cpu").pin_memory()
+
+    def e2e_step():
+        x.copy_(xh, non_blocking=True)
+        step()
+        yh.copy_(y, non_blocking=True)
+
+    for _ in range(2):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_ms, _ = timed(e2e_step, args.steps, flush_between=False)
+    te = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
+    e2e_value = dflops * args.steps * world / (float(te.item()) * 1e-3) / 1e12
+
+    errcode = wino.error_read_clear()
+    if errcode:
+        raise SystemExit(f"device error word {errcode}")
+
+    if rank != 0:
+        return 0
+    peaks = measured_peaks()
+    wflops = wino_flops(n, c, h, w, k)
+    achieved = wflops / (fused_us * 1e-6) / 1e12
+    traffic = committed_traffic()
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        try:
+            r = cpu_reference_sample()
+            cpu = {"value": r["tflops"], "unit": "TFLOP/s", "cores": r["threads"],
+                   "kind": "reference",
+                   "sample": f"{r['images']} of {n} images of the workload, reference conv2dcpu "
+                             f"build '{r['variant']}', {r['seconds']:.1f} s"}
+        except Exception as e:  # noqa: BLE001 - report, do not fail the GPU numbers
+            cpu = {"value": None, "unit": "TFLOP/s", "cores": None, "kind": "reference",
+                   "sample": f"unavailable: {e}"}
+    line = {
+        "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world,
+        "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": max_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f16",
+        "data": "synthetic (seeded ReLU(N(0,1)) input, N(0,2/(9C)) weights)",
+        "config": {"workload": WORKLOAD_NAME, **W, "parallelism": f"replicas x{world}",
+                   "step": "drop-in ABI: filter transform + fused conv + 2 empty slots",
+                   "l2": "flushed between steps (256 MB write)"},
+        "us_per_layer": max_ms / args.steps * 1e3,
+        "fused_us_cached_u": fused_us,
+        "fused_direct_equiv_tflops": dflops / (fused_us * 1e-6) / 1e12,
+        "filter_transform_us": ft_us,
+        "unfused_us": unfused_us,
+        "speedup_vs_unfused": unfused_us / fused_us,
+        "rel_l2": rel_l2, "max_norm": max_norm, "unfused_rel_diff": unf_rel,
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peaks["tflops"],
+                     "unit": "TFLOP/s", "frac": achieved / peaks["tflops"],
+                     "traffic": traffic, "peak_source": peaks["source"],
+                     "kernel": "fused_wino_f16_kernel",
+                     "algorithmic": "Winograd GEMM FLOPs 2*16*K*C*N*ceil(H/2)*ceil(W/2) per launch"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": "TFLOP/s", "h2d_bytes_per_step": x.numel() * 2,
+                "d2h_bytes_per_step": y.numel() * 2},
+        "gpu_launches": 4 * args.steps,
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_only(args):
+    """Launch one kernel family `args.steps` times on the workload with batch
+    `args.n` (for profiler captures; prints nothing measured)."""
+    import numpy as np
+    import torch
+    import oracle
+    wino = importlib.import_module("2024pra_conv_b200")
+    dev = torch.device("cuda", 0)
+    W = dict(WORKLOAD, n=args.n or WORKLOAD["n"])
+    n, c, h, w, k = W["n"], W["c"], W["h"], W["w"], W["k"]
+    x16, w16 = oracle.make_inputs(n, c, h, w, k, seed=0, x_dist="relu_normal",
+                                  w_std=np.sqrt(2.0 / (9 * c)))
+    x = torch.from_numpy(x16).to(dev)
+    wt = torch.from_numpy(w16).to(dev)
+    if args.only == "fused":
+        u = wino.filter_transform(wt)
+        for _ in range(args.steps):
+            wino.conv2d_fused(x, u, k)
+    elif args.only == "unfused":
+        u2 = wino.filter_transform_unfused(wt)
+        ws = wino.UnfusedWorkspace(n, c, h, w, k, dev)
+        for _ in range(args.steps):
+            wino.conv2d_unfused(x, u2, k, ws=ws)
+    else:
+        for _ in range(args.steps):
+            wino.dropin_conv2d(x, wt)
+    torch.cuda.synchronize()
+    code = wino.error_read_clear()
+    print(json.dumps({"only": args.only, "n": n, "launches": args.steps, "device_error": code}))
+    return 1 if code else 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--soak", type=float, default=1.0, help="seconds of untimed load before timing")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--only", choices=["fused", "unfused", "dropin"],
+                    help="only launch this path (profiler captures)")
+    ap.add_argument("--n", type=int, default=0, help="batch size for --only")
+    args = ap.parse_args()
+    if args.only:
+        return run_only(args)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference_arm(args, rank)
+    if world > 1:
+        import datetime
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        return run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

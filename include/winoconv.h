@@ -58,6 +58,19 @@ int wino_filter_transform(const void* weight, void* ucache, int k, int c, void* 
 int wino_conv2d_fused(const void* x, const void* ucache, void* y, int n, int c, int h, int w,
                       int k, void* stream);
 
+/* The plain unfused path, the comparator of the fused kernel: input
+ * transform to V in global memory, the 16 tap GEMMs as one batched tcgen05
+ * GEMM writing M (fp16) to global memory, output transform -- the stage
+ * structure of the reference pipeline (src/preprocessing.cuh:273-424,
+ * src/matrixmul.cuh:139-556, src/conv2d.cpp:17-250).  It reads U in its own
+ * layout, made by wino_filter_transform_unfused; v_ws and m_ws are caller
+ * workspaces of the sizes wino_unfused_workspace_bytes reports. */
+int wino_filter_transform_unfused(const void* weight, void* ucache2, int k, int c, void* stream);
+int wino_unfused_workspace_bytes(int n, int c, int h, int w, int k, size_t* v_bytes,
+                                 size_t* m_bytes);
+int wino_conv2d_unfused(const void* x, const void* ucache2, void* y, void* v_ws, void* m_ws, int n,
+                        int c, int h, int w, int k, void* stream);
+
 /* Launch the four slots of a kernelInfo_t filled by getkernelInfo, in order,
  * on `stream`, each with args[0] = param: the launch sequence of the
  * reference harness (reference src/main.cpp:105-108).  `ki` is `const

@@ -134,5 +134,34 @@ def test_dropin_slots_are_the_expected_kernels(wino, cuda):
     assert ki.slot(2)["lds"] > 48 * 1024  # the fused kernel's pipeline
 
 
-def test_no_device_errors_recorded(wino, cuda):
+def _unfused(wino, x16, w16, dev):
+    import torch
+    x = _t(x16, dev)
+    w = _t(w16, dev)
+    y = wino.conv2d_unfused(x, wino.filter_transform_unfused(w), w.shape[0])
+    torch.cuda.synchronize()
+    return y.cpu().numpy()
+
+
+@pytest.mark.parametrize("shape", [
+    (1, 16, 3, 5, 16), (2, 48, 9, 12, 32), (1, 64, 40, 40, 144), (3, 16, 18, 18, 32),
+    (8, 64, 32, 32, 64),
+])
+def test_unfused_path_parity(wino, cuda, oracle_mod, shape):
+    """The plain unfused comparator (V and M through global memory) meets the
+    same bar as the fused kernel."""
+    n, c, h, w, k = shape
+    x, wt = oracle_mod.make_inputs(n, c, h, w, k, seed=7 + sum(shape), x_dist="uniform")
+    y = _unfused(wino, x, wt, cuda)
+    _check(oracle_mod, y, oracle_mod.conv2d_f64(x, wt), f"unfused {shape}")
+
+
+def test_unfused_large_layer(wino, cuda, oracle_mod):
+    x, w = oracle_mod.make_inputs(128, 256, 28, 28, 256, seed=0, x_dist="relu_normal",
+                                  w_std=np.sqrt(2.0 / (9 * 256)))
+    y = _unfused(wino, x, w, cuda)
+    _check(oracle_mod, y, _fp64_gpu(x, w, cuda), "unfused N128 C256 H28 K256")
+
+
+def test_zz_no_device_errors_recorded(wino, cuda):
     assert wino.error_read_clear() == 0
