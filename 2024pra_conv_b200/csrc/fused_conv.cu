@@ -9,19 +9,25 @@
 //   output transform A^T m A    src/conv2d.cpp:17-250 (store, store1..5)
 // which there run as three kernels with V and M round-tripping through HBM.
 //
-// Work unit ("block"): 128 consecutive Winograd tiles x 32 output channels.
-// The tensor core computes, per tap t,
-//     M_t[tile][k] = sum_c V_t[tile][c] * U_t[k][c]
-// as a 128 x 32 x 16 MMA per 16-channel step, accumulating in TMEM: lane =
-// tile, columns t*32 .. t*32+31 = output channels (16 taps x 32 = 512 cols).
+// Work unit ("block"): 128 output channels x 32 consecutive Winograd tiles.
+// Per tap t the tensor core computes
+//     M_t[k][tile] = sum_c U_t[k][c] * V_t[c][tile]
+// as a 128 x 32 x 16 MMA per 16-channel step (A = U from the U cache, B = V
+// produced on chip), accumulating in TMEM: lane = output channel, columns
+// t*32 .. t*32+31 = tiles (16 taps x 32 = all 512 columns).  All 16 taps of
+// a (k, tile) pair live in one thread's lane, so the output transform is
+// per-thread register arithmetic.  With output channels on the 128-row side
+// each V element feeds 128 channels, which keeps the CUDA-core input
+// transform small next to the MMAs.
 //
-// Warp roles (18 warps):
+// Warp roles (14 warps):
 //   warp 0       TMEM allocation; one thread issues the MMAs
-//   warp 1       one thread bulk-copies the U piece of each 16-channel step
-//   warps 2-9    V producers: B^T d B in packed fp16 straight into the
-//                MN-major shared-memory operand (8 tiles x 8 channels per
-//                core matrix), two stages deep
-//   warps 10-17  epilogue: drain TMEM tap by tap (each drained tap is handed
+//   warp 1       one thread bulk-copies the U piece (16 taps x 128 k x 16 c,
+//                64 KB) of each 16-channel step
+//   warps 2-5    V producers, B^T d B in packed fp16 straight into the
+//                MN-major operand (8 channels x 8 tiles per core matrix);
+//                warps 2-3 fill stage 0, warps 4-5 stage 1
+//   warps 6-13   epilogue: drain TMEM tap by tap (each drained tap is handed
 //                back to the MMA thread at once, so the next block's MMAs
 //                overlap the drain), A^T m A in fp32, fp16 NKPQ stores.
 #include <cuda_runtime.h>
@@ -35,16 +41,16 @@ static __device__ uint32_t g_fused_err;
 
 namespace fused {
 
-constexpr int TILES = 128;             // MMA M: tiles per block
+constexpr int TILES = 32;              // MMA N: tiles per block
 constexpr int NTAP = 16;
-constexpr int V_TAP_BYTES = TILES * 16 * 2;          // 4 KB per tap per step
-constexpr int V_STAGE_BYTES = NTAP * V_TAP_BYTES;    // 64 KB
-constexpr int U_STAGE_BYTES = NTAP * KB * 16 * 2;    // 16 KB (full k-block)
-constexpr int STAGE_BYTES = V_STAGE_BYTES + U_STAGE_BYTES;
+constexpr int V_TAP_BYTES = TILES * 16 * 2;          // 1 KB per tap per step
+constexpr int V_STAGE_BYTES = NTAP * V_TAP_BYTES;    // 16 KB
+constexpr int U_STAGE_BYTES = NTAP * KB * 16 * 2;    // 64 KB (full k-block)
+constexpr int STAGE_BYTES = U_STAGE_BYTES + V_STAGE_BYTES;
 constexpr int NSTAGE = 2;
-constexpr int NWARP = 18;
+constexpr int NWARP = 14;
 constexpr int NTHREAD = NWARP * 32;
-constexpr int WARP_MMA = 0, WARP_U = 1, WARP_V0 = 2, NWARP_V = 8, WARP_E0 = 10, NWARP_E = 8;
+constexpr int WARP_MMA = 0, WARP_U = 1, WARP_V0 = 2, NWARP_V = 4, WARP_E0 = 6, NWARP_E = 8;
 constexpr int SMEM_BYTES = NSTAGE * STAGE_BYTES + 1024;
 
 struct Shared {
@@ -71,13 +77,15 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
   __shared__ Shared sh;
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const Geometry g = make_geometry(p, TILES);
+  const int nKB = (g.K + KB - 1) / KB;
+  const long long nblocks = (long long)g.nTB * nKB;
   const int warp = warp_id();
   const int lane = lane_id();
   uint32_t* err = &g_fused_err;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < NSTAGE; ++s) {
-      mbar_init(&sh.full[s], NWARP_V + 1);
+      mbar_init(&sh.full[s], 2 + 1);  // the stage's two V warps + the U copy
       mbar_init(&sh.empty[s], 1);
     }
     mbar_init(&sh.accf, 1);
@@ -95,16 +103,16 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
   const uint32_t tmem = sh.tmem_base;
   volatile int* abort_flag = &sh.abort_flag;
   const uint32_t smem_base = smem_u32(smem);
-  auto v_stage = [&](int s) { return smem_base + s * STAGE_BYTES; };
-  auto u_stage = [&](int s) { return smem_base + s * STAGE_BYTES + V_STAGE_BYTES; };
+  auto u_stage = [&](int s) { return smem_base + s * STAGE_BYTES; };
+  auto v_stage = [&](int s) { return smem_base + s * STAGE_BYTES + U_STAGE_BYTES; };
 
   if (warp == WARP_MMA) {
     if (lane == 0) {
+      const uint32_t idesc = instr_desc(128, TILES, 0, 0, /*a_mn=*/0, /*b_mn=*/1);
       uint32_t it = 0, bi = 0;
-      for (long long b = blockIdx.x; b < g.nblocks && !*abort_flag; b += gridDim.x, ++bi) {
-        const int kb = (int)(b % g.nKB);
+      for (long long b = blockIdx.x; b < nblocks && !*abort_flag; b += gridDim.x, ++bi) {
+        const int kb = (int)(b % nKB);
         const int kbs = kblock_rows(kb, g.K);
-        const uint32_t idesc = instr_desc(128, kbs, 0, 0, 1, 0);
         for (int s = 0; s < g.CS; ++s, ++it) {
           const int st = it & 1;
           if (!mbar_wait(&sh.full[st], (it >> 1) & 1, abort_flag, err, ERR_WAIT_FULL)) break;
@@ -115,9 +123,9 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
               if (!mbar_wait(&sh.tapfree[t], (bi - 1) & 1, abort_flag, err, ERR_WAIT_DRAIN)) break;
               tc_fence_after();
             }
-            const uint64_t ad = smem_desc(v_stage(st) + t * V_TAP_BYTES, 128, 256);
-            const uint64_t bd = smem_desc(u_stage(st) + t * kbs * 32, 128, 256);
-            mma_f16(tmem + t * KB, ad, bd, idesc, s > 0 ? 1u : 0u);
+            const uint64_t ad = smem_desc(u_stage(st) + t * kbs * 32, 128, 256);
+            const uint64_t bd = smem_desc(v_stage(st) + t * V_TAP_BYTES, 128, 256);
+            mma_f16(tmem + t * TILES, ad, bd, idesc, s > 0 ? 1u : 0u);
           }
           mma_commit(&sh.empty[st]);
         }
@@ -129,8 +137,8 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
     if (lane == 0) {
       const __half* ucache = static_cast<const __half*>(p.transform_filter);
       uint32_t it = 0;
-      for (long long b = blockIdx.x; b < g.nblocks && !*abort_flag; b += gridDim.x) {
-        const int kb = (int)(b % g.nKB);
+      for (long long b = blockIdx.x; b < nblocks && !*abort_flag; b += gridDim.x) {
+        const int kb = (int)(b % nKB);
         const uint32_t bytes = NTAP * kblock_rows(kb, g.K) * 16 * 2;
         for (int s = 0; s < g.CS; ++s, ++it) {
           const int st = it & 1;
@@ -138,25 +146,27 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
               !mbar_wait(&sh.empty[st], ((it >> 1) - 1) & 1, abort_flag, err, ERR_WAIT_EMPTY))
             break;
           mbar_arrive_expect_tx(&sh.full[st], bytes);
-          bulk_g2s(smem + st * STAGE_BYTES + V_STAGE_BYTES, ucache + u_piece(kb, s, g.K, g.C), bytes,
-                   &sh.full[st]);
+          bulk_g2s(smem + st * STAGE_BYTES, ucache + u_piece(kb, s, g.K, g.C), bytes, &sh.full[st]);
         }
       }
       if (*abort_flag) __nanosleep(20000);  // let copies already issued land
     }
     __syncwarp();
   } else if (warp >= WARP_V0 && warp < WARP_V0 + NWARP_V) {
+    // Warps 2-3 produce the even steps (stage 0), warps 4-5 the odd ones.
     const int vw = warp - WARP_V0;
-    const int grp = 2 * vw + (lane >> 4);  // tile group (8 tiles) 0..15
-    const int cl = lane & 15;              // channel inside the step
+    const int my_stage = vw >> 1;
+    const int grp = 2 * (vw & 1) + (lane >> 4);  // tile group (8 tiles) 0..3
+    const int cl = lane & 15;                    // channel inside the step
     const __half* X = static_cast<const __half*>(p.pin);
     uint32_t it = 0;
-    for (long long b = blockIdx.x; b < g.nblocks && !*abort_flag; b += gridDim.x) {
-      const long long tb = b / g.nKB;
+    bool ok = true;
+    for (long long b = blockIdx.x; b < nblocks && ok && !*abort_flag; b += gridDim.x) {
+      const long long tb = b / nKB;
       const long long tile0 = tb * TILES + grp * 8;
-      bool ok = true;
       for (int s = 0; s < g.CS; ++s, ++it) {
         const int st = it & 1;
+        if (st != my_stage) continue;
         if (it >= NSTAGE &&
             !mbar_wait(&sh.empty[st], ((it >> 1) - 1) & 1, abort_flag, err, ERR_WAIT_EMPTY)) {
           ok = false;
@@ -171,74 +181,74 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
         __syncwarp();
         if (lane == 0) mbar_arrive(&sh.full[st]);
       }
-      if (!ok) break;
     }
   } else if (warp >= WARP_E0) {
-    const int quarter = warp & 3;            // TMEM lanes 32*quarter .. +31
-    const int half = (warp - WARP_E0) >> 2;  // output channels 16*half .. +15 of the block
+    const int quarter = warp & 3;            // TMEM lanes 32*quarter .. +31 = channels
+    const int half = (warp - WARP_E0) >> 2;  // tiles 16*half .. +15 of the block
     __half* Y = static_cast<__half*>(p.pout);
     const long long per_img = (long long)g.TP * g.TQ;
+    const bool q_even = (g.Q & 1) == 0;
     uint32_t bi = 0;
-    for (long long b = blockIdx.x; b < g.nblocks; b += gridDim.x, ++bi) {
+    for (long long b = blockIdx.x; b < nblocks; b += gridDim.x, ++bi) {
       if (!mbar_wait(&sh.accf, bi & 1, abort_flag, err, ERR_WAIT_ACCUM)) break;
       tc_fence_after();
-      const long long tb = b / g.nKB;
-      const int kb = (int)(b % g.nKB);
+      const long long tb = b / nKB;
+      const int kb = (int)(b % nKB);
       const int kbs = kblock_rows(kb, g.K);
-      const bool active = half * 16 < kbs;
       float y[16][4];
 #pragma unroll
-      for (int kk = 0; kk < 16; ++kk)
+      for (int j = 0; j < 16; ++j)
 #pragma unroll
-        for (int o = 0; o < 4; ++o) y[kk][o] = 0.f;
+        for (int o = 0; o < 4; ++o) y[j][o] = 0.f;
       const uint32_t tbase = tmem + ((uint32_t)(quarter * 32) << 16) + half * 16;
 #pragma unroll
       for (int t = 0; t < NTAP; ++t) {
         float m[16];
-        if (active) {
-          tmem_ld16(tbase + t * KB, m);
-          tmem_ld_wait();
-        }
+        tmem_ld16(tbase + t * TILES, m);
+        tmem_ld_wait();
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(&sh.tapfree[t]);
-        if (active) {
-          const int a = t >> 2, bcol = t & 3;
-          const int c00 = at_coef(0, a) * at_coef(0, bcol), c01 = at_coef(0, a) * at_coef(1, bcol);
-          const int c10 = at_coef(1, a) * at_coef(0, bcol), c11 = at_coef(1, a) * at_coef(1, bcol);
+        const int a = t >> 2, bc = t & 3;
+        const float c00 = (float)(at_coef(0, a) * at_coef(0, bc));
+        const float c01 = (float)(at_coef(0, a) * at_coef(1, bc));
+        const float c10 = (float)(at_coef(1, a) * at_coef(0, bc));
+        const float c11 = (float)(at_coef(1, a) * at_coef(1, bc));
 #pragma unroll
-          for (int kk = 0; kk < 16; ++kk) {
-            y[kk][0] += (float)c00 * m[kk];
-            y[kk][1] += (float)c01 * m[kk];
-            y[kk][2] += (float)c10 * m[kk];
-            y[kk][3] += (float)c11 * m[kk];
-          }
+        for (int j = 0; j < 16; ++j) {
+          y[j][0] += c00 * m[j];
+          y[j][1] += c01 * m[j];
+          y[j][2] += c10 * m[j];
+          y[j][3] += c11 * m[j];
         }
       }
-      const long long tile = tb * TILES + quarter * 32 + lane;
-      if (active && tile < g.NT) {
-        const int n = (int)(tile / per_img);
-        const int r = (int)(tile - (long long)n * per_img);
-        const int ty = r / g.TQ, tx = r - (r / g.TQ) * g.TQ;
-        const int oy = 2 * ty, ox = 2 * tx;
-        const bool two_cols = ox + 1 < g.Q;
-        const bool two_rows = oy + 1 < g.P;
-        const bool q_even = (g.Q & 1) == 0;
+      const int k = kb * KB + quarter * 32 + lane;
+      if (quarter * 32 + lane < kbs) {
+        long long tile = tb * TILES + half * 16;
+        int n = (int)(tile / per_img);
+        int r = (int)(tile - (long long)n * per_img);
+        int ty = r / g.TQ, tx = r - ty * g.TQ;
 #pragma unroll
-        for (int kk = 0; kk < 16; ++kk) {
-          const int k = kb * KB + half * 16 + kk;
-          if (k >= g.K) break;
-          __half* o = Y + (((size_t)n * g.K + k) * g.P + oy) * (size_t)g.Q + ox;
-          if (two_cols && q_even) {
-            *reinterpret_cast<__half2*>(o) = __floats2half2_rn(y[kk][0], y[kk][1]);
-            if (two_rows) *reinterpret_cast<__half2*>(o + g.Q) = __floats2half2_rn(y[kk][2], y[kk][3]);
-          } else {
-            o[0] = __float2half_rn(y[kk][0]);
-            if (two_cols) o[1] = __float2half_rn(y[kk][1]);
-            if (two_rows) {
-              o[g.Q] = __float2half_rn(y[kk][2]);
-              if (two_cols) o[g.Q + 1] = __float2half_rn(y[kk][3]);
+        for (int j = 0; j < 16; ++j, ++tile) {
+          if (tile < g.NT) {
+            const int oy = 2 * ty, ox = 2 * tx;
+            const bool two_cols = ox + 1 < g.Q, two_rows = oy + 1 < g.P;
+            __half* o = Y + (((size_t)n * g.K + k) * g.P + oy) * (size_t)g.Q + ox;
+            if (two_cols && q_even) {
+              *reinterpret_cast<__half2*>(o) = __floats2half2_rn(y[j][0], y[j][1]);
+              if (two_rows) *reinterpret_cast<__half2*>(o + g.Q) = __floats2half2_rn(y[j][2], y[j][3]);
+            } else {
+              o[0] = __float2half_rn(y[j][0]);
+              if (two_cols) o[1] = __float2half_rn(y[j][1]);
+              if (two_rows) {
+                o[g.Q] = __float2half_rn(y[j][2]);
+                if (two_cols) o[g.Q + 1] = __float2half_rn(y[j][3]);
+              }
             }
+          }
+          if (++tx == g.TQ) {  // advance to the next tile
+            tx = 0;
+            if (++ty == g.TP) { ty = 0; ++n; }
           }
         }
       }

@@ -39,18 +39,26 @@ __device__ __forceinline__ Geometry make_geometry(const KernelParam& p, int tile
 
 // ---- input words ------------------------------------------------------------
 // A "word" is two horizontally adjacent fp16 inputs (cols 2m, 2m+1) of one row,
-// zero outside the image.  `row` points at column 0 of the row (or is null
-// for a row outside the image).
-__device__ __forceinline__ uint32_t load_word(const __half* row, int m, int W, bool w_even) {
-  if (!row) return 0u;
+// zero outside the image.  Loads are branch-free: an out-of-image word is read
+// from a zero word instead of being skipped, so the loads of a task issue
+// back to back and their latencies overlap.
+static __device__ const uint32_t g_zero_words[4] = {0u, 0u, 0u, 0u};
+
+// `row` points at column 0 of input row y (or anywhere when !row_ok).
+__device__ __forceinline__ uint32_t load_word(const __half* row, bool row_ok, int m, int W,
+                                             bool w_even) {
   const int c0 = 2 * m;
   if (w_even) {
-    if (m < 0 || c0 >= W) return 0u;
-    return __ldg(reinterpret_cast<const unsigned int*>(row) + m);
+    const bool ok = row_ok && m >= 0 && c0 < W;
+    const unsigned int* p = ok ? reinterpret_cast<const unsigned int*>(row) + m : g_zero_words;
+    return __ldg(p);
   }
   const unsigned short* r16 = reinterpret_cast<const unsigned short*>(row);
-  uint32_t lo = (c0 >= 0 && c0 < W) ? (uint32_t)__ldg(r16 + c0) : 0u;
-  uint32_t hi = (c0 + 1 >= 0 && c0 + 1 < W) ? (uint32_t)__ldg(r16 + c0 + 1) : 0u;
+  const unsigned short* z16 = reinterpret_cast<const unsigned short*>(g_zero_words);
+  const bool ok0 = row_ok && c0 >= 0 && c0 < W;
+  const bool ok1 = row_ok && c0 + 1 >= 0 && c0 + 1 < W;
+  const uint32_t lo = __ldg(ok0 ? r16 + c0 : z16);
+  const uint32_t hi = __ldg(ok1 ? r16 + c0 + 1 : z16);
   return lo | (hi << 16);
 }
 
@@ -111,9 +119,10 @@ __device__ __forceinline__ void produce_v8(const __half* __restrict__ X, const G
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
       const int y = 2 * ty0 - 1 + i;
-      const __half* row = (y >= 0 && y < g.H) ? plane + (size_t)y * g.W : nullptr;
+      const bool ok = y >= 0 && y < g.H;
+      const __half* row = plane + (size_t)(ok ? y : 0) * g.W;
 #pragma unroll
-      for (int j = 0; j < 10; ++j) d[i][j] = load_word(row, tx0 - 1 + j, g.W, true);
+      for (int j = 0; j < 10; ++j) d[i][j] = load_word(row, ok, tx0 - 1 + j, g.W, true);
     }
 #pragma unroll
     for (int a = 0; a < 4; ++a) {
@@ -137,40 +146,41 @@ __device__ __forceinline__ void produce_v8(const __half* __restrict__ X, const G
   } else {
     // General path: each tile locates its own window (row or image changes
     // inside the group, odd widths, tiles past the end of the batch).  Per
-    // e-row only the two input rows that B^T combines are read.
-    const __half* plane[8];
-    int tyv[8], txv[8];
-#pragma unroll
-    for (int s = 0; s < 8; ++s) {
-      const long long tile = tile0 + s;
-      if (tile < g.NT) {
-        const int n = (int)(tile / per_img);
-        const int r = (int)(tile - (long long)n * per_img);
-        tyv[s] = r / g.TQ;
-        txv[s] = r - tyv[s] * g.TQ;
-        plane[s] = X + ((size_t)n * g.C + c) * (size_t)g.H * g.W;
-      } else {
-        plane[s] = nullptr;
-        tyv[s] = 0;
-        txv[s] = 0;
-      }
+    // e-row only the two input rows that B^T combines are read; tile
+    // coordinates advance incrementally (consecutive tiles step tx, then ty,
+    // then the image).
+    int n1 = 0, ty1 = 0, tx1 = 0;
+    if (tile0 < g.NT) {
+      n1 = (int)(tile0 / per_img);
+      const int r = (int)(tile0 - (long long)n1 * per_img);
+      ty1 = r / g.TQ;
+      tx1 = r - ty1 * g.TQ;
     }
-#pragma unroll
+#pragma unroll 1
     for (int a = 0; a < 4; ++a) {
       // rows combined by Bt[a]: (0,2), (1,2), (2,1), (1,3) as (plus, minus / plus)
       const int ra = (a == 0) ? 0 : (a == 2 ? 2 : 1);
       const int rb = (a == 0) ? 2 : (a == 3 ? 3 : (a == 1 ? 2 : 1));
       uint32_t ew[8][3];
+      int n = n1, ty = ty1, tx = tx1;
 #pragma unroll
       for (int s = 0; s < 8; ++s) {
-        const int ya = 2 * tyv[s] - 1 + ra, yb = 2 * tyv[s] - 1 + rb;
-        const __half* rowa = (plane[s] && ya >= 0 && ya < g.H) ? plane[s] + (size_t)ya * g.W : nullptr;
-        const __half* rowb = (plane[s] && yb >= 0 && yb < g.H) ? plane[s] + (size_t)yb * g.W : nullptr;
+        const bool valid = tile0 + s < g.NT;
+        const int ya = 2 * ty - 1 + ra, yb = 2 * ty - 1 + rb;
+        const bool oka = valid && ya >= 0 && ya < g.H;
+        const bool okb = valid && yb >= 0 && yb < g.H;
+        const __half* base = X + ((size_t)(valid ? n : 0) * g.C + c) * (size_t)g.H * g.W;
+        const __half* rowa = base + (size_t)(oka ? ya : 0) * g.W;
+        const __half* rowb = base + (size_t)(okb ? yb : 0) * g.W;
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
-          const uint32_t wa = load_word(rowa, txv[s] - 1 + j, g.W, w_even);
-          const uint32_t wb = load_word(rowb, txv[s] - 1 + j, g.W, w_even);
+          const uint32_t wa = load_word(rowa, oka, tx - 1 + j, g.W, w_even);
+          const uint32_t wb = load_word(rowb, okb, tx - 1 + j, g.W, w_even);
           ew[s][j] = (a == 1) ? hadd2(wa, wb) : hsub2(wa, wb);
+        }
+        if (++tx == g.TQ) {
+          tx = 0;
+          if (++ty == g.TP) { ty = 0; ++n; }
         }
       }
       uint32_t out[4][4];

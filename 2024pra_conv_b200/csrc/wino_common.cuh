@@ -26,14 +26,14 @@ namespace wino {
 // so that one K-step (16 input channels) of one output-channel block is a
 // single contiguous piece that a CTA fetches with one bulk copy:
 //
-//   k-blocks of KB = 32 output channels (the last one may hold 16),
+//   k-blocks of KB = 128 output channels (the last one may be shorter),
 //   inside a k-block: K-steps cs = c / 16, inside a K-step: taps t = 0..15,
 //   inside a tap: 8-row groups of k (256 bytes) each holding two 8 x 8 core
 //   matrices (channels 0-7 and 8-15 of the step), 8 k-rows x 16 bytes.
 //
 // A (k-block, K-step) piece holds 16 * kbs * 16 elements (kbs = rows of the
 // k-block), taps at a stride of kbs * 16 elements.  Total size 16*K*C.
-constexpr int KB = 32;
+constexpr int KB = 128;
 
 __host__ __device__ __forceinline__ int kblock_rows(int kb, int K) {
   const int r = K - kb * KB;

@@ -87,9 +87,9 @@ def test_check_shape(wino):
 def test_host_u_cache_layout_is_a_bijection():
     """The tile-major U offset formula visits every element exactly once."""
     import numpy as np
-    for K, C in [(32, 16), (48, 32), (16, 48), (80, 64)]:
+    for K, C in [(32, 16), (48, 32), (16, 48), (144, 32), (272, 16)]:
         seen = np.zeros(16 * K * C, np.int32)
-        KB = 32
+        KB = 128
         for t in range(16):
             for k in range(K):
                 for c in range(C):
