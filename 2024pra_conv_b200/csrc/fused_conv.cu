@@ -20,13 +20,17 @@
 // each V element feeds 128 channels, which keeps the CUDA-core input
 // transform small next to the MMAs.
 //
+// Pipelines (shared memory, 192 KB): U in four 32 KB slots, each half of a
+// step's piece (8 taps x 128 k x 16 c), and V in four 16 KB slots, one per
+// step.  Barrier hand-offs cost a few hundred cycles on this part, so each
+// side keeps several slots in flight.
+//
 // Warp roles (14 warps):
 //   warp 0       TMEM allocation; one thread issues the MMAs
-//   warp 1       one thread bulk-copies the U piece (16 taps x 128 k x 16 c,
-//                64 KB) of each 16-channel step
+//   warp 1       one thread bulk-copies the U half-pieces
 //   warps 2-5    V producers, B^T d B in packed fp16 straight into the
 //                MN-major operand (8 channels x 8 tiles per core matrix);
-//                warps 2-3 fill stage 0, warps 4-5 stage 1
+//                warps 2-3 fill the even steps, warps 4-5 the odd ones
 //   warps 6-13   epilogue: drain TMEM tap by tap (each drained tap is handed
 //                back to the MMA thread at once, so the next block's MMAs
 //                overlap the drain), A^T m A in fp32, fp16 NKPQ stores.
@@ -44,18 +48,18 @@ namespace fused {
 constexpr int TILES = 32;              // MMA N: tiles per block
 constexpr int NTAP = 16;
 constexpr int V_TAP_BYTES = TILES * 16 * 2;          // 1 KB per tap per step
-constexpr int V_STAGE_BYTES = NTAP * V_TAP_BYTES;    // 16 KB
-constexpr int U_STAGE_BYTES = NTAP * KB * 16 * 2;    // 64 KB (full k-block)
-constexpr int STAGE_BYTES = U_STAGE_BYTES + V_STAGE_BYTES;
-constexpr int NSTAGE = 2;
+constexpr int V_SLOT_BYTES = NTAP * V_TAP_BYTES;     // 16 KB: one step of V
+constexpr int U_SLOT_BYTES = 8 * KB * 16 * 2;        // 32 KB: 8 taps of a step of U
+constexpr int NVSLOT = 4, NUSLOT = 4;
+constexpr int U_BASE = 0, V_BASE = NUSLOT * U_SLOT_BYTES;
 constexpr int NWARP = 14;
 constexpr int NTHREAD = NWARP * 32;
 constexpr int WARP_MMA = 0, WARP_U = 1, WARP_V0 = 2, NWARP_V = 4, WARP_E0 = 6, NWARP_E = 8;
-constexpr int SMEM_BYTES = NSTAGE * STAGE_BYTES + 1024;
+constexpr int SMEM_BYTES = NUSLOT * U_SLOT_BYTES + NVSLOT * V_SLOT_BYTES + 1024;
 
 struct Shared {
-  uint64_t full[NSTAGE];
-  uint64_t empty[NSTAGE];
+  uint64_t ufull[NUSLOT], uempty[NUSLOT];
+  uint64_t vfull[NVSLOT], vempty[NVSLOT];
   uint64_t accf;
   uint64_t tapfree[NTAP];
   uint32_t tmem_base;
@@ -84,9 +88,13 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
   uint32_t* err = &g_fused_err;
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < NSTAGE; ++s) {
-      mbar_init(&sh.full[s], 2 + 1);  // the stage's two V warps + the U copy
-      mbar_init(&sh.empty[s], 1);
+    for (int s = 0; s < NUSLOT; ++s) {
+      mbar_init(&sh.ufull[s], 1);
+      mbar_init(&sh.uempty[s], 1);
+    }
+    for (int s = 0; s < NVSLOT; ++s) {
+      mbar_init(&sh.vfull[s], 2);  // the step's two V warps
+      mbar_init(&sh.vempty[s], 1);
     }
     mbar_init(&sh.accf, 1);
     for (int t = 0; t < NTAP; ++t) mbar_init(&sh.tapfree[t], NWARP_E);
@@ -103,83 +111,100 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
   const uint32_t tmem = sh.tmem_base;
   volatile int* abort_flag = &sh.abort_flag;
   const uint32_t smem_base = smem_u32(smem);
-  auto u_stage = [&](int s) { return smem_base + s * STAGE_BYTES; };
-  auto v_stage = [&](int s) { return smem_base + s * STAGE_BYTES + U_STAGE_BYTES; };
+  auto u_slot = [&](uint32_t s) { return smem_base + U_BASE + s * U_SLOT_BYTES; };
+  auto v_slot = [&](uint32_t s) { return smem_base + V_BASE + s * V_SLOT_BYTES; };
 
   if (warp == WARP_MMA) {
     if (lane == 0) {
       const uint32_t idesc = instr_desc(128, TILES, 0, 0, /*a_mn=*/0, /*b_mn=*/1);
       uint32_t it = 0, bi = 0;
-      for (long long b = blockIdx.x; b < nblocks && !*abort_flag; b += gridDim.x, ++bi) {
+      bool ok = true;
+      for (long long b = blockIdx.x; b < nblocks && ok; b += gridDim.x, ++bi) {
         const int kb = (int)(b % nKB);
         const int kbs = kblock_rows(kb, g.K);
-        for (int s = 0; s < g.CS; ++s, ++it) {
-          const int st = it & 1;
-          if (!mbar_wait(&sh.full[st], (it >> 1) & 1, abort_flag, err, ERR_WAIT_FULL)) break;
-          tc_fence_after();
+        for (int s = 0; s < g.CS && ok; ++s, ++it) {
+          const uint32_t vs = it % NVSLOT;
+          ok = mbar_wait(&sh.vfull[vs], (it / NVSLOT) & 1, abort_flag, err, ERR_WAIT_FULL);
+          for (int h = 0; h < 2 && ok; ++h) {
+            const uint32_t ui = 2 * it + h, us = ui % NUSLOT;
+            ok = mbar_wait(&sh.ufull[us], (ui / NUSLOT) & 1, abort_flag, err, ERR_WAIT_FULL);
+            if (!ok) break;
+            tc_fence_after();
 #pragma unroll 1
-          for (int t = 0; t < NTAP; ++t) {
-            if (s == 0 && bi > 0) {
-              if (!mbar_wait(&sh.tapfree[t], (bi - 1) & 1, abort_flag, err, ERR_WAIT_DRAIN)) break;
-              tc_fence_after();
+            for (int tt = 0; tt < 8; ++tt) {
+              const int t = 8 * h + tt;
+              if (s == 0 && bi > 0) {
+                ok = mbar_wait(&sh.tapfree[t], (bi - 1) & 1, abort_flag, err, ERR_WAIT_DRAIN);
+                if (!ok) break;
+                tc_fence_after();
+              }
+              const uint64_t ad = smem_desc(u_slot(us) + tt * kbs * 32, 128, 256);
+              const uint64_t bd = smem_desc(v_slot(vs) + t * V_TAP_BYTES, 128, 256);
+              mma_f16(tmem + t * TILES, ad, bd, idesc, s > 0 ? 1u : 0u);
             }
-            const uint64_t ad = smem_desc(u_stage(st) + t * kbs * 32, 128, 256);
-            const uint64_t bd = smem_desc(v_stage(st) + t * V_TAP_BYTES, 128, 256);
-            mma_f16(tmem + t * TILES, ad, bd, idesc, s > 0 ? 1u : 0u);
+            mma_commit(&sh.uempty[us]);
           }
-          mma_commit(&sh.empty[st]);
+          mma_commit(&sh.vempty[vs]);
         }
-        mma_commit(&sh.accf);
+        if (ok) mma_commit(&sh.accf);
       }
     }
     __syncwarp();
   } else if (warp == WARP_U) {
     if (lane == 0) {
-      const __half* ucache = static_cast<const __half*>(p.transform_filter);
-      uint32_t it = 0;
-      for (long long b = blockIdx.x; b < nblocks && !*abort_flag; b += gridDim.x) {
+      const uint8_t* ucache = static_cast<const uint8_t*>(p.transform_filter);
+      uint32_t ui = 0;
+      bool ok = true;
+      for (long long b = blockIdx.x; b < nblocks && ok; b += gridDim.x) {
         const int kb = (int)(b % nKB);
-        const uint32_t bytes = NTAP * kblock_rows(kb, g.K) * 16 * 2;
-        for (int s = 0; s < g.CS; ++s, ++it) {
-          const int st = it & 1;
-          if (it >= NSTAGE &&
-              !mbar_wait(&sh.empty[st], ((it >> 1) - 1) & 1, abort_flag, err, ERR_WAIT_EMPTY))
-            break;
-          mbar_arrive_expect_tx(&sh.full[st], bytes);
-          bulk_g2s(smem + st * STAGE_BYTES, ucache + u_piece(kb, s, g.K, g.C), bytes, &sh.full[st]);
+        const int kbs = kblock_rows(kb, g.K);
+        const uint32_t bytes = 8 * kbs * 16 * 2;
+        for (int s = 0; s < g.CS && ok; ++s) {
+          for (int h = 0; h < 2; ++h, ++ui) {
+            const uint32_t us = ui % NUSLOT;
+            if (ui >= NUSLOT &&
+                !mbar_wait(&sh.uempty[us], (ui / NUSLOT - 1) & 1, abort_flag, err, ERR_WAIT_EMPTY)) {
+              ok = false;
+              break;
+            }
+            mbar_arrive_expect_tx(&sh.ufull[us], bytes);
+            bulk_g2s(smem + U_BASE + us * U_SLOT_BYTES,
+                     ucache + u_piece(kb, s, g.K, g.C) * 2 + (size_t)h * bytes, bytes, &sh.ufull[us]);
+          }
         }
       }
       if (*abort_flag) __nanosleep(20000);  // let copies already issued land
     }
     __syncwarp();
   } else if (warp >= WARP_V0 && warp < WARP_V0 + NWARP_V) {
-    // Warps 2-3 produce the even steps (stage 0), warps 4-5 the odd ones.
+    // Warps 2-3 produce the even steps, warps 4-5 the odd ones.
     const int vw = warp - WARP_V0;
-    const int my_stage = vw >> 1;
+    const uint32_t parity_of_steps = vw >> 1;
     const int grp = 2 * (vw & 1) + (lane >> 4);  // tile group (8 tiles) 0..3
     const int cl = lane & 15;                    // channel inside the step
     const __half* X = static_cast<const __half*>(p.pin);
     uint32_t it = 0;
     bool ok = true;
-    for (long long b = blockIdx.x; b < nblocks && ok && !*abort_flag; b += gridDim.x) {
+    for (long long b = blockIdx.x; b < nblocks && ok; b += gridDim.x) {
       const long long tb = b / nKB;
       const long long tile0 = tb * TILES + grp * 8;
       for (int s = 0; s < g.CS; ++s, ++it) {
-        const int st = it & 1;
-        if (st != my_stage) continue;
-        if (it >= NSTAGE &&
-            !mbar_wait(&sh.empty[st], ((it >> 1) - 1) & 1, abort_flag, err, ERR_WAIT_EMPTY)) {
+        if ((it & 1) != parity_of_steps) continue;
+        const uint32_t vs = it % NVSLOT;
+        if (it >= NVSLOT &&
+            !mbar_wait_warp(&sh.vempty[vs], (it / NVSLOT - 1) & 1, abort_flag, err, ERR_WAIT_EMPTY)) {
           ok = false;
           break;
         }
-        const uint32_t dst = v_stage(st) + grp * 256 + (cl >> 3) * 128 + (cl & 7) * 16;
-        produce_v8(X, g, tile0, s * 16 + cl,
+        const uint32_t dst = v_slot(vs) + grp * 256 + (cl >> 3) * 128 + (cl & 7) * 16;
+        const int next_c = s + 2 < g.CS ? (s + 2) * 16 + cl : -1;
+        produce_v8(X, g, tile0, s * 16 + cl, next_c,
                    [&](int t, uint32_t a, uint32_t b2, uint32_t c2, uint32_t d2) {
                      st_shared_v4(dst + t * V_TAP_BYTES, a, b2, c2, d2);
                    });
         fence_proxy_async_shared();
         __syncwarp();
-        if (lane == 0) mbar_arrive(&sh.full[st]);
+        if (lane == 0) mbar_arrive(&sh.vfull[vs]);
       }
     }
   } else if (warp >= WARP_E0) {
@@ -190,7 +215,7 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
     const bool q_even = (g.Q & 1) == 0;
     uint32_t bi = 0;
     for (long long b = blockIdx.x; b < nblocks; b += gridDim.x, ++bi) {
-      if (!mbar_wait(&sh.accf, bi & 1, abort_flag, err, ERR_WAIT_ACCUM)) break;
+      if (!mbar_wait_warp(&sh.accf, bi & 1, abort_flag, err, ERR_WAIT_ACCUM, 128)) break;
       tc_fence_after();
       const long long tb = b / nKB;
       const int kb = (int)(b % nKB);

@@ -118,6 +118,32 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volati
   return mbar_wait_impl<false>(bar, parity, abort, err, code);
 }
 
+// Warp-wide wait: lane 0 polls (bounded, optional sleep between polls once
+// the wait is long) and the outcome is broadcast; all lanes of the warp call.
+__device__ __forceinline__ bool mbar_wait_warp(uint64_t* bar, uint32_t parity, volatile int* abort,
+                                               uint32_t* err, uint32_t code, uint32_t sleep_ns = 0) {
+  uint32_t ok = 1;
+  if ((threadIdx.x & 31) == 0) {
+    ok = 0;
+    if (mbar_try_wait(bar, parity)) {
+      ok = 1;
+    } else {
+      const uint64_t t0 = globaltimer_ns();
+      for (uint32_t i = 1;; ++i) {
+        if (mbar_try_wait(bar, parity)) { ok = 1; break; }
+        if (abort && *abort) break;
+        if (sleep_ns && i > 8) __nanosleep(sleep_ns);
+        if ((i & 63) == 0 && globaltimer_ns() - t0 > WINO_WAIT_NS) {
+          record_error(err, code);
+          if (abort) *abort = 1;
+          break;
+        }
+      }
+    }
+  }
+  return __shfl_sync(0xffffffffu, ok, 0) != 0;
+}
+
 __device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, uint32_t parity,
                                                   volatile int* abort, uint32_t* err,
                                                   uint32_t code) {
@@ -316,6 +342,11 @@ __device__ __forceinline__ void st_shared_v4(uint32_t addr, uint32_t a, uint32_t
   asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(a), "r"(b), "r"(c),
                "r"(d)
                : "memory");
+}
+
+// Bring the 128-byte line holding `p` into L1 ahead of its use.
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
 }
 
 // Make generic-proxy shared-memory writes visible to the async proxy

@@ -54,7 +54,7 @@ __global__ void __launch_bounds__(256) unfused_input_transform(KernelParam p) {
   uint8_t* v2 = static_cast<uint8_t*>(p.transform_pin);
   const long long tile0 = (long long)tb * TB2 + grp * 8;
   const size_t inner = grp * 256 + (cl >> 3) * 128 + (cl & 7) * 16;
-  produce_v8(static_cast<const __half*>(p.pin), g, tile0, cs * 16 + cl,
+  produce_v8(static_cast<const __half*>(p.pin), g, tile0, cs * 16 + cl, -1,
              [&](int t, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
                uint8_t* dst = v2 + v2_piece(t, tb, cs, g.nTB, g.CS) * 2 + inner;
                *reinterpret_cast<uint4*>(dst) = make_uint4(a, b, c, d);

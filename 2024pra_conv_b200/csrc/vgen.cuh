@@ -94,110 +94,131 @@ __device__ __forceinline__ void bt_cols(uint32_t a0, uint32_t a1, uint32_t a2, u
   v[3] = hsub2(a1, a3);
 }
 
+// Words of one input row for a pair of tiles (A, B = A + 1): tile A needs
+// words txA-1 .. txA+1, tile B words txB-1 .. txB+1.  When B is A's right
+// neighbour those overlap and four loads serve both; when the pair straddles
+// a tile-row (or image) boundary B's three words come from its own row.
+struct PairRow {
+  uint32_t a0, a1, a2, b0, b1, b2;
+};
+
+// Location of one tile: input plane of (image, channel), first window row
+// and first window word; valid == false for tiles past the batch.
+struct TileLoc {
+  const __half* plane;
+  int y0, m0;
+  bool valid;
+};
+
+__device__ __forceinline__ PairRow load_pair_row(const TileLoc& A, const TileLoc& B, bool same_row,
+                                                 int i, const Geometry& g, bool w_even) {
+  PairRow r;
+  const int ya = A.y0 + i;
+  const bool oka = A.valid && ya >= 0 && ya < g.H;
+  const __half* rowa = A.plane + (size_t)(oka ? ya : 0) * g.W;
+  r.a0 = load_word(rowa, oka, A.m0, g.W, w_even);
+  r.a1 = load_word(rowa, oka, A.m0 + 1, g.W, w_even);
+  r.a2 = load_word(rowa, oka, A.m0 + 2, g.W, w_even);
+  if (same_row) {
+    r.b0 = r.a1;
+    r.b1 = r.a2;
+    r.b2 = load_word(rowa, oka, A.m0 + 3, g.W, w_even);
+  } else {
+    const int yb = B.y0 + i;
+    const bool okb = B.valid && yb >= 0 && yb < g.H;
+    const __half* rowb = B.plane + (size_t)(okb ? yb : 0) * g.W;
+    r.b0 = load_word(rowb, okb, B.m0, g.W, w_even);
+    r.b1 = load_word(rowb, okb, B.m0 + 1, g.W, w_even);
+    r.b2 = load_word(rowb, okb, B.m0 + 2, g.W, w_even);
+  }
+  return r;
+}
+
 // Produce V for 8 consecutive tiles (tile0 .. tile0+7) of channel c, all 16
 // taps: sink(t, w0, w1, w2, w3) receives tap t as four words, each two tiles
 // (tile 2i in the low half of w_i, tile 2i+1 in the high half).
-// Each e-row a (taps 4a..4a+3) is stored as soon as it is formed.
-// Fast path: all 8 tiles in one tile row and W even (word loads).
+// If prefetch_c >= 0 the lines the same tiles need for channel prefetch_c are
+// brought into L1 first (the producer's next task), so that task's loads hit.
 template <typename Sink>
 __device__ __forceinline__ void produce_v8(const __half* __restrict__ X, const Geometry& g,
-                                           long long tile0, int c, Sink&& sink) {
+                                           long long tile0, int c, int prefetch_c, Sink&& sink) {
   const bool w_even = (g.W & 1) == 0;
   const long long per_img = (long long)g.TP * g.TQ;
-  bool fast = false;
-  int n0 = 0, ty0 = 0, tx0 = 0;
-  if (tile0 + 7 < g.NT) {
-    n0 = (int)(tile0 / per_img);
-    const int r = (int)(tile0 - (long long)n0 * per_img);
-    ty0 = r / g.TQ;
-    tx0 = r - ty0 * g.TQ;
-    fast = w_even && (tx0 + 7 < g.TQ);
+  const size_t plane_elems = (size_t)g.H * g.W;
+  int n = 0, ty = 0, tx = 0;
+  if (tile0 < g.NT) {
+    n = (int)(tile0 / per_img);
+    const int r = (int)(tile0 - (long long)n * per_img);
+    ty = r / g.TQ;
+    tx = r - ty * g.TQ;
   }
-  if (fast) {
-    const __half* plane = X + ((size_t)n0 * g.C + c) * (size_t)g.H * g.W;
-    uint32_t d[4][10];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int y = 2 * ty0 - 1 + i;
-      const bool ok = y >= 0 && y < g.H;
-      const __half* row = plane + (size_t)(ok ? y : 0) * g.W;
-#pragma unroll
-      for (int j = 0; j < 10; ++j) d[i][j] = load_word(row, ok, tx0 - 1 + j, g.W, true);
+  auto loc = [&](long long tile, int nn, int tyy, int txx) {
+    TileLoc L;
+    L.valid = tile < g.NT;
+    L.plane = X + ((size_t)(L.valid ? nn : 0) * g.C + c) * plane_elems;
+    L.y0 = 2 * tyy - 1;
+    L.m0 = txx - 1;
+    return L;
+  };
+  auto advance = [&](int& nn, int& tyy, int& txx) {
+    if (++txx == g.TQ) {
+      txx = 0;
+      if (++tyy == g.TP) { tyy = 0; ++nn; }
     }
+  };
+  if (prefetch_c >= 0 && tile0 < g.NT) {
+    // the group spans at most a few tile rows: touch each window row once per run
+    const ptrdiff_t dc = (ptrdiff_t)(prefetch_c - c) * (ptrdiff_t)plane_elems;
+    int pn = n, pty = ty, ptx = tx;
 #pragma unroll
-    for (int a = 0; a < 4; ++a) {
-      uint32_t e[10];
+    for (int s = 0; s < 8; ++s) {
+      const long long tile = tile0 + s;
+      if (tile < g.NT && (s == 0 || ptx == 0)) {
+        const __half* pl = X + ((size_t)pn * g.C + c) * plane_elems + dc;
 #pragma unroll
-      for (int j = 0; j < 10; ++j) e[j] = bt_row(a, d[0][j], d[1][j], d[2][j], d[3][j]);
-      uint32_t out[4][4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int u = 2 * q;
-        uint32_t v[4];
-        bt_cols(pk_hi(e[u], e[u + 1]), pk_lo(e[u + 1], e[u + 2]), pk_hi(e[u + 1], e[u + 2]),
-                pk_lo(e[u + 2], e[u + 3]), v);
-#pragma unroll
-        for (int b = 0; b < 4; ++b) out[b][q] = v[b];
-      }
-#pragma unroll
-      for (int b = 0; b < 4; ++b)
-        sink(4 * a + b, out[b][0], out[b][1], out[b][2], out[b][3]);
-    }
-  } else {
-    // General path: each tile locates its own window (row or image changes
-    // inside the group, odd widths, tiles past the end of the batch).  Per
-    // e-row only the two input rows that B^T combines are read; tile
-    // coordinates advance incrementally (consecutive tiles step tx, then ty,
-    // then the image).
-    int n1 = 0, ty1 = 0, tx1 = 0;
-    if (tile0 < g.NT) {
-      n1 = (int)(tile0 / per_img);
-      const int r = (int)(tile0 - (long long)n1 * per_img);
-      ty1 = r / g.TQ;
-      tx1 = r - ty1 * g.TQ;
-    }
-#pragma unroll 1
-    for (int a = 0; a < 4; ++a) {
-      // rows combined by Bt[a]: (0,2), (1,2), (2,1), (1,3) as (plus, minus / plus)
-      const int ra = (a == 0) ? 0 : (a == 2 ? 2 : 1);
-      const int rb = (a == 0) ? 2 : (a == 3 ? 3 : (a == 1 ? 2 : 1));
-      uint32_t ew[8][3];
-      int n = n1, ty = ty1, tx = tx1;
-#pragma unroll
-      for (int s = 0; s < 8; ++s) {
-        const bool valid = tile0 + s < g.NT;
-        const int ya = 2 * ty - 1 + ra, yb = 2 * ty - 1 + rb;
-        const bool oka = valid && ya >= 0 && ya < g.H;
-        const bool okb = valid && yb >= 0 && yb < g.H;
-        const __half* base = X + ((size_t)(valid ? n : 0) * g.C + c) * (size_t)g.H * g.W;
-        const __half* rowa = base + (size_t)(oka ? ya : 0) * g.W;
-        const __half* rowb = base + (size_t)(okb ? yb : 0) * g.W;
-#pragma unroll
-        for (int j = 0; j < 3; ++j) {
-          const uint32_t wa = load_word(rowa, oka, tx - 1 + j, g.W, w_even);
-          const uint32_t wb = load_word(rowb, okb, tx - 1 + j, g.W, w_even);
-          ew[s][j] = (a == 1) ? hadd2(wa, wb) : hsub2(wa, wb);
-        }
-        if (++tx == g.TQ) {
-          tx = 0;
-          if (++ty == g.TP) { ty = 0; ++n; }
+        for (int i = 0; i < 4; ++i) {
+          const int y = 2 * pty - 1 + i;
+          if (y >= 0 && y < g.H) prefetch_l1(pl + (size_t)y * g.W + (ptx > 0 ? 2 * ptx - 2 : 0));
         }
       }
-      uint32_t out[4][4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int s0 = 2 * q, s1 = 2 * q + 1;
-        uint32_t v[4];
-        bt_cols(pk_hi(ew[s0][0], ew[s1][0]), pk_lo(ew[s0][1], ew[s1][1]), pk_hi(ew[s0][1], ew[s1][1]),
-                pk_lo(ew[s0][2], ew[s1][2]), v);
-#pragma unroll
-        for (int b = 0; b < 4; ++b) out[b][q] = v[b];
-      }
-#pragma unroll
-      for (int b = 0; b < 4; ++b)
-        sink(4 * a + b, out[b][0], out[b][1], out[b][2], out[b][3]);
+      advance(pn, pty, ptx);
     }
   }
+  uint32_t out[16][4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const long long ta = tile0 + 2 * q;
+    const TileLoc A = loc(ta, n, ty, tx);
+    const bool same_row = tx + 1 < g.TQ;
+    advance(n, ty, tx);
+    const TileLoc B = loc(ta + 1, n, ty, tx);
+    advance(n, ty, tx);
+    PairRow d[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) d[i] = load_pair_row(A, B, same_row, i, g, w_even);
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      // e-row a of both tiles (B^T across the window rows), on words
+      const uint32_t ea0 = bt_row(a, d[0].a0, d[1].a0, d[2].a0, d[3].a0);
+      const uint32_t ea1 = bt_row(a, d[0].a1, d[1].a1, d[2].a1, d[3].a1);
+      const uint32_t ea2 = bt_row(a, d[0].a2, d[1].a2, d[2].a2, d[3].a2);
+      uint32_t eb0, eb1;
+      if (same_row) {
+        eb0 = ea1;
+        eb1 = ea2;
+      } else {
+        eb0 = bt_row(a, d[0].b0, d[1].b0, d[2].b0, d[3].b0);
+        eb1 = bt_row(a, d[0].b1, d[1].b1, d[2].b1, d[3].b1);
+      }
+      const uint32_t eb2 = bt_row(a, d[0].b2, d[1].b2, d[2].b2, d[3].b2);
+      uint32_t v[4];
+      bt_cols(pk_hi(ea0, eb0), pk_lo(ea1, eb1), pk_hi(ea1, eb1), pk_lo(ea2, eb2), v);
+#pragma unroll
+      for (int b = 0; b < 4; ++b) out[4 * a + b][q] = v[b];
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < 16; ++t) sink(t, out[t][0], out[t][1], out[t][2], out[t][3]);
 }
 
 }  // namespace wino
