@@ -117,30 +117,48 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
   if (warp == WARP_MMA) {
     if (lane == 0) {
       const uint32_t idesc = instr_desc(128, TILES, 0, 0, /*a_mn=*/0, /*b_mn=*/1);
+      // Descriptors are formed once; the start-address field (bits 0-13,
+      // address >> 4) then advances by plain adds (shared addresses < 256 KB,
+      // so the field never carries into the next one).  Keeping the issue
+      // loop to a few instructions per MMA matters: a single thread feeds the
+      // tensor pipe.
+      const uint64_t adesc0 = smem_desc(u_slot(0), 128, 256);
+      const uint64_t bdesc0 = smem_desc(v_slot(0), 128, 256);
+      constexpr uint32_t BSTEP = V_TAP_BYTES >> 4;
       uint32_t it = 0, bi = 0;
       bool ok = true;
       for (long long b = blockIdx.x; b < nblocks && ok; b += gridDim.x, ++bi) {
         const int kb = (int)(b % nKB);
-        const int kbs = kblock_rows(kb, g.K);
+        const uint32_t astep = (uint32_t)(kblock_rows(kb, g.K) * 32) >> 4;
         for (int s = 0; s < g.CS && ok; ++s, ++it) {
           const uint32_t vs = it % NVSLOT;
           ok = mbar_wait(&sh.vfull[vs], (it / NVSLOT) & 1, abort_flag, err, ERR_WAIT_FULL);
-          for (int h = 0; h < 2 && ok; ++h) {
+          const uint32_t acc = s > 0 ? 1u : 0u;
+          const bool first_step = s == 0 && bi > 0;
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            if (!ok) break;
             const uint32_t ui = 2 * it + h, us = ui % NUSLOT;
             ok = mbar_wait(&sh.ufull[us], (ui / NUSLOT) & 1, abort_flag, err, ERR_WAIT_FULL);
             if (!ok) break;
-            tc_fence_after();
-#pragma unroll 1
-            for (int tt = 0; tt < 8; ++tt) {
-              const int t = 8 * h + tt;
-              if (s == 0 && bi > 0) {
-                ok = mbar_wait(&sh.tapfree[t], (bi - 1) & 1, abort_flag, err, ERR_WAIT_DRAIN);
-                if (!ok) break;
+            const uint64_t ad = adesc0 + ((us * U_SLOT_BYTES) >> 4);
+            const uint64_t bd = bdesc0 + ((vs * V_SLOT_BYTES + 8 * h * V_TAP_BYTES) >> 4);
+            const uint32_t d = tmem + 8 * h * TILES;
+            if (first_step) {
+              // the previous block's epilogue hands each tap's columns back in turn
+#pragma unroll
+              for (int tt = 0; tt < 8; ++tt) {
+                if (!mbar_wait(&sh.tapfree[8 * h + tt], (bi - 1) & 1, abort_flag, err, ERR_WAIT_DRAIN)) {
+                  ok = false;
+                  break;
+                }
                 tc_fence_after();
+                mma_f16(d + tt * TILES, ad + tt * astep, bd + tt * BSTEP, idesc, acc);
               }
-              const uint64_t ad = smem_desc(u_slot(us) + tt * kbs * 32, 128, 256);
-              const uint64_t bd = smem_desc(v_slot(vs) + t * V_TAP_BYTES, 128, 256);
-              mma_f16(tmem + t * TILES, ad, bd, idesc, s > 0 ? 1u : 0u);
+            } else {
+#pragma unroll
+              for (int tt = 0; tt < 8; ++tt)
+                mma_f16(d + tt * TILES, ad + tt * astep, bd + tt * BSTEP, idesc, acc);
             }
             mma_commit(&sh.uempty[us]);
           }
@@ -192,7 +210,7 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
         if ((it & 1) != parity_of_steps) continue;
         const uint32_t vs = it % NVSLOT;
         if (it >= NVSLOT &&
-            !mbar_wait_warp(&sh.vempty[vs], (it / NVSLOT - 1) & 1, abort_flag, err, ERR_WAIT_EMPTY)) {
+            !mbar_wait_warp(&sh.vempty[vs], (it / NVSLOT - 1) & 1, abort_flag, err, ERR_WAIT_EMPTY, 32)) {
           ok = false;
           break;
         }
