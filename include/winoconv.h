@@ -29,7 +29,8 @@ enum {
   WINO_EINVAL = 1,        /* null pointer or invalid argument            */
   WINO_EUNSUPPORTED = 2,  /* shape outside the contract above            */
   WINO_ECUDA = 3,         /* a CUDA runtime call failed                  */
-  WINO_EDEVICE = 4        /* a kernel reported an error (see error word) */
+  WINO_EDEVICE = 4,       /* a kernel reported an error (see error word) */
+  WINO_ESCRATCH = 5       /* filter too large for wino_conv2d_noalloc's fixed scratch */
 };
 
 /* Precision variants of the GEMM stage. */
@@ -76,6 +77,21 @@ int wino_conv2d_unfused(const void* x, const void* ucache2, void* y, void* v_ws,
  * reference harness (reference src/main.cpp:105-108).  `ki` is `const
  * kernelInfo_t*` from conv2d.h, passed untyped so this header stands alone. */
 int wino_launch_kernelinfo(const void* ki, void* param, void* stream);
+
+/* Conv for callers that cannot allocate device memory (no counterpart in the
+ * reference).  Plugin hosts that pass only input and output tensors, runtimes
+ * whose device memory is fixed at start-up, and code that must not reach the
+ * allocator mid-call cannot provide the U-cache workspace the other entry
+ * points need; this one keeps U in a fixed array inside the library (8 MiB
+ * held on every GPU that loads the library, for K*C <= wino_noalloc_max_kc())
+ * and runs the filter transform and the fused conv on it.  Larger filters
+ * return WINO_ESCRATCH.  The first call on a device looks the array up, so
+ * make it before any stream capture on that device.  All calls share the
+ * array: calls whose kernels overlap on the GPU race, so serialise them.
+ * Allocates nothing.  x: NCHW fp16, weight: KCRS fp16, y: N K H W fp16. */
+int wino_conv2d_noalloc(const void* x, const void* weight, void* y, int n, int c, int h, int w,
+                        int k, void* stream);
+long long wino_noalloc_max_kc(void);
 
 /* Reads and clears the device error word of the conv kernels (0 = none;
  * otherwise the first wait that ran out or the first bad-shape launch). */
