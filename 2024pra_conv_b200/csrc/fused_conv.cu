@@ -13,24 +13,26 @@
 // Per tap t the tensor core computes
 //     M_t[k][tile] = sum_c U_t[k][c] * V_t[c][tile]
 // as a 128 x 32 x 16 MMA per 16-channel step (A = U from the U cache, B = V
-// produced on chip), accumulating in TMEM: lane = output channel, columns
+// produced on chip, both K-major), accumulating in TMEM: lane = output channel, columns
 // t*32 .. t*32+31 = tiles (16 taps x 32 = all 512 columns).  All 16 taps of
 // a (k, tile) pair live in one thread's lane, so the output transform is
 // per-thread register arithmetic.  With output channels on the 128-row side
 // each V element feeds 128 channels, which keeps the CUDA-core input
 // transform small next to the MMAs.
 //
-// Pipelines (shared memory, 192 KB): U in four 32 KB slots, each half of a
-// step's piece (8 taps x 128 k x 16 c), and V in four 16 KB slots, one per
-// step.  Barrier hand-offs cost a few hundred cycles on this part, so each
-// side keeps several slots in flight.
+// Pipelines (shared memory, 216 KB): U in three 32 KB slots, each half of a
+// step's piece (8 taps x 128 k x 16 c); V in three 16 KB slots, one per
+// step; three 24 KB input slabs.  Barrier hand-offs cost a few hundred
+// cycles on this part, so each side keeps several slots in flight.
 //
 // Warp roles (14 warps):
 //   warp 0       TMEM allocation; one thread issues the MMAs
 //   warp 1       one thread bulk-copies the U half-pieces
-//   warps 2-5    V producers, B^T d B in packed fp16 straight into the
-//                MN-major operand (8 channels x 8 tiles per core matrix);
-//                warps 2-3 fill the even steps, warps 4-5 the odd ones
+//   warps 2-5    V producers, all four on every step: copy the input band
+//                of the step's block into a shared-memory slab two steps
+//                ahead (cp.async), then B^T d B in packed fp16 from the slab
+//                straight into the K-major operand (8 tiles x 8 channels per
+//                core matrix); warp q forms channels 4q..4q+3, lane = tile
 //   warps 6-13   epilogue: drain TMEM tap by tap (each drained tap is handed
 //                back to the MMA thread at once, so the next block's MMAs
 //                overlap the drain), A^T m A in fp32, fp16 NKPQ stores.
@@ -50,16 +52,19 @@ constexpr int NTAP = 16;
 constexpr int V_TAP_BYTES = TILES * 16 * 2;          // 1 KB per tap per step
 constexpr int V_SLOT_BYTES = NTAP * V_TAP_BYTES;     // 16 KB: one step of V
 constexpr int U_SLOT_BYTES = 8 * KB * 16 * 2;        // 32 KB: 8 taps of a step of U
-constexpr int NVSLOT = 4, NUSLOT = 4;
+constexpr int NVSLOT = 3, NUSLOT = 3, NSLAB = 3;
 constexpr int U_BASE = 0, V_BASE = NUSLOT * U_SLOT_BYTES;
+constexpr int SLAB_BASE = V_BASE + NVSLOT * V_SLOT_BYTES;
 constexpr int NWARP = 14;
 constexpr int NTHREAD = NWARP * 32;
 constexpr int WARP_MMA = 0, WARP_U = 1, WARP_V0 = 2, NWARP_V = 4, WARP_E0 = 6, NWARP_E = 8;
-constexpr int SMEM_BYTES = NUSLOT * U_SLOT_BYTES + NVSLOT * V_SLOT_BYTES + 1024;
+constexpr int NPROD = NWARP_V * 32;   // producer threads
+constexpr int SMEM_BYTES = NUSLOT * U_SLOT_BYTES + NVSLOT * V_SLOT_BYTES + NSLAB * SLAB_BYTES + 1024;
 
 struct Shared {
   uint64_t ufull[NUSLOT], uempty[NUSLOT];
   uint64_t vfull[NVSLOT], vempty[NVSLOT];
+  uint64_t slabfull[NSLAB], slabfree[NSLAB];
   uint64_t accf;
   uint64_t tapfree[NTAP];
   uint32_t tmem_base;
@@ -93,8 +98,12 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
       mbar_init(&sh.uempty[s], 1);
     }
     for (int s = 0; s < NVSLOT; ++s) {
-      mbar_init(&sh.vfull[s], 2);  // the step's two V warps
+      mbar_init(&sh.vfull[s], NWARP_V);  // every producer warp
       mbar_init(&sh.vempty[s], 1);
+    }
+    for (int s = 0; s < NSLAB; ++s) {
+      mbar_init(&sh.slabfull[s], NPROD);   // each producer thread's copies
+      mbar_init(&sh.slabfree[s], NWARP_V);
     }
     mbar_init(&sh.accf, 1);
     for (int t = 0; t < NTAP; ++t) mbar_init(&sh.tapfree[t], NWARP_E);
@@ -116,7 +125,7 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
 
   if (warp == WARP_MMA) {
     if (lane == 0) {
-      const uint32_t idesc = instr_desc(128, TILES, 0, 0, /*a_mn=*/0, /*b_mn=*/1);
+      const uint32_t idesc = instr_desc(128, TILES, 0, 0, /*a_mn=*/0, /*b_mn=*/0);
       // Descriptors are formed once; the start-address field (bits 0-13,
       // address >> 4) then advances by plain adds (shared addresses < 256 KB,
       // so the field never carries into the next one).  Keeping the issue
@@ -195,34 +204,80 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
     }
     __syncwarp();
   } else if (warp >= WARP_V0 && warp < WARP_V0 + NWARP_V) {
-    // Warps 2-3 produce the even steps, warps 4-5 the odd ones.
-    const int vw = warp - WARP_V0;
-    const uint32_t parity_of_steps = vw >> 1;
-    const int grp = 2 * (vw & 1) + (lane >> 4);  // tile group (8 tiles) 0..3
-    const int cl = lane & 15;                    // channel inside the step
+    // The four producer warps work on every step together.  Two steps ahead
+    // they copy the input band of the step's block into a slab (cp.async,
+    // completion counted on slabfull); then warp q forms channels 4q..4q+3
+    // of the step's V for all 32 tiles (lane = tile) from the slab.
+    const int q = warp - WARP_V0;
+    const int ptid = threadIdx.x - WARP_V0 * 32;
     const __half* X = static_cast<const __half*>(p.pin);
-    uint32_t it = 0;
+    const int my_blocks =
+        blockIdx.x < nblocks ? (int)((nblocks - blockIdx.x + gridDim.x - 1) / gridDim.x) : 0;
+    const int CS = g.CS;
+    const uint32_t slab0 = smem_base + SLAB_BASE;
+    // Per-block quantities are formed once per block (32-bit math); the
+    // staging side runs two steps ahead, possibly into the next block.
+    auto block_tile0 = [&](int bi) { return (int)((blockIdx.x + (long long)bi * gridDim.x) / nKB) * TILES; };
     bool ok = true;
-    for (long long b = blockIdx.x; b < nblocks && ok; b += gridDim.x) {
-      const long long tb = b / nKB;
-      const long long tile0 = tb * TILES + grp * 8;
-      for (int s = 0; s < g.CS; ++s, ++it) {
-        if ((it & 1) != parity_of_steps) continue;
+    int st_bi = 0, st_s = 0;                      // next step to stage
+    SlabPlan st_pl = slab_plan(g, block_tile0(0), TILES);
+    uint32_t st_it = 0;
+    auto stage_next = [&]() {
+      const uint32_t j = st_it % NSLAB;
+      if (st_it >= NSLAB &&
+          !mbar_wait_warp(&sh.slabfree[j], ((st_it - NSLAB) / NSLAB) & 1, abort_flag, err, ERR_WAIT_EMPTY, 32)) {
+        ok = false;
+        return;
+      }
+      if (slab_fits(g, st_pl)) slab_stage(X, g, st_pl, st_s * 16, slab0 + j * SLAB_BYTES, ptid, NPROD);
+      cp_async_arrive(&sh.slabfull[j]);
+      ++st_it;
+      if (++st_s == CS) {
+        st_s = 0;
+        if (++st_bi < my_blocks) st_pl = slab_plan(g, block_tile0(st_bi), TILES);
+      }
+    };
+    const uint32_t total = (uint32_t)my_blocks * CS;
+    if (total > 0) stage_next();
+    if (total > 1) stage_next();
+    // K-major core matrices: tile group (lane/8) at 256 B, channel half at
+    // 128 B, tile row (lane%8) at 16 B, channel quarter inside the row at 8 B.
+    const uint32_t row_off = (lane >> 3) * 256 + (q >> 1) * 128 + (lane & 7) * 16 + (q & 1) * 8;
+    uint32_t it = 0;
+    for (int bi = 0; bi < my_blocks && ok; ++bi) {
+      const int tile0 = block_tile0(bi);
+      const SlabPlan pl = slab_plan(g, tile0, TILES);
+      const bool use_slab = slab_fits(g, pl);
+      const TileCoord tc = tile_coord(g, tile0 + lane);
+      for (int s = 0; s < CS && ok; ++s, ++it) {
+        if (it + 2 < total) stage_next();
+        if (!ok) break;
+        const uint32_t j = it % NSLAB;
         const uint32_t vs = it % NVSLOT;
+        if (!mbar_wait_warp(&sh.slabfull[j], (it / NSLAB) & 1, abort_flag, err, ERR_WAIT_FULL, 32)) {
+          ok = false;
+          break;
+        }
         if (it >= NVSLOT &&
             !mbar_wait_warp(&sh.vempty[vs], (it / NVSLOT - 1) & 1, abort_flag, err, ERR_WAIT_EMPTY, 32)) {
           ok = false;
           break;
         }
-        const uint32_t dst = v_slot(vs) + grp * 256 + (cl >> 3) * 128 + (cl & 7) * 16;
-        const int next_c = s + 2 < g.CS ? (s + 2) * 16 + cl : -1;
-        produce_v8(X, g, tile0, s * 16 + cl, next_c,
-                   [&](int t, uint32_t a, uint32_t b2, uint32_t c2, uint32_t d2) {
-                     st_shared_v4(dst + t * V_TAP_BYTES, a, b2, c2, d2);
-                   });
+        const uint32_t dst = v_slot(vs) + row_off;
+        auto sink = [&](int t, uint32_t w0, uint32_t w1) {
+          asm volatile("st.shared.v2.b32 [%0], {%1, %2};" ::"r"(dst + t * V_TAP_BYTES), "r"(w0), "r"(w1)
+                       : "memory");
+        };
+        if (use_slab)
+          produce_v_quarter_slab(g, pl, slab0 + j * SLAB_BYTES, tc, 4 * q, sink);
+        else
+          produce_v_quarter_global(X, g, tc, s * 16 + 4 * q, sink);
         fence_proxy_async_shared();
         __syncwarp();
-        if (lane == 0) mbar_arrive(&sh.vfull[vs]);
+        if (lane == 0) {
+          mbar_arrive(&sh.slabfree[j]);
+          mbar_arrive(&sh.vfull[vs]);
+        }
       }
     }
   } else if (warp >= WARP_E0) {
@@ -317,8 +372,9 @@ int wino_fused_smem_bytes() { return fused::SMEM_BYTES; }
 int wino_fused_threads() { return fused::NTHREAD; }
 
 int wino_fused_prepare() {
-  return (int)cudaFuncSetAttribute(fused_wino_f16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   fused::SMEM_BYTES);
+  cudaError_t e = cudaFuncSetAttribute(fused_wino_f16_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, fused::SMEM_BYTES);
+  return (int)e;
 }
 
 // Work blocks of a problem (tile blocks x output-channel blocks).

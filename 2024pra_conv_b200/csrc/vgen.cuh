@@ -13,6 +13,7 @@
 #include <cstdint>
 #include <cuda_fp16.h>
 #include "wino_common.cuh"
+#include "tc_sm100.cuh"
 
 namespace wino {
 
@@ -219,6 +220,329 @@ __device__ __forceinline__ void produce_v8(const __half* __restrict__ X, const G
   }
 #pragma unroll
   for (int t = 0; t < 16; ++t) sink(t, out[t][0], out[t][1], out[t][2], out[t][3]);
+}
+
+// ---------------------------------------------------------------------------
+// One tile x one 16-channel K-step, all 16 taps, for the K-major V operand
+// (core matrix = 8 tiles x 8 channels, a tile's 8 channels one 16-byte row).
+// A warp covers 32 consecutive tiles, so each word load of the warp reads
+// consecutive words of one input row (coalesced).  Two channels are paired
+// per register (c, c+1): window columns are regrouped with byte permutes,
+// then B^T d B runs in packed fp16.
+//
+// sink(t, half, w0, w1, w2, w3): tap t, channels 8*half .. 8*half+7 as four
+// words (channel pair i in w_i, even channel in the low half).
+//
+// If prefetch_c0 >= 0 the rows this tile needs for channels prefetch_c0 ..
+// prefetch_c0+15 are first requested into L1 (the producer's next step), so
+// that step's loads hit.
+template <typename Sink>
+__device__ __forceinline__ void produce_v_tile16(const __half* __restrict__ X, const Geometry& g,
+                                                 long long tile, int c0, int prefetch_c0,
+                                                 Sink&& sink) {
+  const bool w_even = (g.W & 1) == 0;
+  const long long per_img = (long long)g.TP * g.TQ;
+  const size_t plane_elems = (size_t)g.H * g.W;
+  const bool valid = tile < g.NT;
+  int n = 0, ty = 0, tx = 0;
+  if (valid) {
+    n = (int)(tile / per_img);
+    const int r = (int)(tile - (long long)n * per_img);
+    ty = r / g.TQ;
+    tx = r - ty * g.TQ;
+  }
+  const __half* base = X + ((size_t)n * g.C + c0) * plane_elems;
+  const int y0 = 2 * ty - 1, m0 = tx - 1;
+  int rowoff[4];
+  bool rowok[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int y = y0 + i;
+    rowok[i] = valid && y >= 0 && y < g.H;
+    rowoff[i] = (rowok[i] ? y : 0) * g.W;
+  }
+  if (prefetch_c0 >= 0) {
+    const __half* pbase = X + ((size_t)n * g.C + prefetch_c0) * plane_elems + (m0 > 0 ? 2 * m0 : 0);
+#pragma unroll 4
+    for (int ch = 0; ch < 16; ++ch)
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        if (rowok[i]) prefetch_l1(pbase + (size_t)ch * plane_elems + rowoff[i]);
+  }
+#pragma unroll
+  for (int half = 0; half < 2; ++half) {
+    uint32_t out[16][4];
+#pragma unroll
+    for (int cp = 0; cp < 4; ++cp) {
+      const __half* pa = base + (size_t)(8 * half + 2 * cp) * plane_elems;
+      const __half* pb = pa + plane_elems;
+      // 4 rows x 3 words for each of the two channels
+      uint32_t wa[4][3], wb[4][3];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          wa[i][j] = load_word(pa + rowoff[i], rowok[i], m0 + j, g.W, w_even);
+          wb[i][j] = load_word(pb + rowoff[i], rowok[i], m0 + j, g.W, w_even);
+        }
+      // window d[i][col] as (channel c, channel c+1) pairs
+      uint32_t d[4][4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        d[i][0] = pk_hi(wa[i][0], wb[i][0]);
+        d[i][1] = pk_lo(wa[i][1], wb[i][1]);
+        d[i][2] = pk_hi(wa[i][1], wb[i][1]);
+        d[i][3] = pk_lo(wa[i][2], wb[i][2]);
+      }
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        uint32_t e[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) e[j] = bt_row(a, d[0][j], d[1][j], d[2][j], d[3][j]);
+        uint32_t v[4];
+        bt_cols(e[0], e[1], e[2], e[3], v);
+#pragma unroll
+        for (int b = 0; b < 4; ++b) out[4 * a + b][cp] = v[b];
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < 16; ++t) sink(t, half, out[t][0], out[t][1], out[t][2], out[t][3]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Staged input for the fused kernel's cooperative V producers.
+//
+// The 32 consecutive tiles of a block touch, per image they cover, a band of
+// input rows; for every one of a step's 16 channels that band is one
+// contiguous run of memory (NCHW).  The producers copy those runs into a
+// shared-memory "slab" with cp.async two steps ahead, then form V from it.
+//   slab layout: [segment][channel 16][row of the band][W] fp16
+constexpr int SLAB_MAXSEG = 4;
+constexpr int SLAB_BYTES = 24 * 1024;
+
+struct SlabPlan {
+  int nseg, n0, total_rows;
+  int y_lo[SLAB_MAXSEG], rows[SLAB_MAXSEG], row_base[SLAB_MAXSEG];
+};
+
+__device__ __forceinline__ SlabPlan slab_plan(const Geometry& g, int tile0, int tiles_per_block) {
+  SlabPlan pl;
+  const int per_img = g.TP * g.TQ;
+  int last = tile0 + tiles_per_block - 1;
+  if (last >= (int)g.NT) last = (int)g.NT - 1;
+  const int n0 = tile0 / per_img, n1 = last / per_img;
+  const int ty0 = (tile0 - n0 * per_img) / g.TQ;
+  const int ty1 = (last - n1 * per_img) / g.TQ;
+  pl.n0 = n0;
+  pl.nseg = n1 - n0 + 1;
+  int base = 0;
+#pragma unroll
+  for (int k = 0; k < SLAB_MAXSEG; ++k) {
+    const int ta = (k == 0) ? ty0 : 0;
+    const int tb = (k == pl.nseg - 1) ? ty1 : g.TP - 1;
+    const int ylo = max(0, 2 * ta - 1), yhi = min(g.H - 1, 2 * tb + 2);
+    pl.y_lo[k] = ylo;
+    pl.rows[k] = (k < pl.nseg) ? yhi - ylo + 1 : 0;
+    pl.row_base[k] = base;
+    base += 16 * pl.rows[k];
+  }
+  pl.total_rows = base;
+  return pl;
+}
+
+// Window origin of one tile: image, first input row, first word; valid ==
+// false past the end of the batch.  32-bit: tile counts stay below 2^31 for
+// any tensor that fits in device memory.
+struct TileCoord {
+  int n, y0, m0;
+  bool valid;
+};
+
+__device__ __forceinline__ TileCoord tile_coord(const Geometry& g, int tile) {
+  TileCoord tc;
+  tc.valid = tile < (int)g.NT;
+  const int per_img = g.TP * g.TQ;
+  const int t = tc.valid ? tile : 0;
+  tc.n = t / per_img;
+  const int r = t - tc.n * per_img;
+  const int ty = r / g.TQ;
+  tc.y0 = 2 * ty - 1;
+  tc.m0 = r - ty * g.TQ - 1;
+  return tc;
+}
+
+// Whether a block's slab fits (decided per block from its exact plan; blocks
+// that do not fit, and odd widths, read global memory instead).
+__device__ __forceinline__ bool slab_fits(const Geometry& g, const SlabPlan& pl) {
+  return (g.W & 1) == 0 && pl.nseg <= SLAB_MAXSEG &&
+         (long long)pl.total_rows * g.W * 2 <= SLAB_BYTES;
+}
+
+// Arrive on `bar` once all of this thread's earlier cp.async copies landed.
+__device__ __forceinline__ void cp_async_arrive(uint64_t* bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void cp_async4(uint32_t dst_smem, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst_smem), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Copy the slab of channels c0..c0+15 for the block at tile0 (W even).
+// Called by all `nthreads` producer threads; thread `tid` strides the words.
+__device__ __forceinline__ void slab_stage(const __half* __restrict__ X, const Geometry& g,
+                                           const SlabPlan& pl, int c0, uint32_t slab, int tid,
+                                           int nthreads) {
+  const size_t plane = (size_t)g.H * g.W;
+  const int wpr = g.W >> 1;  // words per row
+#pragma unroll 1
+  for (int k = 0; k < pl.nseg; ++k) {
+    const int words = pl.rows[k] * wpr;
+    const __half* src0 = X + ((size_t)(pl.n0 + k) * g.C + c0) * plane + (size_t)pl.y_lo[k] * g.W;
+    const uint32_t dst0 = slab + (uint32_t)pl.row_base[k] * g.W * 2;
+#pragma unroll 1
+    for (int ch = 0; ch < 16; ++ch) {
+      const uint32_t* src = reinterpret_cast<const uint32_t*>(src0 + (size_t)ch * plane);
+      const uint32_t dst = dst0 + (uint32_t)(ch * words) * 4;
+      for (int w = tid; w < words; w += nthreads) cp_async4(dst + 4 * w, src + w);
+    }
+  }
+}
+
+__device__ __forceinline__ uint32_t lds_word_if(uint32_t addr, bool ok) {
+  uint32_t v = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %2, 0;\n\t"
+      "@p ld.shared.u32 %0, [%1];\n\t}"
+      : "+r"(v)
+      : "r"(addr), "r"((uint32_t)ok));
+  return v;
+}
+
+// V of one tile for 4 channels (two pairs) and all 16 taps from the slab.
+// sink(t, w0, w1): tap t, channel pairs (c, c+1), (c+2, c+3).
+template <typename Sink>
+__device__ __forceinline__ void produce_v_quarter_slab(const Geometry& g, const SlabPlan& pl,
+                                                       uint32_t slab, const TileCoord& tc, int cq,
+                                                       Sink&& sink) {
+  const bool valid = tc.valid;
+  int k = tc.n - pl.n0;
+  k = k < 0 ? 0 : (k >= SLAB_MAXSEG ? SLAB_MAXSEG - 1 : k);
+  int y_lo = pl.y_lo[0], rows = pl.rows[0], rbase = pl.row_base[0];
+#pragma unroll
+  for (int j = 1; j < SLAB_MAXSEG; ++j)
+    if (k == j) { y_lo = pl.y_lo[j]; rows = pl.rows[j]; rbase = pl.row_base[j]; }
+  const int wpr = g.W >> 1;
+  const int m0 = tc.m0;
+  bool colok[3];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) colok[j] = m0 + j >= 0 && m0 + j < wpr;
+  int srow[4];
+  bool rowok[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int y = tc.y0 + i;
+    const int r = y - y_lo;
+    rowok[i] = valid && y >= 0 && y < g.H && r >= 0 && r < rows;
+    srow[i] = rowok[i] ? r : 0;
+  }
+  uint32_t out[16][2];
+#pragma unroll
+  for (int cp = 0; cp < 2; ++cp) {
+    const int ca = cq + 2 * cp;
+    uint32_t wa[4][3], wb[4][3];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const uint32_t rowa = slab + (uint32_t)((rbase + ca * rows + srow[i]) * wpr) * 4;
+      const uint32_t rowb = rowa + (uint32_t)(rows * wpr) * 4;
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const bool ok = rowok[i] && colok[j];
+        const uint32_t off = (uint32_t)(ok ? m0 + j : 0) * 4;
+        wa[i][j] = lds_word_if(rowa + off, ok);
+        wb[i][j] = lds_word_if(rowb + off, ok);
+      }
+    }
+    uint32_t d[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      d[i][0] = pk_hi(wa[i][0], wb[i][0]);
+      d[i][1] = pk_lo(wa[i][1], wb[i][1]);
+      d[i][2] = pk_hi(wa[i][1], wb[i][1]);
+      d[i][3] = pk_lo(wa[i][2], wb[i][2]);
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      uint32_t e[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) e[j] = bt_row(a, d[0][j], d[1][j], d[2][j], d[3][j]);
+      uint32_t v[4];
+      bt_cols(e[0], e[1], e[2], e[3], v);
+#pragma unroll
+      for (int b = 0; b < 4; ++b) out[4 * a + b][cp] = v[b];
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < 16; ++t) sink(t, out[t][0], out[t][1]);
+}
+
+// Same from global memory (fallback for problems whose slab does not fit).
+template <typename Sink>
+__device__ __forceinline__ void produce_v_quarter_global(const __half* __restrict__ X,
+                                                         const Geometry& g, const TileCoord& tc,
+                                                         int c, Sink&& sink) {
+  const bool w_even = (g.W & 1) == 0;
+  const size_t plane_elems = (size_t)g.H * g.W;
+  const __half* base = X + ((size_t)tc.n * g.C + c) * plane_elems;
+  const int m0 = tc.m0;
+  int rowoff[4];
+  bool rowok[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int y = tc.y0 + i;
+    rowok[i] = tc.valid && y >= 0 && y < g.H;
+    rowoff[i] = (rowok[i] ? y : 0) * g.W;
+  }
+  uint32_t out[16][2];
+#pragma unroll
+  for (int cp = 0; cp < 2; ++cp) {
+    const __half* pa = base + (size_t)(2 * cp) * plane_elems;
+    const __half* pb = pa + plane_elems;
+    uint32_t wa[4][3], wb[4][3];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        wa[i][j] = load_word(pa + rowoff[i], rowok[i], m0 + j, g.W, w_even);
+        wb[i][j] = load_word(pb + rowoff[i], rowok[i], m0 + j, g.W, w_even);
+      }
+    uint32_t d[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      d[i][0] = pk_hi(wa[i][0], wb[i][0]);
+      d[i][1] = pk_lo(wa[i][1], wb[i][1]);
+      d[i][2] = pk_hi(wa[i][1], wb[i][1]);
+      d[i][3] = pk_lo(wa[i][2], wb[i][2]);
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      uint32_t e[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) e[j] = bt_row(a, d[0][j], d[1][j], d[2][j], d[3][j]);
+      uint32_t v[4];
+      bt_cols(e[0], e[1], e[2], e[3], v);
+#pragma unroll
+      for (int b = 0; b < 4; ++b) out[4 * a + b][cp] = v[b];
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < 16; ++t) sink(t, out[t][0], out[t][1]);
 }
 
 }  // namespace wino
