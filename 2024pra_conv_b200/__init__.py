@@ -78,6 +78,9 @@ def lib():
             "wino_ucache_bytes": ([i, i, i], sz),
             "wino_filter_transform": ([vp, vp, i, i, vp], i),
             "wino_conv2d_fused": ([vp, vp, vp, i, i, i, i, i, vp], i),
+            "wino_fused_workspace_bytes": ([i, i, i, i], sz),
+            "wino_input_layout": ([vp, vp, i, i, i, i, vp], i),
+            "wino_conv2d_fused_ws": ([vp, vp, vp, vp, i, i, i, i, i, vp], i),
             "wino_launch_kernelinfo": ([vp, vp, vp], i),
             "wino_filter_transform_unfused": ([vp, vp, i, i, vp], i),
             "wino_unfused_workspace_bytes": ([i, i, i, i, i, ctypes.POINTER(sz), ctypes.POINTER(sz)], i),
@@ -133,16 +136,31 @@ def make_problem(x, w, y, transform_pin=None, transform_filter=None, mid_result=
                    ptr(mid_result), n, c, h, wd, k, r, s, u, v, p, q)
 
 
-def dropin_conv2d(x, w, stream=None):
+class DropinWorkspaces:
+    """The caller-owned buffers of the reference harness for one shape
+    (src/main.cpp:33-38): transform_pin 4*h*h*n*c, mid_result 4*k*h*w*n and
+    transform_filter 16*k*c fp16 elements."""
+
+    def __init__(self, n, c, h, w, k, device, transform_pin=True):
+        import torch
+        self.transform_pin = (torch.empty(4 * h * h * n * c, dtype=torch.float16, device=device)
+                              if transform_pin else None)
+        self.mid_result = torch.empty(4 * k * h * w * n, dtype=torch.float16, device=device)
+        self.transform_filter = torch.empty(16 * k * c, dtype=torch.float16, device=device)
+
+
+def dropin_conv2d(x, w, stream=None, ws=None, transform_pin=True):
     """Run the drop-in path the way the reference harness does
     (src/main.cpp:33-108): caller-allocated output and workspaces sized as
-    there, getParamsize, getkernelInfo, then the four launch slots."""
+    there, getParamsize, getkernelInfo, then the four launch slots.  With
+    transform_pin=False the caller passes no transform_pin workspace and the
+    fused kernel reads the NCHW input directly."""
     import torch
     n, c, h, wd = x.shape
     k = w.shape[0]
+    ws = ws or DropinWorkspaces(n, c, h, wd, k, x.device, transform_pin)
     y = torch.empty((n, k, h, wd), dtype=torch.float16, device=x.device)
-    tf = torch.empty(16 * k * c, dtype=torch.float16, device=x.device)
-    pr = make_problem(x, w, y, None, tf, None)
+    pr = make_problem(x, w, y, ws.transform_pin, ws.transform_filter, ws.mid_result)
     size = get_param_size(pr)
     param = (ctypes.c_char * size)()
     code, ki = get_kernel_info(pr, param)
@@ -166,13 +184,36 @@ def filter_transform(w, stream=None):
     return u
 
 
-def conv2d_fused(x, ucache, k, out=None, stream=None):
+def fused_workspace_bytes(n, c, h, w) -> int:
+    return int(lib().wino_fused_workspace_bytes(n, c, h, w))
+
+
+def input_layout(x, workspace, stream=None):
+    """The fused path's pre-pass alone: NCHW input -> channel-blocked workspace."""
+    n, c, h, wd = x.shape
+    _check(lib().wino_input_layout(ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(workspace.data_ptr()),
+                                   n, c, h, wd, _stream(stream)), "input_layout")
+
+
+def conv2d_fused(x, ucache, k, out=None, stream=None, workspace=True):
+    """Fused conv on a prepared U cache.  workspace=True (default) allocates
+    (or takes, if a uint8 tensor is given) the channel-blocked input
+    workspace and runs the pre-pass + staged fused kernel; workspace=False
+    runs the fused kernel on the NCHW input directly."""
     import torch
     n, c, h, wd = x.shape
     y = out if out is not None else torch.empty((n, k, h, wd), dtype=torch.float16, device=x.device)
-    _check(lib().wino_conv2d_fused(ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(ucache.data_ptr()),
-                                   ctypes.c_void_p(y.data_ptr()), n, c, h, wd, k, _stream(stream)),
-           "conv2d_fused")
+    if workspace is False or workspace is None:
+        _check(lib().wino_conv2d_fused(ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(ucache.data_ptr()),
+                                       ctypes.c_void_p(y.data_ptr()), n, c, h, wd, k, _stream(stream)),
+               "conv2d_fused")
+        return y
+    if workspace is True:
+        workspace = torch.empty(fused_workspace_bytes(n, c, h, wd), dtype=torch.uint8, device=x.device)
+    _check(lib().wino_conv2d_fused_ws(ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(ucache.data_ptr()),
+                                      ctypes.c_void_p(workspace.data_ptr()),
+                                      ctypes.c_void_p(y.data_ptr()), n, c, h, wd, k, _stream(stream)),
+           "conv2d_fused_ws")
     return y
 
 

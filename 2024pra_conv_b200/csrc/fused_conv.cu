@@ -20,22 +20,29 @@
 // each V element feeds 128 channels, which keeps the CUDA-core input
 // transform small next to the MMAs.
 //
-// Pipelines (shared memory, 216 KB): U in three 32 KB slots, each half of a
-// step's piece (8 taps x 128 k x 16 c); V in three 16 KB slots, one per
-// step; three 24 KB input slabs.  Barrier hand-offs cost a few hundred
-// cycles on this part, so each side keeps several slots in flight.
+// Pipelines (shared memory, 225 KB): U in four 32 KB half-step slots (two
+// steps in flight); V in two 16 KB slots, one per step; three 16 KB input
+// slabs; 16 KB of epilogue store staging.  The MMA thread commits once per step (each tcgen05.commit stalls
+// the MMA pipe for ~90 cycles on this part) to a "step done" barrier that
+// releases that step's U half-slots and V slot together.
 //
-// Warp roles (14 warps):
+// Warp roles (15 warps):
 //   warp 0       TMEM allocation; one thread issues the MMAs
-//   warp 1       one thread bulk-copies the U half-pieces
-//   warps 2-5    V producers, all four on every step: copy the input band
-//                of the step's block into a shared-memory slab two steps
-//                ahead (cp.async), then B^T d B in packed fp16 from the slab
-//                straight into the K-major operand (8 tiles x 8 channels per
-//                core matrix); warp q forms channels 4q..4q+3, lane = tile
+//   warp 1       lanes 0 and 1 bulk-copy the two U halves of a step (one
+//                copy in flight per issuing thread, so two threads)
+//   warps 2-5    V producers, all four on every step: warp q forms channels
+//                4q..4q+3 of the step's V for all 32 tiles (lane = tile):
+//                B^T d B in packed fp16 straight into the K-major operand
+//                (8 tiles x 8 channels per core matrix).  They read the
+//                step's slab, or, without an XB workspace or when a block's
+//                rows exceed a slab, the NCHW input directly.
 //   warps 6-13   epilogue: drain TMEM tap by tap (each drained tap is handed
 //                back to the MMA thread at once, so the next block's MMAs
 //                overlap the drain), A^T m A in fp32, fp16 NKPQ stores.
+//   warp 14      stager: with an XB workspace (p.transform_pin, written by
+//                the pre-pass of input_layout.cu) bulk-copies each step's
+//                input rows into a slab, up to three steps ahead (one copy
+//                per image the block touches, issued from separate lanes).
 #include <cuda_runtime.h>
 #include "tc_sm100.cuh"
 #include "wino_common.cuh"
@@ -51,19 +58,23 @@ constexpr int TILES = 32;              // MMA N: tiles per block
 constexpr int NTAP = 16;
 constexpr int V_TAP_BYTES = TILES * 16 * 2;          // 1 KB per tap per step
 constexpr int V_SLOT_BYTES = NTAP * V_TAP_BYTES;     // 16 KB: one step of V
-constexpr int U_SLOT_BYTES = 8 * KB * 16 * 2;        // 32 KB: 8 taps of a step of U
-constexpr int NVSLOT = 3, NUSLOT = 3, NSLAB = 3;
-constexpr int U_BASE = 0, V_BASE = NUSLOT * U_SLOT_BYTES;
+constexpr int U_HALF_BYTES = 8 * KB * 16 * 2;        // 32 KB: 8 taps of a step of U
+constexpr int NUH = 4;                 // U half-slots: two steps
+constexpr int NVSLOT = 2, NSD = 3, NSLAB = 3;
+constexpr int EPI_WARP_BYTES = 2048;   // epilogue store staging per warp
+constexpr int U_BASE = 0, V_BASE = NUH * U_HALF_BYTES;
 constexpr int SLAB_BASE = V_BASE + NVSLOT * V_SLOT_BYTES;
-constexpr int NWARP = 14;
+constexpr int EPI_BASE = SLAB_BASE + NSLAB * SLAB_BYTES;
+constexpr int NWARP = 15;
 constexpr int NTHREAD = NWARP * 32;
 constexpr int WARP_MMA = 0, WARP_U = 1, WARP_V0 = 2, NWARP_V = 4, WARP_E0 = 6, NWARP_E = 8;
-constexpr int NPROD = NWARP_V * 32;   // producer threads
-constexpr int SMEM_BYTES = NUSLOT * U_SLOT_BYTES + NVSLOT * V_SLOT_BYTES + NSLAB * SLAB_BYTES + 1024;
+constexpr int WARP_S = 14;
+constexpr int SMEM_BYTES = EPI_BASE + 8 * EPI_WARP_BYTES + 1024;
 
 struct Shared {
-  uint64_t ufull[NUSLOT], uempty[NUSLOT];
-  uint64_t vfull[NVSLOT], vempty[NVSLOT];
+  uint64_t ufull[NUH];
+  uint64_t vfull[NVSLOT];
+  uint64_t sdone[NSD];                 // MMAs of step it complete: sdone[it % NSD]
   uint64_t slabfull[NSLAB], slabfree[NSLAB];
   uint64_t accf;
   uint64_t tapfree[NTAP];
@@ -93,16 +104,11 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
   uint32_t* err = &g_fused_err;
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < NUSLOT; ++s) {
-      mbar_init(&sh.ufull[s], 1);
-      mbar_init(&sh.uempty[s], 1);
-    }
-    for (int s = 0; s < NVSLOT; ++s) {
-      mbar_init(&sh.vfull[s], NWARP_V);  // every producer warp
-      mbar_init(&sh.vempty[s], 1);
-    }
+    for (int s = 0; s < NUH; ++s) mbar_init(&sh.ufull[s], 1);
+    for (int s = 0; s < NVSLOT; ++s) mbar_init(&sh.vfull[s], NWARP_V);  // every producer warp
+    for (int s = 0; s < NSD; ++s) mbar_init(&sh.sdone[s], 1);
     for (int s = 0; s < NSLAB; ++s) {
-      mbar_init(&sh.slabfull[s], NPROD);   // each producer thread's copies
+      mbar_init(&sh.slabfull[s], 1);          // the staging lane (plus the copies' bytes)
       mbar_init(&sh.slabfree[s], NWARP_V);
     }
     mbar_init(&sh.accf, 1);
@@ -120,8 +126,14 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
   const uint32_t tmem = sh.tmem_base;
   volatile int* abort_flag = &sh.abort_flag;
   const uint32_t smem_base = smem_u32(smem);
-  auto u_slot = [&](uint32_t s) { return smem_base + U_BASE + s * U_SLOT_BYTES; };
+  auto u_slot = [&](uint32_t s) { return smem_base + U_BASE + s * U_HALF_BYTES; };
   auto v_slot = [&](uint32_t s) { return smem_base + V_BASE + s * V_SLOT_BYTES; };
+  // Slot bookkeeping for step `it` (counted over this CTA's blocks):
+  //   V slot it % NVSLOT, reused at it + NVSLOT (after sdone of step it);
+  //   U half-slots 2 * (it % 2) + h, reused at it + 2 (after sdone of it);
+  //   slab it % NSLAB, reused at it + 3 (after the producers' slabfree).
+  // A waiter on sdone[j] for step it cannot miss its phase: the barrier's
+  // next phase needs operands the waiter has not supplied yet.
 
   if (warp == WARP_MMA) {
     if (lane == 0) {
@@ -147,10 +159,10 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
             if (!ok) break;
-            const uint32_t ui = 2 * it + h, us = ui % NUSLOT;
-            ok = mbar_wait(&sh.ufull[us], (ui / NUSLOT) & 1, abort_flag, err, ERR_WAIT_FULL);
+            const uint32_t us = 2 * (it & 1) + h;
+            ok = mbar_wait(&sh.ufull[us], (it >> 1) & 1, abort_flag, err, ERR_WAIT_FULL);
             if (!ok) break;
-            const uint64_t ad = adesc0 + ((us * U_SLOT_BYTES) >> 4);
+            const uint64_t ad = adesc0 + ((us * U_HALF_BYTES) >> 4);
             const uint64_t bd = bdesc0 + ((vs * V_SLOT_BYTES + 8 * h * V_TAP_BYTES) >> 4);
             const uint32_t d = tmem + 8 * h * TILES;
             if (first_step) {
@@ -169,89 +181,97 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
               for (int tt = 0; tt < 8; ++tt)
                 mma_f16(d + tt * TILES, ad + tt * astep, bd + tt * BSTEP, idesc, acc);
             }
-            mma_commit(&sh.uempty[us]);
           }
-          mma_commit(&sh.vempty[vs]);
+          if (ok) mma_commit(&sh.sdone[it % NSD]);
         }
         if (ok) mma_commit(&sh.accf);
       }
     }
     __syncwarp();
   } else if (warp == WARP_U) {
-    if (lane == 0) {
+    if (lane < 2) {
+      const int h = lane;
       const uint8_t* ucache = static_cast<const uint8_t*>(p.transform_filter);
-      uint32_t ui = 0;
+      uint32_t it = 0;
       bool ok = true;
       for (long long b = blockIdx.x; b < nblocks && ok; b += gridDim.x) {
         const int kb = (int)(b % nKB);
         const int kbs = kblock_rows(kb, g.K);
         const uint32_t bytes = 8 * kbs * 16 * 2;
-        for (int s = 0; s < g.CS && ok; ++s) {
-          for (int h = 0; h < 2; ++h, ++ui) {
-            const uint32_t us = ui % NUSLOT;
-            if (ui >= NUSLOT &&
-                !mbar_wait(&sh.uempty[us], (ui / NUSLOT - 1) & 1, abort_flag, err, ERR_WAIT_EMPTY)) {
-              ok = false;
-              break;
-            }
-            mbar_arrive_expect_tx(&sh.ufull[us], bytes);
-            bulk_g2s(smem + U_BASE + us * U_SLOT_BYTES,
-                     ucache + u_piece(kb, s, g.K, g.C) * 2 + (size_t)h * bytes, bytes, &sh.ufull[us]);
+        for (int s = 0; s < g.CS; ++s, ++it) {
+          if (it >= 2 &&
+              !mbar_wait(&sh.sdone[(it - 2) % NSD], ((it - 2) / NSD) & 1, abort_flag, err, ERR_WAIT_EMPTY)) {
+            ok = false;
+            break;
           }
+          const uint32_t us = 2 * (it & 1) + h;
+          mbar_arrive_expect_tx(&sh.ufull[us], bytes);
+          bulk_g2s(smem + U_BASE + us * U_HALF_BYTES,
+                   ucache + u_piece(kb, s, g.K, g.C) * 2 + (size_t)h * bytes, bytes, &sh.ufull[us]);
         }
       }
       if (*abort_flag) __nanosleep(20000);  // let copies already issued land
     }
     __syncwarp();
+  } else if (warp == WARP_S) {
+    const uint8_t* XB = static_cast<const uint8_t*>(p.transform_pin);
+    const int my_blocks =
+        blockIdx.x < nblocks ? (int)((nblocks - blockIdx.x + gridDim.x - 1) / gridDim.x) : 0;
+    const uint32_t RB = (uint32_t)xb_row_bytes(g.W);
+    const size_t img_stride = (size_t)(g.C >> 4) * xb_rows(g.H) * RB;   // one image of XB
+    const size_t cb_stride = (size_t)xb_rows(g.H) * RB;                  // one channel block
+    uint32_t it = 0;
+    bool ok = true;
+    for (int bi = 0; bi < my_blocks && ok; ++bi) {
+      const int tile0 = (int)((blockIdx.x + (long long)bi * gridDim.x) / nKB) * TILES;
+      const SlabPlan pl = slab_plan(g, tile0, TILES);
+      const bool use = XB != nullptr && slab_fits(g, pl);
+      int ta = 0, rows = 0, rbase = 0;  // this lane's segment
+#pragma unroll
+      for (int k = 0; k < SLAB_MAXSEG; ++k)
+        if (lane == k) { ta = pl.ta[k]; rows = pl.rows[k]; rbase = pl.row_base[k]; }
+      const uint8_t* src0 = XB + (size_t)(pl.n0 + lane) * img_stride + (size_t)(2 * ta) * RB;
+      for (int s = 0; s < g.CS; ++s, ++it) {
+        const uint32_t j = it % NSLAB;
+        if (it >= NSLAB &&
+            !mbar_wait_warp(&sh.slabfree[j], ((it - NSLAB) / NSLAB) & 1, abort_flag, err, ERR_WAIT_EMPTY, 64)) {
+          ok = false;
+          break;
+        }
+        if (use) {
+          if (lane == 0) mbar_arrive_expect_tx(&sh.slabfull[j], (uint32_t)pl.total_rows * RB);
+          __syncwarp();
+          if (lane < pl.nseg)
+            bulk_g2s(smem + SLAB_BASE + j * SLAB_BYTES + (uint32_t)rbase * RB, src0 + (size_t)s * cb_stride,
+                     (uint32_t)rows * RB, &sh.slabfull[j]);
+        } else if (lane == 0) {
+          mbar_arrive(&sh.slabfull[j]);
+        }
+      }
+    }
+    if (*abort_flag) __nanosleep(20000);  // let copies already issued land
+    __syncwarp();
   } else if (warp >= WARP_V0 && warp < WARP_V0 + NWARP_V) {
-    // The four producer warps work on every step together.  Two steps ahead
-    // they copy the input band of the step's block into a slab (cp.async,
-    // completion counted on slabfull); then warp q forms channels 4q..4q+3
-    // of the step's V for all 32 tiles (lane = tile) from the slab.
     const int q = warp - WARP_V0;
-    const int ptid = threadIdx.x - WARP_V0 * 32;
     const __half* X = static_cast<const __half*>(p.pin);
+    const bool have_xb = p.transform_pin != nullptr;
     const int my_blocks =
         blockIdx.x < nblocks ? (int)((nblocks - blockIdx.x + gridDim.x - 1) / gridDim.x) : 0;
     const int CS = g.CS;
     const uint32_t slab0 = smem_base + SLAB_BASE;
-    // Per-block quantities are formed once per block (32-bit math); the
-    // staging side runs two steps ahead, possibly into the next block.
-    auto block_tile0 = [&](int bi) { return (int)((blockIdx.x + (long long)bi * gridDim.x) / nKB) * TILES; };
     bool ok = true;
-    int st_bi = 0, st_s = 0;                      // next step to stage
-    SlabPlan st_pl = slab_plan(g, block_tile0(0), TILES);
-    uint32_t st_it = 0;
-    auto stage_next = [&]() {
-      const uint32_t j = st_it % NSLAB;
-      if (st_it >= NSLAB &&
-          !mbar_wait_warp(&sh.slabfree[j], ((st_it - NSLAB) / NSLAB) & 1, abort_flag, err, ERR_WAIT_EMPTY, 32)) {
-        ok = false;
-        return;
-      }
-      if (slab_fits(g, st_pl)) slab_stage(X, g, st_pl, st_s * 16, slab0 + j * SLAB_BYTES, ptid, NPROD);
-      cp_async_arrive(&sh.slabfull[j]);
-      ++st_it;
-      if (++st_s == CS) {
-        st_s = 0;
-        if (++st_bi < my_blocks) st_pl = slab_plan(g, block_tile0(st_bi), TILES);
-      }
-    };
-    const uint32_t total = (uint32_t)my_blocks * CS;
-    if (total > 0) stage_next();
-    if (total > 1) stage_next();
     // K-major core matrices: tile group (lane/8) at 256 B, channel half at
     // 128 B, tile row (lane%8) at 16 B, channel quarter inside the row at 8 B.
     const uint32_t row_off = (lane >> 3) * 256 + (q >> 1) * 128 + (lane & 7) * 16 + (q & 1) * 8;
     uint32_t it = 0;
     for (int bi = 0; bi < my_blocks && ok; ++bi) {
-      const int tile0 = block_tile0(bi);
+      // per-block quantities once per block, 32-bit
+      const int tile0 = (int)((blockIdx.x + (long long)bi * gridDim.x) / nKB) * TILES;
       const SlabPlan pl = slab_plan(g, tile0, TILES);
-      const bool use_slab = slab_fits(g, pl);
-      const TileCoord tc = tile_coord(g, tile0 + lane);
+      const bool use_slab = have_xb && slab_fits(g, pl);
+      const TileCoord tc = tile_coord(g, tile0 + lane, tile0);
+      const SlabWindow sw = slab_window(g, pl, tc, q);
       for (int s = 0; s < CS && ok; ++s, ++it) {
-        if (it + 2 < total) stage_next();
-        if (!ok) break;
         const uint32_t j = it % NSLAB;
         const uint32_t vs = it % NVSLOT;
         if (!mbar_wait_warp(&sh.slabfull[j], (it / NSLAB) & 1, abort_flag, err, ERR_WAIT_FULL, 32)) {
@@ -259,7 +279,8 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
           break;
         }
         if (it >= NVSLOT &&
-            !mbar_wait_warp(&sh.vempty[vs], (it / NVSLOT - 1) & 1, abort_flag, err, ERR_WAIT_EMPTY, 32)) {
+            !mbar_wait_warp(&sh.sdone[(it - NVSLOT) % NSD], ((it - NVSLOT) / NSD) & 1, abort_flag, err,
+                            ERR_WAIT_EMPTY, 32)) {
           ok = false;
           break;
         }
@@ -269,7 +290,7 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
                        : "memory");
         };
         if (use_slab)
-          produce_v_quarter_slab(g, pl, slab0 + j * SLAB_BYTES, tc, 4 * q, sink);
+          produce_v_quarter_xb(slab0 + j * SLAB_BYTES, sw, sink);
         else
           produce_v_quarter_global(X, g, tc, s * 16 + 4 * q, sink);
         fence_proxy_async_shared();
@@ -280,11 +301,10 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
         }
       }
     }
-  } else if (warp >= WARP_E0) {
+  } else if (warp >= WARP_E0 && warp < WARP_E0 + NWARP_E) {
     const int quarter = warp & 3;            // TMEM lanes 32*quarter .. +31 = channels
     const int half = (warp - WARP_E0) >> 2;  // tiles 16*half .. +15 of the block
     __half* Y = static_cast<__half*>(p.pout);
-    const long long per_img = (long long)g.TP * g.TQ;
     const bool q_even = (g.Q & 1) == 0;
     uint32_t bi = 0;
     for (long long b = blockIdx.x; b < nblocks; b += gridDim.x, ++bi) {
@@ -320,33 +340,56 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
           y[j][3] += c11 * m[j];
         }
       }
-      const int k = kb * KB + quarter * 32 + lane;
-      if (quarter * 32 + lane < kbs) {
-        long long tile = tb * TILES + half * 16;
-        int n = (int)(tile / per_img);
-        int r = (int)(tile - (long long)n * per_img);
-        int ty = r / g.TQ, tx = r - ty * g.TQ;
+      // Stores go through a 2 KB per-warp staging buffer, 8 tiles at a time:
+      // thread k writes its outputs as [k][row][8 tiles] half2 (16-byte
+      // chunks XOR-swizzled by k so the writes are conflict-free), then each
+      // store instruction writes 4 runs of 8 consecutive tiles (32 B of one
+      // output row of one channel) instead of 32 scattered words.
+      const uint32_t ebuf = smem_base + EPI_BASE + (uint32_t)(warp - WARP_E0) * EPI_WARP_BYTES;
+      const int kq = quarter * 32;             // first channel of this warp in the k-block
+      const size_t PQ = (size_t)g.P * g.Q;
 #pragma unroll
-        for (int j = 0; j < 16; ++j, ++tile) {
-          if (tile < g.NT) {
-            const int oy = 2 * ty, ox = 2 * tx;
-            const bool two_cols = ox + 1 < g.Q, two_rows = oy + 1 < g.P;
-            __half* o = Y + (((size_t)n * g.K + k) * g.P + oy) * (size_t)g.Q + ox;
-            if (two_cols && q_even) {
-              *reinterpret_cast<__half2*>(o) = __floats2half2_rn(y[j][0], y[j][1]);
-              if (two_rows) *reinterpret_cast<__half2*>(o + g.Q) = __floats2half2_rn(y[j][2], y[j][3]);
-            } else {
-              o[0] = __float2half_rn(y[j][0]);
-              if (two_cols) o[1] = __float2half_rn(y[j][1]);
-              if (two_rows) {
-                o[g.Q] = __float2half_rn(y[j][2]);
-                if (two_cols) o[g.Q + 1] = __float2half_rn(y[j][3]);
-              }
-            }
+      for (int r = 0; r < 2; ++r) {
+        __syncwarp();  // the previous round's reads are done
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {          // c = row * 2 + tile quad
+          const int row = c >> 1, j0 = 8 * r + 4 * (c & 1);
+          uint32_t w[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const __half2 h2 = __floats2half2_rn(y[j0 + u][2 * row], y[j0 + u][2 * row + 1]);
+            w[u] = *reinterpret_cast<const uint32_t*>(&h2);
           }
-          if (++tx == g.TQ) {  // advance to the next tile
-            tx = 0;
-            if (++ty == g.TP) { ty = 0; ++n; }
+          st_shared_v4(ebuf + lane * 64 + ((c ^ ((lane >> 1) & 3)) << 4), w[0], w[1], w[2], w[3]);
+        }
+        __syncwarp();
+        const int jj = lane & 7;                // tile within the round
+        const int tile = (int)tb * TILES + half * 16 + 8 * r + jj;
+        const bool tvalid = tile < (int)g.NT;
+        const int per_img = g.TP * g.TQ;
+        const int tt = tvalid ? tile : 0;
+        const int n = tt / per_img;
+        const int rr = tt - n * per_img;
+        const int ty = rr / g.TQ;
+        const int oy = 2 * ty, ox = 2 * (rr - ty * g.TQ);
+        const bool two_cols = ox + 1 < g.Q, two_rows = oy + 1 < g.P;
+        __half* o0 = Y + (((size_t)n * g.K + (size_t)(kb * KB + kq)) * g.P + oy) * (size_t)g.Q + ox;
+#pragma unroll 4
+        for (int i = 0; i < 16; ++i) {
+          const int run = 4 * i + (lane >> 3);
+          const int kk = run >> 1, row = run & 1;
+          uint32_t v;
+          asm volatile("ld.shared.b32 %0, [%1];"
+                       : "=r"(v)
+                       : "r"(ebuf + kk * 64 + (((row * 2 + (jj >> 2)) ^ ((kk >> 1) & 3)) << 4) + (jj & 3) * 4));
+          if (tvalid && kq + kk < kbs && (row == 0 || two_rows)) {
+            __half* o = o0 + (size_t)kk * PQ + (size_t)row * g.Q;
+            if (two_cols && q_even) {
+              *reinterpret_cast<uint32_t*>(o) = v;
+            } else {
+              reinterpret_cast<unsigned short*>(o)[0] = (unsigned short)(v & 0xffffu);
+              if (two_cols) reinterpret_cast<unsigned short*>(o)[1] = (unsigned short)(v >> 16);
+            }
           }
         }
       }

@@ -1,0 +1,102 @@
+// Input re-layout pre-pass for the fused kernel: NCHW fp16 -> XB records
+// (layout described in vgen.cuh), zero outside the image.
+//
+// The reference's pipeline also writes an intermediate form of the input into
+// the caller's `transform_pin` workspace before its GEMMs (the transformed
+// tiles V, 4x the input, src/preprocessing.cuh:273-424 writing
+// transform_pin); here that workspace receives the same-size channel-blocked
+// copy of the input and the transform itself happens on chip.
+//
+// One thread per (record row, entry e): it reads columns 2e and 2e+1 of the
+// row for all 16 channels (one 4-byte load per channel when W is even) and
+// writes par-0 entry e (column 2e) and par-1 entry e+1 (column 2e+1) of the
+// four channel quarters; the thread of the last entry also writes the
+// par-1 entry 0 (column -1, zero).  Consecutive threads read consecutive
+// words of each channel row and write consecutive 8-byte words of each
+// (par, quarter) run.  HBM-bound; items are counted in 32 bits (the host
+// checks N*(C/16)*rows*entries < 2^31).
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include "wino_param.h"
+#include "vgen.cuh"
+
+namespace wino {
+
+__global__ void __launch_bounds__(256) xb_layout_kernel(KernelParam p) {
+  const int C = p.c, H = p.h, W = p.w;
+  const int CB = C >> 4, HP = xb_rows(H), E = xb_entries(W);
+  const uint32_t items = (uint32_t)p.n * CB * HP * E;
+  const unsigned short* X = static_cast<const unsigned short*>(p.pin);
+  uint2* XB = static_cast<uint2*>(p.transform_pin);
+  const size_t plane = (size_t)H * W;
+  const bool w_even = (W & 1) == 0;
+  for (uint32_t it = blockIdx.x * blockDim.x + threadIdx.x; it < items; it += gridDim.x * blockDim.x) {
+    const uint32_t rec = it / E;
+    const int e = (int)(it - rec * E);
+    const int r = (int)(rec % HP);
+    const uint32_t ncb = rec / HP;
+    const int cb = (int)(ncb % CB);
+    const int n = (int)(ncb / CB);
+    const int y = r - 1;
+    const int x0 = 2 * e;                         // columns x0 (par 0) and x0 + 1 (par 1)
+    const bool ok0 = y >= 0 && y < H && x0 < W;
+    const bool ok1 = y >= 0 && y < H && x0 + 1 < W;
+    uint32_t lo[16], hi[16];                      // column x0 / x0+1 of channel 16cb + i
+    const unsigned short* src = X + ((size_t)n * C + 16 * cb) * plane + (size_t)(y < 0 ? 0 : y) * W + x0;
+    if (w_even && ok1) {
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const uint32_t v = *reinterpret_cast<const uint32_t*>(src + i * plane);
+        lo[i] = v & 0xffffu;
+        hi[i] = v >> 16;
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        lo[i] = ok0 ? src[i * plane] : 0u;
+        hi[i] = ok1 ? src[i * plane + 1] : 0u;
+      }
+    }
+    uint2* out = XB + (size_t)rec * (8 * E);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      out[q * E + e] = make_uint2(lo[4 * q] | (lo[4 * q + 1] << 16), lo[4 * q + 2] | (lo[4 * q + 3] << 16));
+      if (e + 1 < E)
+        out[(4 + q) * E + e + 1] =
+            make_uint2(hi[4 * q] | (hi[4 * q + 1] << 16), hi[4 * q + 2] | (hi[4 * q + 3] << 16));
+      else
+        out[(4 + q) * E] = make_uint2(0u, 0u);
+    }
+  }
+}
+
+}  // namespace wino
+
+using namespace wino;
+
+extern "C" {
+
+void* wino_xb_layout_kernel_ptr() { return (void*)xb_layout_kernel; }
+
+size_t wino_xb_bytes(int n, int c, int h, int w) { return xb_bytes(n, c, h, w); }
+
+// Items of the pre-pass (one per record row and entry); the kernel counts
+// them in 32 bits.
+long long wino_xb_items(int n, int c, int h, int w) {
+  return (long long)n * (c >> 4) * xb_rows(h) * xb_entries(w);
+}
+
+// Grid of the pre-pass: 256-thread CTAs over the items, capped (the kernel strides).
+unsigned wino_xb_layout_grid(int n, int c, int h, int w) {
+  const long long blocks = (wino_xb_items(n, c, h, w) + 255) / 256;
+  const long long cap = 148LL * 64;
+  return (unsigned)(blocks < cap ? (blocks > 0 ? blocks : 1) : cap);
+}
+
+int wino_launch_xb_layout(const KernelParam* p, cudaStream_t stream) {
+  void* args[] = {const_cast<KernelParam*>(p)};
+  return (int)cudaLaunchKernel((void*)xb_layout_kernel, dim3(wino_xb_layout_grid(p->n, p->c, p->h, p->w)),
+                               dim3(256), args, 0, stream);
+}
+
+}  // extern "C"

@@ -311,19 +311,36 @@ __device__ __forceinline__ void produce_v_tile16(const __half* __restrict__ X, c
 }
 
 // ---------------------------------------------------------------------------
-// Staged input for the fused kernel's cooperative V producers.
+// Channel-blocked input ("XB") for the fused kernel's V producers.
 //
-// The 32 consecutive tiles of a block touch, per image they cover, a band of
-// input rows; for every one of a step's 16 channels that band is one
-// contiguous run of memory (NCHW).  The producers copy those runs into a
-// shared-memory "slab" with cp.async two steps ahead, then form V from it.
-//   slab layout: [segment][channel 16][row of the band][W] fp16
-constexpr int SLAB_MAXSEG = 4;
-constexpr int SLAB_BYTES = 24 * 1024;
+// A pre-pass (input_layout.cu) rewrites the NCHW input once per call as
+// records of one input row of one image and 16 channels:
+//   XB[n][c / 16][r][par][q][e][4]   (fp16)
+// r = y + 1 for y = -1 .. 2*TP (XB_rows(H) = 2*TP + 2 rows), par = column
+// parity, q = channel quarter (channels 4q .. 4q+3), e = entry: par 0 entry e
+// holds column x = 2e, par 1 entry e holds column x = 2e - 1, e = 0 .. TQ
+// (XB_entries(W) = TQ + 1).  Every position outside the image is zero.
+// Then the 4 x 4 window of every tile lies inside the record rows and
+// entries, so the producers read it without bounds checks, one 8-byte word
+// (two channel pairs) per window position, and the window columns of 32
+// consecutive tiles are consecutive words (conflict-free shared loads).
+// The rows of a step's block form one contiguous run per image, which one
+// bulk copy brings into a shared-memory slab.
+__host__ __device__ __forceinline__ int xb_rows(int H) { return 2 * ((H + 1) >> 1) + 2; }
+__host__ __device__ __forceinline__ int xb_entries(int W) { return ((W + 1) >> 1) + 1; }
+__host__ __device__ __forceinline__ int xb_row_bytes(int W) { return 64 * xb_entries(W); }
+__host__ __device__ __forceinline__ size_t xb_bytes(int N, int C, int H, int W) {
+  return (size_t)N * (size_t)(C >> 4) * (size_t)xb_rows(H) * (size_t)xb_row_bytes(W);
+}
 
+constexpr int SLAB_MAXSEG = 4;
+constexpr int SLAB_BYTES = 16 * 1024;
+
+// Rows of one block's slab: per image it covers (segment) the record rows
+// 2*ta .. 2*tb + 3 of its first and last tile rows ta, tb.
 struct SlabPlan {
   int nseg, n0, total_rows;
-  int y_lo[SLAB_MAXSEG], rows[SLAB_MAXSEG], row_base[SLAB_MAXSEG];
+  int ta[SLAB_MAXSEG], rows[SLAB_MAXSEG], row_base[SLAB_MAXSEG];
 };
 
 __device__ __forceinline__ SlabPlan slab_plan(const Geometry& g, int tile0, int tiles_per_block) {
@@ -341,151 +358,101 @@ __device__ __forceinline__ SlabPlan slab_plan(const Geometry& g, int tile0, int 
   for (int k = 0; k < SLAB_MAXSEG; ++k) {
     const int ta = (k == 0) ? ty0 : 0;
     const int tb = (k == pl.nseg - 1) ? ty1 : g.TP - 1;
-    const int ylo = max(0, 2 * ta - 1), yhi = min(g.H - 1, 2 * tb + 2);
-    pl.y_lo[k] = ylo;
-    pl.rows[k] = (k < pl.nseg) ? yhi - ylo + 1 : 0;
+    pl.ta[k] = ta;
+    pl.rows[k] = (k < pl.nseg) ? 2 * (tb - ta) + 4 : 0;
     pl.row_base[k] = base;
-    base += 16 * pl.rows[k];
+    base += pl.rows[k];
   }
   pl.total_rows = base;
   return pl;
 }
 
-// Window origin of one tile: image, first input row, first word; valid ==
-// false past the end of the batch.  32-bit: tile counts stay below 2^31 for
-// any tensor that fits in device memory.
+__device__ __forceinline__ bool slab_fits(const Geometry& g, const SlabPlan& pl) {
+  return pl.nseg <= SLAB_MAXSEG && pl.total_rows * xb_row_bytes(g.W) <= SLAB_BYTES;
+}
+
+// Window origin of one tile; tiles past the end of the batch take the
+// coordinates of `fallback_tile` (a valid tile of the same block), so their
+// reads stay inside the block's slab.  32-bit: tile counts stay below 2^31
+// for any tensor that fits in device memory.
 struct TileCoord {
-  int n, y0, m0;
+  int n, ty, tx, y0, m0;
   bool valid;
 };
 
-__device__ __forceinline__ TileCoord tile_coord(const Geometry& g, int tile) {
+__device__ __forceinline__ TileCoord tile_coord(const Geometry& g, int tile, int fallback_tile) {
   TileCoord tc;
   tc.valid = tile < (int)g.NT;
   const int per_img = g.TP * g.TQ;
-  const int t = tc.valid ? tile : 0;
+  const int t = tc.valid ? tile : fallback_tile;
   tc.n = t / per_img;
   const int r = t - tc.n * per_img;
-  const int ty = r / g.TQ;
-  tc.y0 = 2 * ty - 1;
-  tc.m0 = r - ty * g.TQ - 1;
+  tc.ty = r / g.TQ;
+  tc.tx = r - tc.ty * g.TQ;
+  tc.y0 = 2 * tc.ty - 1;
+  tc.m0 = tc.tx - 1;
   return tc;
 }
 
-// Whether a block's slab fits (decided per block from its exact plan; blocks
-// that do not fit, and odd widths, read global memory instead).
-__device__ __forceinline__ bool slab_fits(const Geometry& g, const SlabPlan& pl) {
-  return (g.W & 1) == 0 && pl.nseg <= SLAB_MAXSEG &&
-         (long long)pl.total_rows * g.W * 2 <= SLAB_BYTES;
-}
+// Shared-memory offsets of one tile's window inside a slab, for channel
+// quarter q: row i of the window at row_off + i * RB; window column j at
+// +col_par1 (j = 0), +col_par0 (j = 1), +col_par1 + 8 (j = 2), +col_par0 + 8
+// (j = 3).
+struct SlabWindow {
+  uint32_t row_off, rb, col_par0, col_par1;
+};
 
-// Arrive on `bar` once all of this thread's earlier cp.async copies landed.
-__device__ __forceinline__ void cp_async_arrive(uint64_t* bar) {
-  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar))
-               : "memory");
-}
-
-__device__ __forceinline__ void cp_async4(uint32_t dst_smem, const void* src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst_smem), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
-// Copy the slab of channels c0..c0+15 for the block at tile0 (W even).
-// Called by all `nthreads` producer threads; thread `tid` strides the words.
-__device__ __forceinline__ void slab_stage(const __half* __restrict__ X, const Geometry& g,
-                                           const SlabPlan& pl, int c0, uint32_t slab, int tid,
-                                           int nthreads) {
-  const size_t plane = (size_t)g.H * g.W;
-  const int wpr = g.W >> 1;  // words per row
-#pragma unroll 1
-  for (int k = 0; k < pl.nseg; ++k) {
-    const int words = pl.rows[k] * wpr;
-    const __half* src0 = X + ((size_t)(pl.n0 + k) * g.C + c0) * plane + (size_t)pl.y_lo[k] * g.W;
-    const uint32_t dst0 = slab + (uint32_t)pl.row_base[k] * g.W * 2;
-#pragma unroll 1
-    for (int ch = 0; ch < 16; ++ch) {
-      const uint32_t* src = reinterpret_cast<const uint32_t*>(src0 + (size_t)ch * plane);
-      const uint32_t dst = dst0 + (uint32_t)(ch * words) * 4;
-      for (int w = tid; w < words; w += nthreads) cp_async4(dst + 4 * w, src + w);
-    }
-  }
-}
-
-__device__ __forceinline__ uint32_t lds_word_if(uint32_t addr, bool ok) {
-  uint32_t v = 0;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %2, 0;\n\t"
-      "@p ld.shared.u32 %0, [%1];\n\t}"
-      : "+r"(v)
-      : "r"(addr), "r"((uint32_t)ok));
-  return v;
-}
-
-// V of one tile for 4 channels (two pairs) and all 16 taps from the slab.
-// sink(t, w0, w1): tap t, channel pairs (c, c+1), (c+2, c+3).
-template <typename Sink>
-__device__ __forceinline__ void produce_v_quarter_slab(const Geometry& g, const SlabPlan& pl,
-                                                       uint32_t slab, const TileCoord& tc, int cq,
-                                                       Sink&& sink) {
-  const bool valid = tc.valid;
+__device__ __forceinline__ SlabWindow slab_window(const Geometry& g, const SlabPlan& pl,
+                                                  const TileCoord& tc, int q) {
+  SlabWindow sw;
   int k = tc.n - pl.n0;
   k = k < 0 ? 0 : (k >= SLAB_MAXSEG ? SLAB_MAXSEG - 1 : k);
-  int y_lo = pl.y_lo[0], rows = pl.rows[0], rbase = pl.row_base[0];
+  int ta = pl.ta[0], rbase = pl.row_base[0];
 #pragma unroll
   for (int j = 1; j < SLAB_MAXSEG; ++j)
-    if (k == j) { y_lo = pl.y_lo[j]; rows = pl.rows[j]; rbase = pl.row_base[j]; }
-  const int wpr = g.W >> 1;
-  const int m0 = tc.m0;
-  bool colok[3];
-#pragma unroll
-  for (int j = 0; j < 3; ++j) colok[j] = m0 + j >= 0 && m0 + j < wpr;
-  int srow[4];
-  bool rowok[4];
+    if (k == j) { ta = pl.ta[j]; rbase = pl.row_base[j]; }
+  const int E = xb_entries(g.W);
+  sw.rb = (uint32_t)xb_row_bytes(g.W);
+  sw.row_off = (uint32_t)(rbase + 2 * (tc.ty - ta)) * sw.rb;
+  sw.col_par0 = (uint32_t)((q * E + tc.tx) * 8);
+  sw.col_par1 = (uint32_t)(((4 + q) * E + tc.tx) * 8);
+  return sw;
+}
+
+__device__ __forceinline__ void lds_v2(uint32_t addr, uint32_t& a, uint32_t& b) {
+  asm volatile("ld.shared.v2.b32 {%0, %1}, [%2];" : "=r"(a), "=r"(b) : "r"(addr));
+}
+
+// V of one tile for 4 channels (two pairs) and all 16 taps from an XB slab.
+// sink(t, w0, w1): tap t, channel pairs (c, c+1), (c+2, c+3).
+template <typename Sink>
+__device__ __forceinline__ void produce_v_quarter_xb(uint32_t slab, const SlabWindow& sw,
+                                                     Sink&& sink) {
+  uint32_t d0[4][4], d1[4][4];  // window (row, col) for channel pair 0 and 1
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    const int y = tc.y0 + i;
-    const int r = y - y_lo;
-    rowok[i] = valid && y >= 0 && y < g.H && r >= 0 && r < rows;
-    srow[i] = rowok[i] ? r : 0;
+    const uint32_t row = slab + sw.row_off + (uint32_t)i * sw.rb;
+    lds_v2(row + sw.col_par1, d0[i][0], d1[i][0]);
+    lds_v2(row + sw.col_par0, d0[i][1], d1[i][1]);
+    lds_v2(row + sw.col_par1 + 8, d0[i][2], d1[i][2]);
+    lds_v2(row + sw.col_par0 + 8, d0[i][3], d1[i][3]);
   }
   uint32_t out[16][2];
 #pragma unroll
-  for (int cp = 0; cp < 2; ++cp) {
-    const int ca = cq + 2 * cp;
-    uint32_t wa[4][3], wb[4][3];
+  for (int a = 0; a < 4; ++a) {
+    uint32_t e0[4], e1[4];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const uint32_t rowa = slab + (uint32_t)((rbase + ca * rows + srow[i]) * wpr) * 4;
-      const uint32_t rowb = rowa + (uint32_t)(rows * wpr) * 4;
-#pragma unroll
-      for (int j = 0; j < 3; ++j) {
-        const bool ok = rowok[i] && colok[j];
-        const uint32_t off = (uint32_t)(ok ? m0 + j : 0) * 4;
-        wa[i][j] = lds_word_if(rowa + off, ok);
-        wb[i][j] = lds_word_if(rowb + off, ok);
-      }
+    for (int j = 0; j < 4; ++j) {
+      e0[j] = bt_row(a, d0[0][j], d0[1][j], d0[2][j], d0[3][j]);
+      e1[j] = bt_row(a, d1[0][j], d1[1][j], d1[2][j], d1[3][j]);
     }
-    uint32_t d[4][4];
+    uint32_t v0[4], v1[4];
+    bt_cols(e0[0], e0[1], e0[2], e0[3], v0);
+    bt_cols(e1[0], e1[1], e1[2], e1[3], v1);
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      d[i][0] = pk_hi(wa[i][0], wb[i][0]);
-      d[i][1] = pk_lo(wa[i][1], wb[i][1]);
-      d[i][2] = pk_hi(wa[i][1], wb[i][1]);
-      d[i][3] = pk_lo(wa[i][2], wb[i][2]);
-    }
-#pragma unroll
-    for (int a = 0; a < 4; ++a) {
-      uint32_t e[4];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) e[j] = bt_row(a, d[0][j], d[1][j], d[2][j], d[3][j]);
-      uint32_t v[4];
-      bt_cols(e[0], e[1], e[2], e[3], v);
-#pragma unroll
-      for (int b = 0; b < 4; ++b) out[4 * a + b][cp] = v[b];
+    for (int b = 0; b < 4; ++b) {
+      out[4 * a + b][0] = v0[b];
+      out[4 * a + b][1] = v1[b];
     }
   }
 #pragma unroll

@@ -55,6 +55,11 @@ int wino_fused_smem_bytes();
 int wino_fused_threads();
 long long wino_fused_nblocks(int n, int h, int w, int k);
 uint32_t wino_fused_error_read_clear();
+void* wino_xb_layout_kernel_ptr();
+size_t wino_xb_bytes(int n, int c, int h, int w);
+unsigned wino_xb_layout_grid(int n, int c, int h, int w);
+long long wino_xb_items(int n, int c, int h, int w);
+int wino_launch_xb_layout(const wino::KernelParam* p, cudaStream_t stream);
 size_t wino_unfused_v_bytes(int n, int c, int h, int w);
 size_t wino_unfused_m_bytes(int n, int k, int h, int w);
 int wino_unfused_prepare();
@@ -107,6 +112,9 @@ wino::KernelParam make_param(const void* x, const void* w, void* y, void* vws, v
   return p;
 }
 
+// The pre-pass counts its items in 32 bits.
+bool xb_items_ok(int n, int c, int h, int w) { return wino_xb_items(n, c, h, w) < (1LL << 31); }
+
 unsigned fused_grid(int n, int h, int w, int k) {
   const long long nb = wino_fused_nblocks(n, h, w, k);
   const long long sms = sm_count();
@@ -153,21 +161,35 @@ int getkernelInfo(problem_t* problem, kernelInfo_t* kernelInfo, void* param) {
 
   if (wino_fused_prepare() != 0) return WINO_ECUDA;
 
+  // The caller's transform_pin workspace holds 4*h*h*n*c fp16 elements
+  // (reference src/main.cpp:36-38); when the channel-blocked input fits
+  // there (and is 16-byte aligned) slot 2 writes it and the fused kernel
+  // stages from it, otherwise the fused kernel reads the NCHW input itself.
+  const size_t pin_ws_bytes = (size_t)4 * pr.h * pr.h * pr.n * pr.c * 2;
+  const bool use_xb = pr.transform_pin != nullptr &&
+                      (reinterpret_cast<uintptr_t>(pr.transform_pin) & 15) == 0 &&
+                      wino_xb_bytes((int)pr.n, (int)pr.c, (int)pr.h, (int)pr.w) <= pin_ws_bytes &&
+                      xb_items_ok((int)pr.n, (int)pr.c, (int)pr.h, (int)pr.w);
+
   std::memset(kernelInfo, 0, sizeof(*kernelInfo));
   const long long kc = (long long)pr.k * pr.c;
   set_slot(kernelInfo, 1, (unsigned)((kc + 255) / 256), 1, 1, 256, 1, 1, 0,
            wino_dropin_filter_kernel_ptr());
-  set_slot(kernelInfo, 2, fused_grid((int)pr.n, (int)pr.h, (int)pr.w, (int)pr.k), 1, 1,
+  if (use_xb)
+    set_slot(kernelInfo, 2, wino_xb_layout_grid((int)pr.n, (int)pr.c, (int)pr.h, (int)pr.w), 1, 1, 256, 1, 1, 0,
+             wino_xb_layout_kernel_ptr());
+  else
+    set_slot(kernelInfo, 2, 1, 1, 1, 32, 1, 1, 0, wino_noop_kernel_ptr());
+  set_slot(kernelInfo, 3, fused_grid((int)pr.n, (int)pr.h, (int)pr.w, (int)pr.k), 1, 1,
            (unsigned)wino_fused_threads(), 1, 1, (unsigned)wino_fused_smem_bytes(),
            wino_fused_kernel_ptr());
-  set_slot(kernelInfo, 3, 1, 1, 1, 32, 1, 1, 0, wino_noop_kernel_ptr());
   set_slot(kernelInfo, 4, 1, 1, 1, 32, 1, 1, 0, wino_noop_kernel_ptr());
 
   mykernelParamType* a = static_cast<mykernelParamType*>(param);
   a->pin = pr.in;
   a->pweight = pr.weight;
   a->pout = pr.out;
-  a->transform_pin = pr.transform_pin;
+  a->transform_pin = use_xb ? pr.transform_pin : nullptr;
   a->transform_filter = pr.transform_filter;
   a->mid_result = pr.mid_result;
   a->n = (short)pr.n; a->c = (short)pr.c; a->h = (short)pr.h; a->w = (short)pr.w;
@@ -233,6 +255,40 @@ extern "C" int wino_conv2d_fused(const void* x, const void* ucache, void* y, int
   if (wino_fused_prepare() != 0) return WINO_ECUDA;
   wino::KernelParam p = make_param(x, nullptr, y, nullptr, const_cast<void*>(ucache), nullptr, n, c,
                                    h, w, k);
+  void* args[] = {&p};
+  const cudaError_t e = cudaLaunchKernel(wino_fused_kernel_ptr(), dim3(fused_grid(n, h, w, k)),
+                                         dim3(wino_fused_threads()), args,
+                                         (size_t)wino_fused_smem_bytes(), (cudaStream_t)stream);
+  return e == cudaSuccess ? WINO_OK : WINO_ECUDA;
+}
+
+extern "C" size_t wino_fused_workspace_bytes(int n, int c, int h, int w) {
+  if (wino_check_shape(n, c, h, w, 16) != WINO_OK) return 0;
+  return wino_xb_bytes(n, c, h, w);
+}
+
+extern "C" int wino_input_layout(const void* x, void* workspace, int n, int c, int h, int w,
+                                 void* stream) {
+  if (!x || !workspace) return WINO_EINVAL;
+  if ((reinterpret_cast<uintptr_t>(workspace) & 15) != 0) return WINO_EINVAL;
+  const int st = wino_check_shape(n, c, h, w, 16);
+  if (st != WINO_OK) return st;
+  if (!xb_items_ok(n, c, h, w)) return WINO_EUNSUPPORTED;
+  wino::KernelParam p = make_param(x, nullptr, nullptr, workspace, nullptr, nullptr, n, c, h, w, 16);
+  return wino_launch_xb_layout(&p, (cudaStream_t)stream) == 0 ? WINO_OK : WINO_ECUDA;
+}
+
+extern "C" int wino_conv2d_fused_ws(const void* x, const void* ucache, void* workspace, void* y,
+                                    int n, int c, int h, int w, int k, void* stream) {
+  if (!x || !ucache || !y || !workspace) return WINO_EINVAL;
+  if ((reinterpret_cast<uintptr_t>(workspace) & 15) != 0) return WINO_EINVAL;
+  const int st = wino_check_shape(n, c, h, w, k);
+  if (st != WINO_OK) return st;
+  if (!xb_items_ok(n, c, h, w)) return WINO_EUNSUPPORTED;
+  if (wino_fused_prepare() != 0) return WINO_ECUDA;
+  wino::KernelParam p = make_param(x, nullptr, y, workspace, const_cast<void*>(ucache), nullptr, n,
+                                   c, h, w, k);
+  if (wino_launch_xb_layout(&p, (cudaStream_t)stream) != 0) return WINO_ECUDA;
   void* args[] = {&p};
   const cudaError_t e = cudaLaunchKernel(wino_fused_kernel_ptr(), dim3(fused_grid(n, h, w, k)),
                                          dim3(wino_fused_threads()), args,

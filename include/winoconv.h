@@ -59,6 +59,18 @@ int wino_filter_transform(const void* weight, void* ucache, int k, int c, void* 
 int wino_conv2d_fused(const void* x, const void* ucache, void* y, int n, int c, int h, int w,
                       int k, void* stream);
 
+/* The same with a caller workspace of wino_fused_workspace_bytes() bytes
+ * (16-byte aligned): a pre-pass writes the input there once in a
+ * channel-blocked layout, which the fused kernel stages into shared memory
+ * with bulk copies -- the fast path.  (The reference likewise hands its
+ * input-transform kernel the caller's transform_pin workspace,
+ * src/main.cpp:36-38, src/preprocessing.cuh:273-424.) */
+size_t wino_fused_workspace_bytes(int n, int c, int h, int w);
+/* The pre-pass alone (input -> workspace), e.g. to time it apart. */
+int wino_input_layout(const void* x, void* workspace, int n, int c, int h, int w, void* stream);
+int wino_conv2d_fused_ws(const void* x, const void* ucache, void* workspace, void* y, int n, int c,
+                         int h, int w, int k, void* stream);
+
 /* The plain unfused path, the comparator of the fused kernel: input
  * transform to V in global memory, the 16 tap GEMMs as one batched tcgen05
  * GEMM writing M (fp16) to global memory, output transform -- the stage

@@ -38,11 +38,33 @@ def _check(oracle_mod, y, y64, what=""):
     return rl2, mxn
 
 
-def _fused(wino, x16, w16, dev):
+def _fused(wino, x16, w16, dev, path="xb"):
+    """path "xb": input re-layout pre-pass + staged fused kernel (default);
+    "direct": the fused kernel reading the NCHW input itself."""
     import torch
-    y = wino.conv2d(_t(x16, dev), _t(w16, dev))
+    x, w = _t(x16, dev), _t(w16, dev)
+    u = wino.filter_transform(w)
+    y = wino.conv2d_fused(x, u, w.shape[0], workspace=(path == "xb"))
     torch.cuda.synchronize()
     return y.cpu().numpy()
+
+
+def _xb_layout_np(x16):
+    """NumPy statement of the channel-blocked input records the pre-pass
+    writes: XB[n][c/16][r][par][q][e][4], r = y + 1 for y = -1 .. 2*TP,
+    par 0 entry e = column 2e, par 1 entry e = column 2e - 1, zero outside."""
+    n, c, h, w = x16.shape
+    tp, tq = (h + 1) // 2, (w + 1) // 2
+    hp, e = 2 * tp + 2, tq + 1
+    pad = np.zeros((n, c, hp, 2 * e + 1), np.float16)       # columns -1 .. 2e-1
+    pad[:, :, 1:h + 1, 1:w + 1] = x16
+    out = np.zeros((n, c // 16, hp, 2, 4, e, 4), np.float16)
+    xs0 = 2 * np.arange(e) + 1          # column 2e   -> padded index 2e + 1
+    xs1 = 2 * np.arange(e)              # column 2e-1 -> padded index 2e
+    v = pad.reshape(n, c // 16, 4, 4, hp, 2 * e + 1)        # n, cb, q, ci, r, col
+    out[:, :, :, 0] = v[..., xs0].transpose(0, 1, 4, 2, 5, 3)
+    out[:, :, :, 1] = v[..., xs1].transpose(0, 1, 4, 2, 5, 3)
+    return out
 
 
 def test_torch_fp64_reference_agrees_with_oracle(cuda, oracle_mod):
@@ -52,10 +74,11 @@ def test_torch_fp64_reference_agrees_with_oracle(cuda, oracle_mod):
     assert np.max(np.abs(yt - y64)) <= 1e-10 * np.max(np.abs(y64))
 
 
+@pytest.mark.parametrize("fpath", ["xb", "direct"])
 @pytest.mark.parametrize("path", golden_cases(), ids=lambda p: p.rsplit("/", 1)[-1])
-def test_fused_vs_reference_golden(wino, cuda, oracle_mod, path):
+def test_fused_vs_reference_golden(wino, cuda, oracle_mod, path, fpath):
     x, w, y_ref = load_golden(path)
-    y = _fused(wino, x, w, cuda)
+    y = _fused(wino, x, w, cuda, fpath)
     y64 = oracle_mod.conv2d_f64(x, w)
     _check(oracle_mod, y, y64, path)
     # and against the reference's own fp16 output (one fp16 rounding apart)
@@ -70,11 +93,15 @@ def test_fused_vs_reference_golden(wino, cuda, oracle_mod, path):
     (3, 16, 18, 18, 32),    # tile groups crossing images
     (1, 64, 40, 40, 64),    # fast path, several tile blocks
     (5, 16, 1, 1, 16),      # one pixel per image
+    (2, 16, 7, 7, 16),      # 16 tiles per image: a block spans two images
+    (1, 16, 6, 224, 16),    # rows wider than a slab: direct reads
+    (40, 16, 2, 2, 16),     # one tile per image: more images than slab segments
 ])
-def test_fused_edge_shapes(wino, cuda, oracle_mod, shape):
+@pytest.mark.parametrize("fpath", ["xb", "direct"])
+def test_fused_edge_shapes(wino, cuda, oracle_mod, shape, fpath):
     n, c, h, w, k = shape
     x, wt = oracle_mod.make_inputs(n, c, h, w, k, seed=sum(shape), x_dist="normal")
-    y = _fused(wino, x, wt, cuda)
+    y = _fused(wino, x, wt, cuda, fpath)
     _check(oracle_mod, y, oracle_mod.conv2d_f64(x, wt), str(shape))
 
 
@@ -117,21 +144,55 @@ def test_dropin_abi_path_and_reference_check(wino, cuda, oracle_mod):
     assert oracle_mod.reference_check(y, cpu16) == 0
 
 
-def test_dropin_slots_are_the_expected_kernels(wino, cuda):
+@pytest.mark.parametrize("with_pin", [True, False])
+def test_dropin_slots_are_the_expected_kernels(wino, cuda, with_pin):
     import ctypes
     import torch
     x = torch.zeros((1, 16, 8, 8), dtype=torch.float16, device=cuda)
     w = torch.zeros((16, 16, 3, 3), dtype=torch.float16, device=cuda)
     y = torch.empty((1, 16, 8, 8), dtype=torch.float16, device=cuda)
-    tf = torch.empty(16 * 16 * 16, dtype=torch.float16, device=cuda)
-    pr = wino.make_problem(x, w, y, None, tf, None)
+    ws = wino.DropinWorkspaces(1, 16, 8, 8, 16, cuda, transform_pin=with_pin)
+    pr = wino.make_problem(x, w, y, ws.transform_pin, ws.transform_filter, ws.mid_result)
     param = (ctypes.c_char * 80)()
     rc, ki = wino.get_kernel_info(pr, param)
     assert rc == 0
     for i in (1, 2, 3, 4):
         s = ki.slot(i)
         assert s["kernel"] and all(g >= 1 for g in s["grid"]) and all(b >= 1 for b in s["block"])
-    assert ki.slot(2)["lds"] > 48 * 1024  # the fused kernel's pipeline
+    assert ki.slot(3)["lds"] > 48 * 1024  # the fused kernel's pipeline
+    # slot 2: the input re-layout pre-pass, or the same no-op kernel as slot 4
+    assert (ki.slot(2)["kernel"] != ki.slot(4)["kernel"]) == with_pin
+
+
+@pytest.mark.parametrize("shape", [(2, 32, 9, 14), (1, 16, 1, 1), (3, 48, 8, 7)])
+def test_input_layout_prepass_bit_exact(wino, cuda, oracle_mod, shape):
+    """The pre-pass output equals the NumPy statement of the layout, bit for bit."""
+    import ctypes
+    import torch
+    n, c, h, w = shape
+    x, _ = oracle_mod.make_inputs(n, c, h, w, 16, seed=3, x_dist="normal")
+    nbytes = wino.fused_workspace_bytes(n, c, h, w)
+    ref = _xb_layout_np(x)
+    assert ref.nbytes == nbytes
+    ws = torch.full((nbytes,), 0xA5, dtype=torch.uint8, device=cuda)   # poison
+    xt = _t(x, cuda)
+    u = torch.zeros(16 * 16 * c, dtype=torch.float16, device=cuda)
+    y = torch.empty((n, 16, h, w), dtype=torch.float16, device=cuda)
+    rc = wino.lib().wino_conv2d_fused_ws(ctypes.c_void_p(xt.data_ptr()), ctypes.c_void_p(u.data_ptr()),
+                                         ctypes.c_void_p(ws.data_ptr()), ctypes.c_void_p(y.data_ptr()),
+                                         n, c, h, w, 16, wino._stream())
+    assert rc == 0
+    torch.cuda.synchronize()
+    got = ws.cpu().numpy().view(np.uint16)
+    assert np.array_equal(got, ref.view(np.uint16).reshape(-1))
+
+
+def test_dropin_without_transform_pin(wino, cuda, oracle_mod):
+    import torch
+    x, w = oracle_mod.make_inputs(2, 32, 12, 10, 32, seed=5, x_dist="normal")
+    y = wino.dropin_conv2d(_t(x, cuda), _t(w, cuda), transform_pin=False)
+    torch.cuda.synchronize()
+    _check(oracle_mod, y.cpu().numpy(), oracle_mod.conv2d_f64(x, w), "drop-in, no transform_pin")
 
 
 def _unfused(wino, x16, w16, dev):
