@@ -21,7 +21,7 @@
 // transform small next to the MMAs.
 //
 // Pipelines (shared memory, 225 KB): U in four 32 KB half-step slots (two
-// steps in flight); V in two 16 KB slots, one per step; three 16 KB input
+// steps in flight); V in three 16 KB slots, one per step; two 16 KB input
 // slabs; 16 KB of epilogue store staging.  The MMA thread commits once per step (each tcgen05.commit stalls
 // the MMA pipe for ~90 cycles on this part) to a "step done" barrier that
 // releases that step's U half-slots and V slot together.
@@ -30,18 +30,21 @@
 //   warp 0       TMEM allocation; one thread issues the MMAs
 //   warp 1       lanes 0 and 1 bulk-copy the two U halves of a step (one
 //                copy in flight per issuing thread, so two threads)
-//   warps 2-5    V producers, all four on every step: warp q forms channels
-//                4q..4q+3 of the step's V for all 32 tiles (lane = tile):
+//   warps 2-5    V producers, all four on every step: warp q forms channel
+//                half q&1 (8 channels) of tap rows 2(q>>1), 2(q>>1)+1 (8
+//                taps) of the step's V for all 32 tiles (lane = tile):
 //                B^T d B in packed fp16 straight into the K-major operand
-//                (8 tiles x 8 channels per core matrix).  They read the
-//                step's slab, or, without an XB workspace or when a block's
-//                rows exceed a slab, the NCHW input directly.
-//   warps 6-13   epilogue: drain TMEM tap by tap (each drained tap is handed
-//                back to the MMA thread at once, so the next block's MMAs
-//                overlap the drain), A^T m A in fp32, fp16 NKPQ stores.
+//                (8 tiles x 8 channels per core matrix, one 16-byte row per
+//                lane and tap).  They read the step's slab, or, without an
+//                XB workspace or when a block's rows exceed a slab, the NCHW
+//                input directly.
+//   warps 6-13   epilogue: drain TMEM one tap half at a time (the block's
+//                last MMAs commit each half separately, and each drained half
+//                goes back to the MMA thread at once, so the drain overlaps
+//                the MMAs on both sides), A^T m A in fp32, fp16 NKPQ stores.
 //   warp 14      stager: with an XB workspace (p.transform_pin, written by
 //                the pre-pass of input_layout.cu) bulk-copies each step's
-//                input rows into a slab, up to three steps ahead (one copy
+//                input rows into a slab, up to two steps ahead (one copy
 //                per image the block touches, issued from separate lanes).
 #include <cuda_runtime.h>
 #include "tc_sm100.cuh"
@@ -60,7 +63,7 @@ constexpr int V_TAP_BYTES = TILES * 16 * 2;          // 1 KB per tap per step
 constexpr int V_SLOT_BYTES = NTAP * V_TAP_BYTES;     // 16 KB: one step of V
 constexpr int U_HALF_BYTES = 8 * KB * 16 * 2;        // 32 KB: 8 taps of a step of U
 constexpr int NUH = 4;                 // U half-slots: two steps
-constexpr int NVSLOT = 2, NSD = 3, NSLAB = 3;
+constexpr int NVSLOT = 3, NSD = 3, NSLAB = 2;
 constexpr int EPI_WARP_BYTES = 2048;   // epilogue store staging per warp
 constexpr int U_BASE = 0, V_BASE = NUH * U_HALF_BYTES;
 constexpr int SLAB_BASE = V_BASE + NVSLOT * V_SLOT_BYTES;
@@ -76,8 +79,8 @@ struct Shared {
   uint64_t vfull[NVSLOT];
   uint64_t sdone[NSD];                 // MMAs of step it complete: sdone[it % NSD]
   uint64_t slabfull[NSLAB], slabfree[NSLAB];
-  uint64_t accf;
-  uint64_t tapfree[NTAP];
+  uint64_t accf[2];                    // last MMAs of a block done, per tap half
+  uint64_t tapfree[2];                 // epilogue drained a tap half of TMEM
   uint32_t tmem_base;
   int abort_flag;
 };
@@ -111,8 +114,10 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
       mbar_init(&sh.slabfull[s], 1);          // the staging lane (plus the copies' bytes)
       mbar_init(&sh.slabfree[s], NWARP_V);
     }
-    mbar_init(&sh.accf, 1);
-    for (int t = 0; t < NTAP; ++t) mbar_init(&sh.tapfree[t], NWARP_E);
+    for (int h = 0; h < 2; ++h) {
+      mbar_init(&sh.accf[h], 1);
+      mbar_init(&sh.tapfree[h], NWARP_E);
+    }
     sh.abort_flag = 0;
     fence_barrier_init();
   }
@@ -131,7 +136,7 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
   // Slot bookkeeping for step `it` (counted over this CTA's blocks):
   //   V slot it % NVSLOT, reused at it + NVSLOT (after sdone of step it);
   //   U half-slots 2 * (it % 2) + h, reused at it + 2 (after sdone of it);
-  //   slab it % NSLAB, reused at it + 3 (after the producers' slabfree).
+  //   slab it % NSLAB, reused at it + NSLAB (after the producers' slabfree).
   // A waiter on sdone[j] for step it cannot miss its phase: the barrier's
   // next phase needs operands the waiter has not supplied yet.
 
@@ -166,25 +171,21 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
             const uint64_t bd = bdesc0 + ((vs * V_SLOT_BYTES + 8 * h * V_TAP_BYTES) >> 4);
             const uint32_t d = tmem + 8 * h * TILES;
             if (first_step) {
-              // the previous block's epilogue hands each tap's columns back in turn
-#pragma unroll
-              for (int tt = 0; tt < 8; ++tt) {
-                if (!mbar_wait(&sh.tapfree[8 * h + tt], (bi - 1) & 1, abort_flag, err, ERR_WAIT_DRAIN)) {
-                  ok = false;
-                  break;
-                }
-                tc_fence_after();
-                mma_f16(d + tt * TILES, ad + tt * astep, bd + tt * BSTEP, idesc, acc);
+              // the previous block's epilogue hands back each tap half of TMEM
+              if (!mbar_wait(&sh.tapfree[h], (bi - 1) & 1, abort_flag, err, ERR_WAIT_DRAIN)) {
+                ok = false;
+                break;
               }
-            } else {
-#pragma unroll
-              for (int tt = 0; tt < 8; ++tt)
-                mma_f16(d + tt * TILES, ad + tt * astep, bd + tt * BSTEP, idesc, acc);
+              tc_fence_after();
             }
+#pragma unroll
+            for (int tt = 0; tt < 8; ++tt)
+              mma_f16(d + tt * TILES, ad + tt * astep, bd + tt * BSTEP, idesc, acc);
+            // after the block's last MMAs of a tap half the epilogue may drain it
+            if (s == g.CS - 1) mma_commit(&sh.accf[h]);
           }
           if (ok) mma_commit(&sh.sdone[it % NSD]);
         }
-        if (ok) mma_commit(&sh.accf);
       }
     }
     __syncwarp();
@@ -253,6 +254,8 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
     __syncwarp();
   } else if (warp >= WARP_V0 && warp < WARP_V0 + NWARP_V) {
     const int q = warp - WARP_V0;
+    const int hh = q & 1;                     // channel half: channels 8hh .. 8hh+7
+    const int ar = q >> 1;                    // tap rows 2ar, 2ar+1 (taps 8ar .. 8ar+7)
     const __half* X = static_cast<const __half*>(p.pin);
     const bool have_xb = p.transform_pin != nullptr;
     const int my_blocks =
@@ -261,8 +264,9 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
     const uint32_t slab0 = smem_base + SLAB_BASE;
     bool ok = true;
     // K-major core matrices: tile group (lane/8) at 256 B, channel half at
-    // 128 B, tile row (lane%8) at 16 B, channel quarter inside the row at 8 B.
-    const uint32_t row_off = (lane >> 3) * 256 + (q >> 1) * 128 + (lane & 7) * 16 + (q & 1) * 8;
+    // 128 B, tile row (lane%8) at 16 B: each lane writes whole 16-byte rows,
+    // eight lanes 128 contiguous bytes (conflict-free).
+    const uint32_t row_off = (lane >> 3) * 256 + hh * 128 + (lane & 7) * 16 + ar * 8 * V_TAP_BYTES;
     uint32_t it = 0;
     for (int bi = 0; bi < my_blocks && ok; ++bi) {
       // per-block quantities once per block, 32-bit
@@ -270,7 +274,7 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
       const SlabPlan pl = slab_plan(g, tile0, TILES);
       const bool use_slab = have_xb && slab_fits(g, pl);
       const TileCoord tc = tile_coord(g, tile0 + lane, tile0);
-      const SlabWindow sw = slab_window(g, pl, tc, q);
+      const SlabWindow sw = slab_window(g, pl, tc, hh);
       for (int s = 0; s < CS && ok; ++s, ++it) {
         const uint32_t j = it % NSLAB;
         const uint32_t vs = it % NVSLOT;
@@ -285,14 +289,27 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
           break;
         }
         const uint32_t dst = v_slot(vs) + row_off;
-        auto sink = [&](int t, uint32_t w0, uint32_t w1) {
-          asm volatile("st.shared.v2.b32 [%0], {%1, %2};" ::"r"(dst + t * V_TAP_BYTES), "r"(w0), "r"(w1)
-                       : "memory");
-        };
-        if (use_slab)
-          produce_v_quarter_xb(slab0 + j * SLAB_BYTES, sw, sink);
-        else
-          produce_v_quarter_global(X, g, tc, s * 16 + 4 * q, sink);
+        if (use_slab) {
+          auto sink = [&](int u, const uint32_t (&w)[4]) {
+            st_shared_v4(dst + u * V_TAP_BYTES, w[0], w[1], w[2], w[3]);
+          };
+          if (ar == 0)
+            produce_v_half_xb<0>(slab0 + j * SLAB_BYTES, sw, sink);
+          else
+            produce_v_half_xb<1>(slab0 + j * SLAB_BYTES, sw, sink);
+        } else {
+          // direct NCHW reads: two channel quarters, keeping this warp's taps
+#pragma unroll 1
+          for (int qq = 0; qq < 2; ++qq) {
+            auto sink = [&](int t, uint32_t w0, uint32_t w1) {
+              if ((t >> 3) == ar)
+                asm volatile("st.shared.v2.b32 [%0], {%1, %2};" ::"r"(dst + (t & 7) * V_TAP_BYTES + qq * 8),
+                             "r"(w0), "r"(w1)
+                             : "memory");
+            };
+            produce_v_quarter_global(X, g, tc, s * 16 + 8 * hh + 4 * qq, sink);
+          }
+        }
         fence_proxy_async_shared();
         __syncwarp();
         if (lane == 0) {
@@ -307,9 +324,8 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
     __half* Y = static_cast<__half*>(p.pout);
     const bool q_even = (g.Q & 1) == 0;
     uint32_t bi = 0;
-    for (long long b = blockIdx.x; b < nblocks; b += gridDim.x, ++bi) {
-      if (!mbar_wait_warp(&sh.accf, bi & 1, abort_flag, err, ERR_WAIT_ACCUM, 128)) break;
-      tc_fence_after();
+    bool ok = true;
+    for (long long b = blockIdx.x; b < nblocks && ok; b += gridDim.x, ++bi) {
       const long long tb = b / nKB;
       const int kb = (int)(b % nKB);
       const int kbs = kblock_rows(kb, g.K);
@@ -321,12 +337,21 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
       const uint32_t tbase = tmem + ((uint32_t)(quarter * 32) << 16) + half * 16;
 #pragma unroll
       for (int t = 0; t < NTAP; ++t) {
+        if ((t & 7) == 0) {
+          if (!mbar_wait_warp(&sh.accf[t >> 3], bi & 1, abort_flag, err, ERR_WAIT_ACCUM, 64)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+        }
         float m[16];
         tmem_ld16(tbase + t * TILES, m);
         tmem_ld_wait();
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&sh.tapfree[t]);
+        if ((t & 7) == 7) {
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&sh.tapfree[t >> 3]);
+        }
         const int a = t >> 2, bc = t & 3;
         const float c00 = (float)(at_coef(0, a) * at_coef(0, bc));
         const float c01 = (float)(at_coef(0, a) * at_coef(1, bc));
@@ -340,6 +365,7 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
           y[j][3] += c11 * m[j];
         }
       }
+      if (!ok) break;
       // Stores go through a 2 KB per-warp staging buffer, 8 tiles at a time:
       // thread k writes its outputs as [k][row][8 tiles] half2 (16-byte
       // chunks XOR-swizzled by k so the writes are conflict-free), then each

@@ -10,10 +10,10 @@
 // One thread per (record row, entry e): it reads columns 2e and 2e+1 of the
 // row for all 16 channels (one 4-byte load per channel when W is even) and
 // writes par-0 entry e (column 2e) and par-1 entry e+1 (column 2e+1) of the
-// four channel quarters; the thread of the last entry also writes the
-// par-1 entry 0 (column -1, zero).  Consecutive threads read consecutive
-// words of each channel row and write consecutive 8-byte words of each
-// (par, quarter) run.  HBM-bound; items are counted in 32 bits (the host
+// two channel halves; the thread of the last entry also writes the par-1
+// entry 0 (column -1, zero).  Consecutive threads read consecutive words of
+// each channel row and write consecutive 16-byte words of each (par, half)
+// run.  HBM-bound; items are counted in 32 bits (the host
 // checks N*(C/16)*rows*entries < 2^31).
 #include <cuda_runtime.h>
 #include <cuda_fp16.h>
@@ -27,7 +27,7 @@ __global__ void __launch_bounds__(256) xb_layout_kernel(KernelParam p) {
   const int CB = C >> 4, HP = xb_rows(H), E = xb_entries(W);
   const uint32_t items = (uint32_t)p.n * CB * HP * E;
   const unsigned short* X = static_cast<const unsigned short*>(p.pin);
-  uint2* XB = static_cast<uint2*>(p.transform_pin);
+  uint4* XB = static_cast<uint4*>(p.transform_pin);
   const size_t plane = (size_t)H * W;
   const bool w_even = (W & 1) == 0;
   for (uint32_t it = blockIdx.x * blockDim.x + threadIdx.x; it < items; it += gridDim.x * blockDim.x) {
@@ -57,15 +57,18 @@ __global__ void __launch_bounds__(256) xb_layout_kernel(KernelParam p) {
         hi[i] = ok1 ? src[i * plane + 1] : 0u;
       }
     }
-    uint2* out = XB + (size_t)rec * (8 * E);
+    uint4* out = XB + (size_t)rec * (4 * E);
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      out[q * E + e] = make_uint2(lo[4 * q] | (lo[4 * q + 1] << 16), lo[4 * q + 2] | (lo[4 * q + 3] << 16));
+    for (int hh = 0; hh < 2; ++hh) {
+      const uint32_t* l = lo + 8 * hh;
+      const uint32_t* u = hi + 8 * hh;
+      out[hh * E + e] = make_uint4(l[0] | (l[1] << 16), l[2] | (l[3] << 16), l[4] | (l[5] << 16),
+                                   l[6] | (l[7] << 16));
       if (e + 1 < E)
-        out[(4 + q) * E + e + 1] =
-            make_uint2(hi[4 * q] | (hi[4 * q + 1] << 16), hi[4 * q + 2] | (hi[4 * q + 3] << 16));
+        out[(2 + hh) * E + e + 1] = make_uint4(u[0] | (u[1] << 16), u[2] | (u[3] << 16),
+                                               u[4] | (u[5] << 16), u[6] | (u[7] << 16));
       else
-        out[(4 + q) * E] = make_uint2(0u, 0u);
+        out[(2 + hh) * E] = make_uint4(0u, 0u, 0u, 0u);
     }
   }
 }

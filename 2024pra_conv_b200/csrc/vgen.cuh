@@ -315,17 +315,17 @@ __device__ __forceinline__ void produce_v_tile16(const __half* __restrict__ X, c
 //
 // A pre-pass (input_layout.cu) rewrites the NCHW input once per call as
 // records of one input row of one image and 16 channels:
-//   XB[n][c / 16][r][par][q][e][4]   (fp16)
-// r = y + 1 for y = -1 .. 2*TP (XB_rows(H) = 2*TP + 2 rows), par = column
-// parity, q = channel quarter (channels 4q .. 4q+3), e = entry: par 0 entry e
-// holds column x = 2e, par 1 entry e holds column x = 2e - 1, e = 0 .. TQ
-// (XB_entries(W) = TQ + 1).  Every position outside the image is zero.
+//   XB[n][c / 16][r][par][hh][e][8]   (fp16)
+// r = y + 1 for y = -1 .. 2*TP (xb_rows(H) = 2*TP + 2 rows), par = column
+// parity, hh = channel half (channels 8hh .. 8hh+7), e = entry: par 0 entry
+// e holds column x = 2e, par 1 entry e holds column x = 2e - 1, e = 0 .. TQ
+// (xb_entries(W) = TQ + 1).  Every position outside the image is zero.
 // Then the 4 x 4 window of every tile lies inside the record rows and
-// entries, so the producers read it without bounds checks, one 8-byte word
-// (two channel pairs) per window position, and the window columns of 32
-// consecutive tiles are consecutive words (conflict-free shared loads).
-// The rows of a step's block form one contiguous run per image, which one
-// bulk copy brings into a shared-memory slab.
+// entries, so the producers read it without bounds checks, one 16-byte word
+// (four channel pairs) per window position; the window columns of
+// consecutive tiles of one tile row are consecutive words.  The rows of a
+// step's block form one contiguous run per image, which one bulk copy
+// brings into a shared-memory slab.
 __host__ __device__ __forceinline__ int xb_rows(int H) { return 2 * ((H + 1) >> 1) + 2; }
 __host__ __device__ __forceinline__ int xb_entries(int W) { return ((W + 1) >> 1) + 1; }
 __host__ __device__ __forceinline__ int xb_row_bytes(int W) { return 64 * xb_entries(W); }
@@ -395,15 +395,15 @@ __device__ __forceinline__ TileCoord tile_coord(const Geometry& g, int tile, int
 }
 
 // Shared-memory offsets of one tile's window inside a slab, for channel
-// quarter q: row i of the window at row_off + i * RB; window column j at
-// +col_par1 (j = 0), +col_par0 (j = 1), +col_par1 + 8 (j = 2), +col_par0 + 8
-// (j = 3).
+// half hh: row i of the window at row_off + i * rb; window column j at
+// +col_par1 (j = 0), +col_par0 (j = 1), +col_par1 + 16 (j = 2),
+// +col_par0 + 16 (j = 3).
 struct SlabWindow {
   uint32_t row_off, rb, col_par0, col_par1;
 };
 
 __device__ __forceinline__ SlabWindow slab_window(const Geometry& g, const SlabPlan& pl,
-                                                  const TileCoord& tc, int q) {
+                                                  const TileCoord& tc, int hh) {
   SlabWindow sw;
   int k = tc.n - pl.n0;
   k = k < 0 ? 0 : (k >= SLAB_MAXSEG ? SLAB_MAXSEG - 1 : k);
@@ -414,49 +414,54 @@ __device__ __forceinline__ SlabWindow slab_window(const Geometry& g, const SlabP
   const int E = xb_entries(g.W);
   sw.rb = (uint32_t)xb_row_bytes(g.W);
   sw.row_off = (uint32_t)(rbase + 2 * (tc.ty - ta)) * sw.rb;
-  sw.col_par0 = (uint32_t)((q * E + tc.tx) * 8);
-  sw.col_par1 = (uint32_t)(((4 + q) * E + tc.tx) * 8);
+  sw.col_par0 = (uint32_t)((hh * E + tc.tx) * 16);
+  sw.col_par1 = (uint32_t)(((2 + hh) * E + tc.tx) * 16);
   return sw;
 }
 
-__device__ __forceinline__ void lds_v2(uint32_t addr, uint32_t& a, uint32_t& b) {
-  asm volatile("ld.shared.v2.b32 {%0, %1}, [%2];" : "=r"(a), "=r"(b) : "r"(addr));
+__device__ __forceinline__ void lds_v4(uint32_t addr, uint32_t (&w)[4]) {
+  asm volatile("ld.shared.v4.b32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3])
+               : "r"(addr));
 }
 
-// V of one tile for 4 channels (two pairs) and all 16 taps from an XB slab.
-// sink(t, w0, w1): tap t, channel pairs (c, c+1), (c+2, c+3).
-template <typename Sink>
-__device__ __forceinline__ void produce_v_quarter_xb(uint32_t slab, const SlabWindow& sw,
-                                                     Sink&& sink) {
-  uint32_t d0[4][4], d1[4][4];  // window (row, col) for channel pair 0 and 1
+// V of one tile for 8 channels (four pairs) and the 8 taps of tap rows
+// 2*ar, 2*ar+1 from an XB slab (tap rows 0-1 use window rows 0-2, tap rows
+// 2-3 window rows 1-3).  sink(u, w[4]): tap 8*ar + u, channel pairs 0..3.
+template <int AR, typename Sink>
+__device__ __forceinline__ void produce_v_half_xb(uint32_t slab, const SlabWindow& sw, Sink&& sink) {
+  constexpr int ar = AR;
+  uint32_t d[3][4][4];  // window row (ar + i), column j, channel pair
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const uint32_t row = slab + sw.row_off + (uint32_t)i * sw.rb;
-    lds_v2(row + sw.col_par1, d0[i][0], d1[i][0]);
-    lds_v2(row + sw.col_par0, d0[i][1], d1[i][1]);
-    lds_v2(row + sw.col_par1 + 8, d0[i][2], d1[i][2]);
-    lds_v2(row + sw.col_par0 + 8, d0[i][3], d1[i][3]);
+  for (int i = 0; i < 3; ++i) {
+    const uint32_t row = slab + sw.row_off + (uint32_t)(ar + i) * sw.rb;
+    lds_v4(row + sw.col_par1, d[i][0]);
+    lds_v4(row + sw.col_par0, d[i][1]);
+    lds_v4(row + sw.col_par1 + 16, d[i][2]);
+    lds_v4(row + sw.col_par0 + 16, d[i][3]);
   }
-  uint32_t out[16][2];
+  uint32_t out[8][4];
 #pragma unroll
-  for (int a = 0; a < 4; ++a) {
-    uint32_t e0[4], e1[4];
+  for (int p = 0; p < 4; ++p) {
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      e0[j] = bt_row(a, d0[0][j], d0[1][j], d0[2][j], d0[3][j]);
-      e1[j] = bt_row(a, d1[0][j], d1[1][j], d1[2][j], d1[3][j]);
-    }
-    uint32_t v0[4], v1[4];
-    bt_cols(e0[0], e0[1], e0[2], e0[3], v0);
-    bt_cols(e1[0], e1[1], e1[2], e1[3], v1);
+    for (int a2 = 0; a2 < 2; ++a2) {
+      uint32_t e[4];
 #pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      out[4 * a + b][0] = v0[b];
-      out[4 * a + b][1] = v1[b];
+      for (int j = 0; j < 4; ++j) {
+        // rows present: ar + 0..2; B^T row a = 2*ar + a2
+        if (AR == 0)
+          e[j] = a2 == 0 ? hsub2(d[0][j][p], d[2][j][p]) : hadd2(d[1][j][p], d[2][j][p]);
+        else
+          e[j] = a2 == 0 ? hsub2(d[1][j][p], d[0][j][p]) : hsub2(d[0][j][p], d[2][j][p]);
+      }
+      uint32_t v[4];
+      bt_cols(e[0], e[1], e[2], e[3], v);
+#pragma unroll
+      for (int b = 0; b < 4; ++b) out[4 * a2 + b][p] = v[b];
     }
   }
 #pragma unroll
-  for (int t = 0; t < 16; ++t) sink(t, out[t][0], out[t][1]);
+  for (int u = 0; u < 8; ++u) sink(u, out[u]);
 }
 
 // Same from global memory (fallback for problems whose slab does not fit).

@@ -51,17 +51,17 @@ def _fused(wino, x16, w16, dev, path="xb"):
 
 def _xb_layout_np(x16):
     """NumPy statement of the channel-blocked input records the pre-pass
-    writes: XB[n][c/16][r][par][q][e][4], r = y + 1 for y = -1 .. 2*TP,
+    writes: XB[n][c/16][r][par][hh][e][8], r = y + 1 for y = -1 .. 2*TP,
     par 0 entry e = column 2e, par 1 entry e = column 2e - 1, zero outside."""
     n, c, h, w = x16.shape
     tp, tq = (h + 1) // 2, (w + 1) // 2
     hp, e = 2 * tp + 2, tq + 1
     pad = np.zeros((n, c, hp, 2 * e + 1), np.float16)       # columns -1 .. 2e-1
     pad[:, :, 1:h + 1, 1:w + 1] = x16
-    out = np.zeros((n, c // 16, hp, 2, 4, e, 4), np.float16)
+    out = np.zeros((n, c // 16, hp, 2, 2, e, 8), np.float16)
     xs0 = 2 * np.arange(e) + 1          # column 2e   -> padded index 2e + 1
     xs1 = 2 * np.arange(e)              # column 2e-1 -> padded index 2e
-    v = pad.reshape(n, c // 16, 4, 4, hp, 2 * e + 1)        # n, cb, q, ci, r, col
+    v = pad.reshape(n, c // 16, 2, 8, hp, 2 * e + 1)        # n, cb, hh, ci, r, col
     out[:, :, :, 0] = v[..., xs0].transpose(0, 1, 4, 2, 5, 3)
     out[:, :, :, 1] = v[..., xs1].transpose(0, 1, 4, 2, 5, 3)
     return out
