@@ -80,6 +80,8 @@ def lib():
             "wino_conv2d_fused": ([vp, vp, vp, i, i, i, i, i, vp], i),
             "wino_fused_workspace_bytes": ([i, i, i, i], sz),
             "wino_input_layout": ([vp, vp, i, i, i, i, vp], i),
+            "wino_variant_workspace_bytes": ([i, i, i, i, i, i], sz),
+            "wino_conv2d_variant": ([i, vp, vp, vp, vp, i, i, i, i, i, vp], i),
             "wino_conv2d_fused_ws": ([vp, vp, vp, vp, i, i, i, i, i, vp], i),
             "wino_launch_kernelinfo": ([vp, vp, vp], i),
             "wino_filter_transform_unfused": ([vp, vp, i, i, vp], i),
@@ -220,6 +222,30 @@ def conv2d_fused(x, ucache, k, out=None, stream=None, workspace=True):
 def conv2d(x, w, stream=None):
     """Filter transform followed by the fused conv (fp16 variant)."""
     return conv2d_fused(x, filter_transform(w, stream), w.shape[0], stream=stream)
+
+
+def variant_workspace_bytes(variant, n, c, h, w, k) -> int:
+    return int(lib().wino_variant_workspace_bytes(variant, n, c, h, w, k))
+
+
+def conv2d_variant(x, w, variant, out=None, workspace=None, stream=None):
+    """Conv with a precision variant of the GEMM stage (VAR_F16, VAR_BF16,
+    VAR_F8, VAR_F16_HILO); filter transform, pre-pass and fused kernel per call."""
+    import torch
+    n, c, h, wd = x.shape
+    k = w.shape[0]
+    y = out if out is not None else torch.empty((n, k, h, wd), dtype=torch.float16, device=x.device)
+    nb = variant_workspace_bytes(variant, n, c, h, wd, k)
+    if nb == 0:
+        raise WinoError(WINO_EUNSUPPORTED, "variant_workspace_bytes")
+    if workspace is None:
+        workspace = torch.empty(nb + 256, dtype=torch.uint8, device=x.device)
+    off = (-workspace.data_ptr()) % 256
+    _check(lib().wino_conv2d_variant(variant, ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(w.data_ptr()),
+                                     ctypes.c_void_p(y.data_ptr()),
+                                     ctypes.c_void_p(workspace.data_ptr() + off), n, c, h, wd, k,
+                                     _stream(stream)), "conv2d_variant")
+    return y
 
 
 def filter_transform_unfused(w, stream=None):

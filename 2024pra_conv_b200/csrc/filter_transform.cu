@@ -87,9 +87,9 @@ __global__ void __launch_bounds__(256) dropin_filter_kernel(KernelParam p) {
 
 // ---- fp8 e4m3 -------------------------------------------------------------
 // Per-(tap, k) scale su[t][k] = amax_c |U'[t][k][c]| / 448 where
-// U'[t][k][c] = U[t][k][c] * sv[t][c] folds the per-(tap, c) input scale of
-// V into the filter (the scales then factor out of the C reduction:
-//   M[t][p][k] = su[t][k] * sum_c q(U'/su)[t][k][c] * q(V/sv)[t][p][c]).
+// U'[t][k][c] = U[t][k][c] * sv[c] folds the per-input-channel scale of V
+// into the filter (the scales then factor out of the C reduction:
+//   M[t][k][tile] = su[t][k] * sum_c q(U'/su)[t][k][c] * q(V/sv)[t][c][tile]).
 // One block per (t, k-group of 8); threads loop over c.
 __global__ void __launch_bounds__(256) filter_transform_f8_kernel(
     const __half* __restrict__ w, const float* __restrict__ sv, uint8_t* __restrict__ u8,
@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(256) filter_transform_f8_kernel(
     float g[9], t16[16];
     load_filter(w, k, c, C, g);
     filter_tile(g, t16);
-    amax = fmaxf(amax, fabsf(t16[t] * sv[t * C + c]));
+    amax = fmaxf(amax, fabsf(t16[t] * sv[c]));
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(256) filter_transform_f8_kernel(
     float g[9], t16[16];
     load_filter(w, k, c, C, g);
     filter_tile(g, t16);
-    const float x = t16[t] * sv[t * C + c] * inv;
+    const float x = t16[t] * sv[c] * inv;
     __nv_fp8_e4m3 q(x);
     u8[u8_offset(t, k, c, K, C)] = *reinterpret_cast<uint8_t*>(&q);
   }

@@ -20,11 +20,24 @@
 // each V element feeds 128 channels, which keeps the CUDA-core input
 // transform small next to the MMAs.
 //
-// Pipelines (shared memory, 225 KB): U in four 32 KB half-step slots (two
-// steps in flight); V in three 16 KB slots, one per step; two 16 KB input
-// slabs; 16 KB of epilogue store staging.  The MMA thread commits once per step (each tcgen05.commit stalls
+// Pipelines (shared memory, 225 KB): U in four 32 KB slots, each holding
+// 8 taps of a step (a step's two halves, two steps in flight); V in three
+// 16 KB slots, one per step; two 16 KB input slabs; 16 KB of epilogue store
+// staging.  The MMA thread commits once per step (each tcgen05.commit stalls
 // the MMA pipe for ~90 cycles on this part) to a "step done" barrier that
-// releases that step's U half-slots and V slot together.
+// releases that step's U slots and V slot together.
+//
+// Precision variants of the GEMM stage (template parameter VAR):
+//   VAR_F16       fp16 U and V (the drop-in path), 16 channels per step;
+//   VAR_BF16      bf16 U and V: V formed in fp16 then rounded to bf16;
+//   VAR_F8        fp8 e4m3 U and V, 32 channels per step (kind::f8f6f4,
+//                 K = 32): V is scaled per input channel (1 / sv[c]) before
+//                 rounding, sv folded into the cached U, and U carries a
+//                 per-(tap, output channel) scale su[t][k] that the
+//                 epilogue applies;
+//   VAR_F16_HILO  fp16 V against U = U_hi + U_lo (two fp16 caches): every
+//                 tap GEMM runs twice into the same accumulator, four U
+//                 pieces per step.
 //
 // Warp roles (15 warps):
 //   warp 0       TMEM allocation; one thread issues the MMAs
@@ -55,14 +68,21 @@ namespace wino {
 
 static __device__ uint32_t g_fused_err;
 
+// Extra operands of the precision variants (unused by VAR_F16).
+struct VariantArgs {
+  const void* u_lo;         // VAR_F16_HILO: residual U cache (fp16, same layout)
+  const float* su;          // VAR_F8: su[t * K + k]
+  const uint32_t* inv_sv2;  // VAR_F8: (1/sv[2i], 1/sv[2i+1]) as fp16x2, i < C/2
+};
+
 namespace fused {
 
 constexpr int TILES = 32;              // MMA N: tiles per block
 constexpr int NTAP = 16;
-constexpr int V_TAP_BYTES = TILES * 16 * 2;          // 1 KB per tap per step
+constexpr int V_TAP_BYTES = TILES * 32;              // 1 KB per tap per step (32 B per tile)
 constexpr int V_SLOT_BYTES = NTAP * V_TAP_BYTES;     // 16 KB: one step of V
-constexpr int U_HALF_BYTES = 8 * KB * 16 * 2;        // 32 KB: 8 taps of a step of U
-constexpr int NUH = 4;                 // U half-slots: two steps
+constexpr int U_HALF_BYTES = 8 * KB * 32;            // 32 KB: 8 taps x 128 k x 32 B
+constexpr int NUH = 4;                 // U slots
 constexpr int NVSLOT = 3, NSD = 3, NSLAB = 2;
 constexpr int EPI_WARP_BYTES = 2048;   // epilogue store staging per warp
 constexpr int U_BASE = 0, V_BASE = NUH * U_HALF_BYTES;
@@ -91,17 +111,45 @@ __host__ __device__ constexpr int at_coef(int i, int a) {
   return i == 0 ? (a == 3 ? 0 : 1) : (a == 0 ? 0 : (a == 1 ? 1 : -1));
 }
 
+// Per-variant constants: channels per step, U pieces (8 taps each) per
+// step, operand format code of the instruction descriptor.
+template <int VAR>
+struct Traits {
+  static constexpr int CH = VAR == VAR_F8 ? 32 : 16;
+  static constexpr int UP = VAR == VAR_F16_HILO ? 4 : 2;
+  static constexpr uint32_t FMT = VAR == VAR_BF16 ? 1u : 0u;  // bf16 / (f16 or e4m3)
+  static constexpr int NCB = CH / 16;                          // XB channel blocks per step
+};
+
+// fp16x2 -> bf16x2 (round to nearest even through fp32).
+__device__ __forceinline__ uint32_t h2_to_bf2(uint32_t w) {
+  const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&w));
+  const __nv_bfloat162 b = __floats2bfloat162_rn(f.x, f.y);
+  return *reinterpret_cast<const uint32_t*>(&b);
+}
+
+// (scale * fp16x2) -> two e4m3 bytes in the low 16 bits (saturating).
+__device__ __forceinline__ uint32_t h2_to_e4m3x2(uint32_t w, uint32_t scale2) {
+  uint32_t x = hmul2_u32(w, scale2);
+  uint16_t r;
+  asm("cvt.rn.satfinite.e4m3x2.f16x2 %0, %1;" : "=h"(r) : "r"(x));
+  return r;
+}
+
 }  // namespace fused
 
 using namespace fused;
 
-__global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam p) {
+template <int VAR>
+__device__ __forceinline__ void fused_body(const KernelParam& p, const VariantArgs& va) {
+  using T = Traits<VAR>;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   __shared__ Shared sh;
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const Geometry g = make_geometry(p, TILES);
   const int nKB = (g.K + KB - 1) / KB;
   const long long nblocks = (long long)g.nTB * nKB;
+  const int CS = g.C / T::CH;          // steps per block
   const int warp = warp_id();
   const int lane = lane_id();
   uint32_t* err = &g_fused_err;
@@ -135,14 +183,15 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
   auto v_slot = [&](uint32_t s) { return smem_base + V_BASE + s * V_SLOT_BYTES; };
   // Slot bookkeeping for step `it` (counted over this CTA's blocks):
   //   V slot it % NVSLOT, reused at it + NVSLOT (after sdone of step it);
-  //   U half-slots 2 * (it % 2) + h, reused at it + 2 (after sdone of it);
+  //   U piece pi = UP * it + j (j < UP) in slot pi % NUH, reused by piece
+  //     pi + NUH (after sdone of step it);
   //   slab it % NSLAB, reused at it + NSLAB (after the producers' slabfree).
   // A waiter on sdone[j] for step it cannot miss its phase: the barrier's
   // next phase needs operands the waiter has not supplied yet.
 
   if (warp == WARP_MMA) {
     if (lane == 0) {
-      const uint32_t idesc = instr_desc(128, TILES, 0, 0, /*a_mn=*/0, /*b_mn=*/0);
+      const uint32_t idesc = instr_desc(128, TILES, T::FMT, T::FMT, /*a_mn=*/0, /*b_mn=*/0);
       // Descriptors are formed once; the start-address field (bits 0-13,
       // address >> 4) then advances by plain adds (shared addresses < 256 KB,
       // so the field never carries into the next one).  Keeping the issue
@@ -156,21 +205,22 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
       for (long long b = blockIdx.x; b < nblocks && ok; b += gridDim.x, ++bi) {
         const int kb = (int)(b % nKB);
         const uint32_t astep = (uint32_t)(kblock_rows(kb, g.K) * 32) >> 4;
-        for (int s = 0; s < g.CS && ok; ++s, ++it) {
+        for (int s = 0; s < CS && ok; ++s, ++it) {
           const uint32_t vs = it % NVSLOT;
           ok = mbar_wait(&sh.vfull[vs], (it / NVSLOT) & 1, abort_flag, err, ERR_WAIT_FULL);
-          const uint32_t acc = s > 0 ? 1u : 0u;
           const bool first_step = s == 0 && bi > 0;
 #pragma unroll
-          for (int h = 0; h < 2; ++h) {
+          for (int j = 0; j < T::UP; ++j) {
             if (!ok) break;
-            const uint32_t us = 2 * (it & 1) + h;
-            ok = mbar_wait(&sh.ufull[us], (it >> 1) & 1, abort_flag, err, ERR_WAIT_FULL);
+            const int h = j & 1;               // tap half
+            const uint32_t pi = T::UP * it + j, us = pi % NUH;
+            ok = mbar_wait(&sh.ufull[us], (pi / NUH) & 1, abort_flag, err, ERR_WAIT_FULL);
             if (!ok) break;
             const uint64_t ad = adesc0 + ((us * U_HALF_BYTES) >> 4);
             const uint64_t bd = bdesc0 + ((vs * V_SLOT_BYTES + 8 * h * V_TAP_BYTES) >> 4);
             const uint32_t d = tmem + 8 * h * TILES;
-            if (first_step) {
+            const uint32_t acc = (s > 0 || j >= 2) ? 1u : 0u;
+            if (first_step && j < 2) {
               // the previous block's epilogue hands back each tap half of TMEM
               if (!mbar_wait(&sh.tapfree[h], (bi - 1) & 1, abort_flag, err, ERR_WAIT_DRAIN)) {
                 ok = false;
@@ -179,10 +229,14 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
               tc_fence_after();
             }
 #pragma unroll
-            for (int tt = 0; tt < 8; ++tt)
-              mma_f16(d + tt * TILES, ad + tt * astep, bd + tt * BSTEP, idesc, acc);
+            for (int tt = 0; tt < 8; ++tt) {
+              if constexpr (VAR == VAR_F8)
+                mma_f8(d + tt * TILES, ad + tt * astep, bd + tt * BSTEP, idesc, acc);
+              else
+                mma_f16(d + tt * TILES, ad + tt * astep, bd + tt * BSTEP, idesc, acc);
+            }
             // after the block's last MMAs of a tap half the epilogue may drain it
-            if (s == g.CS - 1) mma_commit(&sh.accf[h]);
+            if (s == CS - 1 && j >= T::UP - 2) mma_commit(&sh.accf[h]);
           }
           if (ok) mma_commit(&sh.sdone[it % NSD]);
         }
@@ -190,25 +244,33 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
     }
     __syncwarp();
   } else if (warp == WARP_U) {
-    if (lane < 2) {
-      const int h = lane;
-      const uint8_t* ucache = static_cast<const uint8_t*>(p.transform_filter);
+    if (lane < T::UP) {
+      // lane j copies piece j of every step (one copy in flight per thread)
+      const int j = lane;
+      const uint8_t* ubase = static_cast<const uint8_t*>(
+          (VAR == VAR_F16_HILO && j >= 2) ? va.u_lo : p.transform_filter);
       uint32_t it = 0;
       bool ok = true;
       for (long long b = blockIdx.x; b < nblocks && ok; b += gridDim.x) {
         const int kb = (int)(b % nKB);
         const int kbs = kblock_rows(kb, g.K);
-        const uint32_t bytes = 8 * kbs * 16 * 2;
-        for (int s = 0; s < g.CS; ++s, ++it) {
-          if (it >= 2 &&
-              !mbar_wait(&sh.sdone[(it - 2) % NSD], ((it - 2) / NSD) & 1, abort_flag, err, ERR_WAIT_EMPTY)) {
-            ok = false;
-            break;
+        const uint32_t bytes = 8 * kbs * 32;  // 8 taps x kbs rows x 32 B
+        for (int s = 0; s < CS; ++s, ++it) {
+          const uint32_t pi = T::UP * it + j, us = pi % NUH;
+          if (pi >= NUH) {
+            const uint32_t st = (pi - NUH) / T::UP;  // step that last used the slot
+            if (!mbar_wait(&sh.sdone[st % NSD], (st / NSD) & 1, abort_flag, err, ERR_WAIT_EMPTY)) {
+              ok = false;
+              break;
+            }
           }
-          const uint32_t us = 2 * (it & 1) + h;
+          // byte offset of the (k-block, step) piece: a k-block holds 16 x KB x C
+          // elements, a step 16 taps x kbs rows x 32 B
+          const size_t piece = (size_t)kb * KB * 16 * g.C * (VAR == VAR_F8 ? 1 : 2) +
+                               (size_t)s * 16 * kbs * 32;
           mbar_arrive_expect_tx(&sh.ufull[us], bytes);
-          bulk_g2s(smem + U_BASE + us * U_HALF_BYTES,
-                   ucache + u_piece(kb, s, g.K, g.C) * 2 + (size_t)h * bytes, bytes, &sh.ufull[us]);
+          bulk_g2s(smem + U_BASE + us * U_HALF_BYTES, ubase + piece + (size_t)(j & 1) * bytes, bytes,
+                   &sh.ufull[us]);
         }
       }
       if (*abort_flag) __nanosleep(20000);  // let copies already issued land
@@ -223,16 +285,20 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
     const size_t cb_stride = (size_t)xb_rows(g.H) * RB;                  // one channel block
     uint32_t it = 0;
     bool ok = true;
+    // lane = segment + 4 * channel block of the step
+    const int seg = lane & 3, cbi = lane >> 2;
     for (int bi = 0; bi < my_blocks && ok; ++bi) {
       const int tile0 = (int)((blockIdx.x + (long long)bi * gridDim.x) / nKB) * TILES;
       const SlabPlan pl = slab_plan(g, tile0, TILES);
-      const bool use = XB != nullptr && slab_fits(g, pl);
+      const bool use = XB != nullptr && slab_fits(g, pl, T::NCB);
       int ta = 0, rows = 0, rbase = 0;  // this lane's segment
 #pragma unroll
       for (int k = 0; k < SLAB_MAXSEG; ++k)
-        if (lane == k) { ta = pl.ta[k]; rows = pl.rows[k]; rbase = pl.row_base[k]; }
-      const uint8_t* src0 = XB + (size_t)(pl.n0 + lane) * img_stride + (size_t)(2 * ta) * RB;
-      for (int s = 0; s < g.CS; ++s, ++it) {
+        if (seg == k) { ta = pl.ta[k]; rows = pl.rows[k]; rbase = pl.row_base[k]; }
+      const uint8_t* src0 = XB + (size_t)(pl.n0 + seg) * img_stride + (size_t)cbi * cb_stride +
+                            (size_t)(2 * ta) * RB;
+      const uint32_t dst0 = (uint32_t)(cbi * pl.total_rows + rbase) * RB;
+      for (int s = 0; s < CS; ++s, ++it) {
         const uint32_t j = it % NSLAB;
         if (it >= NSLAB &&
             !mbar_wait_warp(&sh.slabfree[j], ((it - NSLAB) / NSLAB) & 1, abort_flag, err, ERR_WAIT_EMPTY, 64)) {
@@ -240,10 +306,10 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
           break;
         }
         if (use) {
-          if (lane == 0) mbar_arrive_expect_tx(&sh.slabfull[j], (uint32_t)pl.total_rows * RB);
+          if (lane == 0) mbar_arrive_expect_tx(&sh.slabfull[j], (uint32_t)(T::NCB * pl.total_rows) * RB);
           __syncwarp();
-          if (lane < pl.nseg)
-            bulk_g2s(smem + SLAB_BASE + j * SLAB_BYTES + (uint32_t)rbase * RB, src0 + (size_t)s * cb_stride,
+          if (seg < pl.nseg && cbi < T::NCB)
+            bulk_g2s(smem + SLAB_BASE + j * SLAB_BYTES + dst0, src0 + (size_t)s * T::NCB * cb_stride,
                      (uint32_t)rows * RB, &sh.slabfull[j]);
         } else if (lane == 0) {
           mbar_arrive(&sh.slabfull[j]);
@@ -254,27 +320,30 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
     __syncwarp();
   } else if (warp >= WARP_V0 && warp < WARP_V0 + NWARP_V) {
     const int q = warp - WARP_V0;
-    const int hh = q & 1;                     // channel half: channels 8hh .. 8hh+7
+    const int hh = q & 1;                     // K half of the step's operand row
     const int ar = q >> 1;                    // tap rows 2ar, 2ar+1 (taps 8ar .. 8ar+7)
     const __half* X = static_cast<const __half*>(p.pin);
     const bool have_xb = p.transform_pin != nullptr;
     const int my_blocks =
         blockIdx.x < nblocks ? (int)((nblocks - blockIdx.x + gridDim.x - 1) / gridDim.x) : 0;
-    const int CS = g.CS;
     const uint32_t slab0 = smem_base + SLAB_BASE;
     bool ok = true;
-    // K-major core matrices: tile group (lane/8) at 256 B, channel half at
-    // 128 B, tile row (lane%8) at 16 B: each lane writes whole 16-byte rows,
-    // eight lanes 128 contiguous bytes (conflict-free).
+    // K-major core matrices: tile group (lane/8) at 256 B, K half at 128 B,
+    // tile row (lane%8) at 16 B: each lane writes whole 16-byte rows, eight
+    // lanes 128 contiguous bytes (conflict-free).
     const uint32_t row_off = (lane >> 3) * 256 + hh * 128 + (lane & 7) * 16 + ar * 8 * V_TAP_BYTES;
     uint32_t it = 0;
     for (int bi = 0; bi < my_blocks && ok; ++bi) {
       // per-block quantities once per block, 32-bit
       const int tile0 = (int)((blockIdx.x + (long long)bi * gridDim.x) / nKB) * TILES;
       const SlabPlan pl = slab_plan(g, tile0, TILES);
-      const bool use_slab = have_xb && slab_fits(g, pl);
+      const bool use_slab = have_xb && slab_fits(g, pl, T::NCB);
       const TileCoord tc = tile_coord(g, tile0 + lane, tile0);
-      const SlabWindow sw = slab_window(g, pl, tc, hh);
+      // fp8: this warp's K half is a whole XB channel block (two 8-channel
+      // halves), the second block of the step's slab for hh = 1
+      const uint32_t cb_off = VAR == VAR_F8 ? (uint32_t)(hh * pl.total_rows) * (uint32_t)xb_row_bytes(g.W) : 0u;
+      const SlabWindow sw0 = slab_window(g, pl, tc, VAR == VAR_F8 ? 0 : hh);
+      const SlabWindow sw1 = slab_window(g, pl, tc, 1);
       for (int s = 0; s < CS && ok; ++s, ++it) {
         const uint32_t j = it % NSLAB;
         const uint32_t vs = it % NVSLOT;
@@ -289,25 +358,71 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
           break;
         }
         const uint32_t dst = v_slot(vs) + row_off;
-        if (use_slab) {
-          auto sink = [&](int u, const uint32_t (&w)[4]) {
-            st_shared_v4(dst + u * V_TAP_BYTES, w[0], w[1], w[2], w[3]);
-          };
-          if (ar == 0)
-            produce_v_half_xb<0>(slab0 + j * SLAB_BYTES, sw, sink);
-          else
-            produce_v_half_xb<1>(slab0 + j * SLAB_BYTES, sw, sink);
-        } else {
-          // direct NCHW reads: two channel quarters, keeping this warp's taps
-#pragma unroll 1
-          for (int qq = 0; qq < 2; ++qq) {
-            auto sink = [&](int t, uint32_t w0, uint32_t w1) {
-              if ((t >> 3) == ar)
-                asm volatile("st.shared.v2.b32 [%0], {%1, %2};" ::"r"(dst + (t & 7) * V_TAP_BYTES + qq * 8),
-                             "r"(w0), "r"(w1)
-                             : "memory");
+        const uint32_t slab = slab0 + j * SLAB_BYTES + cb_off;
+        if constexpr (VAR == VAR_F8) {
+          // 16 channels c0 .. c0+15, two 8-channel halves, 8 bytes each
+          const int c0 = s * 32 + 16 * hh;
+#pragma unroll
+          for (int half = 0; half < 2; ++half) {
+            uint32_t sc[4];
+#pragma unroll
+            for (int pp = 0; pp < 4; ++pp) sc[pp] = va.inv_sv2[(c0 + 8 * half) / 2 + pp];
+            auto sink = [&](int u, const uint32_t (&w)[4]) {
+              const uint32_t lo = h2_to_e4m3x2(w[0], sc[0]) | (h2_to_e4m3x2(w[1], sc[1]) << 16);
+              const uint32_t hi = h2_to_e4m3x2(w[2], sc[2]) | (h2_to_e4m3x2(w[3], sc[3]) << 16);
+              asm volatile("st.shared.v2.b32 [%0], {%1, %2};" ::"r"(dst + u * V_TAP_BYTES + half * 8),
+                           "r"(lo), "r"(hi)
+                           : "memory");
             };
-            produce_v_quarter_global(X, g, tc, s * 16 + 8 * hh + 4 * qq, sink);
+            if (use_slab) {
+              const SlabWindow& sw = half ? sw1 : sw0;
+              if (ar == 0) produce_v_half_xb<0>(slab, sw, sink);
+              else produce_v_half_xb<1>(slab, sw, sink);
+            } else {
+#pragma unroll 1
+              for (int qq = 0; qq < 2; ++qq) {
+                auto qsink = [&](int t, uint32_t w0, uint32_t w1) {
+                  if ((t >> 3) == ar) {
+                    const uint32_t v = h2_to_e4m3x2(w0, sc[2 * qq]) | (h2_to_e4m3x2(w1, sc[2 * qq + 1]) << 16);
+                    asm volatile("st.shared.b32 [%0], %1;" ::"r"(dst + (t & 7) * V_TAP_BYTES + half * 8 + qq * 4),
+                                 "r"(v)
+                                 : "memory");
+                  }
+                };
+                produce_v_quarter_global(X, g, tc, c0 + 8 * half + 4 * qq, qsink);
+              }
+            }
+          }
+        } else {
+          if (use_slab) {
+            auto sink = [&](int u, const uint32_t (&w)[4]) {
+              if constexpr (VAR == VAR_BF16)
+                st_shared_v4(dst + u * V_TAP_BYTES, h2_to_bf2(w[0]), h2_to_bf2(w[1]), h2_to_bf2(w[2]),
+                             h2_to_bf2(w[3]));
+              else
+                st_shared_v4(dst + u * V_TAP_BYTES, w[0], w[1], w[2], w[3]);
+            };
+            if (ar == 0)
+              produce_v_half_xb<0>(slab, sw0, sink);
+            else
+              produce_v_half_xb<1>(slab, sw0, sink);
+          } else {
+            // direct NCHW reads: two channel quarters, keeping this warp's taps
+#pragma unroll 1
+            for (int qq = 0; qq < 2; ++qq) {
+              auto sink = [&](int t, uint32_t w0, uint32_t w1) {
+                if ((t >> 3) == ar) {
+                  if constexpr (VAR == VAR_BF16) {
+                    w0 = h2_to_bf2(w0);
+                    w1 = h2_to_bf2(w1);
+                  }
+                  asm volatile("st.shared.v2.b32 [%0], {%1, %2};" ::"r"(dst + (t & 7) * V_TAP_BYTES + qq * 8),
+                               "r"(w0), "r"(w1)
+                               : "memory");
+                }
+              };
+              produce_v_quarter_global(X, g, tc, s * 16 + 8 * hh + 4 * qq, sink);
+            }
           }
         }
         fence_proxy_async_shared();
@@ -335,6 +450,13 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
 #pragma unroll
         for (int o = 0; o < 4; ++o) y[j][o] = 0.f;
       const uint32_t tbase = tmem + ((uint32_t)(quarter * 32) << 16) + half * 16;
+      // fp8: per-(tap, output channel) scale of U
+      float su[NTAP];
+      if constexpr (VAR == VAR_F8) {
+        const int kc = min(kb * KB + quarter * 32 + lane, g.K - 1);
+#pragma unroll
+        for (int t = 0; t < NTAP; ++t) su[t] = va.su[t * g.K + kc];
+      }
 #pragma unroll
       for (int t = 0; t < NTAP; ++t) {
         if ((t & 7) == 0) {
@@ -351,6 +473,10 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
           tc_fence_before();
           __syncwarp();
           if (lane == 0) mbar_arrive(&sh.tapfree[t >> 3]);
+        }
+        if constexpr (VAR == VAR_F8) {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) m[j] *= su[t];
         }
         const int a = t >> 2, bc = t & 3;
         const float c00 = (float)(at_coef(0, a) * at_coef(0, bc));
@@ -430,6 +556,20 @@ __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam 
   }
 }
 
+// The drop-in kernel: its only argument is the plugin's parameter struct.
+__global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam p) {
+  fused_body<VAR_F16>(p, VariantArgs{nullptr, nullptr, nullptr});
+}
+
+template <int VAR>
+__global__ void __launch_bounds__(NTHREAD, 1) fused_wino_var_kernel(KernelParam p, VariantArgs va) {
+  fused_body<VAR>(p, va);
+}
+
+template __global__ void fused_wino_var_kernel<VAR_BF16>(KernelParam, VariantArgs);
+template __global__ void fused_wino_var_kernel<VAR_F8>(KernelParam, VariantArgs);
+template __global__ void fused_wino_var_kernel<VAR_F16_HILO>(KernelParam, VariantArgs);
+
 }  // namespace wino
 
 using namespace wino;
@@ -443,6 +583,32 @@ int wino_fused_threads() { return fused::NTHREAD; }
 int wino_fused_prepare() {
   cudaError_t e = cudaFuncSetAttribute(fused_wino_f16_kernel,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, fused::SMEM_BYTES);
+  return (int)e;
+}
+
+static void* var_kernel(int variant) {
+  switch (variant) {
+    case VAR_F16: return (void*)fused_wino_f16_kernel;
+    case VAR_BF16: return (void*)fused_wino_var_kernel<VAR_BF16>;
+    case VAR_F8: return (void*)fused_wino_var_kernel<VAR_F8>;
+    case VAR_F16_HILO: return (void*)fused_wino_var_kernel<VAR_F16_HILO>;
+    default: return nullptr;
+  }
+}
+
+// Launch the fused kernel of a precision variant on `grid` CTAs.
+int wino_fused_launch_variant(int variant, const KernelParam* p, const VariantArgs* va, unsigned grid,
+                              cudaStream_t stream) {
+  void* fn = var_kernel(variant);
+  if (!fn) return (int)cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, fused::SMEM_BYTES);
+  if (e != cudaSuccess) return (int)e;
+  KernelParam pc = *p;
+  VariantArgs vc = va ? *va : VariantArgs{nullptr, nullptr, nullptr};
+  void* args2[] = {&pc, &vc};
+  void* args1[] = {&pc};
+  e = cudaLaunchKernel(fn, dim3(grid), dim3(fused::NTHREAD), variant == VAR_F16 ? args1 : args2,
+                       (size_t)fused::SMEM_BYTES, stream);
   return (int)e;
 }
 

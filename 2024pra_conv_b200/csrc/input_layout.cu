@@ -1,5 +1,6 @@
 // Input re-layout pre-pass for the fused kernel: NCHW fp16 -> XB records
-// (layout described in vgen.cuh), zero outside the image.
+// (layout described in vgen.cuh), zero outside the image.  For the fp8
+// variant it also records the per-channel max |x| (p.mid_result non-null).
 //
 // The reference's pipeline also writes an intermediate form of the input into
 // the caller's `transform_pin` workspace before its GEMMs (the transformed
@@ -30,6 +31,8 @@ __global__ void __launch_bounds__(256) xb_layout_kernel(KernelParam p) {
   uint4* XB = static_cast<uint4*>(p.transform_pin);
   const size_t plane = (size_t)H * W;
   const bool w_even = (W & 1) == 0;
+  // optional (fp8 variant): per-channel max |x| as fp16 magnitude bits
+  unsigned* amax = static_cast<unsigned*>(p.mid_result);
   for (uint32_t it = blockIdx.x * blockDim.x + threadIdx.x; it < items; it += gridDim.x * blockDim.x) {
     const uint32_t rec = it / E;
     const int e = (int)(it - rec * E);
@@ -57,6 +60,23 @@ __global__ void __launch_bounds__(256) xb_layout_kernel(KernelParam p) {
         hi[i] = ok1 ? src[i * plane + 1] : 0u;
       }
     }
+    if (amax != nullptr) {
+      // per-channel max |x| (fp16 magnitude bits order like the values):
+      // reduced over the warp when all its lanes hold the same channel block
+      const unsigned act = __activemask();
+      const int cb0 = __shfl_sync(act, cb, __ffs(act) - 1);
+      const bool uni = __all_sync(act, cb == cb0);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        uint32_t m = max(lo[i] & 0x7fffu, hi[i] & 0x7fffu);
+        if (uni) {
+          m = __reduce_max_sync(act, m);
+          if ((int)threadIdx.x % 32 == __ffs(act) - 1 && m) atomicMax(amax + 16 * cb + i, m);
+        } else if (m) {
+          atomicMax(amax + 16 * cb + i, m);
+        }
+      }
+    }
     uint4* out = XB + (size_t)rec * (4 * E);
 #pragma unroll
     for (int hh = 0; hh < 2; ++hh) {
@@ -71,6 +91,30 @@ __global__ void __launch_bounds__(256) xb_layout_kernel(KernelParam p) {
         out[(2 + hh) * E] = make_uint4(0u, 0u, 0u, 0u);
     }
   }
+}
+
+// fp8 scales from the per-channel input maxima: |V| <= 4 max|x_c| (each
+// V element is a signed sum of four inputs), so V / sv[c] with
+// sv[c] = 4 max|x_c| / 448 stays inside e4m3's range.  The producers multiply
+// by inv = fp16(1 / sv[c]) (clamped to fp16's range), so sv[c] is recorded as
+// exactly 1 / inv for folding into U.  One thread per channel pair.
+__global__ void xb_f8_scales_kernel(const unsigned* __restrict__ amax, float* __restrict__ sv,
+                                    uint32_t* __restrict__ inv_sv2, int C) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (2 * i >= C) return;
+  uint32_t packed = 0;
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const int c = 2 * i + k;
+    const unsigned short bits = (unsigned short)amax[c];
+    const float a = __half2float(*reinterpret_cast<const __half*>(&bits));
+    float inv = a > 0.f ? 448.f / (4.f * a) : 1.f;
+    inv = fminf(inv, 65504.f);
+    const __half hinv = __float2half_rn(inv);
+    sv[c] = 1.f / __half2float(hinv);
+    packed |= (uint32_t)(*reinterpret_cast<const unsigned short*>(&hinv)) << (16 * k);
+  }
+  inv_sv2[i] = packed;
 }
 
 }  // namespace wino
@@ -94,6 +138,12 @@ unsigned wino_xb_layout_grid(int n, int c, int h, int w) {
   const long long blocks = (wino_xb_items(n, c, h, w) + 255) / 256;
   const long long cap = 148LL * 64;
   return (unsigned)(blocks < cap ? (blocks > 0 ? blocks : 1) : cap);
+}
+
+int wino_launch_xb_f8_scales(const unsigned* amax, float* sv, uint32_t* inv_sv2, int C,
+                             cudaStream_t stream) {
+  xb_f8_scales_kernel<<<(C / 2 + 127) / 128, 128, 0, stream>>>(amax, sv, inv_sv2, C);
+  return (int)cudaGetLastError();
 }
 
 int wino_launch_xb_layout(const KernelParam* p, cudaStream_t stream) {

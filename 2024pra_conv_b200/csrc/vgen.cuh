@@ -67,6 +67,10 @@ __device__ __forceinline__ uint32_t hadd2(uint32_t a, uint32_t b) {
   __half2 r = __hadd2(*reinterpret_cast<__half2*>(&a), *reinterpret_cast<__half2*>(&b));
   return *reinterpret_cast<uint32_t*>(&r);
 }
+__device__ __forceinline__ uint32_t hmul2_u32(uint32_t a, uint32_t b) {
+  __half2 r = __hmul2(*reinterpret_cast<__half2*>(&a), *reinterpret_cast<__half2*>(&b));
+  return *reinterpret_cast<uint32_t*>(&r);
+}
 __device__ __forceinline__ uint32_t hsub2(uint32_t a, uint32_t b) {
   __half2 r = __hsub2(*reinterpret_cast<__half2*>(&a), *reinterpret_cast<__half2*>(&b));
   return *reinterpret_cast<uint32_t*>(&r);
@@ -367,8 +371,9 @@ __device__ __forceinline__ SlabPlan slab_plan(const Geometry& g, int tile0, int 
   return pl;
 }
 
-__device__ __forceinline__ bool slab_fits(const Geometry& g, const SlabPlan& pl) {
-  return pl.nseg <= SLAB_MAXSEG && pl.total_rows * xb_row_bytes(g.W) <= SLAB_BYTES;
+// ncb: XB channel blocks a step stages (16 channels each).
+__device__ __forceinline__ bool slab_fits(const Geometry& g, const SlabPlan& pl, int ncb = 1) {
+  return pl.nseg <= SLAB_MAXSEG && ncb * pl.total_rows * xb_row_bytes(g.W) <= SLAB_BYTES;
 }
 
 // Window origin of one tile; tiles past the end of the batch take the

@@ -60,6 +60,21 @@ size_t wino_xb_bytes(int n, int c, int h, int w);
 unsigned wino_xb_layout_grid(int n, int c, int h, int w);
 long long wino_xb_items(int n, int c, int h, int w);
 int wino_launch_xb_layout(const wino::KernelParam* p, cudaStream_t stream);
+int wino_launch_xb_f8_scales(const unsigned* amax, float* sv, uint32_t* inv_sv2, int C,
+                             cudaStream_t stream);
+int wino_launch_filter_transform_f8(const void* weight, const float* sv, void* u8, float* su, int K,
+                                    int C, cudaStream_t stream);
+}
+namespace wino {
+struct VariantArgs {
+  const void* u_lo;
+  const float* su;
+  const uint32_t* inv_sv2;
+};
+}
+extern "C" {
+int wino_fused_launch_variant(int variant, const wino::KernelParam* p, const wino::VariantArgs* va,
+                              unsigned grid, cudaStream_t stream);
 size_t wino_unfused_v_bytes(int n, int c, int h, int w);
 size_t wino_unfused_m_bytes(int n, int k, int h, int w);
 int wino_unfused_prepare();
@@ -294,6 +309,93 @@ extern "C" int wino_conv2d_fused_ws(const void* x, const void* ucache, void* wor
                                          dim3(wino_fused_threads()), args,
                                          (size_t)wino_fused_smem_bytes(), (cudaStream_t)stream);
   return e == cudaSuccess ? WINO_OK : WINO_ECUDA;
+}
+
+// ------------------------------------------------ precision variants ----
+namespace {
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// Workspace of wino_conv2d_variant: XB | U (| U_lo) (| su | amax | sv | inv_sv2).
+struct VarLayout {
+  size_t xb, u, ulo, su, amax, sv, inv, total;
+};
+
+VarLayout var_layout(int variant, int n, int c, int h, int w, int k) {
+  VarLayout L{};
+  size_t off = 0;
+  L.xb = off; off += align256(wino_xb_bytes(n, c, h, w));
+  L.u = off; off += align256(wino_ucache_bytes(k, c, variant == WINO_VAR_F8 ? WINO_VAR_F8 : WINO_VAR_F16));
+  if (variant == WINO_VAR_F16_HILO) { L.ulo = off; off += align256((size_t)16 * k * c * 2); }
+  if (variant == WINO_VAR_F8) {
+    L.su = off; off += align256((size_t)16 * k * sizeof(float));
+    L.amax = off; off += align256((size_t)c * sizeof(unsigned));
+    L.sv = off; off += align256((size_t)c * sizeof(float));
+    L.inv = off; off += align256((size_t)(c / 2) * sizeof(uint32_t));
+  }
+  L.total = off;
+  return L;
+}
+
+int check_variant(int variant, int n, int c, int h, int w, int k) {
+  if (variant < WINO_VAR_F16 || variant > WINO_VAR_F16_HILO) return WINO_EINVAL;
+  const int st = wino_check_shape(n, c, h, w, k);
+  if (st != WINO_OK) return st;
+  if (variant == WINO_VAR_F8 && c % 32 != 0) return WINO_EUNSUPPORTED;
+  if (!xb_items_ok(n, c, h, w)) return WINO_EUNSUPPORTED;
+  return WINO_OK;
+}
+
+}  // namespace
+
+extern "C" size_t wino_variant_workspace_bytes(int variant, int n, int c, int h, int w, int k) {
+  if (check_variant(variant, n, c, h, w, k) != WINO_OK) return 0;
+  return var_layout(variant, n, c, h, w, k).total;
+}
+
+extern "C" int wino_conv2d_variant(int variant, const void* x, const void* weight, void* y,
+                                   void* workspace, int n, int c, int h, int w, int k, void* stream) {
+  if (!x || !weight || !y || !workspace) return WINO_EINVAL;
+  if ((reinterpret_cast<uintptr_t>(workspace) & 255) != 0) return WINO_EINVAL;
+  const int st = check_variant(variant, n, c, h, w, k);
+  if (st != WINO_OK) return st;
+  const cudaStream_t s = (cudaStream_t)stream;
+  const VarLayout L = var_layout(variant, n, c, h, w, k);
+  uint8_t* ws = static_cast<uint8_t*>(workspace);
+  wino::KernelParam p = make_param(x, nullptr, y, ws + L.xb, ws + L.u, nullptr, n, c, h, w, k);
+  wino::VariantArgs va{nullptr, nullptr, nullptr};
+  int rc = 0;
+  switch (variant) {
+    case WINO_VAR_F16:
+      rc = wino_launch_filter_transform(weight, ws + L.u, nullptr, k, c, 0, 0, s);
+      break;
+    case WINO_VAR_BF16:
+      rc = wino_launch_filter_transform(weight, ws + L.u, nullptr, k, c, 1, 0, s);
+      break;
+    case WINO_VAR_F16_HILO:
+      rc = wino_launch_filter_transform(weight, ws + L.u, ws + L.ulo, k, c, 0, 0, s);
+      va.u_lo = ws + L.ulo;
+      break;
+    default: {  // WINO_VAR_F8: input maxima first (pre-pass), then scales, then U8
+      unsigned* amax = reinterpret_cast<unsigned*>(ws + L.amax);
+      if (cudaMemsetAsync(amax, 0, (size_t)c * sizeof(unsigned), s) != cudaSuccess) return WINO_ECUDA;
+      wino::KernelParam pl = p;
+      pl.mid_result = amax;
+      if (wino_launch_xb_layout(&pl, s) != 0) return WINO_ECUDA;
+      float* sv = reinterpret_cast<float*>(ws + L.sv);
+      uint32_t* inv = reinterpret_cast<uint32_t*>(ws + L.inv);
+      float* su = reinterpret_cast<float*>(ws + L.su);
+      if (wino_launch_xb_f8_scales(amax, sv, inv, c, s) != 0) return WINO_ECUDA;
+      rc = wino_launch_filter_transform_f8(weight, sv, ws + L.u, su, k, c, s);
+      va.su = su;
+      va.inv_sv2 = inv;
+      break;
+    }
+  }
+  if (rc != 0) return WINO_ECUDA;
+  if (variant != WINO_VAR_F8 && wino_launch_xb_layout(&p, s) != 0) return WINO_ECUDA;
+  return wino_fused_launch_variant(variant, &p, &va, fused_grid(n, h, w, k), s) == 0 ? WINO_OK
+                                                                                      : WINO_ECUDA;
 }
 
 // Launch the four slots of a filled kernelInfo_t in order on one stream, each

@@ -84,6 +84,18 @@ int wino_unfused_workspace_bytes(int n, int c, int h, int w, int k, size_t* v_by
 int wino_conv2d_unfused(const void* x, const void* ucache2, void* y, void* v_ws, void* m_ws, int n,
                         int c, int h, int w, int k, void* stream);
 
+/* Conv with a precision variant of the GEMM stage (WINO_VAR_*), everything
+ * per call: the variant's filter transform (bf16 U; U_hi + U_lo; or fp8 U
+ * with the input's per-channel scales folded in and per-(tap, k) scales),
+ * the input pre-pass (for fp8 also the per-channel max |x|), then the fused
+ * kernel of the variant.  workspace: wino_variant_workspace_bytes() bytes,
+ * 256-byte aligned.  fp8 needs c % 32 == 0.  x: NCHW fp16, weight: KCRS
+ * fp16, y: N K H W fp16.  (The reference computes in fp16 only,
+ * src/matrixmul.cuh:28-35; these variants have no counterpart there.) */
+size_t wino_variant_workspace_bytes(int variant, int n, int c, int h, int w, int k);
+int wino_conv2d_variant(int variant, const void* x, const void* weight, void* y, void* workspace,
+                        int n, int c, int h, int w, int k, void* stream);
+
 /* Launch the four slots of a kernelInfo_t filled by getkernelInfo, in order,
  * on `stream`, each with args[0] = param: the launch sequence of the
  * reference harness (reference src/main.cpp:105-108).  `ki` is `const

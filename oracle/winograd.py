@@ -90,18 +90,65 @@ def _bf16(a):
     return b.astype(np.uint32).view(np.float32).astype(np.float64)
 
 
+def input_transform_f16(x):
+    """B^T d B as the fused kernel's producers compute it: packed fp16
+    arithmetic, each two-term +- sum rounded to fp16 once (rows of B^T d,
+    then the columns of that times B)."""
+    d = input_windows(x)
+    n, c, tp, tq = d.shape[:4]
+    e = _f16(np.einsum("ai,nctqij->nctqaj", BT, d))
+    v = _f16(np.einsum("nctqaj,bj->abntqc", e, BT))
+    return v.reshape(16, n * tp * tq, c)
+
+
+def _e4m3(a):
+    """Round to fp8 e4m3 (3 mantissa bits, min normal 2^-6, subnormal step
+    2^-9), nearest-even, saturating at 448 (the .satfinite conversion)."""
+    a = np.asarray(a, np.float64)
+    mag = np.abs(a)
+    e = np.floor(np.log2(np.maximum(mag, 2.0 ** -6)))
+    step = np.where(mag < 2.0 ** -6, 2.0 ** -9, 2.0 ** (e - 3))
+    r = np.round(mag / step) * step
+    return np.sign(a) * np.minimum(r, 448.0)
+
+
+def conv2d_winograd_f8_emulated(x, w):
+    """The fp8 e4m3 variant's quantization, step by step (a model of the
+    fused kernel's fp8 path, not of the reference, which has no fp8 path):
+    per input channel c, inv_c = fp16(min(448 / (4 max|x_c|), 65504)) and
+    sv_c = 1 / inv_c (|V| <= 4 max|x_c|); V8 = e4m3(fp16(V) * inv_c);
+    U'[t][k][c] = U * sv_c, su[t][k] = max_c |U'| / 448, U8 = e4m3(U' / su);
+    M = su * sum_c U8 V8 (wide accumulation); output transform in wide
+    precision."""
+    n, c, h, wd = x.shape
+    k = w.shape[0]
+    amax = np.abs(np.asarray(x, np.float64)).max(axis=(0, 2, 3))
+    inv = np.where(amax > 0, 448.0 / (4.0 * np.where(amax > 0, amax, 1.0)), 1.0)
+    inv = _f16(np.minimum(inv, 65504.0))
+    sv = 1.0 / inv
+    v8 = _e4m3(_f16(input_transform_f16(x) * inv[None, None, :]))
+    u1 = filter_transform(w) * sv[None, None, :]
+    su = np.abs(u1).max(axis=2) / 448.0
+    su = np.where(su > 0, su, 1.0)
+    u8 = _e4m3(u1 / su[:, :, None])
+    m = gemm(u8, v8) * su[:, None, :]
+    return output_transform(m, n, k, h, wd)
+
+
 def conv2d_winograd_emulated(x, w, operand="f16"):
     """Winograd with the rounding points of the fused fp16/bf16 kernels.
 
-    U and V are formed exactly (fp32 is exact for these +-1/2 combinations of
-    fp16 values up to one rounding) and rounded once to the GEMM operand type;
-    M is accumulated in wide precision (the tensor core accumulates in fp32);
-    the output transform is done before the single fp16 rounding of Y.
+    U is formed exactly (fp32 is exact for these +-1/2 combinations of fp16
+    values up to one rounding) and rounded once to the operand type; V is
+    formed in packed fp16 arithmetic (input_transform_f16) and, for bf16,
+    rounded once more; M is accumulated in wide precision (the tensor core
+    accumulates in fp32); the output transform is done before the single fp16
+    rounding of Y.
     """
     rnd = _f16 if operand == "f16" else _bf16
     n, c, h, wd = x.shape
     k = w.shape[0]
     u = rnd(filter_transform(w))
-    v = rnd(input_transform(x))
+    v = rnd(input_transform_f16(x))
     m = gemm(u, v).astype(np.float32).astype(np.float64)
     return output_transform(m, n, k, h, wd)

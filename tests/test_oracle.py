@@ -59,3 +59,13 @@ def test_reference_cpu_multithreaded_matches_single(oracle_mod):
     a = oracle_mod.ref_conv2dcpu(x, w, threads=1)
     b = oracle_mod.ref_conv2dcpu(x, w, threads=4)
     assert np.array_equal(a, b)
+
+
+def test_e4m3_rounding_known_values():
+    """fp8 e4m3 rounding of the variant model: nearest-even on a 3-bit
+    mantissa, subnormal step 2^-9, saturation at 448."""
+    from oracle.winograd import _e4m3
+    vals = np.array([1.0, 1.0625, 1.1875, -1.0625, 448.0, 500.0, 2.0 ** -9, 2.0 ** -10 * 1.5,
+                     0.0, 240.0, 0.017578125])
+    want = np.array([1.0, 1.0, 1.25, -1.0, 448.0, 448.0, 2.0 ** -9, 2.0 ** -9, 0.0, 240.0, 0.017578125])
+    assert np.array_equal(_e4m3(vals), want)
