@@ -81,6 +81,22 @@ def lib():
             "wino_fused_workspace_bytes": ([i, i, i, i], sz),
             "wino_input_layout": ([vp, vp, i, i, i, i, vp], i),
             "wino_variant_workspace_bytes": ([i, i, i, i, i, i], sz),
+            "wino_conv2d_fused_cfg": ([vp, vp, vp, vp, i, i, i, i, i, i, vp], i),
+            "wino_tune_layer": ([vp, vp, vp, vp, i, i, i, i, i, i, ctypes.POINTER(ctypes.c_float),
+                                 ctypes.POINTER(i), vp], i),
+            "wino_batch_create": ([ctypes.POINTER(vp)], i),
+            "wino_batch_destroy": ([vp], i),
+            "wino_batch_add_layer": ([vp, vp, vp, vp, vp, i, i, i, i, i], i),
+            "wino_batch_num_layers": ([vp], i),
+            "wino_batch_set_config": ([vp, i, i], i),
+            "wino_batch_get_config": ([vp, i, ctypes.POINTER(i)], i),
+            "wino_batch_set_order": ([vp, ctypes.POINTER(i), i], i),
+            "wino_batch_get_order": ([vp, ctypes.POINTER(i), i], i),
+            "wino_batch_commit": ([vp], i),
+            "wino_batch_run": ([vp, vp], i),
+            "wino_batch_tune": ([vp, i, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float), vp], i),
+            "wino_batch_graph_capture": ([vp, vp], i),
+            "wino_batch_graph_launch": ([vp, vp], i),
             "wino_conv2d_variant": ([i, vp, vp, vp, vp, i, i, i, i, i, vp], i),
             "wino_conv2d_fused_ws": ([vp, vp, vp, vp, i, i, i, i, i, vp], i),
             "wino_launch_kernelinfo": ([vp, vp, vp], i),
@@ -281,6 +297,108 @@ def conv2d_unfused(x, ucache2, k, ws=None, out=None, stream=None):
                                      ctypes.c_void_p(ws.m.data_ptr()), n, c, h, wd, k, _stream(stream)),
            "conv2d_unfused")
     return y
+
+
+CFG_KMAJOR, CFG_DIRECT, NCFG = 1, 2, 4
+
+# The uneven ResNet-style 3x3 stride-1 pad-1 layer set of the batched launch,
+# as (C, K, H=W): two each of the four square stages plus the four C != K
+# transitions.
+RESNET_LAYER_SET = [(64, 64, 56), (64, 64, 56), (128, 128, 28), (128, 128, 28),
+                    (256, 256, 14), (256, 256, 14), (512, 512, 7), (512, 512, 7),
+                    (64, 128, 56), (128, 256, 28), (256, 512, 14), (512, 256, 7)]
+
+
+def _p(t):
+    return ctypes.c_void_p(0 if t is None else t.data_ptr())
+
+
+def conv2d_fused_cfg(x, ucache, k, cfg, workspace=None, out=None, stream=None):
+    """Fused fp16 conv on a cached U with a schedule configuration (CFG_* bits)."""
+    import torch
+    n, c, h, wd = x.shape
+    y = out if out is not None else torch.empty((n, k, h, wd), dtype=torch.float16, device=x.device)
+    if workspace is None and not (cfg & CFG_DIRECT):
+        workspace = torch.empty(fused_workspace_bytes(n, c, h, wd), dtype=torch.uint8, device=x.device)
+    _check(lib().wino_conv2d_fused_cfg(_p(x), _p(ucache), _p(workspace), _p(y), n, c, h, wd, k, cfg,
+                                       _stream(stream)), "conv2d_fused_cfg")
+    return y
+
+
+def tune_layer(x, ucache, k, workspace, out, reps=3, stream=None):
+    """Exhaustive tuning of one layer: (per-config mean us list, best cfg)."""
+    n, c, h, wd = x.shape
+    us = (ctypes.c_float * NCFG)()
+    best = ctypes.c_int(-1)
+    _check(lib().wino_tune_layer(_p(x), _p(ucache), _p(workspace), _p(out), n, c, h, wd, k, reps, us,
+                                 ctypes.byref(best), _stream(stream)), "tune_layer")
+    return [float(v) for v in us], best.value
+
+
+class Batch:
+    """Uneven fp16 layers run as one persistent launch (optionally a CUDA graph).
+
+    Each layer owns its input, U cache (filter_transform), output and pre-pass
+    workspace; the Python object keeps references so they outlive the batch."""
+
+    def __init__(self):
+        self._h = ctypes.c_void_p(0)
+        _check(lib().wino_batch_create(ctypes.byref(self._h)), "batch_create")
+        self._keep = []
+
+    def add(self, x, ucache, k, out, workspace=None):
+        n, c, h, wd = x.shape
+        _check(lib().wino_batch_add_layer(self._h, _p(x), _p(ucache), _p(workspace), _p(out), n, c, h,
+                                          wd, k), "batch_add_layer")
+        self._keep.append((x, ucache, out, workspace))
+
+    def __len__(self):
+        return lib().wino_batch_num_layers(self._h)
+
+    def set_config(self, layer, cfg):
+        _check(lib().wino_batch_set_config(self._h, layer, cfg), "batch_set_config")
+
+    def config(self, layer):
+        v = ctypes.c_int(0)
+        _check(lib().wino_batch_get_config(self._h, layer, ctypes.byref(v)), "batch_get_config")
+        return v.value
+
+    def set_order(self, order):
+        arr = (ctypes.c_int * len(order))(*order)
+        _check(lib().wino_batch_set_order(self._h, arr, len(order)), "batch_set_order")
+
+    def order(self):
+        n = len(self)
+        arr = (ctypes.c_int * n)()
+        _check(lib().wino_batch_get_order(self._h, arr, n), "batch_get_order")
+        return list(arr)
+
+    def run(self, stream=None):
+        _check(lib().wino_batch_run(self._h, _stream(stream)), "batch_run")
+
+    def tune(self, reps=3, stream=None):
+        n = len(self)
+        lu = (ctypes.c_float * (n * NCFG))()
+        ou = (ctypes.c_float * 3)()
+        _check(lib().wino_batch_tune(self._h, reps, lu, ou, _stream(stream)), "batch_tune")
+        return [list(lu[i * NCFG:(i + 1) * NCFG]) for i in range(n)], list(ou)
+
+    def capture(self, stream=None):
+        _check(lib().wino_batch_graph_capture(self._h, _stream(stream)), "batch_graph_capture")
+
+    def launch(self, stream=None):
+        _check(lib().wino_batch_graph_launch(self._h, _stream(stream)), "batch_graph_launch")
+
+    def close(self):
+        if self._h:
+            lib().wino_batch_destroy(self._h)
+            self._h = ctypes.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 - interpreter shutdown
+            pass
 
 
 def error_read_clear() -> int:

@@ -63,6 +63,7 @@
 #include "tc_sm100.cuh"
 #include "wino_common.cuh"
 #include "vgen.cuh"
+#include "wino_batch.h"
 
 namespace wino {
 
@@ -140,16 +141,81 @@ __device__ __forceinline__ uint32_t h2_to_e4m3x2(uint32_t w, uint32_t scale2) {
 
 using namespace fused;
 
-template <int VAR>
-__device__ __forceinline__ void fused_body(const KernelParam& p, const VariantArgs& va) {
+// ---- work blocks --------------------------------------------------------
+// A persistent CTA walks work blocks b = blockIdx.x, + gridDim.x, ...; every
+// role walks the same sequence and asks its block source for the block's
+// layer arguments and coordinates, so one kernel serves one layer or a
+// table of layers (schedule configuration bits CFG_* in wino_batch.h).
+struct BlockInfo {
+  Geometry g;
+  const __half* x;          // NCHW input
+  __half* y;                // NKPQ output
+  const uint8_t* xb;        // XB records, or null (direct reads)
+  const uint8_t* u;         // U cache
+  int tb, kb;               // tile block, k block
+};
+
+__device__ __forceinline__ void block_coords(long long lb, const Geometry& g, int cfg, int& tb, int& kb) {
+  if (cfg & CFG_KMAJOR) {
+    kb = (int)(lb / g.nTB);
+    tb = (int)(lb - (long long)kb * g.nTB);
+  } else {
+    tb = (int)(lb / g.nKB);
+    kb = (int)(lb - (long long)tb * g.nKB);
+  }
+}
+
+__device__ __forceinline__ BlockInfo make_block(const KernelParam& p, const Geometry& g, int cfg, long long lb) {
+  BlockInfo B;
+  B.g = g;
+  B.x = static_cast<const __half*>(p.pin);
+  B.y = static_cast<__half*>(p.pout);
+  B.xb = (cfg & CFG_DIRECT) ? nullptr : static_cast<const uint8_t*>(p.transform_pin);
+  B.u = static_cast<const uint8_t*>(p.transform_filter);
+  block_coords(lb, g, cfg, B.tb, B.kb);
+  return B;
+}
+
+// One layer (the drop-in and single-conv entry points).
+struct OneLayer {
+  KernelParam p;
+  Geometry g;
+  int cfg;
+  __device__ long long total() const { return g.nblocks; }
+  __device__ BlockInfo get(long long b) const { return make_block(p, g, cfg, b); }
+};
+
+// A table of layers in global memory, blocks concatenated in table order
+// (the batched persistent launch); entries are read through the read-only
+// cache.
+struct LayerTable {
+  const BatchTable* t;
+  long long tot;
+  __device__ long long total() const { return tot; }
+  __device__ BlockInfo get(long long b) const {
+    int l = 0;
+    const int nl = __ldg(&t->nlayers);
+    while (l + 1 < nl && __ldg(&t->layer[l + 1].block_begin) <= b) ++l;
+    const LayerDesc& d = t->layer[l];
+    KernelParam p;
+    p.pin = (void*)__ldg((const unsigned long long*)&d.p.pin);
+    p.pout = (void*)__ldg((const unsigned long long*)&d.p.pout);
+    p.transform_pin = (void*)__ldg((const unsigned long long*)&d.p.transform_pin);
+    p.transform_filter = (void*)__ldg((const unsigned long long*)&d.p.transform_filter);
+    p.n = __ldg(&d.p.n); p.c = __ldg(&d.p.c); p.h = __ldg(&d.p.h); p.w = __ldg(&d.p.w);
+    p.k = __ldg(&d.p.k); p.Oh = __ldg(&d.p.Oh); p.Ow = __ldg(&d.p.Ow);
+    const Geometry g = make_geometry(p, TILES);
+    return make_block(p, g, __ldg(&d.cfg), b - __ldg(&d.block_begin));
+  }
+};
+
+template <int VAR, typename Sched>
+__device__ __forceinline__ void fused_body(const Sched& sched, const VariantArgs& va) {
   using T = Traits<VAR>;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   __shared__ Shared sh;
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  const Geometry g = make_geometry(p, TILES);
-  const int nKB = (g.K + KB - 1) / KB;
-  const long long nblocks = (long long)g.nTB * nKB;
-  const int CS = g.C / T::CH;          // steps per block
+  const long long nblocks = sched.total();
   const int warp = warp_id();
   const int lane = lane_id();
   uint32_t* err = &g_fused_err;
@@ -203,8 +269,9 @@ __device__ __forceinline__ void fused_body(const KernelParam& p, const VariantAr
       uint32_t it = 0, bi = 0;
       bool ok = true;
       for (long long b = blockIdx.x; b < nblocks && ok; b += gridDim.x, ++bi) {
-        const int kb = (int)(b % nKB);
-        const uint32_t astep = (uint32_t)(kblock_rows(kb, g.K) * 32) >> 4;
+        const BlockInfo B = sched.get(b);
+        const int CS = B.g.C / T::CH;          // steps of the block
+        const uint32_t astep = (uint32_t)(kblock_rows(B.kb, B.g.K) * 32) >> 4;
         for (int s = 0; s < CS && ok; ++s, ++it) {
           const uint32_t vs = it % NVSLOT;
           ok = mbar_wait(&sh.vfull[vs], (it / NVSLOT) & 1, abort_flag, err, ERR_WAIT_FULL);
@@ -247,12 +314,14 @@ __device__ __forceinline__ void fused_body(const KernelParam& p, const VariantAr
     if (lane < T::UP) {
       // lane j copies piece j of every step (one copy in flight per thread)
       const int j = lane;
-      const uint8_t* ubase = static_cast<const uint8_t*>(
-          (VAR == VAR_F16_HILO && j >= 2) ? va.u_lo : p.transform_filter);
       uint32_t it = 0;
       bool ok = true;
       for (long long b = blockIdx.x; b < nblocks && ok; b += gridDim.x) {
-        const int kb = (int)(b % nKB);
+        const BlockInfo B = sched.get(b);
+        const Geometry& g = B.g;
+        const int CS = g.C / T::CH;
+        const uint8_t* ubase = (VAR == VAR_F16_HILO && j >= 2) ? static_cast<const uint8_t*>(va.u_lo) : B.u;
+        const int kb = B.kb;
         const int kbs = kblock_rows(kb, g.K);
         const uint32_t bytes = 8 * kbs * 32;  // 8 taps x kbs rows x 32 B
         for (int s = 0; s < CS; ++s, ++it) {
@@ -277,18 +346,19 @@ __device__ __forceinline__ void fused_body(const KernelParam& p, const VariantAr
     }
     __syncwarp();
   } else if (warp == WARP_S) {
-    const uint8_t* XB = static_cast<const uint8_t*>(p.transform_pin);
-    const int my_blocks =
-        blockIdx.x < nblocks ? (int)((nblocks - blockIdx.x + gridDim.x - 1) / gridDim.x) : 0;
-    const uint32_t RB = (uint32_t)xb_row_bytes(g.W);
-    const size_t img_stride = (size_t)(g.C >> 4) * xb_rows(g.H) * RB;   // one image of XB
-    const size_t cb_stride = (size_t)xb_rows(g.H) * RB;                  // one channel block
     uint32_t it = 0;
     bool ok = true;
     // lane = segment + 4 * channel block of the step
     const int seg = lane & 3, cbi = lane >> 2;
-    for (int bi = 0; bi < my_blocks && ok; ++bi) {
-      const int tile0 = (int)((blockIdx.x + (long long)bi * gridDim.x) / nKB) * TILES;
+    for (long long b = blockIdx.x; b < nblocks && ok; b += gridDim.x) {
+      const BlockInfo B = sched.get(b);
+      const Geometry& g = B.g;
+      const int CS = g.C / T::CH;
+      const uint8_t* XB = B.xb;
+      const uint32_t RB = (uint32_t)xb_row_bytes(g.W);
+      const size_t img_stride = (size_t)(g.C >> 4) * xb_rows(g.H) * RB;   // one image of XB
+      const size_t cb_stride = (size_t)xb_rows(g.H) * RB;                  // one channel block
+      const int tile0 = B.tb * TILES;
       const SlabPlan pl = slab_plan(g, tile0, TILES);
       const bool use = XB != nullptr && slab_fits(g, pl, T::NCB);
       int ta = 0, rows = 0, rbase = 0;  // this lane's segment
@@ -322,10 +392,6 @@ __device__ __forceinline__ void fused_body(const KernelParam& p, const VariantAr
     const int q = warp - WARP_V0;
     const int hh = q & 1;                     // K half of the step's operand row
     const int ar = q >> 1;                    // tap rows 2ar, 2ar+1 (taps 8ar .. 8ar+7)
-    const __half* X = static_cast<const __half*>(p.pin);
-    const bool have_xb = p.transform_pin != nullptr;
-    const int my_blocks =
-        blockIdx.x < nblocks ? (int)((nblocks - blockIdx.x + gridDim.x - 1) / gridDim.x) : 0;
     const uint32_t slab0 = smem_base + SLAB_BASE;
     bool ok = true;
     // K-major core matrices: tile group (lane/8) at 256 B, K half at 128 B,
@@ -333,11 +399,15 @@ __device__ __forceinline__ void fused_body(const KernelParam& p, const VariantAr
     // lanes 128 contiguous bytes (conflict-free).
     const uint32_t row_off = (lane >> 3) * 256 + hh * 128 + (lane & 7) * 16 + ar * 8 * V_TAP_BYTES;
     uint32_t it = 0;
-    for (int bi = 0; bi < my_blocks && ok; ++bi) {
+    for (long long b = blockIdx.x; b < nblocks && ok; b += gridDim.x) {
       // per-block quantities once per block, 32-bit
-      const int tile0 = (int)((blockIdx.x + (long long)bi * gridDim.x) / nKB) * TILES;
+      const BlockInfo B = sched.get(b);
+      const Geometry& g = B.g;
+      const int CS = g.C / T::CH;
+      const __half* X = B.x;
+      const int tile0 = B.tb * TILES;
       const SlabPlan pl = slab_plan(g, tile0, TILES);
-      const bool use_slab = have_xb && slab_fits(g, pl, T::NCB);
+      const bool use_slab = B.xb != nullptr && slab_fits(g, pl, T::NCB);
       const TileCoord tc = tile_coord(g, tile0 + lane, tile0);
       // fp8: this warp's K half is a whole XB channel block (two 8-channel
       // halves), the second block of the step's slab for hh = 1
@@ -436,13 +506,15 @@ __device__ __forceinline__ void fused_body(const KernelParam& p, const VariantAr
   } else if (warp >= WARP_E0 && warp < WARP_E0 + NWARP_E) {
     const int quarter = warp & 3;            // TMEM lanes 32*quarter .. +31 = channels
     const int half = (warp - WARP_E0) >> 2;  // tiles 16*half .. +15 of the block
-    __half* Y = static_cast<__half*>(p.pout);
-    const bool q_even = (g.Q & 1) == 0;
     uint32_t bi = 0;
     bool ok = true;
     for (long long b = blockIdx.x; b < nblocks && ok; b += gridDim.x, ++bi) {
-      const long long tb = b / nKB;
-      const int kb = (int)(b % nKB);
+      const BlockInfo B = sched.get(b);
+      const Geometry& g = B.g;
+      __half* Y = B.y;
+      const bool q_even = (g.Q & 1) == 0;
+      const long long tb = B.tb;
+      const int kb = B.kb;
       const int kbs = kblock_rows(kb, g.K);
       float y[16][4];
 #pragma unroll
@@ -558,17 +630,27 @@ __device__ __forceinline__ void fused_body(const KernelParam& p, const VariantAr
 
 // The drop-in kernel: its only argument is the plugin's parameter struct.
 __global__ void __launch_bounds__(NTHREAD, 1) fused_wino_f16_kernel(KernelParam p) {
-  fused_body<VAR_F16>(p, VariantArgs{nullptr, nullptr, nullptr});
+  const OneLayer one{p, make_geometry(p, TILES), 0};
+  fused_body<VAR_F16>(one, VariantArgs{nullptr, nullptr, nullptr});
 }
 
+// Precision variants and schedule configurations of one layer.
 template <int VAR>
-__global__ void __launch_bounds__(NTHREAD, 1) fused_wino_var_kernel(KernelParam p, VariantArgs va) {
-  fused_body<VAR>(p, va);
+__global__ void __launch_bounds__(NTHREAD, 1) fused_wino_var_kernel(KernelParam p, VariantArgs va, int cfg) {
+  const OneLayer one{p, make_geometry(p, TILES), cfg};
+  fused_body<VAR>(one, va);
 }
 
-template __global__ void fused_wino_var_kernel<VAR_BF16>(KernelParam, VariantArgs);
-template __global__ void fused_wino_var_kernel<VAR_F8>(KernelParam, VariantArgs);
-template __global__ void fused_wino_var_kernel<VAR_F16_HILO>(KernelParam, VariantArgs);
+template __global__ void fused_wino_var_kernel<VAR_F16>(KernelParam, VariantArgs, int);
+template __global__ void fused_wino_var_kernel<VAR_BF16>(KernelParam, VariantArgs, int);
+template __global__ void fused_wino_var_kernel<VAR_F8>(KernelParam, VariantArgs, int);
+template __global__ void fused_wino_var_kernel<VAR_F16_HILO>(KernelParam, VariantArgs, int);
+
+// A table of fp16 layers in one persistent launch.
+__global__ void __launch_bounds__(NTHREAD, 1) fused_wino_batch_kernel(const BatchTable* t, long long total) {
+  const LayerTable lt{t, total};
+  fused_body<VAR_F16>(lt, VariantArgs{nullptr, nullptr, nullptr});
+}
 
 }  // namespace wino
 
@@ -586,9 +668,21 @@ int wino_fused_prepare() {
   return (int)e;
 }
 
+static void* var_kernel(int variant);
+
+// Dynamic shared memory limit of a variant's kernel, set once per variant.
+int wino_fused_prepare_variant(int variant) {
+  static int done[4] = {-1, -1, -1, -1};
+  if (variant < 0 || variant > 3) return (int)cudaErrorInvalidValue;
+  if (done[variant] < 0)
+    done[variant] = (int)cudaFuncSetAttribute(var_kernel(variant), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              fused::SMEM_BYTES);
+  return done[variant];
+}
+
 static void* var_kernel(int variant) {
   switch (variant) {
-    case VAR_F16: return (void*)fused_wino_f16_kernel;
+    case VAR_F16: return (void*)fused_wino_var_kernel<VAR_F16>;
     case VAR_BF16: return (void*)fused_wino_var_kernel<VAR_BF16>;
     case VAR_F8: return (void*)fused_wino_var_kernel<VAR_F8>;
     case VAR_F16_HILO: return (void*)fused_wino_var_kernel<VAR_F16_HILO>;
@@ -596,18 +690,42 @@ static void* var_kernel(int variant) {
   }
 }
 
-// Launch the fused kernel of a precision variant on `grid` CTAs.
-int wino_fused_launch_variant(int variant, const KernelParam* p, const VariantArgs* va, unsigned grid,
-                              cudaStream_t stream) {
+// Launch the fused kernel of a precision variant and schedule configuration
+// (CFG_* bits) on `grid` CTAs.
+int wino_fused_launch_variant(int variant, const KernelParam* p, const VariantArgs* va, int cfg,
+                              unsigned grid, cudaStream_t stream) {
   void* fn = var_kernel(variant);
   if (!fn) return (int)cudaErrorInvalidValue;
-  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, fused::SMEM_BYTES);
+  cudaError_t e = (cudaError_t)wino_fused_prepare_variant(variant);
   if (e != cudaSuccess) return (int)e;
   KernelParam pc = *p;
   VariantArgs vc = va ? *va : VariantArgs{nullptr, nullptr, nullptr};
-  void* args2[] = {&pc, &vc};
-  void* args1[] = {&pc};
-  e = cudaLaunchKernel(fn, dim3(grid), dim3(fused::NTHREAD), variant == VAR_F16 ? args1 : args2,
+  int cf = cfg;
+  void* args[] = {&pc, &vc, &cf};
+  e = cudaLaunchKernel(fn, dim3(grid), dim3(fused::NTHREAD), args, (size_t)fused::SMEM_BYTES, stream);
+  return (int)e;
+}
+
+// The batched persistent launch over a device-resident layer table.
+size_t wino_batch_table_bytes() { return sizeof(BatchTable); }
+int wino_batch_max_layers() { return BATCH_MAX; }
+size_t wino_batch_layer_desc_bytes() { return sizeof(LayerDesc); }
+
+// Dynamic shared memory limits, set outside any stream capture.
+int wino_fused_prepare_batch() {
+  return (int)cudaFuncSetAttribute(fused_wino_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   fused::SMEM_BYTES);
+}
+
+int wino_fused_launch_batch(const void* table_dev, long long total_blocks, unsigned grid,
+                            cudaStream_t stream) {
+  static const int prepared = wino_fused_prepare_batch();
+  if (prepared != 0) return prepared;
+  cudaError_t e;
+  const BatchTable* t = static_cast<const BatchTable*>(table_dev);
+  long long tot = total_blocks;
+  void* args[] = {&t, &tot};
+  e = cudaLaunchKernel((void*)fused_wino_batch_kernel, dim3(grid), dim3(fused::NTHREAD), args,
                        (size_t)fused::SMEM_BYTES, stream);
   return (int)e;
 }

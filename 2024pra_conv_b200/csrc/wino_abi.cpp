@@ -74,7 +74,7 @@ struct VariantArgs {
 }
 extern "C" {
 int wino_fused_launch_variant(int variant, const wino::KernelParam* p, const wino::VariantArgs* va,
-                              unsigned grid, cudaStream_t stream);
+                              int cfg, unsigned grid, cudaStream_t stream);
 size_t wino_unfused_v_bytes(int n, int c, int h, int w);
 size_t wino_unfused_m_bytes(int n, int k, int h, int w);
 int wino_unfused_prepare();
@@ -394,8 +394,8 @@ extern "C" int wino_conv2d_variant(int variant, const void* x, const void* weigh
   }
   if (rc != 0) return WINO_ECUDA;
   if (variant != WINO_VAR_F8 && wino_launch_xb_layout(&p, s) != 0) return WINO_ECUDA;
-  return wino_fused_launch_variant(variant, &p, &va, fused_grid(n, h, w, k), s) == 0 ? WINO_OK
-                                                                                      : WINO_ECUDA;
+  return wino_fused_launch_variant(variant, &p, &va, 0, fused_grid(n, h, w, k), s) == 0 ? WINO_OK
+                                                                                         : WINO_ECUDA;
 }
 
 // Launch the four slots of a filled kernelInfo_t in order on one stream, each

@@ -1,0 +1,399 @@
+// Batched persistent launch, schedule configurations and the autotuner.
+//
+// A batch holds the uneven 3x3 conv layers of a network (each with its own
+// input, cached U, output and XB workspace).  Running it issues the input
+// pre-pass of every layer that uses one and then ONE persistent fused-kernel
+// launch whose CTAs walk the concatenated work blocks of all layers through
+// a device-resident layer table; the whole sequence can be captured into a
+// CUDA graph and replayed.  The reference has no counterpart: its harness
+// runs one hard-wired shape per launch sequence (src/main.cpp:105-124,
+// src/conv2d.cpp:458-494).
+//
+// The autotuner times every schedule configuration of every layer (CFG_*
+// bits of wino_batch.h) with CUDA events, keeps the fastest per layer, then
+// times whole-batch launches under three layer orders and keeps the fastest.
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <new>
+#include <numeric>
+#include <vector>
+#include <cuda_runtime.h>
+
+#include "winoconv.h"
+#include "wino_param.h"
+#include "wino_batch.h"
+
+namespace wino {
+struct VariantArgs {
+  const void* u_lo;
+  const float* su;
+  const uint32_t* inv_sv2;
+};
+}  // namespace wino
+
+extern "C" {
+int wino_fused_launch_variant(int variant, const wino::KernelParam* p, const wino::VariantArgs* va,
+                              int cfg, unsigned grid, cudaStream_t stream);
+int wino_fused_launch_batch(const void* table_dev, long long total_blocks, unsigned grid,
+                            cudaStream_t stream);
+int wino_launch_xb_layout(const wino::KernelParam* p, cudaStream_t stream);
+int wino_fused_prepare_batch();
+int wino_fused_prepare_variant(int variant);
+size_t wino_xb_bytes(int n, int c, int h, int w);
+long long wino_xb_items(int n, int c, int h, int w);
+long long wino_fused_nblocks(int n, int h, int w, int k);
+}
+
+namespace {
+
+using wino::BatchTable;
+using wino::KernelParam;
+using wino::LayerDesc;
+
+int sm_count() {
+  int dev = 0, n = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+  if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+    return 148;
+  return n;
+}
+
+KernelParam layer_param(const void* x, const void* ucache, void* xb, void* y, int n, int c, int h,
+                        int w, int k) {
+  KernelParam p;
+  std::memset(&p, 0, sizeof(p));
+  p.pin = const_cast<void*>(x);
+  p.pout = y;
+  p.transform_pin = xb;
+  p.transform_filter = const_cast<void*>(ucache);
+  p.n = (short)n; p.c = (short)c; p.h = (short)h; p.w = (short)w; p.k = (short)k;
+  p.r = 3; p.s = 3; p.u = 1; p.v = 1; p.p = 1; p.q = 1;
+  p.Oh = (short)h; p.Ow = (short)w;
+  return p;
+}
+
+unsigned grid_for(long long blocks) {
+  const long long sms = sm_count();
+  return (unsigned)std::max<long long>(1, std::min(blocks, sms));
+}
+
+// One layer with a schedule configuration: its pre-pass (unless direct) and
+// the fused kernel.
+int run_layer_cfg(const KernelParam& p0, int cfg, cudaStream_t s) {
+  KernelParam p = p0;
+  if (!p.transform_pin) cfg |= wino::CFG_DIRECT;
+  if (cfg & wino::CFG_DIRECT) {
+    p.transform_pin = nullptr;
+  } else if (wino_launch_xb_layout(&p, s) != 0) {
+    return WINO_ECUDA;
+  }
+  const long long nb = wino_fused_nblocks(p.n, p.h, p.w, p.k);
+  return wino_fused_launch_variant(WINO_VAR_F16, &p, nullptr, cfg, grid_for(nb), s) == 0 ? WINO_OK
+                                                                                          : WINO_ECUDA;
+}
+
+// Mean microseconds of `fn` over `reps` launches after one warm-up, on `s`.
+template <typename F>
+int time_us(F&& fn, int reps, cudaStream_t s, float* us) {
+  cudaEvent_t a, b;
+  if (cudaEventCreate(&a) != cudaSuccess) return WINO_ECUDA;
+  if (cudaEventCreate(&b) != cudaSuccess) {
+    cudaEventDestroy(a);
+    return WINO_ECUDA;
+  }
+  int rc = fn();
+  if (rc == WINO_OK) {
+    cudaEventRecord(a, s);
+    for (int i = 0; i < reps && rc == WINO_OK; ++i) rc = fn();
+    cudaEventRecord(b, s);
+    if (cudaEventSynchronize(b) != cudaSuccess) rc = WINO_ECUDA;
+    float ms = 0.f;
+    if (rc == WINO_OK && cudaEventElapsedTime(&ms, a, b) != cudaSuccess) rc = WINO_ECUDA;
+    if (rc == WINO_OK) *us = ms * 1000.f / (float)std::max(reps, 1);
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return rc;
+}
+
+struct Layer {
+  KernelParam p;
+  int cfg = 0;
+  long long blocks = 0;
+  float tuned_us = 0.f;
+};
+
+struct Batch {
+  std::vector<Layer> layers;
+  std::vector<int> order;        // table order of the layers
+  BatchTable* table_dev = nullptr;
+  long long total = 0;
+  bool dirty = true;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+
+  void drop_graph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+  }
+
+  // Build the table in `order` and copy it to the device (synchronous: never
+  // called inside a stream capture).
+  int commit() {
+    if (!dirty) return WINO_OK;
+    if (!table_dev && cudaMalloc(&table_dev, sizeof(BatchTable)) != cudaSuccess) return WINO_ECUDA;
+    BatchTable t;
+    std::memset(&t, 0, sizeof(t));
+    t.nlayers = (int)order.size();
+    long long begin = 0;
+    for (size_t i = 0; i < order.size(); ++i) {
+      const Layer& L = layers[order[i]];
+      LayerDesc& d = t.layer[i];
+      d.p = L.p;
+      int cfg = L.cfg;
+      if (!d.p.transform_pin) cfg |= wino::CFG_DIRECT;
+      if (cfg & wino::CFG_DIRECT) d.p.transform_pin = nullptr;
+      d.cfg = cfg;
+      d.block_begin = begin;
+      begin += L.blocks;
+    }
+    t.total = begin;
+    total = begin;
+    if (cudaMemcpy(table_dev, &t, sizeof(t), cudaMemcpyHostToDevice) != cudaSuccess) return WINO_ECUDA;
+    dirty = false;
+    drop_graph();
+    return WINO_OK;
+  }
+
+  int run(cudaStream_t s) {
+    if (dirty) return WINO_EINVAL;  // commit first (outside any capture)
+    for (int li : order) {
+      const Layer& L = layers[li];
+      if (L.p.transform_pin && !(L.cfg & wino::CFG_DIRECT) && wino_launch_xb_layout(&L.p, s) != 0)
+        return WINO_ECUDA;
+    }
+    return wino_fused_launch_batch(table_dev, total, grid_for(total), s) == 0 ? WINO_OK : WINO_ECUDA;
+  }
+};
+
+Batch* as_batch(void* h) { return static_cast<Batch*>(h); }
+
+}  // namespace
+
+extern "C" {
+
+int wino_conv2d_fused_cfg(const void* x, const void* ucache, void* workspace, void* y, int n, int c,
+                          int h, int w, int k, int cfg, void* stream) {
+  if (!x || !ucache || !y) return WINO_EINVAL;
+  if (cfg < 0 || cfg >= wino::NCFG) return WINO_EINVAL;
+  if (workspace && (reinterpret_cast<uintptr_t>(workspace) & 15) != 0) return WINO_EINVAL;
+  const int st = wino_check_shape(n, c, h, w, k);
+  if (st != WINO_OK) return st;
+  if (workspace && wino_xb_items(n, c, h, w) >= (1LL << 31)) return WINO_EUNSUPPORTED;
+  return run_layer_cfg(layer_param(x, ucache, workspace, y, n, c, h, w, k), cfg, (cudaStream_t)stream);
+}
+
+int wino_tune_layer(const void* x, const void* ucache, void* workspace, void* y, int n, int c, int h,
+                    int w, int k, int reps, float* us_out, int* best_cfg, void* stream) {
+  if (!x || !ucache || !y || !us_out || !best_cfg) return WINO_EINVAL;
+  const int st = wino_check_shape(n, c, h, w, k);
+  if (st != WINO_OK) return st;
+  const KernelParam p = layer_param(x, ucache, workspace, y, n, c, h, w, k);
+  const cudaStream_t s = (cudaStream_t)stream;
+  int best = -1;
+  for (int cfg = 0; cfg < wino::NCFG; ++cfg) {
+    us_out[cfg] = -1.f;
+    if (!workspace && !(cfg & wino::CFG_DIRECT)) continue;
+    float us = 0.f;
+    const int rc = time_us([&] { return run_layer_cfg(p, cfg, s); }, reps, s, &us);
+    if (rc != WINO_OK) return rc;
+    us_out[cfg] = us;
+    if (best < 0 || us < us_out[best]) best = cfg;
+  }
+  *best_cfg = best;
+  return WINO_OK;
+}
+
+int wino_batch_create(void** out) {
+  if (!out) return WINO_EINVAL;
+  *out = new (std::nothrow) Batch();
+  return *out ? WINO_OK : WINO_EINVAL;
+}
+
+int wino_batch_destroy(void* h) {
+  Batch* b = as_batch(h);
+  if (!b) return WINO_EINVAL;
+  b->drop_graph();
+  if (b->table_dev) cudaFree(b->table_dev);
+  delete b;
+  return WINO_OK;
+}
+
+int wino_batch_add_layer(void* h, const void* x, const void* ucache, void* xb_ws, void* y, int n,
+                         int c, int hh, int w, int k) {
+  Batch* b = as_batch(h);
+  if (!b || !x || !ucache || !y) return WINO_EINVAL;
+  if ((int)b->layers.size() >= wino::BATCH_MAX) return WINO_EUNSUPPORTED;
+  const int st = wino_check_shape(n, c, hh, w, k);
+  if (st != WINO_OK) return st;
+  if (xb_ws && ((reinterpret_cast<uintptr_t>(xb_ws) & 15) != 0 || wino_xb_items(n, c, hh, w) >= (1LL << 31)))
+    return WINO_EINVAL;
+  Layer L;
+  L.p = layer_param(x, ucache, xb_ws, y, n, c, hh, w, k);
+  L.blocks = wino_fused_nblocks(n, hh, w, k);
+  L.cfg = xb_ws ? 0 : wino::CFG_DIRECT;
+  b->order.push_back((int)b->layers.size());
+  b->layers.push_back(L);
+  b->dirty = true;
+  return WINO_OK;
+}
+
+int wino_batch_num_layers(void* h) {
+  Batch* b = as_batch(h);
+  return b ? (int)b->layers.size() : -1;
+}
+
+int wino_batch_set_config(void* h, int layer, int cfg) {
+  Batch* b = as_batch(h);
+  if (!b || layer < 0 || layer >= (int)b->layers.size() || cfg < 0 || cfg >= wino::NCFG)
+    return WINO_EINVAL;
+  b->layers[layer].cfg = cfg;
+  b->dirty = true;
+  return WINO_OK;
+}
+
+int wino_batch_get_config(void* h, int layer, int* cfg) {
+  Batch* b = as_batch(h);
+  if (!b || !cfg || layer < 0 || layer >= (int)b->layers.size()) return WINO_EINVAL;
+  *cfg = b->layers[layer].cfg;
+  return WINO_OK;
+}
+
+int wino_batch_set_order(void* h, const int* order, int n) {
+  Batch* b = as_batch(h);
+  if (!b || !order || n != (int)b->layers.size()) return WINO_EINVAL;
+  std::vector<int> o(order, order + n), sorted(o);
+  std::sort(sorted.begin(), sorted.end());
+  for (int i = 0; i < n; ++i)
+    if (sorted[i] != i) return WINO_EINVAL;  // must be a permutation
+  b->order = o;
+  b->dirty = true;
+  return WINO_OK;
+}
+
+int wino_batch_get_order(void* h, int* order, int n) {
+  Batch* b = as_batch(h);
+  if (!b || !order || n != (int)b->layers.size()) return WINO_EINVAL;
+  std::copy(b->order.begin(), b->order.end(), order);
+  return WINO_OK;
+}
+
+int wino_batch_commit(void* h) {
+  Batch* b = as_batch(h);
+  return b ? b->commit() : WINO_EINVAL;
+}
+
+int wino_batch_run(void* h, void* stream) {
+  Batch* b = as_batch(h);
+  if (!b || b->layers.empty()) return WINO_EINVAL;
+  const int rc = b->commit();
+  if (rc != WINO_OK) return rc;
+  return b->run((cudaStream_t)stream);
+}
+
+// Autotune: per-layer configurations (exhaustive over CFG_*), then the layer
+// order of the table among {as added, longest first, longest/shortest
+// interleaved}.  layer_us: nlayers x NCFG timings (-1 = not applicable);
+// order_us: the three whole-batch timings.  Leaves the best choice set.
+int wino_batch_tune(void* h, int reps, float* layer_us, float* order_us, void* stream) {
+  Batch* b = as_batch(h);
+  if (!b || b->layers.empty()) return WINO_EINVAL;
+  const cudaStream_t s = (cudaStream_t)stream;
+  const int nl = (int)b->layers.size();
+  for (int i = 0; i < nl; ++i) {
+    Layer& L = b->layers[i];
+    float us[wino::NCFG];
+    int best = 0;
+    const int rc = wino_tune_layer(L.p.pin, L.p.transform_filter, L.p.transform_pin, L.p.pout, L.p.n,
+                                   L.p.c, L.p.h, L.p.w, L.p.k, reps, us, &best, stream);
+    if (rc != WINO_OK) return rc;
+    L.cfg = best;
+    L.tuned_us = us[best];
+    if (layer_us)
+      for (int c = 0; c < wino::NCFG; ++c) layer_us[i * wino::NCFG + c] = us[c];
+  }
+  std::vector<int> natural(nl), longest(nl), inter;
+  std::iota(natural.begin(), natural.end(), 0);
+  longest = natural;
+  std::stable_sort(longest.begin(), longest.end(),
+                   [&](int a, int c) { return b->layers[a].tuned_us > b->layers[c].tuned_us; });
+  for (int lo = 0, hi = nl - 1; lo <= hi;) {
+    inter.push_back(longest[lo++]);
+    if (lo <= hi) inter.push_back(longest[hi--]);
+  }
+  const std::vector<int>* orders[3] = {&natural, &longest, &inter};
+  int best_o = 0;
+  float best_us = 0.f;
+  for (int o = 0; o < 3; ++o) {
+    b->order = *orders[o];
+    b->dirty = true;
+    int rc = b->commit();
+    if (rc != WINO_OK) return rc;
+    float us = 0.f;
+    rc = time_us([&] { return b->run(s); }, reps, s, &us);
+    if (rc != WINO_OK) return rc;
+    if (order_us) order_us[o] = us;
+    if (o == 0 || us < best_us) {
+      best_us = us;
+      best_o = o;
+    }
+  }
+  b->order = *orders[best_o];
+  b->dirty = true;
+  return b->commit();
+}
+
+// Capture one run (pre-passes + the persistent launch) into a CUDA graph.
+// The capture uses a stream of its own (the legacy default stream cannot be
+// captured); the graph may then be launched on any stream.  `stream` is
+// accepted for symmetry and unused.
+int wino_batch_graph_capture(void* h, void* stream) {
+  (void)stream;
+  Batch* b = as_batch(h);
+  if (!b || b->layers.empty()) return WINO_EINVAL;
+  int rc = b->commit();
+  if (rc != WINO_OK) return rc;
+  if (wino_fused_prepare_batch() != 0) return WINO_ECUDA;
+  b->drop_graph();
+  cudaStream_t s = nullptr;
+  if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return WINO_ECUDA;
+  if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaStreamDestroy(s);
+    return WINO_ECUDA;
+  }
+  rc = b->run(s);
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(s, &g);
+  cudaStreamDestroy(s);
+  if (rc != WINO_OK || e != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return rc != WINO_OK ? rc : WINO_ECUDA;
+  }
+  if (cudaGraphInstantiate(&b->exec, g, 0) != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return WINO_ECUDA;
+  }
+  b->graph = g;
+  return WINO_OK;
+}
+
+int wino_batch_graph_launch(void* h, void* stream) {
+  Batch* b = as_batch(h);
+  if (!b || !b->exec || b->dirty) return WINO_EINVAL;
+  return cudaGraphLaunch(b->exec, (cudaStream_t)stream) == cudaSuccess ? WINO_OK : WINO_ECUDA;
+}
+
+}  // extern "C"

@@ -96,6 +96,53 @@ size_t wino_variant_workspace_bytes(int variant, int n, int c, int h, int w, int
 int wino_conv2d_variant(int variant, const void* x, const void* weight, void* y, void* workspace,
                         int n, int c, int h, int w, int k, void* stream);
 
+/* Schedule configurations of the fused kernel (bits): WINO_CFG_KMAJOR orders
+ * the work blocks k-block-major (consecutive blocks share U) instead of
+ * tile-major (they share input tiles); WINO_CFG_DIRECT makes the producers
+ * read the NCHW input directly instead of the pre-pass workspace.  Every
+ * configuration computes bit-identical results. */
+enum { WINO_CFG_KMAJOR = 1, WINO_CFG_DIRECT = 2, WINO_NCFG = 4 };
+
+/* One fp16 conv on a cached U with a schedule configuration; workspace
+ * (wino_fused_workspace_bytes, may be NULL for WINO_CFG_DIRECT) receives the
+ * pre-pass output. */
+int wino_conv2d_fused_cfg(const void* x, const void* ucache, void* workspace, void* y, int n, int c,
+                          int h, int w, int k, int cfg, void* stream);
+
+/* Exhaustive tuning of one layer: mean microseconds of every configuration
+ * (us_out[WINO_NCFG]; -1 where not applicable, i.e. no workspace) over
+ * `reps` runs after one warm-up, and the fastest in *best_cfg.  Synchronises
+ * `stream`; not inside a stream capture. */
+int wino_tune_layer(const void* x, const void* ucache, void* workspace, void* y, int n, int c, int h,
+                    int w, int k, int reps, float* us_out, int* best_cfg, void* stream);
+
+/* Batched persistent launch (no counterpart in the reference, whose harness
+ * runs one hard-wired shape per launch sequence, src/main.cpp:105-124).  A
+ * batch holds up to 32 fp16 layers, each with its input, cached U, output
+ * and (optional) pre-pass workspace; wino_batch_run issues the pre-passes and
+ * ONE persistent fused-kernel launch over all layers' work blocks (a device
+ * layer table); wino_batch_graph_capture records that sequence in a CUDA
+ * graph, wino_batch_graph_launch replays it.  wino_batch_tune runs the
+ * autotuner: per layer the fastest configuration (exhaustive), then the
+ * fastest table order among {as added, longest first, longest/shortest
+ * interleaved}; layer_us receives nlayers x WINO_NCFG timings, order_us the
+ * three whole-batch timings (either may be NULL).  Configuration and order
+ * changes invalidate a captured graph. */
+int wino_batch_create(void** batch);
+int wino_batch_destroy(void* batch);
+int wino_batch_add_layer(void* batch, const void* x, const void* ucache, void* workspace, void* y,
+                         int n, int c, int h, int w, int k);
+int wino_batch_num_layers(void* batch);
+int wino_batch_set_config(void* batch, int layer, int cfg);
+int wino_batch_get_config(void* batch, int layer, int* cfg);
+int wino_batch_set_order(void* batch, const int* order, int n);
+int wino_batch_get_order(void* batch, int* order, int n);
+int wino_batch_commit(void* batch);
+int wino_batch_run(void* batch, void* stream);
+int wino_batch_tune(void* batch, int reps, float* layer_us, float* order_us, void* stream);
+int wino_batch_graph_capture(void* batch, void* stream);
+int wino_batch_graph_launch(void* batch, void* stream);
+
 /* Launch the four slots of a kernelInfo_t filled by getkernelInfo, in order,
  * on `stream`, each with args[0] = param: the launch sequence of the
  * reference harness (reference src/main.cpp:105-108).  `ki` is `const

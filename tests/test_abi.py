@@ -100,3 +100,31 @@ def test_host_u_cache_layout_is_a_bijection():
                            (cc >> 3) * 64 + (kr & 7) * 8 + (cc & 7))
                     seen[off] += 1
         assert (seen == 1).all()
+
+
+def test_batch_host_validation(wino):
+    """Batch object bookkeeping that needs no GPU: shape checks, the layer
+    cap, order permutations, configuration ranges."""
+    L = wino.lib()
+    h = ctypes.c_void_p(0)
+    assert L.wino_batch_create(ctypes.byref(h)) == 0
+    dummy = ctypes.c_void_p(0x1000)
+    assert L.wino_batch_add_layer(h, dummy, dummy, None, dummy, 2, 64, 14, 14, 64) == 0
+    assert L.wino_batch_add_layer(h, dummy, dummy, None, dummy, 2, 24, 14, 14, 64) == 2   # C % 16
+    assert L.wino_batch_add_layer(h, None, dummy, None, dummy, 2, 64, 14, 14, 64) == 1    # null input
+    assert L.wino_batch_add_layer(h, dummy, dummy, ctypes.c_void_p(0x1008), dummy, 2, 64, 14, 14, 64) == 1
+    assert L.wino_batch_add_layer(h, dummy, dummy, None, dummy, 1, 32, 7, 7, 32) == 0
+    assert L.wino_batch_num_layers(h) == 2
+    bad = (ctypes.c_int * 2)(0, 0)
+    good = (ctypes.c_int * 2)(1, 0)
+    assert L.wino_batch_set_order(h, bad, 2) == 1
+    assert L.wino_batch_set_order(h, good, 2) == 0
+    out = (ctypes.c_int * 2)()
+    assert L.wino_batch_get_order(h, out, 2) == 0 and list(out) == [1, 0]
+    assert L.wino_batch_set_config(h, 0, 4) == 1
+    assert L.wino_batch_set_config(h, 2, 0) == 1
+    assert L.wino_batch_set_config(h, 1, 3) == 0
+    for _ in range(30):
+        assert L.wino_batch_add_layer(h, dummy, dummy, None, dummy, 1, 16, 4, 4, 16) == 0
+    assert L.wino_batch_add_layer(h, dummy, dummy, None, dummy, 1, 16, 4, 4, 16) == 2     # 33rd
+    assert L.wino_batch_destroy(h) == 0

@@ -1,0 +1,98 @@
+"""Schedule configurations, the batched persistent launch, its CUDA graph
+and the autotuner.
+
+Every configuration and every layer order computes the same arithmetic, so
+outputs must be bit-identical to the single-layer default path; each layer
+is also checked against FP64 (rel-L2 <= 2e-3, max-normalised <= 1e-2).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _fp64_check(x, w, y):
+    import torch
+    y64 = torch.nn.functional.conv2d(x.double(), w.double(), padding=1)
+    yd = y.double()
+    rl2 = float(torch.linalg.vector_norm(yd - y64) / torch.linalg.vector_norm(y64))
+    mxn = float((yd - y64).abs().max() / y64.abs().max())
+    assert rl2 <= 2e-3 and mxn <= 1e-2, (rl2, mxn)
+
+
+@pytest.mark.parametrize("shape", [(4, 64, 20, 20, 144), (2, 32, 7, 7, 32), (1, 16, 6, 224, 16)])
+def test_configs_bit_identical(wino, cuda, oracle_mod, shape):
+    import torch
+    n, c, h, w, k = shape
+    x16, w16 = oracle_mod.make_inputs(n, c, h, w, k, seed=7, x_dist="normal")
+    x = torch.from_numpy(x16).to(cuda)
+    wt = torch.from_numpy(w16).to(cuda)
+    u = wino.filter_transform(wt)
+    ref = wino.conv2d_fused(x, u, k)
+    for cfg in range(wino.NCFG):
+        y = wino.conv2d_fused_cfg(x, u, k, cfg)
+        torch.cuda.synchronize()
+        assert torch.equal(y.view(torch.int16), ref.view(torch.int16)), cfg
+    _fp64_check(x, wt, ref)
+    assert wino.error_read_clear() == 0
+
+
+def _layer_set(wino, oracle_mod, cuda, n):
+    import torch
+    layers = []
+    for i, (c, k, h) in enumerate(wino.RESNET_LAYER_SET):
+        x16, w16 = oracle_mod.make_inputs(n, c, h, h, k, seed=100 + i, x_dist="uniform",
+                                          w_std=np.sqrt(2.0 / (9 * c)))
+        x = torch.from_numpy(x16).to(cuda)
+        wt = torch.from_numpy(w16).to(cuda)
+        u = wino.filter_transform(wt)
+        ws = torch.empty(wino.fused_workspace_bytes(n, c, h, h), dtype=torch.uint8, device=cuda)
+        y = torch.full((n, k, h, h), float("nan"), dtype=torch.float16, device=cuda)
+        layers.append((x, wt, u, ws, y, k))
+    return layers
+
+
+def test_batched_layer_set_one_launch_graph_and_tuner(wino, cuda, oracle_mod):
+    """The 12-layer ResNet-style set at N=32 in one persistent launch."""
+    import torch
+    layers = _layer_set(wino, oracle_mod, cuda, 32)
+    refs = [wino.conv2d_fused(x, u, k) for (x, wt, u, ws, y, k) in layers]
+    b = wino.Batch()
+    for (x, wt, u, ws, y, k) in layers:
+        b.add(x, u, k, y, workspace=ws)
+    assert len(b) == 12
+
+    def check(tag):
+        torch.cuda.synchronize()
+        for i, ((x, wt, u, ws, y, k), r) in enumerate(zip(layers, refs)):
+            assert torch.equal(y.view(torch.int16), r.view(torch.int16)), (tag, i)
+            y.fill_(float("nan"))
+
+    b.run()
+    check("run")
+    for (x, wt, u, ws, y, k), r in zip(layers, refs):
+        _fp64_check(x, wt, r)
+    # mixed configurations and a reversed table order
+    for i in range(12):
+        b.set_config(i, i % wino.NCFG)
+    b.set_order(list(range(11, -1, -1)))
+    b.run()
+    check("mixed configs, reversed order")
+    # autotuner: timings for every configuration, then the best order
+    layer_us, order_us = b.tune(reps=2)
+    assert all(min(t for t in row if t > 0) > 0 for row in layer_us)
+    assert all(t > 0 for t in order_us)
+    for i in range(12):
+        row = layer_us[i]
+        assert row[b.config(i)] == min(t for t in row if t > 0)
+    assert sorted(b.order()) == list(range(12))
+    b.run()
+    check("tuned")
+    # CUDA graph of pre-passes + the persistent launch, replayed twice
+    b.capture()
+    b.launch()
+    check("graph 1")
+    b.launch()
+    check("graph 2")
+    b.close()
+    assert wino.error_read_clear() == 0
