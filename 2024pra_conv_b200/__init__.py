@@ -82,6 +82,8 @@ def lib():
             "wino_input_layout": ([vp, vp, i, i, i, i, vp], i),
             "wino_variant_workspace_bytes": ([i, i, i, i, i, i], sz),
             "wino_conv2d_fused_cfg": ([vp, vp, vp, vp, i, i, i, i, i, i, vp], i),
+            "wino_fused_cfg_workspace_bytes": ([i, i, i, i, i, i], sz),
+            "wino_fused_tune_workspace_bytes": ([i, i, i, i, i], sz),
             "wino_tune_layer": ([vp, vp, vp, vp, i, i, i, i, i, i, ctypes.POINTER(ctypes.c_float),
                                  ctypes.POINTER(i), vp], i),
             "wino_batch_create": ([ctypes.POINTER(vp)], i),
@@ -299,7 +301,11 @@ def conv2d_unfused(x, ucache2, k, ws=None, out=None, stream=None):
     return y
 
 
-CFG_KMAJOR, CFG_DIRECT, NCFG = 1, 2, 4
+CFG_KMAJOR, CFG_DIRECT, CFG_SPLIT_SHIFT, NCFG = 1, 2, 2, 16
+
+
+def cfg_split(level):
+    return level << CFG_SPLIT_SHIFT
 
 # The uneven ResNet-style 3x3 stride-1 pad-1 layer set of the batched launch,
 # as (C, K, H=W): two each of the four square stages plus the four C != K
@@ -313,20 +319,40 @@ def _p(t):
     return ctypes.c_void_p(0 if t is None else t.data_ptr())
 
 
+def _aligned_ws(nbytes, device):
+    """A uint8 workspace view starting on a 256-byte boundary (None for 0 bytes)."""
+    import torch
+    if nbytes == 0:
+        return None
+    buf = torch.empty(nbytes + 256, dtype=torch.uint8, device=device)
+    off = (-buf.data_ptr()) % 256
+    return buf[off:off + nbytes]
+
+
+def cfg_workspace_bytes(n, c, h, w, k, cfg) -> int:
+    return int(lib().wino_fused_cfg_workspace_bytes(n, c, h, w, k, cfg))
+
+
+def tune_workspace_bytes(n, c, h, w, k) -> int:
+    return int(lib().wino_fused_tune_workspace_bytes(n, c, h, w, k))
+
+
 def conv2d_fused_cfg(x, ucache, k, cfg, workspace=None, out=None, stream=None):
     """Fused fp16 conv on a cached U with a schedule configuration (CFG_* bits)."""
     import torch
     n, c, h, wd = x.shape
     y = out if out is not None else torch.empty((n, k, h, wd), dtype=torch.float16, device=x.device)
-    if workspace is None and not (cfg & CFG_DIRECT):
-        workspace = torch.empty(fused_workspace_bytes(n, c, h, wd), dtype=torch.uint8, device=x.device)
+    if workspace is None:
+        workspace = _aligned_ws(cfg_workspace_bytes(n, c, h, wd, k, cfg), x.device)
     _check(lib().wino_conv2d_fused_cfg(_p(x), _p(ucache), _p(workspace), _p(y), n, c, h, wd, k, cfg,
                                        _stream(stream)), "conv2d_fused_cfg")
     return y
 
 
 def tune_layer(x, ucache, k, workspace, out, reps=3, stream=None):
-    """Exhaustive tuning of one layer: (per-config mean us list, best cfg)."""
+    """Exhaustive tuning of one layer: (per-config mean us list, -1 outside
+    the tuning space; best cfg).  workspace: tune_workspace_bytes() bytes,
+    256-byte aligned (see _aligned_ws), or None for the direct configurations."""
     n, c, h, wd = x.shape
     us = (ctypes.c_float * NCFG)()
     best = ctypes.c_int(-1)

@@ -150,10 +150,24 @@ struct BlockInfo {
   Geometry g;
   const __half* x;          // NCHW input
   __half* y;                // NKPQ output
+  float* y32;               // split blocks: fp32 partial-sum output, else null
   const uint8_t* xb;        // XB records, or null (direct reads)
   const uint8_t* u;         // U cache
   int tb, kb;               // tile block, k block
+  int split, per;           // split index, 16-channel steps per split (per = 0: all)
 };
+
+// Steps [s0, s1) of a block for a kernel stepping `ch` channels at a time.
+__device__ __forceinline__ void block_steps(const BlockInfo& B, int ch, int& s0, int& s1) {
+  const int cs = B.g.C / ch;
+  if (B.per == 0) {
+    s0 = 0;
+    s1 = cs;
+  } else {
+    s0 = B.split * B.per;
+    s1 = min(cs, s0 + B.per);
+  }
+}
 
 __device__ __forceinline__ void block_coords(long long lb, const Geometry& g, int cfg, int& tb, int& kb) {
   if (cfg & CFG_KMAJOR) {
@@ -165,6 +179,7 @@ __device__ __forceinline__ void block_coords(long long lb, const Geometry& g, in
   }
 }
 
+// Work blocks of a layer: (tile block, k block, split), splits innermost.
 __device__ __forceinline__ BlockInfo make_block(const KernelParam& p, const Geometry& g, int cfg, long long lb) {
   BlockInfo B;
   B.g = g;
@@ -172,8 +187,26 @@ __device__ __forceinline__ BlockInfo make_block(const KernelParam& p, const Geom
   B.y = static_cast<__half*>(p.pout);
   B.xb = (cfg & CFG_DIRECT) ? nullptr : static_cast<const uint8_t*>(p.transform_pin);
   B.u = static_cast<const uint8_t*>(p.transform_filter);
+  int nsplit, per;
+  split_plan(cfg, g.CS, nsplit, per);
+  if (nsplit > 1) {
+    B.split = (int)(lb % nsplit);
+    lb /= nsplit;
+    B.per = per;
+    B.y32 = static_cast<float*>(p.mid_result);
+  } else {
+    B.split = 0;
+    B.per = 0;
+    B.y32 = nullptr;
+  }
   block_coords(lb, g, cfg, B.tb, B.kb);
   return B;
+}
+
+__device__ __forceinline__ long long layer_blocks(const Geometry& g, int cfg) {
+  int nsplit, per;
+  split_plan(cfg, g.CS, nsplit, per);
+  return g.nblocks * nsplit;
 }
 
 // One layer (the drop-in and single-conv entry points).
@@ -181,7 +214,7 @@ struct OneLayer {
   KernelParam p;
   Geometry g;
   int cfg;
-  __device__ long long total() const { return g.nblocks; }
+  __device__ long long total() const { return layer_blocks(g, cfg); }
   __device__ BlockInfo get(long long b) const { return make_block(p, g, cfg, b); }
 };
 
@@ -270,12 +303,13 @@ __device__ __forceinline__ void fused_body(const Sched& sched, const VariantArgs
       bool ok = true;
       for (long long b = blockIdx.x; b < nblocks && ok; b += gridDim.x, ++bi) {
         const BlockInfo B = sched.get(b);
-        const int CS = B.g.C / T::CH;          // steps of the block
+        int s0, s1;                            // steps of the block
+        block_steps(B, T::CH, s0, s1);
         const uint32_t astep = (uint32_t)(kblock_rows(B.kb, B.g.K) * 32) >> 4;
-        for (int s = 0; s < CS && ok; ++s, ++it) {
+        for (int s = s0; s < s1 && ok; ++s, ++it) {
           const uint32_t vs = it % NVSLOT;
           ok = mbar_wait(&sh.vfull[vs], (it / NVSLOT) & 1, abort_flag, err, ERR_WAIT_FULL);
-          const bool first_step = s == 0 && bi > 0;
+          const bool first_step = s == s0 && bi > 0;
 #pragma unroll
           for (int j = 0; j < T::UP; ++j) {
             if (!ok) break;
@@ -286,7 +320,7 @@ __device__ __forceinline__ void fused_body(const Sched& sched, const VariantArgs
             const uint64_t ad = adesc0 + ((us * U_HALF_BYTES) >> 4);
             const uint64_t bd = bdesc0 + ((vs * V_SLOT_BYTES + 8 * h * V_TAP_BYTES) >> 4);
             const uint32_t d = tmem + 8 * h * TILES;
-            const uint32_t acc = (s > 0 || j >= 2) ? 1u : 0u;
+            const uint32_t acc = (s > s0 || j >= 2) ? 1u : 0u;
             if (first_step && j < 2) {
               // the previous block's epilogue hands back each tap half of TMEM
               if (!mbar_wait(&sh.tapfree[h], (bi - 1) & 1, abort_flag, err, ERR_WAIT_DRAIN)) {
@@ -303,7 +337,7 @@ __device__ __forceinline__ void fused_body(const Sched& sched, const VariantArgs
                 mma_f16(d + tt * TILES, ad + tt * astep, bd + tt * BSTEP, idesc, acc);
             }
             // after the block's last MMAs of a tap half the epilogue may drain it
-            if (s == CS - 1 && j >= T::UP - 2) mma_commit(&sh.accf[h]);
+            if (s == s1 - 1 && j >= T::UP - 2) mma_commit(&sh.accf[h]);
           }
           if (ok) mma_commit(&sh.sdone[it % NSD]);
         }
@@ -319,12 +353,13 @@ __device__ __forceinline__ void fused_body(const Sched& sched, const VariantArgs
       for (long long b = blockIdx.x; b < nblocks && ok; b += gridDim.x) {
         const BlockInfo B = sched.get(b);
         const Geometry& g = B.g;
-        const int CS = g.C / T::CH;
+        int s0, s1;
+        block_steps(B, T::CH, s0, s1);
         const uint8_t* ubase = (VAR == VAR_F16_HILO && j >= 2) ? static_cast<const uint8_t*>(va.u_lo) : B.u;
         const int kb = B.kb;
         const int kbs = kblock_rows(kb, g.K);
         const uint32_t bytes = 8 * kbs * 32;  // 8 taps x kbs rows x 32 B
-        for (int s = 0; s < CS; ++s, ++it) {
+        for (int s = s0; s < s1; ++s, ++it) {
           const uint32_t pi = T::UP * it + j, us = pi % NUH;
           if (pi >= NUH) {
             const uint32_t st = (pi - NUH) / T::UP;  // step that last used the slot
@@ -353,7 +388,8 @@ __device__ __forceinline__ void fused_body(const Sched& sched, const VariantArgs
     for (long long b = blockIdx.x; b < nblocks && ok; b += gridDim.x) {
       const BlockInfo B = sched.get(b);
       const Geometry& g = B.g;
-      const int CS = g.C / T::CH;
+      int s0, s1;
+      block_steps(B, T::CH, s0, s1);
       const uint8_t* XB = B.xb;
       const uint32_t RB = (uint32_t)xb_row_bytes(g.W);
       const size_t img_stride = (size_t)(g.C >> 4) * xb_rows(g.H) * RB;   // one image of XB
@@ -368,7 +404,7 @@ __device__ __forceinline__ void fused_body(const Sched& sched, const VariantArgs
       const uint8_t* src0 = XB + (size_t)(pl.n0 + seg) * img_stride + (size_t)cbi * cb_stride +
                             (size_t)(2 * ta) * RB;
       const uint32_t dst0 = (uint32_t)(cbi * pl.total_rows + rbase) * RB;
-      for (int s = 0; s < CS; ++s, ++it) {
+      for (int s = s0; s < s1; ++s, ++it) {
         const uint32_t j = it % NSLAB;
         if (it >= NSLAB &&
             !mbar_wait_warp(&sh.slabfree[j], ((it - NSLAB) / NSLAB) & 1, abort_flag, err, ERR_WAIT_EMPTY, 64)) {
@@ -403,7 +439,8 @@ __device__ __forceinline__ void fused_body(const Sched& sched, const VariantArgs
       // per-block quantities once per block, 32-bit
       const BlockInfo B = sched.get(b);
       const Geometry& g = B.g;
-      const int CS = g.C / T::CH;
+      int s0, s1;
+      block_steps(B, T::CH, s0, s1);
       const __half* X = B.x;
       const int tile0 = B.tb * TILES;
       const SlabPlan pl = slab_plan(g, tile0, TILES);
@@ -414,7 +451,7 @@ __device__ __forceinline__ void fused_body(const Sched& sched, const VariantArgs
       const uint32_t cb_off = VAR == VAR_F8 ? (uint32_t)(hh * pl.total_rows) * (uint32_t)xb_row_bytes(g.W) : 0u;
       const SlabWindow sw0 = slab_window(g, pl, tc, VAR == VAR_F8 ? 0 : hh);
       const SlabWindow sw1 = slab_window(g, pl, tc, 1);
-      for (int s = 0; s < CS && ok; ++s, ++it) {
+      for (int s = s0; s < s1 && ok; ++s, ++it) {
         const uint32_t j = it % NSLAB;
         const uint32_t vs = it % NVSLOT;
         if (!mbar_wait_warp(&sh.slabfull[j], (it / NSLAB) & 1, abort_flag, err, ERR_WAIT_FULL, 32)) {
@@ -564,6 +601,31 @@ __device__ __forceinline__ void fused_body(const Sched& sched, const VariantArgs
         }
       }
       if (!ok) break;
+      if (B.y32 != nullptr) {
+        // split block: add this block's fp32 partial outputs
+        const int kk = quarter * 32 + lane;
+        if (kk < kbs) {
+          const int per_img = g.TP * g.TQ;
+#pragma unroll
+          for (int jt = 0; jt < 16; ++jt) {
+            const int tile = (int)tb * TILES + half * 16 + jt;
+            if (tile < (int)g.NT) {
+              const int n = tile / per_img;
+              const int rr = tile - n * per_img;
+              const int ty = rr / g.TQ;
+              const int oy = 2 * ty, ox = 2 * (rr - ty * g.TQ);
+              float* o = B.y32 + (((size_t)n * g.K + (size_t)(kb * KB + kk)) * g.P + oy) * (size_t)g.Q + ox;
+              atomicAdd(o, y[jt][0]);
+              if (ox + 1 < g.Q) atomicAdd(o + 1, y[jt][1]);
+              if (oy + 1 < g.P) {
+                atomicAdd(o + g.Q, y[jt][2]);
+                if (ox + 1 < g.Q) atomicAdd(o + g.Q + 1, y[jt][3]);
+              }
+            }
+          }
+        }
+        continue;
+      }
       // Stores go through a 2 KB per-warp staging buffer, 8 tiles at a time:
       // thread k writes its outputs as [k][row][8 tiles] half2 (16-byte
       // chunks XOR-swizzled by k so the writes are conflict-free), then each
@@ -626,6 +688,13 @@ __device__ __forceinline__ void fused_body(const Sched& sched, const VariantArgs
     tc_fence_after();
     tmem_dealloc(tmem, 512);
   }
+}
+
+// Rounds the fp32 sums of split blocks to the fp16 output.
+__global__ void y32_to_f16_kernel(const float* __restrict__ y32, __half* __restrict__ y, long long count) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < count;
+       i += (long long)gridDim.x * blockDim.x)
+    y[i] = __float2half_rn(y32[i]);
 }
 
 // The drop-in kernel: its only argument is the plugin's parameter struct.
@@ -734,6 +803,26 @@ int wino_fused_launch_batch(const void* table_dev, long long total_blocks, unsig
 long long wino_fused_nblocks(int n, int h, int w, int k) {
   const long long nt = (long long)n * ((h + 1) / 2) * ((w + 1) / 2);
   return ((nt + fused::TILES - 1) / fused::TILES) * ((k + KB - 1) / KB);
+}
+
+// ... and with a schedule configuration (splits multiply the blocks).
+long long wino_fused_nblocks_cfg(int n, int c, int h, int w, int k, int cfg) {
+  int nsplit, per;
+  split_plan(cfg, c / 16, nsplit, per);
+  return wino_fused_nblocks(n, h, w, k) * nsplit;
+}
+
+int wino_fused_cfg_splits(int c, int cfg) {
+  int nsplit, per;
+  split_plan(cfg, c / 16, nsplit, per);
+  return nsplit;
+}
+
+int wino_launch_y32_to_f16(const float* y32, void* y, long long count, cudaStream_t stream) {
+  const long long blocks = (count + 255) / 256;
+  y32_to_f16_kernel<<<(unsigned)(blocks < (1LL << 20) ? blocks : (1LL << 20)), 256, 0, stream>>>(
+      y32, static_cast<__half*>(y), count);
+  return (int)cudaGetLastError();
 }
 
 uint32_t wino_fused_error_read_clear() {

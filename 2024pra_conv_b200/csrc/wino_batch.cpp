@@ -43,6 +43,9 @@ int wino_fused_prepare_variant(int variant);
 size_t wino_xb_bytes(int n, int c, int h, int w);
 long long wino_xb_items(int n, int c, int h, int w);
 long long wino_fused_nblocks(int n, int h, int w, int k);
+long long wino_fused_nblocks_cfg(int n, int c, int h, int w, int k, int cfg);
+int wino_fused_cfg_splits(int c, int cfg);
+int wino_launch_y32_to_f16(const float* y32, void* y, long long count, cudaStream_t stream);
 }
 
 namespace {
@@ -78,19 +81,40 @@ unsigned grid_for(long long blocks) {
   return (unsigned)std::max<long long>(1, std::min(blocks, sms));
 }
 
-// One layer with a schedule configuration: its pre-pass (unless direct) and
-// the fused kernel.
-int run_layer_cfg(const KernelParam& p0, int cfg, cudaStream_t s) {
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// Workspace of a configuration: the XB records (unless direct), then the
+// fp32 partial-sum output of split configurations.
+size_t cfg_workspace_bytes(int n, int c, int h, int w, int k, int cfg) {
+  size_t b = (cfg & wino::CFG_DIRECT) ? 0 : align256(wino_xb_bytes(n, c, h, w));
+  if (wino_fused_cfg_splits(c, cfg) > 1) b += (size_t)n * k * h * w * sizeof(float);
+  return b;
+}
+
+// One layer with a schedule configuration: zero the fp32 sums (split), the
+// pre-pass (unless direct), the fused kernel, the fp16 rounding (split).
+// `ws` holds cfg_workspace_bytes(..., cfg) bytes (may be null for a
+// direct, unsplit configuration).
+int run_layer_cfg(const KernelParam& p0, void* ws, int cfg, cudaStream_t s) {
   KernelParam p = p0;
-  if (!p.transform_pin) cfg |= wino::CFG_DIRECT;
-  if (cfg & wino::CFG_DIRECT) {
-    p.transform_pin = nullptr;
-  } else if (wino_launch_xb_layout(&p, s) != 0) {
-    return WINO_ECUDA;
+  if (!ws) cfg = (cfg | wino::CFG_DIRECT) & ~(3 << wino::CFG_SPLIT_SHIFT);
+  uint8_t* w8 = static_cast<uint8_t*>(ws);
+  const bool split = wino_fused_cfg_splits(p.c, cfg) > 1;
+  const long long ycount = (long long)p.n * p.k * p.h * p.w;
+  p.transform_pin = (cfg & wino::CFG_DIRECT) ? nullptr : w8;
+  p.mid_result = nullptr;
+  if (split) {
+    float* y32 = reinterpret_cast<float*>(
+        w8 + ((cfg & wino::CFG_DIRECT) ? 0 : align256(wino_xb_bytes(p.n, p.c, p.h, p.w))));
+    p.mid_result = y32;
+    if (cudaMemsetAsync(y32, 0, (size_t)ycount * sizeof(float), s) != cudaSuccess) return WINO_ECUDA;
   }
-  const long long nb = wino_fused_nblocks(p.n, p.h, p.w, p.k);
-  return wino_fused_launch_variant(WINO_VAR_F16, &p, nullptr, cfg, grid_for(nb), s) == 0 ? WINO_OK
-                                                                                          : WINO_ECUDA;
+  if (p.transform_pin && wino_launch_xb_layout(&p, s) != 0) return WINO_ECUDA;
+  const long long nb = wino_fused_nblocks_cfg(p.n, p.c, p.h, p.w, p.k, cfg);
+  if (wino_fused_launch_variant(WINO_VAR_F16, &p, nullptr, cfg, grid_for(nb), s) != 0) return WINO_ECUDA;
+  if (split && wino_launch_y32_to_f16(static_cast<const float*>(p.mid_result), p.pout, ycount, s) != 0)
+    return WINO_ECUDA;
+  return WINO_OK;
 }
 
 // Mean microseconds of `fn` over `reps` launches after one warm-up, on `s`.
@@ -185,30 +209,55 @@ Batch* as_batch(void* h) { return static_cast<Batch*>(h); }
 
 extern "C" {
 
+size_t wino_fused_cfg_workspace_bytes(int n, int c, int h, int w, int k, int cfg) {
+  if (cfg < 0 || cfg >= wino::NCFG || wino_check_shape(n, c, h, w, k) != WINO_OK) return 0;
+  return cfg_workspace_bytes(n, c, h, w, k, cfg);
+}
+
+// Bytes that serve every configuration (the tuner's workspace).
+size_t wino_fused_tune_workspace_bytes(int n, int c, int h, int w, int k) {
+  size_t m = 0;
+  for (int cfg = 0; cfg < wino::NCFG; ++cfg)
+    m = std::max(m, wino_fused_cfg_workspace_bytes(n, c, h, w, k, cfg));
+  return m;
+}
+
 int wino_conv2d_fused_cfg(const void* x, const void* ucache, void* workspace, void* y, int n, int c,
                           int h, int w, int k, int cfg, void* stream) {
   if (!x || !ucache || !y) return WINO_EINVAL;
   if (cfg < 0 || cfg >= wino::NCFG) return WINO_EINVAL;
-  if (workspace && (reinterpret_cast<uintptr_t>(workspace) & 15) != 0) return WINO_EINVAL;
+  if (workspace && (reinterpret_cast<uintptr_t>(workspace) & 255) != 0) return WINO_EINVAL;
   const int st = wino_check_shape(n, c, h, w, k);
   if (st != WINO_OK) return st;
-  if (workspace && wino_xb_items(n, c, h, w) >= (1LL << 31)) return WINO_EUNSUPPORTED;
-  return run_layer_cfg(layer_param(x, ucache, workspace, y, n, c, h, w, k), cfg, (cudaStream_t)stream);
+  if (!workspace && cfg_workspace_bytes(n, c, h, w, k, cfg) != 0) return WINO_EINVAL;
+  if (!(cfg & wino::CFG_DIRECT) && wino_xb_items(n, c, h, w) >= (1LL << 31)) return WINO_EUNSUPPORTED;
+  return run_layer_cfg(layer_param(x, ucache, nullptr, y, n, c, h, w, k), workspace, cfg,
+                       (cudaStream_t)stream);
 }
 
+// The tuning space: with a workspace every configuration without
+// CFG_DIRECT (direct reads never win when the pre-pass is available);
+// without one, the direct unsplit configurations.
 int wino_tune_layer(const void* x, const void* ucache, void* workspace, void* y, int n, int c, int h,
                     int w, int k, int reps, float* us_out, int* best_cfg, void* stream) {
   if (!x || !ucache || !y || !us_out || !best_cfg) return WINO_EINVAL;
   const int st = wino_check_shape(n, c, h, w, k);
   if (st != WINO_OK) return st;
-  const KernelParam p = layer_param(x, ucache, workspace, y, n, c, h, w, k);
+  if (workspace && (reinterpret_cast<uintptr_t>(workspace) & 255) != 0) return WINO_EINVAL;
+  const KernelParam p = layer_param(x, ucache, nullptr, y, n, c, h, w, k);
   const cudaStream_t s = (cudaStream_t)stream;
   int best = -1;
   for (int cfg = 0; cfg < wino::NCFG; ++cfg) {
     us_out[cfg] = -1.f;
-    if (!workspace && !(cfg & wino::CFG_DIRECT)) continue;
+    if (workspace ? (cfg & wino::CFG_DIRECT) != 0
+                  : (!(cfg & wino::CFG_DIRECT) || wino::cfg_split_level(cfg) != 0))
+      continue;
+    // a split level that gives the same splits as a lower one is skipped
+    if (wino::cfg_split_level(cfg) > 0 &&
+        wino_fused_cfg_splits(c, cfg) == wino_fused_cfg_splits(c, cfg - (1 << wino::CFG_SPLIT_SHIFT)))
+      continue;
     float us = 0.f;
-    const int rc = time_us([&] { return run_layer_cfg(p, cfg, s); }, reps, s, &us);
+    const int rc = time_us([&] { return run_layer_cfg(p, workspace, cfg, s); }, reps, s, &us);
     if (rc != WINO_OK) return rc;
     us_out[cfg] = us;
     if (best < 0 || us < us_out[best]) best = cfg;
@@ -258,7 +307,8 @@ int wino_batch_num_layers(void* h) {
 
 int wino_batch_set_config(void* h, int layer, int cfg) {
   Batch* b = as_batch(h);
-  if (!b || layer < 0 || layer >= (int)b->layers.size() || cfg < 0 || cfg >= wino::NCFG)
+  if (!b || layer < 0 || layer >= (int)b->layers.size() || cfg < 0 || cfg >= wino::NCFG ||
+      wino::cfg_split_level(cfg) != 0)
     return WINO_EINVAL;
   b->layers[layer].cfg = cfg;
   b->dirty = true;
@@ -317,9 +367,18 @@ int wino_batch_tune(void* h, int reps, float* layer_us, float* order_us, void* s
     Layer& L = b->layers[i];
     float us[wino::NCFG];
     int best = 0;
-    const int rc = wino_tune_layer(L.p.pin, L.p.transform_filter, L.p.transform_pin, L.p.pout, L.p.n,
-                                   L.p.c, L.p.h, L.p.w, L.p.k, reps, us, &best, stream);
-    if (rc != WINO_OK) return rc;
+    // batch layers run unsplit: time the configurations without splits
+    best = -1;
+    for (int cfg = 0; cfg < wino::NCFG; ++cfg) {
+      us[cfg] = -1.f;
+      if (wino::cfg_split_level(cfg) != 0) continue;
+      if (!L.p.transform_pin && !(cfg & wino::CFG_DIRECT)) continue;
+      float t = 0.f;
+      const int rc = time_us([&] { return run_layer_cfg(L.p, L.p.transform_pin, cfg, s); }, reps, s, &t);
+      if (rc != WINO_OK) return rc;
+      us[cfg] = t;
+      if (best < 0 || t < us[best]) best = cfg;
+    }
     L.cfg = best;
     L.tuned_us = us[best];
     if (layer_us)

@@ -357,8 +357,125 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": 4 * args.steps,
         "clocks": clocks,
     }
+    if world == 1 and not args.no_extras:
+        line["north_star"] = north_star_legs(wino, dev, flush, ev, peaks, max(args.steps, 5))
     print(json.dumps(line), flush=True)
     return 0
+
+
+def north_star_legs(wino, dev, flush, ev, peaks, steps):
+    """Rank-0 extras on the other workloads: the batched 12-layer ResNet-style
+    set (autotuned, one persistent launch, CUDA graph), the precision
+    variants on N64 C=K256 H14 with their errors against FP64, and the
+    learned cost model judged against exhaustive tuning on the committed
+    timings.  Not part of `value`."""
+    import numpy as np
+    import torch
+    import oracle
+    out = {}
+    stream = torch.cuda.current_stream()
+
+    def timed(fn, iters, do_flush=True):
+        ts = []
+        for _ in range(iters):
+            if do_flush:
+                flush.zero_()
+            a, b = ev(), ev()
+            a.record(stream)
+            fn()
+            b.record(stream)
+            b.synchronize()
+            ts.append(a.elapsed_time(b))
+        return statistics.median(ts) * 1e3  # us
+
+    # --- batched layer set, N=32
+    n = 32
+    layers = []
+    dfl = 0.0
+    t_roof = 0.0          # sum over layers of max(t_HBM, t_tensor)
+    n_tc = 0
+    for i, (c, k, h) in enumerate(wino.RESNET_LAYER_SET):
+        x16, w16 = oracle.make_inputs(n, c, h, h, k, seed=100 + i, x_dist="uniform",
+                                      w_std=np.sqrt(2.0 / (9 * c)))
+        x = torch.from_numpy(x16).to(dev)
+        wt = torch.from_numpy(w16).to(dev)
+        u = wino.filter_transform(wt)
+        ws = torch.empty(wino.fused_workspace_bytes(n, c, h, h), dtype=torch.uint8, device=dev)
+        y = torch.empty((n, k, h, h), dtype=torch.float16, device=dev)
+        layers.append((x, wt, u, ws, y, c, k, h))
+        dfl += direct_flops(n, c, h, h, k)
+        byt = 2.0 * (n * c * h * h + n * k * h * h + 16 * k * c)
+        t_hbm = byt / (peaks["hbm_gbs"] * 1e9)
+        t_tc = wino_flops(n, c, h, h, k) / (peaks["tflops"] * 1e12)
+        t_roof += max(t_hbm, t_tc)
+        n_tc += t_tc > t_hbm
+    seq_us = timed(lambda: [wino.conv2d_fused(x, u, k, out=y, workspace=ws)
+                            for (x, wt, u, ws, y, c, k, h) in layers], steps)
+    b = wino.Batch()
+    for (x, wt, u, ws, y, c, k, h) in layers:
+        b.add(x, u, k, y, workspace=ws)
+    b.run()
+    untuned_us = timed(b.run, steps)
+    layer_us, order_us = b.tune(reps=3)
+    b.capture()
+    b.launch()
+    torch.cuda.synchronize()
+    graph_us = timed(b.launch, steps)
+    worst = 0.0
+    for (x, wt, u, ws, y, c, k, h) in layers:
+        y64 = torch.nn.functional.conv2d(x.double(), wt.double(), padding=1)
+        worst = max(worst, float(torch.linalg.vector_norm(y.double() - y64) / torch.linalg.vector_norm(y64)))
+    out["layer_set"] = {
+        "workload": "12 ResNet-style 3x3 s1 p1 layers at N=32, (C,K,H): " +
+                    ", ".join(f"({c},{k},{h})" for (c, k, h) in wino.RESNET_LAYER_SET),
+        "us_graph_tuned": graph_us, "us_persistent_untuned": untuned_us, "us_sequential_launches": seq_us,
+        "direct_equiv_tflops": dfl / (graph_us * 1e-6) / 1e12,
+        "configs": [b.config(i) for i in range(len(layers))], "order": b.order(),
+        "order_us": order_us, "worst_rel_l2": worst,
+        "roofline": {"per_layer_bound": f"{n_tc} of 12 layers tensor-bound, the rest HBM-bound",
+                     "target_us": t_roof * 1e6, "frac": t_roof * 1e6 / graph_us,
+                     "definition": "sum over layers of max(HBM bytes / hbm_gbs, Winograd FLOPs / "
+                                   "bf16_tflops) over the measured time"},
+        "l2": "flushed between steps"}
+    b.close()
+    del layers
+
+    # --- precision variants, N64 C=K256 H14 (uniform inputs)
+    x16, w16 = oracle.make_inputs(64, 256, 14, 14, 256, seed=0, x_dist="uniform",
+                                  w_std=np.sqrt(2.0 / (9 * 256)))
+    x = torch.from_numpy(x16).to(dev)
+    wt = torch.from_numpy(w16).to(dev)
+    y64 = torch.nn.functional.conv2d(x.double(), wt.double(), padding=1)
+    var = {}
+    for name, v in [("f16", wino.VAR_F16), ("bf16", wino.VAR_BF16), ("f8_e4m3", wino.VAR_F8),
+                    ("f16_hilo", wino.VAR_F16_HILO)]:
+        ws = torch.empty(wino.variant_workspace_bytes(v, 64, 256, 14, 14, 256) + 256, dtype=torch.uint8,
+                         device=dev)
+        y = torch.empty((64, 256, 14, 14), dtype=torch.float16, device=dev)
+        wino.conv2d_variant(x, wt, v, out=y, workspace=ws)
+        torch.cuda.synchronize()
+        d = y.double() - y64
+        us = timed(lambda: wino.conv2d_variant(x, wt, v, out=y, workspace=ws), steps)
+        var[name] = {"us_per_call": us, "rel_l2": float(torch.linalg.vector_norm(d) / torch.linalg.vector_norm(y64)),
+                     "max_norm": float(d.abs().max() / y64.abs().max()),
+                     "direct_equiv_tflops": direct_flops(64, 256, 14, 14, 256) / (us * 1e-6) / 1e12}
+    out["variants"] = {"workload": "N64 C256 H14 W14 K256, x ~ U[-1,1]; per call: filter transform "
+                                   "+ input pre-pass + fused kernel", **var}
+
+    # --- learned cost model vs exhaustive tuning (committed timings)
+    path = os.path.join(ROOT, "tests", "golden", "tuning_timings.json")
+    if os.path.exists(path):
+        cm = importlib.import_module("2024pra_conv_b200.costmodel")
+        with open(path) as f:
+            rows = json.load(f)["rows"]
+        r = cm.evaluate(rows)
+        r.pop("regret")
+        out["cost_model"] = {"data": "exhaustive tuning timings of 400 seeded shapes "
+                                     "(tests/golden/tuning_timings.json), 300 train / 100 held out", **r}
+    err = wino.error_read_clear()
+    if err:
+        raise SystemExit(f"device error word {err}")
+    return out
 
 
 def run_only(args):
@@ -401,6 +518,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--soak", type=float, default=1.0, help="seconds of untimed load before timing")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the layer-set / variants / cost-model legs")
     ap.add_argument("--only", choices=["fused", "unfused", "dropin"],
                     help="only launch this path (profiler captures)")
     ap.add_argument("--n", type=int, default=0, help="batch size for --only")

@@ -99,20 +99,34 @@ int wino_conv2d_variant(int variant, const void* x, const void* weight, void* y,
 /* Schedule configurations of the fused kernel (bits): WINO_CFG_KMAJOR orders
  * the work blocks k-block-major (consecutive blocks share U) instead of
  * tile-major (they share input tiles); WINO_CFG_DIRECT makes the producers
- * read the NCHW input directly instead of the pre-pass workspace.  Every
- * configuration computes bit-identical results. */
-enum { WINO_CFG_KMAJOR = 1, WINO_CFG_DIRECT = 2, WINO_NCFG = 4 };
+ * read the NCHW input directly instead of the pre-pass workspace; bits 2-3
+ * (WINO_CFG_SPLIT(L)) split each block's 16-channel steps over up to 4^L CTAs
+ * that add fp32 partial outputs, rounded to fp16 by a second pass -- for
+ * layers with too few blocks to fill the GPU.  Unsplit configurations
+ * compute bit-identical results; split ones differ only in the fp32
+ * summation order. */
+enum { WINO_CFG_KMAJOR = 1, WINO_CFG_DIRECT = 2, WINO_CFG_SPLIT_SHIFT = 2, WINO_NCFG = 16 };
+#define WINO_CFG_SPLIT(level) ((level) << WINO_CFG_SPLIT_SHIFT)
 
-/* One fp16 conv on a cached U with a schedule configuration; workspace
- * (wino_fused_workspace_bytes, may be NULL for WINO_CFG_DIRECT) receives the
- * pre-pass output. */
+/* Workspace of one configuration (pre-pass records unless direct, then the
+ * fp32 sums of split configurations; 0 = none needed) and the size that
+ * serves every configuration (for wino_tune_layer). */
+size_t wino_fused_cfg_workspace_bytes(int n, int c, int h, int w, int k, int cfg);
+size_t wino_fused_tune_workspace_bytes(int n, int c, int h, int w, int k);
+
+/* One fp16 conv on a cached U with a schedule configuration; workspace:
+ * wino_fused_cfg_workspace_bytes() bytes, 256-byte aligned (NULL allowed
+ * when that is 0). */
 int wino_conv2d_fused_cfg(const void* x, const void* ucache, void* workspace, void* y, int n, int c,
                           int h, int w, int k, int cfg, void* stream);
 
 /* Exhaustive tuning of one layer: mean microseconds of every configuration
- * (us_out[WINO_NCFG]; -1 where not applicable, i.e. no workspace) over
- * `reps` runs after one warm-up, and the fastest in *best_cfg.  Synchronises
- * `stream`; not inside a stream capture. */
+ * of the tuning space (us_out[WINO_NCFG], -1 for configurations outside it)
+ * over `reps` runs after one warm-up, and the fastest in *best_cfg.  With a
+ * workspace (wino_fused_tune_workspace_bytes) the space is every
+ * configuration without WINO_CFG_DIRECT, split levels that give the same
+ * number of splits as a lower one left out; without one, the two direct
+ * unsplit configurations.  Synchronises `stream`; not inside a capture. */
 int wino_tune_layer(const void* x, const void* ucache, void* workspace, void* y, int n, int c, int h,
                     int w, int k, int reps, float* us_out, int* best_cfg, void* stream);
 
@@ -122,8 +136,9 @@ int wino_tune_layer(const void* x, const void* ucache, void* workspace, void* y,
  * and (optional) pre-pass workspace; wino_batch_run issues the pre-passes and
  * ONE persistent fused-kernel launch over all layers' work blocks (a device
  * layer table); wino_batch_graph_capture records that sequence in a CUDA
- * graph, wino_batch_graph_launch replays it.  wino_batch_tune runs the
- * autotuner: per layer the fastest configuration (exhaustive), then the
+ * graph, wino_batch_graph_launch replays it.  Batch layers run unsplit.
+ * wino_batch_tune runs the autotuner: per layer the fastest unsplit
+ * configuration (exhaustive), then the
  * fastest table order among {as added, longest first, longest/shortest
  * interleaved}; layer_us receives nlayers x WINO_NCFG timings, order_us the
  * three whole-batch timings (either may be NULL).  Configuration and order

@@ -20,8 +20,11 @@ def _fp64_check(x, w, y):
     assert rl2 <= 2e-3 and mxn <= 1e-2, (rl2, mxn)
 
 
-@pytest.mark.parametrize("shape", [(4, 64, 20, 20, 144), (2, 32, 7, 7, 32), (1, 16, 6, 224, 16)])
-def test_configs_bit_identical(wino, cuda, oracle_mod, shape):
+@pytest.mark.parametrize("shape", [(4, 64, 20, 20, 144), (2, 32, 7, 7, 32), (1, 16, 6, 224, 16),
+                                   (1, 256, 10, 10, 64)])
+def test_configs(wino, cuda, oracle_mod, shape):
+    """Unsplit configurations: bit-identical to the default path.  Split
+    ones (fp32 partial sums added in another order): FP64 parity."""
     import torch
     n, c, h, w, k = shape
     x16, w16 = oracle_mod.make_inputs(n, c, h, w, k, seed=7, x_dist="normal")
@@ -32,8 +35,29 @@ def test_configs_bit_identical(wino, cuda, oracle_mod, shape):
     for cfg in range(wino.NCFG):
         y = wino.conv2d_fused_cfg(x, u, k, cfg)
         torch.cuda.synchronize()
-        assert torch.equal(y.view(torch.int16), ref.view(torch.int16)), cfg
+        if (cfg >> wino.CFG_SPLIT_SHIFT) == 0 or c == 16:
+            assert torch.equal(y.view(torch.int16), ref.view(torch.int16)), cfg
+        else:
+            _fp64_check(x, wt, y)
     _fp64_check(x, wt, ref)
+    assert wino.error_read_clear() == 0
+
+
+def test_tune_layer_space(wino, cuda, oracle_mod):
+    import torch
+    n, c, h, w, k = 1, 512, 14, 14, 128
+    x16, w16 = oracle_mod.make_inputs(n, c, h, w, k, seed=9, x_dist="uniform")
+    x = torch.from_numpy(x16).to(cuda)
+    u = wino.filter_transform(torch.from_numpy(w16).to(cuda))
+    y = torch.empty((n, k, h, w), dtype=torch.float16, device=cuda)
+    ws = wino._aligned_ws(wino.tune_workspace_bytes(n, c, h, w, k), cuda)
+    us, best = wino.tune_layer(x, u, k, ws, y, reps=1)
+    timed = [i for i, t in enumerate(us) if t > 0]
+    assert all(not (i & wino.CFG_DIRECT) for i in timed)
+    assert {0, 1, wino.cfg_split(1), wino.cfg_split(2), wino.cfg_split(3)} <= set(timed)
+    assert best in timed and us[best] == min(us[i] for i in timed)
+    us2, best2 = wino.tune_layer(x, u, k, None, y, reps=1)
+    assert [i for i, t in enumerate(us2) if t > 0] == [wino.CFG_DIRECT, wino.CFG_DIRECT | 1]
     assert wino.error_read_clear() == 0
 
 
@@ -74,7 +98,7 @@ def test_batched_layer_set_one_launch_graph_and_tuner(wino, cuda, oracle_mod):
         _fp64_check(x, wt, r)
     # mixed configurations and a reversed table order
     for i in range(12):
-        b.set_config(i, i % wino.NCFG)
+        b.set_config(i, i % 4)      # unsplit configurations: batch layers run unsplit
     b.set_order(list(range(11, -1, -1)))
     b.run()
     check("mixed configs, reversed order")
