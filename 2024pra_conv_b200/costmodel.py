@@ -130,12 +130,11 @@ def _stream():
     return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
 
 
-def mlp_forward(params, x):
+def mlp_forward(params, x, O=NCFG):
     """params, x: cuda float32 tensors -> predictions [B, O]."""
     import torch
     L = _lib()
     B = x.shape[0]
-    O = NCFG
     y = torch.empty((B, O), dtype=torch.float32, device=x.device)
     rc = L.wino_mlp_forward(_ptr(params), _ptr(x), _ptr(y), B, x.shape[1], O, _stream())
     if rc:

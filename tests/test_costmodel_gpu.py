@@ -32,7 +32,7 @@ def test_mlp_forward_and_gradient_match_cpu_oracle(cuda, seed):
     cm = _cm()
     p, x, t, m = _batch(seed)
     T = lambda a: torch.from_numpy(a).to(cuda)
-    y = cm.mlp_forward(T(p), T(x)).cpu().numpy()
+    y = cm.mlp_forward(T(p), T(x), O=4).cpu().numpy()
     y64, _ = M.forward(p.astype(np.float64), x.astype(np.float64), 6, 4)
     assert np.allclose(y, y64, rtol=1e-4, atol=1e-5)
     loss, g = cm.mlp_grad(T(p), T(x), T(t), T(m))
