@@ -1,6 +1,8 @@
 // Input re-layout pre-pass for the fused kernel: NCHW fp16 -> XB records
 // (layout described in vgen.cuh), zero outside the image.  For the fp8
-// variant it also records the per-channel max |x| (p.mid_result non-null).
+// variant a second instantiation also records the per-channel max |x| into
+// p.mid_result (the plain one never touches that field, which in the
+// drop-in parameter struct is the caller's workspace).
 //
 // The reference's pipeline also writes an intermediate form of the input into
 // the caller's `transform_pin` workspace before its GEMMs (the transformed
@@ -23,6 +25,7 @@
 
 namespace wino {
 
+template <bool AMAX>
 __global__ void __launch_bounds__(256) xb_layout_kernel(KernelParam p) {
   const int C = p.c, H = p.h, W = p.w;
   const int CB = C >> 4, HP = xb_rows(H), E = xb_entries(W);
@@ -32,7 +35,7 @@ __global__ void __launch_bounds__(256) xb_layout_kernel(KernelParam p) {
   const size_t plane = (size_t)H * W;
   const bool w_even = (W & 1) == 0;
   // optional (fp8 variant): per-channel max |x| as fp16 magnitude bits
-  unsigned* amax = static_cast<unsigned*>(p.mid_result);
+  unsigned* amax = AMAX ? static_cast<unsigned*>(p.mid_result) : nullptr;
   for (uint32_t it = blockIdx.x * blockDim.x + threadIdx.x; it < items; it += gridDim.x * blockDim.x) {
     const uint32_t rec = it / E;
     const int e = (int)(it - rec * E);
@@ -60,7 +63,7 @@ __global__ void __launch_bounds__(256) xb_layout_kernel(KernelParam p) {
         hi[i] = ok1 ? src[i * plane + 1] : 0u;
       }
     }
-    if (amax != nullptr) {
+    if (AMAX) {
       // per-channel max |x| (fp16 magnitude bits order like the values):
       // reduced over the warp when all its lanes hold the same channel block
       const unsigned act = __activemask();
@@ -123,7 +126,7 @@ using namespace wino;
 
 extern "C" {
 
-void* wino_xb_layout_kernel_ptr() { return (void*)xb_layout_kernel; }
+void* wino_xb_layout_kernel_ptr() { return (void*)xb_layout_kernel<false>; }
 
 size_t wino_xb_bytes(int n, int c, int h, int w) { return xb_bytes(n, c, h, w); }
 
@@ -148,8 +151,16 @@ int wino_launch_xb_f8_scales(const unsigned* amax, float* sv, uint32_t* inv_sv2,
 
 int wino_launch_xb_layout(const KernelParam* p, cudaStream_t stream) {
   void* args[] = {const_cast<KernelParam*>(p)};
-  return (int)cudaLaunchKernel((void*)xb_layout_kernel, dim3(wino_xb_layout_grid(p->n, p->c, p->h, p->w)),
-                               dim3(256), args, 0, stream);
+  return (int)cudaLaunchKernel((void*)xb_layout_kernel<false>,
+                               dim3(wino_xb_layout_grid(p->n, p->c, p->h, p->w)), dim3(256), args, 0, stream);
+}
+
+// The fp8 variant's pre-pass: also the per-channel max |x| into p->mid_result
+// (C unsigned words, zeroed by the caller).
+int wino_launch_xb_layout_amax(const KernelParam* p, cudaStream_t stream) {
+  void* args[] = {const_cast<KernelParam*>(p)};
+  return (int)cudaLaunchKernel((void*)xb_layout_kernel<true>,
+                               dim3(wino_xb_layout_grid(p->n, p->c, p->h, p->w)), dim3(256), args, 0, stream);
 }
 
 }  // extern "C"

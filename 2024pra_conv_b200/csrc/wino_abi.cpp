@@ -60,6 +60,7 @@ size_t wino_xb_bytes(int n, int c, int h, int w);
 unsigned wino_xb_layout_grid(int n, int c, int h, int w);
 long long wino_xb_items(int n, int c, int h, int w);
 int wino_launch_xb_layout(const wino::KernelParam* p, cudaStream_t stream);
+int wino_launch_xb_layout_amax(const wino::KernelParam* p, cudaStream_t stream);
 int wino_launch_xb_f8_scales(const unsigned* amax, float* sv, uint32_t* inv_sv2, int C,
                              cudaStream_t stream);
 int wino_launch_filter_transform_f8(const void* weight, const float* sv, void* u8, float* su, int K,
@@ -381,7 +382,7 @@ extern "C" int wino_conv2d_variant(int variant, const void* x, const void* weigh
       if (cudaMemsetAsync(amax, 0, (size_t)c * sizeof(unsigned), s) != cudaSuccess) return WINO_ECUDA;
       wino::KernelParam pl = p;
       pl.mid_result = amax;
-      if (wino_launch_xb_layout(&pl, s) != 0) return WINO_ECUDA;
+      if (wino_launch_xb_layout_amax(&pl, s) != 0) return WINO_ECUDA;
       float* sv = reinterpret_cast<float*>(ws + L.sv);
       uint32_t* inv = reinterpret_cast<uint32_t*>(ws + L.inv);
       float* su = reinterpret_cast<float*>(ws + L.su);

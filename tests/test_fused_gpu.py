@@ -187,6 +187,20 @@ def test_input_layout_prepass_bit_exact(wino, cuda, oracle_mod, shape):
     assert np.array_equal(got, ref.view(np.uint16).reshape(-1))
 
 
+def test_dropin_leaves_caller_mid_result_untouched(wino, cuda, oracle_mod):
+    """The drop-in kernels write only transform_filter (U), transform_pin
+    (the pre-pass records) and the output; the caller's mid_result workspace
+    keeps its contents."""
+    import torch
+    x, w = oracle_mod.make_inputs(2, 32, 12, 10, 32, seed=6, x_dist="normal")
+    ws = wino.DropinWorkspaces(2, 32, 12, 10, 32, cuda)
+    ws.mid_result.fill_(1.25)
+    y = wino.dropin_conv2d(_t(x, cuda), _t(w, cuda), ws=ws)
+    torch.cuda.synchronize()
+    assert bool((ws.mid_result == 1.25).all())
+    _check(oracle_mod, y.cpu().numpy(), oracle_mod.conv2d_f64(x, w), "drop-in")
+
+
 def test_dropin_without_transform_pin(wino, cuda, oracle_mod):
     import torch
     x, w = oracle_mod.make_inputs(2, 32, 12, 10, 32, seed=5, x_dist="normal")
