@@ -65,6 +65,18 @@
 #include "vgen.cuh"
 #include "wino_batch.h"
 
+// Back-off (ns) between polls of a waiting warp once its wait is long:
+// producers, stager, epilogue.
+#ifndef WINO_SLEEP_PROD
+#define WINO_SLEEP_PROD 32
+#endif
+#ifndef WINO_SLEEP_STAGE
+#define WINO_SLEEP_STAGE 64
+#endif
+#ifndef WINO_SLEEP_EPI
+#define WINO_SLEEP_EPI 64
+#endif
+
 namespace wino {
 
 static __device__ uint32_t g_fused_err;
@@ -407,7 +419,7 @@ __device__ __forceinline__ void fused_body(const Sched& sched, const VariantArgs
       for (int s = s0; s < s1; ++s, ++it) {
         const uint32_t j = it % NSLAB;
         if (it >= NSLAB &&
-            !mbar_wait_warp(&sh.slabfree[j], ((it - NSLAB) / NSLAB) & 1, abort_flag, err, ERR_WAIT_EMPTY, 64)) {
+            !mbar_wait_warp(&sh.slabfree[j], ((it - NSLAB) / NSLAB) & 1, abort_flag, err, ERR_WAIT_EMPTY, WINO_SLEEP_STAGE)) {
           ok = false;
           break;
         }
@@ -454,13 +466,13 @@ __device__ __forceinline__ void fused_body(const Sched& sched, const VariantArgs
       for (int s = s0; s < s1 && ok; ++s, ++it) {
         const uint32_t j = it % NSLAB;
         const uint32_t vs = it % NVSLOT;
-        if (!mbar_wait_warp(&sh.slabfull[j], (it / NSLAB) & 1, abort_flag, err, ERR_WAIT_FULL, 32)) {
+        if (!mbar_wait_warp(&sh.slabfull[j], (it / NSLAB) & 1, abort_flag, err, ERR_WAIT_FULL, WINO_SLEEP_PROD)) {
           ok = false;
           break;
         }
         if (it >= NVSLOT &&
             !mbar_wait_warp(&sh.sdone[(it - NVSLOT) % NSD], ((it - NVSLOT) / NSD) & 1, abort_flag, err,
-                            ERR_WAIT_EMPTY, 32)) {
+                            ERR_WAIT_EMPTY, WINO_SLEEP_PROD)) {
           ok = false;
           break;
         }
@@ -569,7 +581,7 @@ __device__ __forceinline__ void fused_body(const Sched& sched, const VariantArgs
 #pragma unroll
       for (int t = 0; t < NTAP; ++t) {
         if ((t & 7) == 0) {
-          if (!mbar_wait_warp(&sh.accf[t >> 3], bi & 1, abort_flag, err, ERR_WAIT_ACCUM, 64)) {
+          if (!mbar_wait_warp(&sh.accf[t >> 3], bi & 1, abort_flag, err, ERR_WAIT_ACCUM, WINO_SLEEP_EPI)) {
             ok = false;
             break;
           }
