@@ -128,3 +128,33 @@ def test_batch_host_validation(wino):
         assert L.wino_batch_add_layer(h, dummy, dummy, None, dummy, 1, 16, 4, 4, 16) == 0
     assert L.wino_batch_add_layer(h, dummy, dummy, None, dummy, 1, 16, 4, 4, 16) == 2     # 33rd
     assert L.wino_batch_destroy(h) == 0
+
+
+def test_split_configuration_sizes(wino):
+    """Host arithmetic of the schedule configurations (no GPU): workspace
+    bytes, split counts (every split non-empty) and work blocks."""
+    L = wino.lib()
+    L.wino_fused_nblocks_cfg.argtypes = [ctypes.c_int] * 6
+    L.wino_fused_nblocks_cfg.restype = ctypes.c_longlong
+    L.wino_fused_cfg_splits.argtypes = [ctypes.c_int, ctypes.c_int]
+    L.wino_fused_nblocks.argtypes = [ctypes.c_int] * 4
+    L.wino_fused_nblocks.restype = ctypes.c_longlong
+    n, c, h, w, k = 2, 256, 14, 14, 64
+    xb = wino.fused_workspace_bytes(n, c, h, w)
+    al = lambda b: (b + 255) // 256 * 256
+    y32 = n * k * h * w * 4
+    assert wino.cfg_workspace_bytes(n, c, h, w, k, 0) == al(xb)
+    assert wino.cfg_workspace_bytes(n, c, h, w, k, wino.CFG_KMAJOR) == al(xb)
+    assert wino.cfg_workspace_bytes(n, c, h, w, k, wino.CFG_DIRECT) == 0
+    assert wino.cfg_workspace_bytes(n, c, h, w, k, wino.cfg_split(1)) == al(xb) + y32
+    assert wino.cfg_workspace_bytes(n, c, h, w, k, wino.CFG_DIRECT | wino.cfg_split(2)) == y32
+    assert wino.tune_workspace_bytes(n, c, h, w, k) == al(xb) + y32
+    # 16 steps: 4^L wanted -> 1, 4, 16, 16 splits; 1 step: never split
+    assert [L.wino_fused_cfg_splits(256, wino.cfg_split(l)) for l in range(4)] == [1, 4, 16, 16]
+    assert [L.wino_fused_cfg_splits(16, wino.cfg_split(l)) for l in range(4)] == [1, 1, 1, 1]
+    assert L.wino_fused_cfg_splits(48, wino.cfg_split(1)) == 3          # 3 steps, one each
+    assert wino.cfg_workspace_bytes(1, 16, 8, 8, 16, wino.cfg_split(3)) == al(wino.fused_workspace_bytes(1, 16, 8, 8))
+    base = L.wino_fused_nblocks(n, h, w, k)
+    assert L.wino_fused_nblocks_cfg(n, c, h, w, k, wino.cfg_split(2)) == 16 * base
+    assert L.wino_fused_nblocks_cfg(n, c, h, w, k, wino.CFG_KMAJOR) == base
+    assert wino.cfg_workspace_bytes(n, 24, h, w, k, 0) == 0               # bad shape
