@@ -7,7 +7,7 @@ log-time per configuration (16 outputs, masked to the configurations
 timed) -- is trained on those timings with the
 library's own CUDA kernels (csrc/mlp.cu: forward, backward, Adam) and picks
 a configuration for unseen shapes without timing them; exhaustive tuning
-stays the fallback and the judge of its picks.  The reference has no
+stays the fallback and the yardstick of its picks.  The reference has no
 counterpart (one hard-wired kernel set per shape, src/conv2d.cpp:458-494).
 
 Shape space (400 seeded shapes, 300 train / 100 held out): N in {1, 8, 32,

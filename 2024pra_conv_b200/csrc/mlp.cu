@@ -2,7 +2,7 @@
 // outputs, fp32) trained and evaluated with hand-written CUDA kernels.  It
 // maps shape features of a conv layer to the predicted log-time of each
 // schedule configuration; the autotuner's exhaustive timings are its
-// training data and remain the fallback and the judge of its picks.  The
+// training data and remain the fallback and the yardstick of its picks.  The
 // reference has no counterpart (it hard-wires one kernel set per shape,
 // src/conv2d.cpp:458-494).
 //

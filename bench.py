@@ -358,16 +358,16 @@ def run_ours(args, rank, world, local_rank):
         "clocks": clocks,
     }
     if world == 1 and not args.no_extras:
-        line["north_star"] = north_star_legs(wino, dev, flush, ev, peaks, max(args.steps, 5))
+        line["extensions"] = extension_legs(wino, dev, flush, ev, peaks, max(args.steps, 5))
     print(json.dumps(line), flush=True)
     return 0
 
 
-def north_star_legs(wino, dev, flush, ev, peaks, steps):
+def extension_legs(wino, dev, flush, ev, peaks, steps):
     """Rank-0 extras on the other workloads: the batched 12-layer ResNet-style
     set (autotuned, one persistent launch, CUDA graph), the precision
     variants on N64 C=K256 H14 with their errors against FP64, and the
-    learned cost model judged against exhaustive tuning on the committed
+    learned cost model measured against exhaustive tuning on the committed
     timings.  Not part of `value`."""
     import numpy as np
     import torch

@@ -56,7 +56,7 @@ def test_mlp_training_on_gpu_reduces_loss(cuda):
 
 @pytest.mark.skipif(not os.path.exists(TIMINGS), reason="timings fixture not generated")
 def test_cost_model_picks_within_10pct_of_exhaustive_and_beats_default(cuda, capsys):
-    """Trained on 300 shapes' exhaustive timings, judged on 100 held out."""
+    """Trained on 300 shapes' exhaustive timings, evaluated on 100 held out."""
     cm = _cm()
     with open(TIMINGS) as f:
         rows = json.load(f)["rows"]
