@@ -142,7 +142,10 @@ int wino_tune_layer(const void* x, const void* ucache, void* workspace, void* y,
  * fastest table order among {as added, longest first, longest/shortest
  * interleaved}; layer_us receives nlayers x WINO_NCFG timings, order_us the
  * three whole-batch timings (either may be NULL).  Configuration and order
- * changes invalidate a captured graph. */
+ * changes invalidate a captured graph.  Each layer needs its own workspace
+ * (wino_fused_workspace_bytes of its shape, or NULL for direct reads): the
+ * pre-passes of a run write all workspaces before the one launch reads
+ * them, so layers sharing one would overwrite each other. */
 int wino_batch_create(void** batch);
 int wino_batch_destroy(void* batch);
 int wino_batch_add_layer(void* batch, const void* x, const void* ucache, void* workspace, void* y,
