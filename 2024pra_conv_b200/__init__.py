@@ -80,6 +80,7 @@ def lib():
             "wino_conv2d_fused": ([vp, vp, vp, i, i, i, i, i, vp], i),
             "wino_fused_workspace_bytes": ([i, i, i, i], sz),
             "wino_input_layout": ([vp, vp, i, i, i, i, vp], i),
+            "wino_conv2d_fused_epilogue": ([vp, vp, vp, vp, vp, vp, i, i, i, i, i, i, vp], i),
             "wino_variant_workspace_bytes": ([i, i, i, i, i, i], sz),
             "wino_conv2d_fused_cfg": ([vp, vp, vp, vp, i, i, i, i, i, i, vp], i),
             "wino_fused_cfg_workspace_bytes": ([i, i, i, i, i, i], sz),
@@ -234,6 +235,23 @@ def conv2d_fused(x, ucache, k, out=None, stream=None, workspace=True):
                                       ctypes.c_void_p(workspace.data_ptr()),
                                       ctypes.c_void_p(y.data_ptr()), n, c, h, wd, k, _stream(stream)),
            "conv2d_fused_ws")
+    return y
+
+
+def conv2d_fused_epilogue(x, ucache, k, bias=None, residual=None, relu=False, out=None,
+                          workspace=None, stream=None):
+    """relu?(conv(x) + bias[k] + residual) in one fused kernel (plus the input
+    pre-pass).  bias: float32 [K] tensor or None; residual: fp16 tensor of the
+    output's shape or None (may be `out` itself)."""
+    import torch
+    n, c, h, wd = x.shape
+    y = out if out is not None else torch.empty((n, k, h, wd), dtype=torch.float16, device=x.device)
+    if workspace is None:
+        workspace = torch.empty(fused_workspace_bytes(n, c, h, wd), dtype=torch.uint8, device=x.device)
+    ptr = lambda t: ctypes.c_void_p(0 if t is None else t.data_ptr())
+    _check(lib().wino_conv2d_fused_epilogue(ptr(x), ptr(ucache), ptr(workspace), ptr(y), ptr(bias),
+                                            ptr(residual), 1 if relu else 0, n, c, h, wd, k, _stream(stream)),
+           "conv2d_fused_epilogue")
     return y
 
 

@@ -81,12 +81,6 @@ namespace wino {
 
 static __device__ uint32_t g_fused_err;
 
-// Extra operands of the precision variants (unused by VAR_F16).
-struct VariantArgs {
-  const void* u_lo;         // VAR_F16_HILO: residual U cache (fp16, same layout)
-  const float* su;          // VAR_F8: su[t * K + k]
-  const uint32_t* inv_sv2;  // VAR_F8: (1/sv[2i], 1/sv[2i+1]) as fp16x2, i < C/2
-};
 
 namespace fused {
 
@@ -646,6 +640,24 @@ __device__ __forceinline__ void fused_body(const Sched& sched, const VariantArgs
       const uint32_t ebuf = smem_base + EPI_BASE + (uint32_t)(warp - WARP_E0) * EPI_WARP_BYTES;
       const int kq = quarter * 32;             // first channel of this warp in the k-block
       const size_t PQ = (size_t)g.P * g.Q;
+      // Fused epilogue (optional): + bias[k] in fp32 here; + residual and
+      // ReLU at the coalesced store below (ReLU here when there is no
+      // residual).
+      constexpr bool kEpi = VAR == VAR_F16;   // the fused epilogue is an fp16-path option
+      if (kEpi && va.bias != nullptr) {
+        const float bk = va.bias[min(kb * KB + kq + lane, g.K - 1)];
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+#pragma unroll
+          for (int o = 0; o < 4; ++o) y[j][o] += bk;
+      }
+      if (kEpi && va.relu && va.residual == nullptr) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+#pragma unroll
+          for (int o = 0; o < 4; ++o) y[j][o] = fmaxf(y[j][o], 0.f);
+      }
+      const __half* R = kEpi ? static_cast<const __half*>(va.residual) : nullptr;
 #pragma unroll
       for (int r = 0; r < 2; ++r) {
         __syncwarp();  // the previous round's reads are done
@@ -682,6 +694,23 @@ __device__ __forceinline__ void fused_body(const Sched& sched, const VariantArgs
                        : "r"(ebuf + kk * 64 + (((row * 2 + (jj >> 2)) ^ ((kk >> 1) & 3)) << 4) + (jj & 3) * 4));
           if (tvalid && kq + kk < kbs && (row == 0 || two_rows)) {
             __half* o = o0 + (size_t)kk * PQ + (size_t)row * g.Q;
+            if (kEpi && R != nullptr) {
+              // + residual (same layout as y, read where y is written), then ReLU
+              const __half* ro = R + (o - Y);
+              const unsigned short* r16 = reinterpret_cast<const unsigned short*>(ro);
+              const uint32_t rw = (two_cols && q_even) ? *reinterpret_cast<const uint32_t*>(ro)
+                                                       : (uint32_t)r16[0] | (two_cols ? (uint32_t)r16[1] << 16 : 0u);
+              float2 f = __half22float2(*reinterpret_cast<const __half2*>(&v));
+              const float2 rf = __half22float2(*reinterpret_cast<const __half2*>(&rw));
+              f.x += rf.x;
+              f.y += rf.y;
+              if (va.relu) {
+                f.x = fmaxf(f.x, 0.f);
+                f.y = fmaxf(f.y, 0.f);
+              }
+              const __half2 h2 = __floats2half2_rn(f.x, f.y);
+              v = *reinterpret_cast<const uint32_t*>(&h2);
+            }
             if (two_cols && q_even) {
               *reinterpret_cast<uint32_t*>(o) = v;
             } else {

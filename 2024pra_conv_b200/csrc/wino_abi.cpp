@@ -66,13 +66,6 @@ int wino_launch_xb_f8_scales(const unsigned* amax, float* sv, uint32_t* inv_sv2,
 int wino_launch_filter_transform_f8(const void* weight, const float* sv, void* u8, float* su, int K,
                                     int C, cudaStream_t stream);
 }
-namespace wino {
-struct VariantArgs {
-  const void* u_lo;
-  const float* su;
-  const uint32_t* inv_sv2;
-};
-}
 extern "C" {
 int wino_fused_launch_variant(int variant, const wino::KernelParam* p, const wino::VariantArgs* va,
                               int cfg, unsigned grid, cudaStream_t stream);
@@ -397,6 +390,29 @@ extern "C" int wino_conv2d_variant(int variant, const void* x, const void* weigh
   if (variant != WINO_VAR_F8 && wino_launch_xb_layout(&p, s) != 0) return WINO_ECUDA;
   return wino_fused_launch_variant(variant, &p, &va, 0, fused_grid(n, h, w, k), s) == 0 ? WINO_OK
                                                                                          : WINO_ECUDA;
+}
+
+// Fused conv with the epilogue of the next ResNet step folded in:
+// y = relu?(conv(x) + bias[k] + residual).
+extern "C" int wino_conv2d_fused_epilogue(const void* x, const void* ucache, void* workspace, void* y,
+                                          const float* bias, const void* residual, int relu, int n, int c,
+                                          int h, int w, int k, void* stream) {
+  if (!x || !ucache || !y || !workspace) return WINO_EINVAL;
+  if ((reinterpret_cast<uintptr_t>(workspace) & 15) != 0) return WINO_EINVAL;
+  if (residual && (reinterpret_cast<uintptr_t>(residual) & 3) != 0) return WINO_EINVAL;
+  const int st = wino_check_shape(n, c, h, w, k);
+  if (st != WINO_OK) return st;
+  if (!xb_items_ok(n, c, h, w)) return WINO_EUNSUPPORTED;
+  const cudaStream_t s = (cudaStream_t)stream;
+  wino::KernelParam p = make_param(x, nullptr, y, workspace, const_cast<void*>(ucache), nullptr, n, c, h,
+                                   w, k);
+  if (wino_launch_xb_layout(&p, s) != 0) return WINO_ECUDA;
+  wino::VariantArgs va{};
+  va.bias = bias;
+  va.residual = residual;
+  va.relu = relu ? 1 : 0;
+  return wino_fused_launch_variant(WINO_VAR_F16, &p, &va, 0, fused_grid(n, h, w, k), s) == 0 ? WINO_OK
+                                                                                          : WINO_ECUDA;
 }
 
 // Launch the four slots of a filled kernelInfo_t in order on one stream, each

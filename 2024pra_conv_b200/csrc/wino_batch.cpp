@@ -24,13 +24,6 @@
 #include "wino_param.h"
 #include "wino_batch.h"
 
-namespace wino {
-struct VariantArgs {
-  const void* u_lo;
-  const float* su;
-  const uint32_t* inv_sv2;
-};
-}  // namespace wino
 
 extern "C" {
 int wino_fused_launch_variant(int variant, const wino::KernelParam* p, const wino::VariantArgs* va,

@@ -22,6 +22,17 @@ struct KernelParam {
 };
 
 static_assert(sizeof(KernelParam) == 80, "KernelParam must stay 80 bytes");
+
+// Extra arguments of the non-drop-in fused kernels (zero = unused).
+struct VariantArgs {
+  const void* u_lo;          // VAR_F16_HILO: residual U cache (fp16, same layout)
+  const float* su;           // VAR_F8: su[t * K + k]
+  const uint32_t* inv_sv2;   // VAR_F8: (1/sv[2i], 1/sv[2i+1]) as fp16x2, i < C/2
+  const float* bias;         // epilogue: + bias[k]
+  const void* residual;      // epilogue: + residual (fp16, the output's layout; may alias it)
+  int relu;                  // epilogue: max(., 0) last
+  int pad;
+};
 static_assert(offsetof(KernelParam, n) == 48, "dims start after six pointers");
 static_assert(offsetof(KernelParam, Ow) == 72, "thirteen shorts");
 

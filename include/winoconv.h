@@ -71,6 +71,18 @@ int wino_input_layout(const void* x, void* workspace, int n, int c, int h, int w
 int wino_conv2d_fused_ws(const void* x, const void* ucache, void* workspace, void* y, int n, int c,
                          int h, int w, int k, void* stream);
 
+/* The fast path with the step that follows a conv in a ResNet block folded
+ * into its output transform (the reference stops at the conv, writing M and
+ * transforming it in a separate kernel, src/conv2d.cpp:17-250):
+ *   y = relu ? max(conv(x) + bias[k] + residual, 0) : conv(x) + bias[k] + residual
+ * bias: fp32 per output channel, or NULL; residual: fp16 in y's N K H W
+ * layout (4-byte aligned, may be y itself), or NULL.  conv + bias is
+ * rounded to fp16 before the residual is added (in fp32) and the result
+ * rounded again.  workspace as for wino_conv2d_fused_ws. */
+int wino_conv2d_fused_epilogue(const void* x, const void* ucache, void* workspace, void* y,
+                               const float* bias, const void* residual, int relu, int n, int c, int h,
+                               int w, int k, void* stream);
+
 /* The plain unfused path, the comparator of the fused kernel: input
  * transform to V in global memory, the 16 tap GEMMs as one batched tcgen05
  * GEMM writing M (fp16) to global memory, output transform -- the stage

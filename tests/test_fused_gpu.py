@@ -240,3 +240,39 @@ def test_unfused_large_layer(wino, cuda, oracle_mod):
 
 def test_zz_no_device_errors_recorded(wino, cuda):
     assert wino.error_read_clear() == 0
+
+
+@pytest.mark.parametrize("shape", [(4, 64, 14, 14, 64), (2, 48, 9, 12, 144), (1, 32, 7, 7, 32)])
+@pytest.mark.parametrize("mode", ["bias", "residual", "bias_relu", "all", "all_in_place"])
+def test_fused_epilogue(wino, cuda, oracle_mod, shape, mode):
+    """relu?(conv + bias + residual) from the fused kernel's output transform
+    against FP64 (bar: rel-L2 <= 2e-3, max-normalised <= 1e-2 of the result)."""
+    import torch
+    n, c, h, w, k = shape
+    x16, w16 = oracle_mod.make_inputs(n, c, h, w, k, seed=11, x_dist="normal")
+    x, wt = _t(x16, cuda), _t(w16, cuda)
+    g = torch.Generator(device=cuda)
+    g.manual_seed(3)
+    bias = torch.randn(k, device=cuda, generator=g) * 0.5 if "bias" in mode or "all" in mode else None
+    res = (torch.randn((n, k, h, w), device=cuda, generator=g) * 0.5).half() \
+        if "residual" in mode or "all" in mode else None
+    relu = "relu" in mode or "all" in mode
+    u = wino.filter_transform(wt)
+    y64 = torch.nn.functional.conv2d(x.double(), wt.double(), padding=1)
+    if bias is not None:
+        y64 = y64 + bias.double().view(1, k, 1, 1)
+    if res is not None:
+        y64 = y64 + res.double()
+    if relu:
+        y64 = torch.relu(y64)
+    if mode == "all_in_place":
+        out = res.clone()
+        y = wino.conv2d_fused_epilogue(x, u, k, bias=bias, residual=out, relu=True, out=out)
+    else:
+        y = wino.conv2d_fused_epilogue(x, u, k, bias=bias, residual=res, relu=relu)
+    torch.cuda.synchronize()
+    d = y.double() - y64
+    rl2 = float(torch.linalg.vector_norm(d) / torch.linalg.vector_norm(y64))
+    mxn = float(d.abs().max() / y64.abs().max())
+    assert rl2 <= REL_L2 and mxn <= MAX_NORM, (mode, rl2, mxn)
+    assert wino.error_read_clear() == 0
