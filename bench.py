@@ -462,6 +462,29 @@ def extension_legs(wino, dev, flush, ev, peaks, steps):
     out["variants"] = {"workload": "N64 C256 H14 W14 K256, x ~ U[-1,1]; per call: filter transform "
                                    "+ input pre-pass + fused kernel", **var}
 
+    # --- fused epilogue (bias + residual + ReLU) vs the conv then separate elementwise ops
+    n, c, h, k = 128, 256, 28, 256
+    x16, w16 = oracle.make_inputs(n, c, h, h, k, seed=0, x_dist="relu_normal", w_std=np.sqrt(2.0 / (9 * c)))
+    x = torch.from_numpy(x16).to(dev)
+    wt = torch.from_numpy(w16).to(dev)
+    u = wino.filter_transform(wt)
+    ws = torch.empty(wino.fused_workspace_bytes(n, c, h, h), dtype=torch.uint8, device=dev)
+    bias = torch.randn(k, device=dev) * 0.1
+    res = torch.randn((n, k, h, h), device=dev).half()
+    y = torch.empty((n, k, h, h), dtype=torch.float16, device=dev)
+    bias16 = bias.half().view(1, k, 1, 1)
+    fused_ep = timed(lambda: wino.conv2d_fused_epilogue(x, u, k, bias=bias, residual=res, relu=True, out=y,
+                                                        workspace=ws), steps)
+
+    def separate():
+        wino.conv2d_fused(x, u, k, out=y, workspace=ws)
+        torch.relu_(y.add_(bias16).add_(res))
+
+    sep = timed(separate, steps)
+    out["fused_epilogue"] = {"workload": "N128 C256 H28 K256: relu(conv + bias + residual)",
+                             "us_fused": fused_ep, "us_conv_then_torch_elementwise": sep}
+    del x, wt, u, ws, res, y
+
     # --- learned cost model vs exhaustive tuning (committed timings)
     path = os.path.join(ROOT, "tests", "golden", "tuning_timings.json")
     if os.path.exists(path):
