@@ -81,6 +81,7 @@ def lib():
             "wino_fused_workspace_bytes": ([i, i, i, i], sz),
             "wino_input_layout": ([vp, vp, i, i, i, i, vp], i),
             "wino_conv2d_fused_epilogue": ([vp, vp, vp, vp, vp, vp, i, i, i, i, i, i, vp], i),
+            "wino_conv2d_direct": ([vp, vp, vp] + [i] * 11 + [vp], i),
             "wino_variant_workspace_bytes": ([i, i, i, i, i, i], sz),
             "wino_conv2d_fused_cfg": ([vp, vp, vp, vp, i, i, i, i, i, i, vp], i),
             "wino_fused_cfg_workspace_bytes": ([i, i, i, i, i, i], sz),
@@ -170,7 +171,7 @@ class DropinWorkspaces:
         self.transform_filter = torch.empty(16 * k * c, dtype=torch.float16, device=device)
 
 
-def dropin_conv2d(x, w, stream=None, ws=None, transform_pin=True):
+def dropin_conv2d(x, w, stream=None, ws=None, transform_pin=True, stride=1, pad=None):
     """Run the drop-in path the way the reference harness does
     (src/main.cpp:33-108): caller-allocated output and workspaces sized as
     there, getParamsize, getkernelInfo, then the four launch slots.  With
@@ -178,10 +179,13 @@ def dropin_conv2d(x, w, stream=None, ws=None, transform_pin=True):
     fused kernel reads the NCHW input directly."""
     import torch
     n, c, h, wd = x.shape
-    k = w.shape[0]
+    k, _, r, s = w.shape
+    pad = (r // 2) if pad is None else pad
+    oh, ow = (h - r + 2 * pad) // stride + 1, (wd - s + 2 * pad) // stride + 1
     ws = ws or DropinWorkspaces(n, c, h, wd, k, x.device, transform_pin)
-    y = torch.empty((n, k, h, wd), dtype=torch.float16, device=x.device)
-    pr = make_problem(x, w, y, ws.transform_pin, ws.transform_filter, ws.mid_result)
+    y = torch.empty((n, k, oh, ow), dtype=torch.float16, device=x.device)
+    pr = make_problem(x, w, y, ws.transform_pin, ws.transform_filter, ws.mid_result,
+                      r=r, s=s, u=stride, v=stride, p=pad, q=pad)
     size = get_param_size(pr)
     param = (ctypes.c_char * size)()
     code, ki = get_kernel_info(pr, param)
@@ -252,6 +256,20 @@ def conv2d_fused_epilogue(x, ucache, k, bias=None, residual=None, relu=False, ou
     _check(lib().wino_conv2d_fused_epilogue(ptr(x), ptr(ucache), ptr(workspace), ptr(y), ptr(bias),
                                             ptr(residual), 1 if relu else 0, n, c, h, wd, k, _stream(stream)),
            "conv2d_fused_epilogue")
+    return y
+
+
+def conv2d_direct(x, w, stride=1, pad=1, out=None, stream=None):
+    """Direct convolution of any filter size / stride / padding (fp16 in and
+    out, fp32 accumulation)."""
+    import torch
+    n, c, h, wd = x.shape
+    k, _, r, s = w.shape
+    oh, ow = (h - r + 2 * pad) // stride + 1, (wd - s + 2 * pad) // stride + 1
+    y = out if out is not None else torch.empty((n, k, oh, ow), dtype=torch.float16, device=x.device)
+    _check(lib().wino_conv2d_direct(ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(w.data_ptr()),
+                                    ctypes.c_void_p(y.data_ptr()), n, c, h, wd, k, r, s, stride, stride,
+                                    pad, pad, _stream(stream)), "conv2d_direct")
     return y
 
 

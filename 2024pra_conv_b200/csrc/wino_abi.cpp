@@ -55,6 +55,9 @@ int wino_fused_smem_bytes();
 int wino_fused_threads();
 long long wino_fused_nblocks(int n, int h, int w, int k);
 uint32_t wino_fused_error_read_clear();
+void* wino_direct_kernel_ptr();
+void wino_direct_grid(int n, int k, int oh, int ow, unsigned* gx, unsigned* gy);
+int wino_launch_direct(const wino::KernelParam* p, cudaStream_t stream);
 void* wino_xb_layout_kernel_ptr();
 size_t wino_xb_bytes(int n, int c, int h, int w);
 unsigned wino_xb_layout_grid(int n, int c, int h, int w);
@@ -157,16 +160,59 @@ int getParamsize(problem_t* problem, int* paramSize) {
   return WINO_OK;
 }
 
+// Validation shared by the drop-in and the direct-conv entry point: positive
+// dims within the `short` fields, a filter no larger than the padded input.
+int check_general(long long n, long long c, long long h, long long w, long long k, long long r,
+                  long long s, long long u, long long v, long long p, long long q, int* oh, int* ow) {
+  if (n < 1 || c < 1 || h < 1 || w < 1 || k < 1 || r < 1 || s < 1 || u < 1 || v < 1 || p < 0 || q < 0)
+    return WINO_EINVAL;
+  if (n > kMaxDim || c > kMaxDim || h > kMaxDim || w > kMaxDim || k > kMaxDim || r > kMaxDim ||
+      s > kMaxDim || u > kMaxDim || v > kMaxDim || p > kMaxDim || q > kMaxDim)
+    return WINO_EUNSUPPORTED;
+  if (h + 2 * p < r || w + 2 * q < s) return WINO_EINVAL;
+  const long long oh_ = (h - r + 2 * p) / u + 1, ow_ = (w - s + 2 * q) / v + 1;
+  if (oh_ > kMaxDim || ow_ > kMaxDim) return WINO_EUNSUPPORTED;
+  if (n * oh_ * ow_ / 64 >= (1LL << 31)) return WINO_EUNSUPPORTED;  // direct kernel's grid.x
+  *oh = (int)oh_;
+  *ow = (int)ow_;
+  return WINO_OK;
+}
+
 int getkernelInfo(problem_t* problem, kernelInfo_t* kernelInfo, void* param) {
   if (!problem || !kernelInfo || !param) return WINO_EINVAL;
   const problem_t& pr = *problem;
-  if (pr.r != 3 || pr.s != 3 || pr.u != 1 || pr.v != 1 || pr.p != 1 || pr.q != 1)
-    return WINO_EUNSUPPORTED;
-  const int st = wino_check_shape((int)pr.n, (int)pr.c, (int)pr.h, (int)pr.w, (int)pr.k);
+  int oh = 0, ow = 0;
+  const int st = check_general(pr.n, pr.c, pr.h, pr.w, pr.k, pr.r, pr.s, pr.u, pr.v, pr.p, pr.q, &oh, &ow);
   if (st != WINO_OK) return st;
-  if (!pr.in || !pr.weight || !pr.out || !pr.transform_filter) return WINO_EINVAL;
-  const int oh = ((int)pr.h - (int)pr.r + 2 * (int)pr.p) / (int)pr.u + 1;
-  const int ow = ((int)pr.w - (int)pr.s + 2 * (int)pr.q) / (int)pr.v + 1;
+  if (!pr.in || !pr.weight || !pr.out) return WINO_EINVAL;
+  // Winograd F(2x2,3x3) for 3x3 / stride 1 / pad 1 with 16-channel multiples
+  // and a U-cache workspace; every other shape goes to the direct kernel.
+  const bool wino = pr.r == 3 && pr.s == 3 && pr.u == 1 && pr.v == 1 && pr.p == 1 && pr.q == 1 &&
+                    wino_check_shape((int)pr.n, (int)pr.c, (int)pr.h, (int)pr.w, (int)pr.k) == WINO_OK &&
+                    pr.transform_filter != nullptr;
+
+  mykernelParamType* a = static_cast<mykernelParamType*>(param);
+  a->pin = pr.in;
+  a->pweight = pr.weight;
+  a->pout = pr.out;
+  a->transform_filter = pr.transform_filter;
+  a->mid_result = pr.mid_result;
+  a->n = (short)pr.n; a->c = (short)pr.c; a->h = (short)pr.h; a->w = (short)pr.w;
+  a->k = (short)pr.k; a->r = (short)pr.r; a->s = (short)pr.s; a->u = (short)pr.u;
+  a->v = (short)pr.v; a->p = (short)pr.p; a->q = (short)pr.q;
+  a->Oh = (short)oh; a->Ow = (short)ow;
+  std::memset(kernelInfo, 0, sizeof(*kernelInfo));
+
+  if (!wino) {
+    unsigned gx, gy;
+    wino_direct_grid((int)pr.n, (int)pr.k, oh, ow, &gx, &gy);
+    a->transform_pin = nullptr;
+    set_slot(kernelInfo, 1, 1, 1, 1, 32, 1, 1, 0, wino_noop_kernel_ptr());
+    set_slot(kernelInfo, 2, 1, 1, 1, 32, 1, 1, 0, wino_noop_kernel_ptr());
+    set_slot(kernelInfo, 3, gx, gy, 1, 256, 1, 1, 0, wino_direct_kernel_ptr());
+    set_slot(kernelInfo, 4, 1, 1, 1, 32, 1, 1, 0, wino_noop_kernel_ptr());
+    return WINO_OK;
+  }
 
   if (wino_fused_prepare() != 0) return WINO_ECUDA;
 
@@ -179,8 +225,8 @@ int getkernelInfo(problem_t* problem, kernelInfo_t* kernelInfo, void* param) {
                       (reinterpret_cast<uintptr_t>(pr.transform_pin) & 15) == 0 &&
                       wino_xb_bytes((int)pr.n, (int)pr.c, (int)pr.h, (int)pr.w) <= pin_ws_bytes &&
                       xb_items_ok((int)pr.n, (int)pr.c, (int)pr.h, (int)pr.w);
+  a->transform_pin = use_xb ? pr.transform_pin : nullptr;
 
-  std::memset(kernelInfo, 0, sizeof(*kernelInfo));
   const long long kc = (long long)pr.k * pr.c;
   set_slot(kernelInfo, 1, (unsigned)((kc + 255) / 256), 1, 1, 256, 1, 1, 0,
            wino_dropin_filter_kernel_ptr());
@@ -193,18 +239,6 @@ int getkernelInfo(problem_t* problem, kernelInfo_t* kernelInfo, void* param) {
            (unsigned)wino_fused_threads(), 1, 1, (unsigned)wino_fused_smem_bytes(),
            wino_fused_kernel_ptr());
   set_slot(kernelInfo, 4, 1, 1, 1, 32, 1, 1, 0, wino_noop_kernel_ptr());
-
-  mykernelParamType* a = static_cast<mykernelParamType*>(param);
-  a->pin = pr.in;
-  a->pweight = pr.weight;
-  a->pout = pr.out;
-  a->transform_pin = use_xb ? pr.transform_pin : nullptr;
-  a->transform_filter = pr.transform_filter;
-  a->mid_result = pr.mid_result;
-  a->n = (short)pr.n; a->c = (short)pr.c; a->h = (short)pr.h; a->w = (short)pr.w;
-  a->k = (short)pr.k; a->r = (short)pr.r; a->s = (short)pr.s; a->u = (short)pr.u;
-  a->v = (short)pr.v; a->p = (short)pr.p; a->q = (short)pr.q;
-  a->Oh = (short)oh; a->Ow = (short)ow;
   return WINO_OK;
 }
 
@@ -413,6 +447,20 @@ extern "C" int wino_conv2d_fused_epilogue(const void* x, const void* ucache, voi
   va.relu = relu ? 1 : 0;
   return wino_fused_launch_variant(WINO_VAR_F16, &p, &va, 0, fused_grid(n, h, w, k), s) == 0 ? WINO_OK
                                                                                           : WINO_ECUDA;
+}
+
+// Direct convolution of any filter size, stride and padding (the shapes the
+// Winograd path does not take).
+extern "C" int wino_conv2d_direct(const void* x, const void* weight, void* y, int n, int c, int h,
+                                  int w, int k, int r, int s, int u, int v, int p, int q, void* stream) {
+  if (!x || !weight || !y) return WINO_EINVAL;
+  int oh = 0, ow = 0;
+  const int st = check_general(n, c, h, w, k, r, s, u, v, p, q, &oh, &ow);
+  if (st != WINO_OK) return st;
+  wino::KernelParam pk = make_param(x, weight, y, nullptr, nullptr, nullptr, n, c, h, w, k);
+  pk.r = (short)r; pk.s = (short)s; pk.u = (short)u; pk.v = (short)v; pk.p = (short)p; pk.q = (short)q;
+  pk.Oh = (short)oh; pk.Ow = (short)ow;
+  return wino_launch_direct(&pk, (cudaStream_t)stream) == 0 ? WINO_OK : WINO_ECUDA;
 }
 
 // Launch the four slots of a filled kernelInfo_t in order on one stream, each

@@ -10,8 +10,9 @@
  * caller can keep U resident and so that tests and benchmarks can reach each
  * stage.  Each function cites the reference stage it implements.
  *
- * Shape contract (all entry points): 3x3 filter, stride 1, pad 1,
- * c % 16 == 0, k % 16 == 0, n, c, h, w, k in [1, 32767].
+ * Shape contract (all Winograd entry points): 3x3 filter, stride 1, pad 1,
+ * c % 16 == 0, k % 16 == 0, n, c, h, w, k in [1, 32767].  Other shapes:
+ * wino_conv2d_direct, and getkernelInfo dispatches them there itself.
  * Return: 0 on success or one of the WINO_E* codes below.
  */
 #ifndef WINO_WINOCONV_H
@@ -82,6 +83,14 @@ int wino_conv2d_fused_ws(const void* x, const void* ucache, void* workspace, voi
 int wino_conv2d_fused_epilogue(const void* x, const void* ucache, void* workspace, void* y,
                                const float* bias, const void* residual, int relu, int n, int c, int h,
                                int w, int k, void* stream);
+
+/* Direct convolution for any filter size r x s, stride (u, v) and padding
+ * (p, q) and any channel counts (implicit GEMM on CUDA cores, fp32
+ * accumulation); y: N K OH OW with OH = (h - r + 2p)/u + 1, OW likewise.
+ * getkernelInfo dispatches every shape outside the Winograd contract here
+ * (the reference ignores r, s, u, v, p, q, src/conv2d.cpp:254-271). */
+int wino_conv2d_direct(const void* x, const void* weight, void* y, int n, int c, int h, int w, int k,
+                       int r, int s, int u, int v, int p, int q, void* stream);
 
 /* The plain unfused path, the comparator of the fused kernel: input
  * transform to V in global memory, the 16 tap GEMMs as one batched tcgen05

@@ -7,6 +7,8 @@ import os
 import re
 import subprocess
 
+import numpy as np
+
 import pytest
 
 from conftest import ROOT
@@ -65,15 +67,34 @@ def _problem(wino, **kw):
 
 
 @pytest.mark.parametrize("field,value,code", [
-    ("r", 5, 2), ("s", 1, 2), ("u", 2, 2), ("v", 2, 2), ("p", 0, 2), ("q", 2, 2),
-    ("c", 8, 2), ("k", 27, 2), ("c", 3, 2), ("h", 40000, 2), ("n", 0, 1), ("w", 0, 1),
-    ("in_", 0, 1), ("weight", 0, 1), ("out", 0, 1), ("transform_filter", 0, 1),
+    ("h", 40000, 2), ("n", 0, 1), ("w", 0, 1), ("r", 0, 1), ("u", 0, 1), ("r", 40, 1),
+    ("in_", 0, 1), ("weight", 0, 1), ("out", 0, 1),
 ])
-def test_getkernelinfo_rejects_unsupported(wino, field, value, code):
+def test_getkernelinfo_rejects_invalid(wino, field, value, code):
     pr = _problem(wino, **{field: value})
     param = (ctypes.c_char * 80)()
     rc, _ = wino.get_kernel_info(pr, param)
     assert rc == code
+
+
+@pytest.mark.parametrize("field,value", [
+    ("r", 5), ("s", 1), ("u", 2), ("v", 2), ("p", 0), ("q", 2), ("c", 8), ("k", 27), ("c", 3),
+    ("transform_filter", 0),
+])
+def test_getkernelinfo_sends_other_shapes_to_the_direct_kernel(wino, field, value):
+    """Shapes outside the Winograd contract get the direct kernel in slot 3
+    and empty kernels elsewhere (needs no GPU: no attribute is set)."""
+    pr = _problem(wino, **{field: value})
+    param = (ctypes.c_char * 80)()
+    rc, ki = wino.get_kernel_info(pr, param)
+    assert rc == 0
+    L = wino.lib()
+    L.wino_direct_kernel_ptr.restype = ctypes.c_void_p
+    assert ki.slot(3)["kernel"] == L.wino_direct_kernel_ptr()
+    assert ki.slot(1)["kernel"] == ki.slot(2)["kernel"] == ki.slot(4)["kernel"]
+    dims = np.frombuffer(bytes(param)[48:74], dtype=np.int16)
+    n, c, h, w, k, r, s, u, v, p, q, oh, ow = dims
+    assert oh == (h - r + 2 * p) // u + 1 and ow == (w - s + 2 * q) // v + 1
 
 
 def test_check_shape(wino):
