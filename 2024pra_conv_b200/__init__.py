@@ -21,6 +21,7 @@ LIB_PATH = os.path.join(HERE, "_build", "libwinoconv.so")
 
 # Error codes of include/winoconv.h.
 WINO_OK, WINO_EINVAL, WINO_EUNSUPPORTED, WINO_ECUDA, WINO_EDEVICE = 0, 1, 2, 3, 4
+WINO_ESCRATCH, WINO_ESTALE, WINO_EIO = 5, 6, 7
 VAR_F16, VAR_BF16, VAR_F8, VAR_F16_HILO = 0, 1, 2, 3
 
 
@@ -82,6 +83,9 @@ def lib():
             "wino_input_layout": ([vp, vp, i, i, i, i, vp], i),
             "wino_conv2d_fused_epilogue": ([vp, vp, vp, vp, vp, vp, i, i, i, i, i, i, vp], i),
             "wino_conv2d_direct": ([vp, vp, vp] + [i] * 11 + [vp], i),
+            "wino_weight_tag": ([vp, i, i, ctypes.POINTER(ctypes.c_ulonglong), vp], i),
+            "wino_ucache_save": ([ctypes.c_char_p, vp, i, i, ctypes.c_ulonglong], i),
+            "wino_ucache_load": ([ctypes.c_char_p, vp, i, i, ctypes.c_ulonglong], i),
             "wino_variant_workspace_bytes": ([i, i, i, i, i, i], sz),
             "wino_conv2d_fused_cfg": ([vp, vp, vp, vp, i, i, i, i, i, i, vp], i),
             "wino_fused_cfg_workspace_bytes": ([i, i, i, i, i, i], sz),
@@ -300,6 +304,34 @@ def conv2d_variant(x, w, variant, out=None, workspace=None, stream=None):
                                      ctypes.c_void_p(workspace.data_ptr() + off), n, c, h, wd, k,
                                      _stream(stream)), "conv2d_variant")
     return y
+
+
+def weight_tag(w, stream=None) -> int:
+    """64-bit content tag of fp16 KCRS weights (computed on the GPU)."""
+    k, c = w.shape[:2]
+    t = ctypes.c_ulonglong(0)
+    _check(lib().wino_weight_tag(ctypes.c_void_p(w.data_ptr()), k, c, ctypes.byref(t), _stream(stream)),
+           "weight_tag")
+    return t.value
+
+
+def filter_transform_persistent(w, path, stream=None):
+    """The U cache of `w`, loaded from `path` when the file holds the U of
+    exactly these weights, else computed and written there.  Returns
+    (ucache, loaded)."""
+    import torch
+    k, c = w.shape[:2]
+    tag = weight_tag(w, stream)
+    u = torch.empty(16 * k * c, dtype=torch.float16, device=w.device)
+    rc = lib().wino_ucache_load(os.fsencode(path), ctypes.c_void_p(u.data_ptr()), k, c, tag)
+    if rc == WINO_OK:
+        return u, True
+    if rc not in (WINO_ESTALE, WINO_EIO):
+        raise WinoError(rc, "ucache_load")
+    u = filter_transform(w, stream)
+    torch.cuda.current_stream().synchronize()
+    _check(lib().wino_ucache_save(os.fsencode(path), ctypes.c_void_p(u.data_ptr()), k, c, tag), "ucache_save")
+    return u, False
 
 
 def filter_transform_unfused(w, stream=None):

@@ -31,7 +31,9 @@ enum {
   WINO_EUNSUPPORTED = 2,  /* shape outside the contract above            */
   WINO_ECUDA = 3,         /* a CUDA runtime call failed                  */
   WINO_EDEVICE = 4,       /* a kernel reported an error (see error word) */
-  WINO_ESCRATCH = 5       /* filter too large for wino_conv2d_noalloc's fixed scratch */
+  WINO_ESCRATCH = 5,      /* filter too large for wino_conv2d_noalloc's fixed scratch */
+  WINO_ESTALE = 6,        /* persisted U cache is for other weights, shape or layout */
+  WINO_EIO = 7            /* file could not be read or written */
 };
 
 /* Precision variants of the GEMM stage. */
@@ -52,6 +54,18 @@ size_t wino_ucache_bytes(int k, int c, int variant);
  * fp16 U cache (reference src/preprocessing.cuh:75-270, GgGT*).  One-shot:
  * the result stays valid for as long as the weights do. */
 int wino_filter_transform(const void* weight, void* ucache, int k, int c, void* stream);
+
+/* Persistence of the fp16 U cache across calls and processes (the reference
+ * re-runs its filter transform on every iteration, src/main.cpp:121):
+ * wino_weight_tag computes a 64-bit content tag of fp16 KCRS weights on the
+ * GPU (synchronises `stream`); wino_ucache_save writes a U cache with its
+ * shape, layout version and that tag; wino_ucache_load fills a caller's U
+ * buffer from such a file and returns WINO_ESTALE -- leaving the buffer
+ * untouched -- when the file belongs to other weights (tag), another shape or
+ * another layout version, so a caller re-runs wino_filter_transform then. */
+int wino_weight_tag(const void* weight, int k, int c, unsigned long long* tag, void* stream);
+int wino_ucache_save(const char* path, const void* ucache, int k, int c, unsigned long long tag);
+int wino_ucache_load(const char* path, void* ucache, int k, int c, unsigned long long tag);
 
 /* Fused conv on a prepared fp16 U cache: input transform, tensor-core tap
  * GEMMs and output transform in one persistent kernel (reference

@@ -179,3 +179,16 @@ def test_split_configuration_sizes(wino):
     assert L.wino_fused_nblocks_cfg(n, c, h, w, k, wino.cfg_split(2)) == 16 * base
     assert L.wino_fused_nblocks_cfg(n, c, h, w, k, wino.CFG_KMAJOR) == base
     assert wino.cfg_workspace_bytes(n, 24, h, w, k, 0) == 0               # bad shape
+
+
+def test_ucache_load_refuses_missing_and_foreign_files(wino, tmp_path):
+    """No GPU needed: the header is checked before any device copy."""
+    L = wino.lib()
+    dummy = ctypes.c_void_p(0x1000)
+    missing = os.fsencode(str(tmp_path / "none.bin"))
+    assert L.wino_ucache_load(missing, dummy, 32, 32, 1) == 7           # WINO_EIO
+    p = tmp_path / "foreign.bin"
+    p.write_bytes(b"NOTAUCAC" + bytes(40))
+    assert L.wino_ucache_load(os.fsencode(str(p)), dummy, 32, 32, 1) == 6  # WINO_ESTALE
+    assert L.wino_ucache_load(os.fsencode(str(p)), dummy, 32, 24, 1) == 2  # bad shape
+    assert L.wino_ucache_load(None, dummy, 32, 32, 1) == 1
