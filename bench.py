@@ -52,6 +52,20 @@ def wino_flops(n, c, h, w, k):
     return 2.0 * 16 * k * c * n * ((h + 1) // 2) * ((w + 1) // 2)
 
 
+def replica_throughput(local_ms, flops_per_rank, world, device):
+    """Whole-job throughput of `world` independent replicas: every rank did
+    `flops_per_rank` in `local_ms`; the job ends with its slowest rank, so the
+    time is the max over ranks (all_reduce MAX; every rank calls this) and the
+    value all ranks' FLOPs over it.  Returns (max_ms, TFLOP/s)."""
+    max_ms = float(local_ms)
+    if world > 1:
+        import torch
+        t = torch.tensor([max_ms], dtype=torch.float64, device=device)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        max_ms = float(t.item())
+    return max_ms, flops_per_rank * world / (max_ms * 1e-3) / 1e12
+
+
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -251,12 +265,8 @@ def run_ours(args, rank, world, local_rank):
             torch.distributed.barrier()
     clocks = sampler.summary()
 
-    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    max_ms = float(t.item())
     dflops = direct_flops(n, c, h, w, k)
-    value = dflops * args.steps * world / (max_ms * 1e-3) / 1e12
+    max_ms, value = replica_throughput(total_ms, dflops * args.steps, world, dev)
 
     # --- parity of the timed path (outside the timed region)
     y64 = torch.nn.functional.conv2d(x.double(), wt.double(), padding=1)
@@ -303,10 +313,7 @@ def run_ours(args, rank, world, local_rank):
         e2e_step()
     torch.cuda.synchronize()
     e2e_ms, _ = timed(e2e_step, args.steps, flush_between=False)
-    te = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
-    e2e_value = dflops * args.steps * world / (float(te.item()) * 1e-3) / 1e12
+    _, e2e_value = replica_throughput(e2e_ms, dflops * args.steps, world, dev)
 
     errcode = wino.error_read_clear()
     if errcode:
