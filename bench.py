@@ -273,7 +273,8 @@ def run_ours(args, rank, world, local_rank):
     yd = y.double()
     rel_l2 = float(torch.linalg.vector_norm(yd - y64) / torch.linalg.vector_norm(y64))
     max_norm = float((yd - y64).abs().max() / y64.abs().max())
-    del y64, yd
+    y64_ref = y64                               # kept for the end-to-end check below
+    del yd
 
     # --- per-kernel pieces: filter transform, fused conv on cached U, unfused path
     ucache = wino.filter_transform(wt)
@@ -299,21 +300,67 @@ def run_ours(args, rank, world, local_rank):
     unfused_us = unf_ms / iters * 1e3
     ft_us = ft_ms / iters * 1e3
 
-    # --- end to end through the C-ABI with host buffers
+    # --- end to end through the C-ABI with host buffers.  Every step uploads
+    # its input from pinned host memory, runs the drop-in slots and downloads
+    # its output; consecutive steps are pipelined over two buffer sets and
+    # three streams (upload / compute / download), so step i's download
+    # overlaps step i+1's upload and compute (PCIe is full duplex).
     xh = torch.empty_like(x, device="cpu").pin_memory()
     xh.copy_(x)
-    yh = torch.empty_like(y, device="cpu").pin_memory()
+    yh = [torch.empty_like(y, device="cpu").pin_memory() for _ in range(2)]
+    xd = [x, torch.empty_like(x)]
+    yd = [y, torch.empty_like(y)]
+    dws2 = wino.DropinWorkspaces(n, c, h, w, k, dev)
+    params, kis = [], []
+    for bset in range(2):
+        ws_b = dws if bset == 0 else dws2
+        pr_b = wino.make_problem(xd[bset], wt, yd[bset], ws_b.transform_pin, ws_b.transform_filter,
+                                 ws_b.mid_result)
+        prm = (ctypes.c_char * wino.get_param_size(pr_b))()
+        code, ki_b = wino.get_kernel_info(pr_b, prm)
+        if code != 0:
+            raise SystemExit(f"getkernelInfo failed: {code}")
+        params.append(prm)
+        kis.append(ki_b)
+    s_up, s_comp, s_down = torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream()
+    up_done = [torch.cuda.Event() for _ in range(2)]
+    comp_done = [torch.cuda.Event() for _ in range(2)]
+    down_done = [torch.cuda.Event() for _ in range(2)]
+    started = [False, False]
 
-    def e2e_step():
-        x.copy_(xh, non_blocking=True)
-        step()
-        yh.copy_(y, non_blocking=True)
+    def e2e_run(steps_):
+        for i in range(steps_):
+            bset = i % 2
+            with torch.cuda.stream(s_up):
+                if started[bset]:
+                    s_up.wait_event(comp_done[bset])       # the compute has read xd[bset]
+                xd[bset].copy_(xh, non_blocking=True)
+                up_done[bset].record(s_up)
+            s_comp.wait_event(up_done[bset])
+            if started[bset]:
+                s_comp.wait_event(down_done[bset])         # the download has read yd[bset]
+            wino.launch_kernel_info(kis[bset], params[bset], s_comp)
+            comp_done[bset].record(s_comp)
+            with torch.cuda.stream(s_down):
+                s_down.wait_event(comp_done[bset])
+                yh[bset].copy_(yd[bset], non_blocking=True)
+                down_done[bset].record(s_down)
+            started[bset] = True
 
-    for _ in range(2):
-        e2e_step()
+    e2e_run(2)
     torch.cuda.synchronize()
-    e2e_ms, _ = timed(e2e_step, args.steps, flush_between=False)
+    a_ev, b_ev = ev(), ev()
+    a_ev.record(s_up)
+    e2e_run(args.steps)
+    s_down.wait_stream(s_up)
+    s_down.wait_stream(s_comp)
+    b_ev.record(s_down)
+    b_ev.synchronize()
+    e2e_ms = a_ev.elapsed_time(b_ev)
+    torch.cuda.synchronize()
+    e2e_err = float((yh[(args.steps - 1) % 2].to(dev).double() - y64_ref).norm() / y64_ref.norm())
     _, e2e_value = replica_throughput(e2e_ms, dflops * args.steps, world, dev)
+    del dws2, xd, yd
 
     errcode = wino.error_read_clear()
     if errcode:
@@ -360,7 +407,8 @@ def run_ours(args, rank, world, local_rank):
                      "algorithmic": "Winograd GEMM FLOPs 2*16*K*C*N*ceil(H/2)*ceil(W/2) per launch"},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": "TFLOP/s", "h2d_bytes_per_step": x.numel() * 2,
-                "d2h_bytes_per_step": y.numel() * 2},
+                "d2h_bytes_per_step": y.numel() * 2, "rel_l2_of_downloaded_output": e2e_err,
+                "pipelining": "2 buffer sets, upload / compute / download streams"},
         "gpu_launches": 4 * args.steps,
         "clocks": clocks,
     }
