@@ -1,14 +1,21 @@
-// Winograd input transform B^T d B for groups of 8 consecutive tiles, in
-// packed fp16 arithmetic, shared by the fused kernel (into shared memory)
-// and the unfused input-transform kernel (into global memory).
+// Winograd input transform B^T d B in packed fp16 arithmetic (two channels
+// or two tiles per 32-bit word), for the fused and unfused kernels.
 //
 // Reference: calculate_transform_pin / prefetch_input / init_mask of
-// src/preprocessing.cuh:6-72 (one tile per thread, mask-based padding,
-// fp16 arithmetic).  Here a thread forms 8 tiles x 16 taps of one channel:
-// the B^T row combination runs on pairs of adjacent input columns, and a
-// byte permute regroups them into pairs of adjacent tiles, so each tap's 8
-// tiles leave as one 16-byte row of an MN-major core matrix.  Padding is
-// handled by zero words outside the image.
+// src/preprocessing.cuh:6-72 (one tile per thread, mask-based padding, fp16
+// arithmetic).  Three producers:
+//   produce_v8                 unfused input transform: a thread forms 8
+//                              tiles x 16 taps of one channel from NCHW
+//                              input (the B^T rows on pairs of adjacent
+//                              columns, a byte permute into pairs of adjacent
+//                              tiles), each tap's 8 tiles leaving as one
+//                              16-byte row of an MN-major core matrix;
+//   produce_v_half_xb          fused kernel: one tile, 8 channels, the 8 taps
+//                              of two tap rows, from a shared-memory slab of
+//                              the channel-blocked XB input (no bounds checks);
+//   produce_v_quarter_global   fused kernel without XB: one tile, 4 channels,
+//                              16 taps, straight from NCHW input.
+// Padding is zero: zero words outside the image, or XB's zero records.
 #pragma once
 #include <cstdint>
 #include <cuda_fp16.h>
@@ -224,94 +231,6 @@ __device__ __forceinline__ void produce_v8(const __half* __restrict__ X, const G
   }
 #pragma unroll
   for (int t = 0; t < 16; ++t) sink(t, out[t][0], out[t][1], out[t][2], out[t][3]);
-}
-
-// ---------------------------------------------------------------------------
-// One tile x one 16-channel K-step, all 16 taps, for the K-major V operand
-// (core matrix = 8 tiles x 8 channels, a tile's 8 channels one 16-byte row).
-// A warp covers 32 consecutive tiles, so each word load of the warp reads
-// consecutive words of one input row (coalesced).  Two channels are paired
-// per register (c, c+1): window columns are regrouped with byte permutes,
-// then B^T d B runs in packed fp16.
-//
-// sink(t, half, w0, w1, w2, w3): tap t, channels 8*half .. 8*half+7 as four
-// words (channel pair i in w_i, even channel in the low half).
-//
-// If prefetch_c0 >= 0 the rows this tile needs for channels prefetch_c0 ..
-// prefetch_c0+15 are first requested into L1 (the producer's next step), so
-// that step's loads hit.
-template <typename Sink>
-__device__ __forceinline__ void produce_v_tile16(const __half* __restrict__ X, const Geometry& g,
-                                                 long long tile, int c0, int prefetch_c0,
-                                                 Sink&& sink) {
-  const bool w_even = (g.W & 1) == 0;
-  const long long per_img = (long long)g.TP * g.TQ;
-  const size_t plane_elems = (size_t)g.H * g.W;
-  const bool valid = tile < g.NT;
-  int n = 0, ty = 0, tx = 0;
-  if (valid) {
-    n = (int)(tile / per_img);
-    const int r = (int)(tile - (long long)n * per_img);
-    ty = r / g.TQ;
-    tx = r - ty * g.TQ;
-  }
-  const __half* base = X + ((size_t)n * g.C + c0) * plane_elems;
-  const int y0 = 2 * ty - 1, m0 = tx - 1;
-  int rowoff[4];
-  bool rowok[4];
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int y = y0 + i;
-    rowok[i] = valid && y >= 0 && y < g.H;
-    rowoff[i] = (rowok[i] ? y : 0) * g.W;
-  }
-  if (prefetch_c0 >= 0) {
-    const __half* pbase = X + ((size_t)n * g.C + prefetch_c0) * plane_elems + (m0 > 0 ? 2 * m0 : 0);
-#pragma unroll 4
-    for (int ch = 0; ch < 16; ++ch)
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-        if (rowok[i]) prefetch_l1(pbase + (size_t)ch * plane_elems + rowoff[i]);
-  }
-#pragma unroll
-  for (int half = 0; half < 2; ++half) {
-    uint32_t out[16][4];
-#pragma unroll
-    for (int cp = 0; cp < 4; ++cp) {
-      const __half* pa = base + (size_t)(8 * half + 2 * cp) * plane_elems;
-      const __half* pb = pa + plane_elems;
-      // 4 rows x 3 words for each of the two channels
-      uint32_t wa[4][3], wb[4][3];
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j) {
-          wa[i][j] = load_word(pa + rowoff[i], rowok[i], m0 + j, g.W, w_even);
-          wb[i][j] = load_word(pb + rowoff[i], rowok[i], m0 + j, g.W, w_even);
-        }
-      // window d[i][col] as (channel c, channel c+1) pairs
-      uint32_t d[4][4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        d[i][0] = pk_hi(wa[i][0], wb[i][0]);
-        d[i][1] = pk_lo(wa[i][1], wb[i][1]);
-        d[i][2] = pk_hi(wa[i][1], wb[i][1]);
-        d[i][3] = pk_lo(wa[i][2], wb[i][2]);
-      }
-#pragma unroll
-      for (int a = 0; a < 4; ++a) {
-        uint32_t e[4];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) e[j] = bt_row(a, d[0][j], d[1][j], d[2][j], d[3][j]);
-        uint32_t v[4];
-        bt_cols(e[0], e[1], e[2], e[3], v);
-#pragma unroll
-        for (int b = 0; b < 4; ++b) out[4 * a + b][cp] = v[b];
-      }
-    }
-#pragma unroll
-    for (int t = 0; t < 16; ++t) sink(t, half, out[t][0], out[t][1], out[t][2], out[t][3]);
-  }
 }
 
 // ---------------------------------------------------------------------------
