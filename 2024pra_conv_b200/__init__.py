@@ -477,6 +477,18 @@ class Batch:
         _check(lib().wino_batch_tune(self._h, reps, lu, ou, _stream(stream)), "batch_tune")
         return [list(lu[i * NCFG:(i + 1) * NCFG]) for i in range(n)], list(ou)
 
+    def tuning_state(self):
+        """The autotuner's choices, to be saved (JSON-able) and restored later."""
+        return {"version": 1, "configs": [self.config(i) for i in range(len(self))], "order": self.order()}
+
+    def restore(self, state):
+        """Re-applies tuning_state() output (the same layer list) without re-tuning."""
+        if state.get("version") != 1 or len(state["configs"]) != len(self):
+            raise ValueError("tuning state of another version or layer list")
+        for i, c in enumerate(state["configs"]):
+            self.set_config(i, c)
+        self.set_order(state["order"])
+
     def capture(self, stream=None):
         _check(lib().wino_batch_graph_capture(self._h, _stream(stream)), "batch_graph_capture")
 

@@ -217,6 +217,53 @@ def evaluate(rows, epochs=3000, lr=3e-3, seed=0, default_cfg=0):
             "loss_last": float(hist[-1]), "held_out": len(te), "train": len(tr)}
 
 
+def train(rows, idx=None, epochs=3000, lr=3e-3, seed=0):
+    """Train on the given rows (default: the training split) with the CUDA
+    kernels; returns a model dict {params (float32 numpy), mu, sd}."""
+    import torch
+    idx = split(len(rows))[0] if idx is None else idx
+    x, t, m, _, norm = dataset(rows, idx)
+    dev = torch.device("cuda", 0)
+    p = torch.from_numpy(init_params(seed=seed)).to(dev)
+    mlp_train(p, torch.from_numpy(x).to(dev), torch.from_numpy(t).to(dev), torch.from_numpy(m).to(dev),
+              epochs=epochs, lr=lr)
+    return {"params": p.cpu().numpy(), "mu": norm.mu, "sd": norm.sd}
+
+
+def pick(model, shapes, allowed=None):
+    """Predicted-fastest configuration per shape (n, c, h, k) with the CUDA
+    inference kernel; `allowed`: configurations to choose from (default: the
+    tuning space, i.e. every configuration without CFG_DIRECT)."""
+    import torch
+    allowed = [c for c in range(NCFG) if not (c & 2)] if allowed is None else allowed
+    norm = Normaliser([[0.0] * F])
+    norm.mu, norm.sd = np.asarray(model["mu"]), np.asarray(model["sd"])
+    x = norm([raw_features(tuple(s)) for s in shapes])
+    dev = torch.device("cuda", 0)
+    pred = mlp_forward(torch.from_numpy(np.asarray(model["params"], np.float32)).to(dev),
+                       torch.from_numpy(x).to(dev)).cpu().numpy()
+    mask = np.full(NCFG, np.inf)
+    mask[allowed] = 0.0
+    return [int(v) for v in (pred + mask).argmin(1)]
+
+
+MODEL_VERSION = 1
+
+
+def save_model(model, path):
+    """Versioned checkpoint of a trained model (NumPy .npz)."""
+    np.savez(path, version=MODEL_VERSION, features=F, outputs=NCFG, params=model["params"],
+             mu=model["mu"], sd=model["sd"])
+
+
+def load_model(path):
+    """A checkpoint written by save_model; refuses other versions or shapes."""
+    d = np.load(path)
+    if int(d["version"]) != MODEL_VERSION or int(d["features"]) != F or int(d["outputs"]) != NCFG:
+        raise ValueError(f"{path}: cost-model checkpoint of another version or shape")
+    return {"params": d["params"].astype(np.float32), "mu": d["mu"], "sd": d["sd"]}
+
+
 def main(argv):
     if len(argv) >= 2 and argv[0] == "collect":
         rows = collect(random_shapes(), log=lambda s: print(s, flush=True))

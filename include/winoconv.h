@@ -217,6 +217,14 @@ int wino_conv2d_noalloc(const void* x, const void* weight, void* y, int n, int c
                         int k, void* stream);
 long long wino_noalloc_max_kc(void);
 
+/* Self-test of the failure detection (no counterpart in the reference, which
+ * has none): a kernel whose two bounded waits -- warp-wide and single-thread,
+ * the forms the conv kernels use -- wait on mbarriers nothing signals, so
+ * both run out after their time limit (~1 s), record their codes
+ * (code[0] = 1, code[1] = 2 expected) and return normally.  Returns a
+ * cudaError_t (0 = the kernel ended without a fault). */
+int wino_selftest_wait_timeout(uint32_t* code);
+
 /* Reads and clears the device error word of the conv kernels (0 = none;
  * otherwise the first wait that ran out or the first bad-shape launch). */
 int wino_error_read_clear(uint32_t* code);

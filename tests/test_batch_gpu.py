@@ -120,3 +120,30 @@ def test_batched_layer_set_one_launch_graph_and_tuner(wino, cuda, oracle_mod):
     check("graph 2")
     b.close()
     assert wino.error_read_clear() == 0
+
+
+def test_tuning_state_save_and_restore(wino, cuda, oracle_mod, tmp_path):
+    """Tuned choices survive a JSON round trip and re-apply without tuning."""
+    import json
+    import torch
+    layers = _layer_set(wino, oracle_mod, cuda, 4)
+    refs = [wino.conv2d_fused(x, u, k) for (x, wt, u, ws, y, k) in layers]
+    b = wino.Batch()
+    for (x, wt, u, ws, y, k) in layers:
+        b.add(x, u, k, y, workspace=ws)
+    b.tune(reps=1)
+    path = tmp_path / "tuning.json"
+    path.write_text(json.dumps(b.tuning_state()))
+    b.close()
+    b2 = wino.Batch()
+    for (x, wt, u, ws, y, k) in layers:
+        b2.add(x, u, k, y, workspace=ws)
+    state = json.loads(path.read_text())
+    b2.restore(state)
+    assert b2.tuning_state() == state
+    b2.run()
+    torch.cuda.synchronize()
+    for (x, wt, u, ws, y, k), r in zip(layers, refs):
+        assert torch.equal(y.view(torch.int16), r.view(torch.int16))
+    b2.close()
+    assert wino.error_read_clear() == 0

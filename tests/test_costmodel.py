@@ -38,3 +38,18 @@ def test_shape_space_and_split():
     assert f.shape == (400, cm.F) and np.isfinite(f).all()
     p = cm.init_params()
     assert np.array_equal(p, M.init_params(cm.F, cm.NCFG, seed=0))
+
+
+def test_model_checkpoint_round_trip(tmp_path):
+    cm = importlib.import_module("2024pra_conv_b200.costmodel")
+    model = {"params": cm.init_params(seed=3), "mu": np.arange(cm.F, dtype=np.float64),
+             "sd": np.ones(cm.F)}
+    path = str(tmp_path / "model.npz")
+    cm.save_model(model, path)
+    back = cm.load_model(path)
+    assert np.array_equal(back["params"], model["params"]) and np.array_equal(back["mu"], model["mu"])
+    np.savez(path, version=99, features=cm.F, outputs=cm.NCFG, params=model["params"], mu=model["mu"],
+             sd=model["sd"])
+    import pytest
+    with pytest.raises(ValueError):
+        cm.load_model(path)

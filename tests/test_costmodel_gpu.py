@@ -66,3 +66,17 @@ def test_cost_model_picks_within_10pct_of_exhaustive_and_beats_default(cuda, cap
     assert r["loss_last"] < r["loss_first"]
     assert r["regret_geomean"] <= 1.10
     assert r["gain_geomean"] >= 1.0
+
+
+@pytest.mark.skipif(not os.path.exists(TIMINGS), reason="timings fixture not generated")
+def test_trained_model_checkpoint_gives_the_same_picks(cuda, tmp_path):
+    cm = _cm()
+    with open(TIMINGS) as f:
+        rows = json.load(f)["rows"]
+    model = cm.train(rows, epochs=500)
+    shapes = [tuple(r["shape"]) for r in rows[:50]]
+    picks = cm.pick(model, shapes)
+    assert all(not (p & 2) for p in picks)                   # inside the tuning space
+    path = str(tmp_path / "m.npz")
+    cm.save_model(model, path)
+    assert cm.pick(cm.load_model(path), shapes) == picks
