@@ -41,9 +41,9 @@
 //
 // Warp roles (15 warps):
 //   warp 0       TMEM allocation; one thread issues the MMAs
-//   warp 1       lanes 0 and 1 bulk-copy the two U halves of a step (one
+//   warp 4       lanes 0 and 1 bulk-copy the two U halves of a step (one
 //                copy in flight per issuing thread, so two threads)
-//   warps 2-5    V producers, all four on every step: warp q forms channel
+//   warps 1,2,3,5 V producers, all four on every step: producer q forms channel
 //                half q&1 (8 channels) of tap rows 2(q>>1), 2(q>>1)+1 (8
 //                taps) of the step's V for all 32 tiles (lane = tile):
 //                B^T d B in packed fp16 straight into the K-major operand
@@ -51,11 +51,11 @@
 //                lane and tap).  They read the step's slab, or, without an
 //                XB workspace or when a block's rows exceed a slab, the NCHW
 //                input directly.
-//   warps 6-13   epilogue: drain TMEM one tap half at a time (the block's
+//   warps 7-14   epilogue: drain TMEM one tap half at a time (the block's
 //                last MMAs commit each half separately, and each drained half
 //                goes back to the MMA thread at once, so the drain overlaps
 //                the MMAs on both sides), A^T m A in fp32, fp16 NKPQ stores.
-//   warp 14      stager: with an XB workspace (p.transform_pin, written by
+//   warp 6       stager: with an XB workspace (p.transform_pin, written by
 //                the pre-pass of input_layout.cu) bulk-copies each step's
 //                input rows into a slab, up to two steps ahead (one copy
 //                per image the block touches, issued from separate lanes).
@@ -97,8 +97,17 @@ constexpr int SLAB_BASE = V_BASE + NVSLOT * V_SLOT_BYTES;
 constexpr int EPI_BASE = SLAB_BASE + NSLAB * SLAB_BYTES;
 constexpr int NWARP = 15;
 constexpr int NTHREAD = NWARP * 32;
-constexpr int WARP_MMA = 0, WARP_U = 1, WARP_V0 = 2, NWARP_V = 4, WARP_E0 = 6, NWARP_E = 8;
-constexpr int WARP_S = 14;
+// Warp w issues from scheduler (SMSP) w % 4.  The single MMA-issuing thread
+// must not share its scheduler with a busy warp (it was measured starved to
+// ~95 cycles per MMA next to a V producer), so scheduler 0 holds only the MMA
+// warp, the mostly waiting U loader and the two epilogue warps that TMEM lane
+// access pins there (warp w reads TMEM lanes 32*(w%4) ..): producers run on
+// schedulers 1-3.
+constexpr int WARP_MMA = 0, WARP_U = 4, WARP_S = 6, NWARP_V = 4, WARP_E0 = 7, NWARP_E = 8;
+// producer index of a warp (warps 1, 2, 3, 5), or -1
+__device__ __forceinline__ int producer_index(int warp) {
+  return warp >= 1 && warp <= 3 ? warp - 1 : (warp == 5 ? 3 : -1);
+}
 constexpr int SMEM_BYTES = EPI_BASE + 8 * EPI_WARP_BYTES + 1024;
 
 struct Shared {
@@ -430,8 +439,8 @@ __device__ __forceinline__ void fused_body(const Sched& sched, const VariantArgs
     }
     if (*abort_flag) __nanosleep(20000);  // let copies already issued land
     __syncwarp();
-  } else if (warp >= WARP_V0 && warp < WARP_V0 + NWARP_V) {
-    const int q = warp - WARP_V0;
+  } else if (producer_index(warp) >= 0) {
+    const int q = producer_index(warp);
     const int hh = q & 1;                     // K half of the step's operand row
     const int ar = q >> 1;                    // tap rows 2ar, 2ar+1 (taps 8ar .. 8ar+7)
     const uint32_t slab0 = smem_base + SLAB_BASE;
