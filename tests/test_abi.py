@@ -192,3 +192,30 @@ def test_ucache_load_refuses_missing_and_foreign_files(wino, tmp_path):
     assert L.wino_ucache_load(os.fsencode(str(p)), dummy, 32, 32, 1) == 6  # WINO_ESTALE
     assert L.wino_ucache_load(os.fsencode(str(p)), dummy, 32, 24, 1) == 2  # bad shape
     assert L.wino_ucache_load(None, dummy, 32, 32, 1) == 1
+
+
+def test_new_entry_points_validate_before_launching(wino):
+    """Argument checks of the extension entry points return codes without any
+    CUDA call (so they run here without a GPU)."""
+    L = wino.lib()
+    d = ctypes.c_void_p(0x10000)
+    odd = ctypes.c_void_p(0x10002)
+    # fused epilogue: null pointers, misaligned workspace/residual, bad shape
+    assert L.wino_conv2d_fused_epilogue(None, d, d, d, None, None, 0, 1, 16, 8, 8, 16, None) == 1
+    assert L.wino_conv2d_fused_epilogue(d, d, odd, d, None, None, 0, 1, 16, 8, 8, 16, None) == 1
+    assert L.wino_conv2d_fused_epilogue(d, d, d, d, None, odd, 0, 1, 16, 8, 8, 16, None) == 1
+    assert L.wino_conv2d_fused_epilogue(d, d, d, d, None, None, 0, 1, 24, 8, 8, 16, None) == 2
+    # direct conv: general shapes accepted by validation, invalid ones refused
+    assert L.wino_conv2d_direct(None, d, d, 1, 3, 8, 8, 4, 3, 3, 1, 1, 1, 1, None) == 1
+    assert L.wino_conv2d_direct(d, d, d, 1, 3, 2, 2, 4, 5, 5, 1, 1, 0, 0, None) == 1   # filter > input
+    assert L.wino_conv2d_direct(d, d, d, 1, 3, 8, 8, 4, 3, 3, 0, 1, 1, 1, None) == 1   # stride 0
+    assert L.wino_conv2d_direct(d, d, d, 1, 3, 40000, 8, 4, 3, 3, 1, 1, 1, 1, None) == 2
+    # variants: fp8 needs C % 32 == 0; bad variant id
+    assert L.wino_variant_workspace_bytes(2, 1, 48, 8, 8, 16) == 0
+    assert L.wino_variant_workspace_bytes(9, 1, 64, 8, 8, 16) == 0
+    assert L.wino_conv2d_variant(9, d, d, d, d, 1, 64, 8, 8, 16, None) == 1
+    assert L.wino_conv2d_variant(0, d, d, d, odd, 1, 64, 8, 8, 16, None) == 1           # ws alignment
+    # schedule configurations: cfg out of range, missing workspace
+    assert L.wino_conv2d_fused_cfg(d, d, None, d, 1, 64, 8, 8, 16, 16, None) == 1
+    assert L.wino_conv2d_fused_cfg(d, d, None, d, 1, 64, 8, 8, 16, 0, None) == 1
+    assert L.wino_conv2d_fused_ws(d, d, None, d, 1, 64, 8, 8, 16, None) == 1
