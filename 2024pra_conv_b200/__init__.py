@@ -112,6 +112,10 @@ def lib():
             "wino_unfused_workspace_bytes": ([i, i, i, i, i, ctypes.POINTER(sz), ctypes.POINTER(sz)], i),
             "wino_conv2d_unfused": ([vp, vp, vp, vp, vp, i, i, i, i, i, vp], i),
             "wino_error_read_clear": ([ctypes.POINTER(ctypes.c_uint32)], i),
+            "wino_f4_filter_bytes": ([i, i, i], sz),
+            "wino_f4_workspace_bytes": ([i, i, i, i, i, i], sz),
+            "wino_f4_filter_transform": ([vp, i, i, i, vp, sz, vp], i),
+            "wino_conv2d_f4": ([vp, vp, i, i, i, i, i, i, vp, sz, vp], i),
         }
         for name, (args, res) in sigs.items():
             fn = getattr(L, name)
@@ -395,6 +399,53 @@ def _aligned_ws(nbytes, device):
     buf = torch.empty(nbytes + 256, dtype=torch.uint8, device=device)
     off = (-buf.data_ptr()) % 256
     return buf[off:off + nbytes]
+
+
+# ------------------------------------------------------ F(4x4,3x3) path ---
+def f4_workspace_bytes(n, c, h, w, k, hilo=True) -> int:
+    return int(lib().wino_f4_workspace_bytes(n, c, h, w, k, int(bool(hilo))))
+
+
+class ConvF4:
+    """Winograd F(4x4,3x3) conv of one weight tensor over inputs of one shape.
+
+    The filter transform runs once (constructor / set_weight) into the head of
+    the workspace; every call runs input transform, 36-tap GEMM and output
+    transform.  hilo=True stores U and V as fp16 hi + lo pairs (the accurate
+    form); hilo=False as single fp16 values (about ten times larger error)."""
+
+    def __init__(self, w, n, h, wd, hilo=True, stream=None):
+        self.k, self.c = w.shape[:2]
+        self.n, self.h, self.wd, self.hilo = n, h, wd, int(bool(hilo))
+        self.nbytes = f4_workspace_bytes(n, self.c, h, wd, self.k, self.hilo)
+        self.ws = _aligned_ws(self.nbytes, w.device)
+        self.set_weight(w, stream)
+
+    def set_weight(self, w, stream=None):
+        if tuple(w.shape) != (self.k, self.c, 3, 3) or w.dtype.itemsize != 2:
+            raise WinoError(WINO_EINVAL, "ConvF4.set_weight: weight shape")
+        self._w = w
+        _check(lib().wino_f4_filter_transform(ctypes.c_void_p(w.data_ptr()), self.k, self.c, self.hilo,
+                                              ctypes.c_void_p(self.ws.data_ptr()), self.nbytes,
+                                              _stream(stream)), "f4_filter_transform")
+
+    def __call__(self, x, out=None, stream=None):
+        import torch
+        if tuple(x.shape) != (self.n, self.c, self.h, self.wd):
+            raise WinoError(WINO_EINVAL, "ConvF4: input shape")
+        y = out if out is not None else torch.empty((self.n, self.k, self.h, self.wd), dtype=torch.float16,
+                                                   device=x.device)
+        _check(lib().wino_conv2d_f4(ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(y.data_ptr()), self.n,
+                                    self.c, self.h, self.wd, self.k, self.hilo,
+                                    ctypes.c_void_p(self.ws.data_ptr()), self.nbytes, _stream(stream)),
+               "conv2d_f4")
+        return y
+
+
+def conv2d_f4(x, w, hilo=True, out=None, stream=None):
+    """One F(4x4,3x3) conv (filter transform included)."""
+    n, c, h, wd = x.shape
+    return ConvF4(w, n, h, wd, hilo, stream)(x, out, stream)
 
 
 def cfg_workspace_bytes(n, c, h, w, k, cfg) -> int:

@@ -64,13 +64,19 @@ __global__ void __launch_bounds__(256) unfused_input_transform(KernelParam p) {
 // ------------------------------------------------------------- tap GEMMs ---
 using namespace unfused;
 
-__global__ void __launch_bounds__(NTHREAD, 1) unfused_gemm(KernelParam p) {
+// One batched tap GEMM: for every tap t, M[t][k][tile] = sum_c V2[t][tile][c]
+// * U2[t][k][c] over `c_red` reduction channels, M stored as fp16 (M32 false)
+// or fp32 (M32 true).  The F(2x2) comparator runs it with 16 taps and c_red =
+// C; the F(4x4,3x3) path with 36 taps and c_red = C or 3C (hi+lo pieces).
+template <bool M32>
+__device__ __forceinline__ void tap_gemm_body(const TapGemm& tg) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   __shared__ unfused::Shared sh;
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  const Geometry g = make_geometry(p, TB2);
+  struct { int nTB, CS, K, C; } g;
+  g.nTB = tg.ntb; g.CS = tg.c_red >> 4; g.K = tg.k; g.C = tg.c_red;
   const int nKB2 = (g.K + KB2 - 1) / KB2;
-  const long long nunits = 16LL * g.nTB * nKB2;
+  const long long nunits = (long long)tg.taps * g.nTB * nKB2;
   const int nst = (g.CS + SK - 1) / SK;  // stages per unit
   const int warp = warp_id(), lane = lane_id();
   uint32_t* err = &g_unfused_err;
@@ -97,8 +103,8 @@ __global__ void __launch_bounds__(NTHREAD, 1) unfused_gemm(KernelParam p) {
 
   if (warp == 0) {
     if (lane == 0) {
-      const uint8_t* v2 = static_cast<const uint8_t*>(p.transform_pin);
-      const uint8_t* u2 = static_cast<const uint8_t*>(p.transform_filter);
+      const uint8_t* v2 = static_cast<const uint8_t*>(tg.v2);
+      const uint8_t* u2 = static_cast<const uint8_t*>(tg.u2);
       uint32_t it = 0;
       for (long long u = blockIdx.x; u < nunits && !*abort_flag; u += gridDim.x) {
         int t, tb, kb;
@@ -152,7 +158,6 @@ __global__ void __launch_bounds__(NTHREAD, 1) unfused_gemm(KernelParam p) {
     __syncwarp();
   } else {
     const int quarter = warp & 3;
-    __half* m16 = static_cast<__half*>(p.mid_result);
     const size_t ntp = (size_t)g.nTB * TB2;
     uint32_t ui = 0;
     for (long long u = blockIdx.x; u < nunits; u += gridDim.x, ++ui) {
@@ -168,9 +173,16 @@ __global__ void __launch_bounds__(NTHREAD, 1) unfused_gemm(KernelParam p) {
         float v[16];
         tmem_ld16(taddr + c0, v);
         tmem_ld_wait();
-        __half* dst = m16 + ((size_t)t * g.K + (size_t)kb * KB2 + c0) * ntp + tile;
+        const size_t row = ((size_t)t * g.K + (size_t)kb * KB2 + c0) * ntp + tile;
+        if constexpr (M32) {
+          float* dst = static_cast<float*>(tg.m) + row;
 #pragma unroll
-        for (int j = 0; j < 16; ++j) dst[(size_t)j * ntp] = __float2half_rn(v[j]);
+          for (int j = 0; j < 16; ++j) dst[(size_t)j * ntp] = v[j];
+        } else {
+          __half* dst = static_cast<__half*>(tg.m) + row;
+#pragma unroll
+          for (int j = 0; j < 16; ++j) dst[(size_t)j * ntp] = __float2half_rn(v[j]);
+        }
       }
       tc_fence_before();
       __syncwarp();
@@ -184,6 +196,16 @@ __global__ void __launch_bounds__(NTHREAD, 1) unfused_gemm(KernelParam p) {
     tmem_dealloc(tmem, 256);
   }
 }
+
+__global__ void __launch_bounds__(NTHREAD, 1) unfused_gemm(KernelParam p) {
+  const Geometry g = make_geometry(p, TB2);
+  TapGemm s;
+  s.v2 = p.transform_pin; s.u2 = p.transform_filter; s.m = p.mid_result;
+  s.taps = 16; s.ntb = g.nTB; s.c_red = g.C; s.k = g.K;
+  tap_gemm_body<false>(s);
+}
+
+__global__ void __launch_bounds__(NTHREAD, 1) tap_gemm_f32(TapGemm s) { tap_gemm_body<true>(s); }
 
 // ------------------------------------------------------ output transform ---
 // grid (ceil(tiles/256), K): thread = (tile, k); reads the 16 taps of M16.
@@ -264,6 +286,16 @@ int wino_unfused_launch(const KernelParam* p, int sms, cudaStream_t stream) {
   const int grid = (int)(units < sms ? units : sms);
   unfused_gemm<<<grid, NTHREAD, unfused::SMEM_BYTES, stream>>>(*p);
   unfused_output_transform<<<dim3((unsigned)((nt + 255) / 256), p->k), 256, 0, stream>>>(*p);
+  return (int)cudaGetLastError();
+}
+
+int wino_tap_gemm_f32_launch(const TapGemm* s, int sms, void* stream) {
+  static const cudaError_t attr = cudaFuncSetAttribute(
+      tap_gemm_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, unfused::SMEM_BYTES);
+  if (attr != cudaSuccess) return (int)attr;
+  const long long units = (long long)s->taps * s->ntb * ((s->k + KB2 - 1) / KB2);
+  const int grid = (int)(units < sms ? units : sms);
+  tap_gemm_f32<<<grid, NTHREAD, unfused::SMEM_BYTES, (cudaStream_t)stream>>>(*s);
   return (int)cudaGetLastError();
 }
 

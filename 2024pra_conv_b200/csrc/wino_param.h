@@ -36,4 +36,17 @@ struct VariantArgs {
 static_assert(offsetof(KernelParam, n) == 48, "dims start after six pointers");
 static_assert(offsetof(KernelParam, Ow) == 72, "thirteen shorts");
 
+// Arguments of one batched tap GEMM of the unfused layouts (V2 / U2 of
+// wino_common.cuh): `taps` taps, `ntb` 128-tile blocks, `c_red` reduction
+// channels (a multiple of 16), `k` output channels (a multiple of 16).
+struct TapGemm {
+  const void* v2;
+  const void* u2;
+  void* m;                   // M[t][k][tile], tiles padded to ntb * 128
+  int taps, ntb, c_red, k;
+};
+
 }  // namespace wino
+
+// fp32-M instance of the tap GEMM (unfused_conv.cu), on `sms` persistent CTAs.
+extern "C" int wino_tap_gemm_f32_launch(const wino::TapGemm* s, int sms, void* stream);

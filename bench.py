@@ -421,7 +421,8 @@ def run_ours(args, rank, world, local_rank):
 def extension_legs(wino, dev, flush, ev, peaks, steps):
     """Rank-0 extras on the other workloads: the batched 12-layer ResNet-style
     set (autotuned, one persistent launch, CUDA graph), the precision
-    variants on N64 C=K256 H14 with their errors against FP64, and the
+    variants on N64 C=K256 H14 with their errors against FP64, Winograd
+    F(4x4,3x3) beside F(2x2) on N128 C256 H28, the fused epilogue, and the
     learned cost model measured against exhaustive tuning on the committed
     timings.  Not part of `value`."""
     import numpy as np
@@ -517,6 +518,41 @@ def extension_legs(wino, dev, flush, ev, peaks, steps):
     out["variants"] = {"workload": "N64 C256 H14 W14 K256, x ~ U[-1,1]; per call: filter transform "
                                    "+ input pre-pass + fused kernel", **var}
 
+    # --- Winograd F(4x4,3x3), hi+lo and plain, on N128 C256 H28 K256 against F(2x2) fused
+    n, c, h, k = 128, 256, 28, 256
+    x16, w16 = oracle.make_inputs(n, c, h, h, k, seed=0, x_dist="relu_normal", w_std=np.sqrt(2.0 / (9 * c)))
+    x = torch.from_numpy(x16).to(dev)
+    wt = torch.from_numpy(w16).to(dev)
+    y64 = torch.nn.functional.conv2d(x.double(), wt.double(), padding=1)
+    y = torch.empty((n, k, h, h), dtype=torch.float16, device=dev)
+    f4 = {}
+    for name, hilo in [("f4_hilo", True), ("f4_f16", False)]:
+        conv = wino.ConvF4(wt, n, h, h, hilo=hilo)
+        conv(x, out=y)
+        torch.cuda.synchronize()
+        d = y.double() - y64
+        us = timed(lambda: conv(x, out=y), steps)
+        f4[name] = {"us_per_call": us,
+                    "rel_l2": float(torch.linalg.vector_norm(d) / torch.linalg.vector_norm(y64)),
+                    "max_norm": float(d.abs().max() / y64.abs().max()),
+                    "direct_equiv_tflops": direct_flops(n, c, h, h, k) / (us * 1e-6) / 1e12,
+                    "workspace_bytes": conv.nbytes}
+        del conv
+    u = wino.filter_transform(wt)
+    ws = torch.empty(wino.fused_workspace_bytes(n, c, h, h), dtype=torch.uint8, device=dev)
+    wino.conv2d_fused(x, u, k, out=y, workspace=ws)
+    torch.cuda.synchronize()
+    d = y.double() - y64
+    us = timed(lambda: wino.conv2d_fused(x, u, k, out=y, workspace=ws), steps)
+    f4["f2_fused_f16"] = {"us_per_call": us,
+                          "rel_l2": float(torch.linalg.vector_norm(d) / torch.linalg.vector_norm(y64)),
+                          "max_norm": float(d.abs().max() / y64.abs().max()),
+                          "direct_equiv_tflops": direct_flops(n, c, h, h, k) / (us * 1e-6) / 1e12}
+    out["winograd_f4"] = {"workload": "N128 C256 H28 K256, x = relu(N(0,1)); transformed filter cached; "
+                                      "per call: input transform + 36-tap GEMM + output transform (F4), "
+                                      "pre-pass + fused kernel (F2)", **f4}
+    del x, wt, y64, y, u, ws
+
     # --- fused epilogue (bias + residual + ReLU) vs the conv then separate elementwise ops
     n, c, h, k = 128, 256, 28, 256
     x16, w16 = oracle.make_inputs(n, c, h, h, k, seed=0, x_dist="relu_normal", w_std=np.sqrt(2.0 / (9 * c)))
@@ -579,6 +615,10 @@ def run_only(args):
         ws = wino.UnfusedWorkspace(n, c, h, w, k, dev)
         for _ in range(args.steps):
             wino.conv2d_unfused(x, u2, k, ws=ws)
+    elif args.only == "f4":
+        conv = wino.ConvF4(wt, n, h, w, hilo=True)
+        for _ in range(args.steps):
+            conv(x)
     else:
         for _ in range(args.steps):
             wino.dropin_conv2d(x, wt)
@@ -598,7 +638,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the layer-set / variants / cost-model legs")
-    ap.add_argument("--only", choices=["fused", "unfused", "dropin"],
+    ap.add_argument("--only", choices=["fused", "unfused", "dropin", "f4"],
                     help="only launch this path (profiler captures)")
     ap.add_argument("--n", type=int, default=0, help="batch size for --only")
     args = ap.parse_args()

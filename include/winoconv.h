@@ -31,7 +31,7 @@ enum {
   WINO_EUNSUPPORTED = 2,  /* shape outside the contract above            */
   WINO_ECUDA = 3,         /* a CUDA runtime call failed                  */
   WINO_EDEVICE = 4,       /* a kernel reported an error (see error word) */
-  WINO_ESCRATCH = 5,      /* filter too large for wino_conv2d_noalloc's fixed scratch */
+  WINO_ESCRATCH = 5,      /* scratch or caller workspace too small for the shape */
   WINO_ESTALE = 6,        /* persisted U cache is for other weights, shape or layout */
   WINO_EIO = 7            /* file could not be read or written */
 };
@@ -130,6 +130,24 @@ int wino_conv2d_unfused(const void* x, const void* ucache2, void* y, void* v_ws,
 size_t wino_variant_workspace_bytes(int variant, int n, int c, int h, int w, int k);
 int wino_conv2d_variant(int variant, const void* x, const void* weight, void* y, void* workspace,
                         int n, int c, int h, int w, int k, void* stream);
+
+/* Winograd F(4x4,3x3) (36 taps, 4x4 output tiles; no counterpart in the
+ * reference, which has F(2x2,3x3) only: src/preprocessing.cuh:75-424,
+ * src/matrixmul.cuh:139-556, src/conv2d.cpp:17-250).  U and V are formed in
+ * fp32 and stored as fp16: one piece (hilo = 0) or a hi + lo pair (hilo = 1,
+ * products hi*hi + lo*hi + hi*lo accumulated in fp32); M stays fp32 and the
+ * output transform is fp32.  Same shape contract as the fused path (3x3,
+ * stride 1, pad 1, c and k multiples of 16).  workspace: 256-byte aligned,
+ * wino_f4_workspace_bytes() bytes; its first wino_f4_filter_bytes() bytes
+ * hold the transformed filter, written by wino_f4_filter_transform() once
+ * per weight tensor and read by every wino_conv2d_f4() after it (the rest
+ * holds V and M).  Too small a workspace returns WINO_ESCRATCH. */
+size_t wino_f4_filter_bytes(int k, int c, int hilo);
+size_t wino_f4_workspace_bytes(int n, int c, int h, int w, int k, int hilo);
+int wino_f4_filter_transform(const void* weight, int k, int c, int hilo, void* workspace,
+                             size_t workspace_bytes, void* stream);
+int wino_conv2d_f4(const void* x, void* y, int n, int c, int h, int w, int k, int hilo,
+                   void* workspace, size_t workspace_bytes, void* stream);
 
 /* Schedule configurations of the fused kernel (bits): WINO_CFG_KMAJOR orders
  * the work blocks k-block-major (consecutive blocks share U) instead of

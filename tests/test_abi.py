@@ -219,3 +219,30 @@ def test_new_entry_points_validate_before_launching(wino):
     assert L.wino_conv2d_fused_cfg(d, d, None, d, 1, 64, 8, 8, 16, 16, None) == 1
     assert L.wino_conv2d_fused_cfg(d, d, None, d, 1, 64, 8, 8, 16, 0, None) == 1
     assert L.wino_conv2d_fused_ws(d, d, None, d, 1, 64, 8, 8, 16, None) == 1
+
+
+def test_f4_entry_points_validate_and_size(wino):
+    """Winograd F(4x4,3x3) entry points: workspace arithmetic and the argument
+    checks that return before any CUDA call."""
+    L = wino.lib()
+    d = ctypes.c_void_p(0x10000)
+    odd = ctypes.c_void_p(0x10010)          # 16- but not 256-byte aligned
+    r256 = lambda b: (b + 255) // 256 * 256
+    # N128 C256 H28 K256: 7 x 7 tiles per image -> 6272 tiles, 49 blocks of 128
+    ntp = 49 * 128
+    for hilo, cr in ((0, 256), (1, 768)):
+        u, v, m = r256(36 * 256 * cr * 2), r256(36 * ntp * cr * 2), r256(36 * 256 * ntp * 4)
+        assert L.wino_f4_filter_bytes(256, 256, hilo) == u
+        assert L.wino_f4_workspace_bytes(128, 256, 28, 28, 256, hilo) == u + v + m
+    full = L.wino_f4_workspace_bytes(1, 16, 8, 8, 16, 1)
+    fb = L.wino_f4_filter_bytes(16, 16, 1)
+    assert L.wino_f4_filter_transform(None, 16, 16, 1, d, fb, None) == 1
+    assert L.wino_f4_filter_transform(d, 16, 24, 1, d, fb, None) == 2        # C % 16
+    assert L.wino_f4_filter_transform(d, 16, 16, 2, d, fb, None) == 1        # hilo not 0/1
+    assert L.wino_f4_filter_transform(d, 16, 16, 1, d, fb - 1, None) == 5    # workspace too small
+    assert L.wino_f4_filter_transform(d, 16, 16, 1, odd, fb, None) == 1      # alignment
+    assert L.wino_conv2d_f4(None, d, 1, 16, 8, 8, 16, 1, d, full, None) == 1
+    assert L.wino_conv2d_f4(d, d, 1, 16, 8, 8, 24, 1, d, full, None) == 2    # K % 16
+    assert L.wino_conv2d_f4(d, d, 0, 16, 8, 8, 16, 1, d, full, None) == 1    # n = 0
+    assert L.wino_conv2d_f4(d, d, 1, 16, 8, 8, 16, 1, d, full - 1, None) == 5
+    assert L.wino_conv2d_f4(d, d, 1, 16, 8, 8, 16, 1, odd, full, None) == 1

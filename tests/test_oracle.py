@@ -69,3 +69,39 @@ def test_e4m3_rounding_known_values():
                      0.0, 240.0, 0.017578125])
     want = np.array([1.0, 1.0, 1.25, -1.0, 448.0, 448.0, 2.0 ** -9, 2.0 ** -9, 0.0, 240.0, 0.017578125])
     assert np.array_equal(_e4m3(vals), want)
+
+
+@pytest.mark.parametrize("shape", [(1, 16, 9, 7, 16), (2, 16, 4, 5, 32), (1, 32, 1, 1, 16), (1, 16, 13, 12, 16)])
+def test_winograd_f4_restatement_is_exact(oracle_mod, shape):
+    """F(4x4,3x3) in fp64 equals the direct conv, ragged tiles included."""
+    from oracle import winograd_f4 as F4
+    n, c, h, w, k = shape
+    x, wt = oracle_mod.make_inputs(n, c, h, w, k, seed=4)
+    y64 = oracle_mod.conv2d_f64(x, wt)
+    assert np.max(np.abs(F4.conv2d_f4_f64(x, wt) - y64)) <= 1e-12 * np.max(np.abs(y64))
+
+
+@pytest.mark.parametrize("dist", ["uniform", "relu_normal", "student_t3"])
+def test_winograd_f4_error_columns(oracle_mod, dist):
+    """F(4x4) with single fp16 U and V misses the 2e-3 target (transform
+    coefficients up to 5, 1/24 and 8); the hi+lo pieces bring it to the fp16
+    output-rounding floor, below F(2x2)'s fp16 error."""
+    from oracle import winograd as W, winograd_f4 as F4
+    x, w = oracle_mod.make_inputs(2, 64, 20, 20, 32, seed=6, x_dist=dist)
+    y64 = oracle_mod.conv2d_f64(x, w)
+    plain = oracle_mod.rel_l2(F4.conv2d_f4_emulated(x, w, hilo=False).astype(np.float16), y64)
+    hilo = oracle_mod.rel_l2(F4.conv2d_f4_emulated(x, w, hilo=True).astype(np.float16), y64)
+    f2 = oracle_mod.rel_l2(W.conv2d_winograd_emulated(x, w, "f16").astype(np.float16), y64)
+    floor = oracle_mod.rel_l2(y64.astype(np.float16), y64)
+    assert plain > 2e-3
+    assert hilo < 1.2 * floor < f2
+
+
+def test_winograd_f4_hilo_split():
+    from oracle import winograd_f4 as F4
+    a = np.array([1 / 3, -1 / 6, 1e-3 / 7, 1234.567, 0.0])
+    hi, lo = F4.split_hilo(a)
+    assert np.all(hi.astype(np.float16).astype(np.float64) == hi)
+    # lo's own rounding: half an fp16 step of |a - hi| <= 2^-12 |a|, or half
+    # the fp16 subnormal step 2^-24 where lo is subnormal
+    assert np.all(np.abs(hi + lo - a.astype(np.float32)) <= np.maximum(2.0 ** -22 * np.abs(a), 2.0 ** -25))
