@@ -7,8 +7,9 @@
 //
 //   unfused_input_transform   X (NCHW) -> V2 (tile-major, fp16)
 //   unfused_gemm              16 x [tiles x C] * [C x K]^T on tcgen05 with
-//                             128 x 128 output tiles (the full-rate MMA
-//                             shape), double-buffered TMEM, fp32 accumulate
+//                             128 x 256 output tiles (two 128 x 128 MMAs per
+//                             K-step sharing the tile operand), double-
+//                             buffered TMEM, fp32 accumulate
 //                             -> M16[t][k][tile] fp16
 //   unfused_output_transform  M16 -> Y (N K P Q), A^T m A in fp32
 //
@@ -28,10 +29,12 @@ namespace unfused {
 
 constexpr int NSTAGE = 4;
 constexpr int SK = 4;                         // K-steps (16 channels each) per stage
+constexpr int KPU = 2;                        // 128-row k-blocks per work unit (share A)
 constexpr int A_STEP = TB2 * 16 * 2;          // 4 KB: one K-step of a 128-tile block
 constexpr int B_STEP_MAX = KB2 * 16 * 2;      // 4 KB: one K-step of a 128-row k-block
 constexpr int STAGE_A = SK * A_STEP;
-constexpr int STAGE_BYTES = SK * (A_STEP + B_STEP_MAX);
+constexpr int STAGE_B = SK * B_STEP_MAX;      // one k-block's operand of a stage
+constexpr int STAGE_BYTES = STAGE_A + KPU * STAGE_B;
 constexpr int SMEM_BYTES = NSTAGE * STAGE_BYTES + 1024;
 constexpr int NTHREAD = 6 * 32;               // producer, MMA, 4 epilogue warps
 
@@ -68,6 +71,9 @@ using namespace unfused;
 // * U2[t][k][c] over `c_red` reduction channels, M stored as fp16 (M32 false)
 // or fp32 (M32 true).  The F(2x2) comparator runs it with 16 taps and c_red =
 // C; the F(4x4,3x3) path with 36 taps and c_red = C or 3C (hi+lo pieces).
+// A work unit is (tap, 128-tile block, pair of 128-row k-blocks): each K-step
+// issues two M=128 N<=128 MMAs that share the V operand, into two 128-column
+// TMEM accumulators; units are double-buffered in TMEM (512 columns).
 template <bool M32>
 __device__ __forceinline__ void tap_gemm_body(const TapGemm& tg) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -76,7 +82,8 @@ __device__ __forceinline__ void tap_gemm_body(const TapGemm& tg) {
   struct { int nTB, CS, K, C; } g;
   g.nTB = tg.ntb; g.CS = tg.c_red >> 4; g.K = tg.k; g.C = tg.c_red;
   const int nKB2 = (g.K + KB2 - 1) / KB2;
-  const long long nunits = (long long)tg.taps * g.nTB * nKB2;
+  const int nKP = (nKB2 + KPU - 1) / KPU;
+  const long long nunits = (long long)tg.taps * g.nTB * nKP;
   const int nst = (g.CS + SK - 1) / SK;  // stages per unit
   const int warp = warp_id(), lane = lane_id();
   uint32_t* err = &g_unfused_err;
@@ -87,7 +94,7 @@ __device__ __forceinline__ void tap_gemm_body(const TapGemm& tg) {
     sh.abort_flag = 0;
     fence_barrier_init();
   }
-  if (warp == 1) { tmem_alloc(&sh.tmem_base, 256); tmem_relinquish(); }
+  if (warp == 1) { tmem_alloc(&sh.tmem_base, 512); tmem_relinquish(); }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -95,10 +102,14 @@ __device__ __forceinline__ void tap_gemm_body(const TapGemm& tg) {
   volatile int* abort_flag = &sh.abort_flag;
   const uint32_t sbase = smem_u32(smem);
 
-  auto unit_coords = [&](long long u, int& t, int& tb, int& kb) {
-    kb = (int)(u % nKB2);
-    tb = (int)((u / nKB2) % g.nTB);
-    t = (int)(u / ((long long)nKB2 * g.nTB));
+  // kb = first k-block of the unit; kbs[i] = rows of its i-th k-block (0: absent)
+  auto unit_coords = [&](long long u, int& t, int& tb, int& kb, int (&kbs)[KPU]) {
+    const int kp = (int)(u % nKP);
+    tb = (int)((u / nKP) % g.nTB);
+    t = (int)(u / ((long long)nKP * g.nTB));
+    kb = kp * KPU;
+#pragma unroll
+    for (int i = 0; i < KPU; ++i) kbs[i] = kb + i < nKB2 ? kblock2_rows(kb + i, g.K) : 0;
   };
 
   if (warp == 0) {
@@ -107,21 +118,26 @@ __device__ __forceinline__ void tap_gemm_body(const TapGemm& tg) {
       const uint8_t* u2 = static_cast<const uint8_t*>(tg.u2);
       uint32_t it = 0;
       for (long long u = blockIdx.x; u < nunits && !*abort_flag; u += gridDim.x) {
-        int t, tb, kb;
-        unit_coords(u, t, tb, kb);
-        const int kbs = kblock2_rows(kb, g.K);
+        int t, tb, kb, kbs[KPU];
+        unit_coords(u, t, tb, kb, kbs);
         for (int j = 0; j < nst; ++j, ++it) {
           const int st = it % NSTAGE;
           if (it >= NSTAGE &&
               !mbar_wait(&sh.empty[st], (it / NSTAGE - 1) & 1, abort_flag, err, ERR_WAIT_EMPTY))
             break;
           const int nk = min(SK, g.CS - j * SK);
-          const uint32_t abytes = nk * A_STEP, bbytes = nk * kbs * 32;
-          mbar_arrive_expect_tx(&sh.full[st], abytes + bbytes);
+          const uint32_t abytes = nk * A_STEP;
+          uint32_t tx = abytes;
+#pragma unroll
+          for (int i = 0; i < KPU; ++i) tx += nk * kbs[i] * 32;
+          mbar_arrive_expect_tx(&sh.full[st], tx);
           bulk_g2s(smem + st * STAGE_BYTES, v2 + v2_piece(t, tb, j * SK, g.nTB, g.CS) * 2, abytes,
                    &sh.full[st]);
-          bulk_g2s(smem + st * STAGE_BYTES + STAGE_A, u2 + u2_piece(t, kb, j * SK, g.K, g.C) * 2,
-                   bbytes, &sh.full[st]);
+#pragma unroll
+          for (int i = 0; i < KPU; ++i)
+            if (kbs[i])
+              bulk_g2s(smem + st * STAGE_BYTES + STAGE_A + i * STAGE_B,
+                       u2 + u2_piece(t, kb + i, j * SK, g.K, g.C) * 2, nk * kbs[i] * 32, &sh.full[st]);
         }
       }
       if (*abort_flag) __nanosleep(20000);
@@ -131,24 +147,29 @@ __device__ __forceinline__ void tap_gemm_body(const TapGemm& tg) {
     if (lane == 0) {
       uint32_t it = 0, ui = 0;
       for (long long u = blockIdx.x; u < nunits && !*abort_flag; u += gridDim.x, ++ui) {
-        int t, tb, kb;
-        unit_coords(u, t, tb, kb);
-        const int kbs = kblock2_rows(kb, g.K);
-        const uint32_t idesc = instr_desc(128, kbs, 0, 0, 1, 0);
+        int t, tb, kb, kbs[KPU];
+        unit_coords(u, t, tb, kb, kbs);
+        uint32_t idesc[KPU];
+#pragma unroll
+        for (int i = 0; i < KPU; ++i) idesc[i] = instr_desc(128, kbs[i] ? kbs[i] : 16, 0, 0, 1, 0);
         const int ab = ui & 1;
         if (ui >= 2 && !mbar_wait(&sh.accempty[ab], ((ui >> 1) - 1) & 1, abort_flag, err, ERR_WAIT_DRAIN))
           break;
         tc_fence_after();
-        const uint32_t d = tmem + ab * 128;
+        const uint32_t d = tmem + ab * (KPU * 128);
         for (int j = 0; j < nst; ++j, ++it) {
           const int st = it % NSTAGE;
           if (!mbar_wait(&sh.full[st], (it / NSTAGE) & 1, abort_flag, err, ERR_WAIT_FULL)) break;
           tc_fence_after();
           const int nk = min(SK, g.CS - j * SK);
-          const uint32_t a0 = sbase + st * STAGE_BYTES, b0 = a0 + STAGE_A;
+          const uint32_t a0 = sbase + st * STAGE_BYTES;
           for (int kk = 0; kk < nk; ++kk) {
-            mma_f16(d, smem_desc(a0 + kk * A_STEP, 128, 256), smem_desc(b0 + kk * kbs * 32, 128, 256),
-                    idesc, (j > 0 || kk > 0) ? 1u : 0u);
+            const uint64_t adesc = smem_desc(a0 + kk * A_STEP, 128, 256);
+#pragma unroll
+            for (int i = 0; i < KPU; ++i)
+              if (kbs[i])
+                mma_f16(d + i * 128, adesc, smem_desc(a0 + STAGE_A + i * STAGE_B + kk * kbs[i] * 32, 128, 256),
+                        idesc[i], (j > 0 || kk > 0) ? 1u : 0u);
           }
           mma_commit(&sh.empty[st]);
         }
@@ -161,19 +182,21 @@ __device__ __forceinline__ void tap_gemm_body(const TapGemm& tg) {
     const size_t ntp = (size_t)g.nTB * TB2;
     uint32_t ui = 0;
     for (long long u = blockIdx.x; u < nunits; u += gridDim.x, ++ui) {
-      int t, tb, kb;
-      unit_coords(u, t, tb, kb);
-      const int kbs = kblock2_rows(kb, g.K);
+      int t, tb, kb, kbs[KPU];
+      unit_coords(u, t, tb, kb, kbs);
       const int ab = ui & 1;
       if (!mbar_wait(&sh.accfull[ab], (ui >> 1) & 1, abort_flag, err, ERR_WAIT_ACCUM)) break;
       tc_fence_after();
       const size_t tile = (size_t)tb * TB2 + quarter * 32 + lane;
-      const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + ab * 128;
-      for (int c0 = 0; c0 < kbs; c0 += 16) {
+      const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + ab * (KPU * 128);
+      // columns i * 128 + c of the unit's accumulators = output channel (kb + i) * 128 + c
+      for (int cc = 0; cc < KPU * 128; cc += 16) {
+        const int i = cc >> 7, c0 = cc & 127;
+        if (c0 >= kbs[i]) continue;
         float v[16];
-        tmem_ld16(taddr + c0, v);
+        tmem_ld16(taddr + cc, v);
         tmem_ld_wait();
-        const size_t row = ((size_t)t * g.K + (size_t)kb * KB2 + c0) * ntp + tile;
+        const size_t row = ((size_t)t * g.K + (size_t)(kb + i) * KB2 + c0) * ntp + tile;
         if constexpr (M32) {
           float* dst = static_cast<float*>(tg.m) + row;
 #pragma unroll
@@ -193,7 +216,7 @@ __device__ __forceinline__ void tap_gemm_body(const TapGemm& tg) {
   __syncthreads();
   if (warp == 1) {
     tc_fence_after();
-    tmem_dealloc(tmem, 256);
+    tmem_dealloc(tmem, 512);
   }
 }
 
@@ -282,7 +305,7 @@ int wino_unfused_launch(const KernelParam* p, int sms, cudaStream_t stream) {
   const int ntb = (int)((nt + TB2 - 1) / TB2);
   const int cs = p->c / 16;
   unfused_input_transform<<<dim3(ntb, cs), 256, 0, stream>>>(*p);
-  const long long units = 16LL * ntb * ((p->k + KB2 - 1) / KB2);
+  const long long units = 16LL * ntb * (((p->k + KB2 - 1) / KB2 + KPU - 1) / KPU);
   const int grid = (int)(units < sms ? units : sms);
   unfused_gemm<<<grid, NTHREAD, unfused::SMEM_BYTES, stream>>>(*p);
   unfused_output_transform<<<dim3((unsigned)((nt + 255) / 256), p->k), 256, 0, stream>>>(*p);
@@ -293,7 +316,7 @@ int wino_tap_gemm_f32_launch(const TapGemm* s, int sms, void* stream) {
   static const cudaError_t attr = cudaFuncSetAttribute(
       tap_gemm_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, unfused::SMEM_BYTES);
   if (attr != cudaSuccess) return (int)attr;
-  const long long units = (long long)s->taps * s->ntb * ((s->k + KB2 - 1) / KB2);
+  const long long units = (long long)s->taps * s->ntb * (((s->k + KB2 - 1) / KB2 + KPU - 1) / KPU);
   const int grid = (int)(units < sms ? units : sms);
   tap_gemm_f32<<<grid, NTHREAD, unfused::SMEM_BYTES, (cudaStream_t)stream>>>(*s);
   return (int)cudaGetLastError();
