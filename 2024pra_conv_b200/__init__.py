@@ -112,6 +112,13 @@ def lib():
             "wino_unfused_workspace_bytes": ([i, i, i, i, i, ctypes.POINTER(sz), ctypes.POINTER(sz)], i),
             "wino_conv2d_unfused": ([vp, vp, vp, vp, vp, i, i, i, i, i, vp], i),
             "wino_error_read_clear": ([ctypes.POINTER(ctypes.c_uint32)], i),
+            "wino_twostage_workspace_bytes": ([i, i, i, i, i], sz),
+            "wino_conv2d_twostage": ([vp, vp, vp, vp, i, i, i, i, i, vp], i),
+            "wino_twostage_stage": ([i, vp, vp, vp, vp, i, i, i, i, i, vp], i),
+            "wino_twostage_gemm_kernel_ptr": ([], vp),
+            "wino_dropin_filter_u2_kernel_ptr": ([], vp),
+            "wino_twostage_output_kernel_ptr": ([], vp),
+            "wino_fused_kernel_ptr": ([], vp),
             "wino_f4_filter_bytes": ([i, i, i], sz),
             "wino_f4_workspace_bytes": ([i, i, i, i, i, i], sz),
             "wino_f4_filter_transform": ([vp, i, i, i, vp, sz, vp], i),
@@ -347,6 +354,39 @@ def filter_transform_unfused(w, stream=None):
                                                ctypes.c_void_p(u.data_ptr()), k, c, _stream(stream)),
            "filter_transform_unfused")
     return u
+
+
+def twostage_workspace_bytes(n, c, h, w, k) -> int:
+    return int(lib().wino_twostage_workspace_bytes(n, c, h, w, k))
+
+
+def conv2d_twostage(x, ucache2, k, out=None, workspace=None, stream=None):
+    """Two-stage conv on a U cache in the unfused layout (filter_transform_unfused):
+    input pre-pass, input transform fused into full-rate tap GEMMs writing
+    fp16 M, then the output transform.  workspace: uint8 tensor of
+    twostage_workspace_bytes() bytes (allocated when None)."""
+    import torch
+    n, c, h, wd = x.shape
+    y = out if out is not None else torch.empty((n, k, h, wd), dtype=torch.float16, device=x.device)
+    nb = twostage_workspace_bytes(n, c, h, wd, k)
+    if nb == 0:
+        raise WinoError(WINO_EUNSUPPORTED, "twostage_workspace_bytes")
+    if workspace is None:
+        workspace = _aligned_ws(nb, x.device)
+    _check(lib().wino_conv2d_twostage(ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(ucache2.data_ptr()),
+                                      ctypes.c_void_p(workspace.data_ptr()), ctypes.c_void_p(y.data_ptr()),
+                                      n, c, h, wd, k, _stream(stream)), "conv2d_twostage")
+    return y
+
+
+def twostage_stage(stage, x, ucache2, k, out, workspace, stream=None):
+    """One stage of conv2d_twostage (0 pre-pass, 1 tap GEMM, 2 output
+    transform) on a workspace of twostage_workspace_bytes()."""
+    n, c, h, wd = x.shape
+    _check(lib().wino_twostage_stage(stage, ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(ucache2.data_ptr()),
+                                     ctypes.c_void_p(workspace.data_ptr()), ctypes.c_void_p(out.data_ptr()),
+                                     n, c, h, wd, k, _stream(stream)), "twostage_stage")
+    return out
 
 
 class UnfusedWorkspace:

@@ -85,6 +85,22 @@ __global__ void __launch_bounds__(256) dropin_filter_kernel(KernelParam p) {
   for (int t = 0; t < 16; ++t) u[u_offset(t, k, c, K, C)] = __float2half_rn(t16[t]);
 }
 
+// Drop-in slot-1 kernel of the two-stage route: weight -> transform_filter
+// in the tap GEMM's U2 layout (u2_offset).
+__global__ void __launch_bounds__(256) dropin_filter_u2_kernel(KernelParam p) {
+  const int K = p.k, C = p.c;
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (size_t)K * C) return;
+  int k, c;
+  uorder_kc(idx, K, k, c);
+  float g[9], t16[16];
+  load_filter(static_cast<const __half*>(p.pweight), k, c, C, g);
+  filter_tile(g, t16);
+  __half* u = static_cast<__half*>(p.transform_filter);
+#pragma unroll
+  for (int t = 0; t < 16; ++t) u[u2_offset(t, k, c, K, C)] = __float2half_rn(t16[t]);
+}
+
 // ---- fp8 e4m3 -------------------------------------------------------------
 // Per-(tap, k) scale su[t][k] = amax_c |U'[t][k][c]| / 448 where
 // U'[t][k][c] = U[t][k][c] * sv[c] folds the per-input-channel scale of V
@@ -127,6 +143,7 @@ using namespace wino;
 extern "C" {
 
 void* wino_dropin_filter_kernel_ptr() { return (void*)dropin_filter_kernel; }
+void* wino_dropin_filter_u2_kernel_ptr() { return (void*)dropin_filter_u2_kernel; }
 
 int wino_launch_filter_transform(const void* weight, void* ucache, void* ucache_lo, int K, int C,
                                  int bf16, int layout, cudaStream_t stream) {

@@ -79,6 +79,16 @@ int wino_unfused_launch(const wino::KernelParam* p, int sms, cudaStream_t stream
 uint32_t wino_unfused_error_read_clear();
 int wino_launch_filter_transform(const void* weight, void* ucache, void* ucache_lo, int K, int C,
                                  int bf16, int layout, cudaStream_t stream);
+void* wino_dropin_filter_u2_kernel_ptr();
+void* wino_twostage_gemm_kernel_ptr();
+void* wino_twostage_output_kernel_ptr();
+int wino_twostage_threads();
+int wino_twostage_smem_bytes();
+int wino_twostage_prepare();
+size_t wino_twostage_m_bytes(int n, int h, int w, int k);
+unsigned wino_twostage_gemm_grid(int n, int h, int w, int k, int sms);
+void wino_twostage_output_grid(int n, int h, int w, int k, unsigned* gx, unsigned* gy);
+uint32_t wino_twostage_error_read_clear();
 }
 
 namespace {
@@ -228,6 +238,27 @@ int getkernelInfo(problem_t* problem, kernelInfo_t* kernelInfo, void* param) {
   a->transform_pin = use_xb ? pr.transform_pin : nullptr;
 
   const long long kc = (long long)pr.k * pr.c;
+  // Two-stage route (input transform fused into full-width tap GEMMs, M in
+  // the caller's mid_result, output transform in slot 4) whenever M fits the
+  // reference's mid_result size of 4*k*h*w*n fp16 elements (even H and W)
+  // and the channel-blocked input fits transform_pin.
+  const bool two_stage = use_xb && pr.mid_result != nullptr &&
+                         wino_twostage_m_bytes((int)pr.n, (int)pr.h, (int)pr.w, (int)pr.k) <=
+                             (size_t)4 * pr.k * pr.h * pr.w * pr.n * 2 &&
+                         wino_twostage_prepare() == 0;
+  if (two_stage) {
+    set_slot(kernelInfo, 1, (unsigned)((kc + 255) / 256), 1, 1, 256, 1, 1, 0,
+             wino_dropin_filter_u2_kernel_ptr());
+    set_slot(kernelInfo, 2, wino_xb_layout_grid((int)pr.n, (int)pr.c, (int)pr.h, (int)pr.w), 1, 1, 256, 1, 1, 0,
+             wino_xb_layout_kernel_ptr());
+    set_slot(kernelInfo, 3, wino_twostage_gemm_grid((int)pr.n, (int)pr.h, (int)pr.w, (int)pr.k, sm_count()), 1, 1,
+             (unsigned)wino_twostage_threads(), 1, 1, (unsigned)wino_twostage_smem_bytes(),
+             wino_twostage_gemm_kernel_ptr());
+    unsigned ox, oy;
+    wino_twostage_output_grid((int)pr.n, (int)pr.h, (int)pr.w, (int)pr.k, &ox, &oy);
+    set_slot(kernelInfo, 4, ox, oy, 1, 256, 1, 1, 0, wino_twostage_output_kernel_ptr());
+    return WINO_OK;
+  }
   set_slot(kernelInfo, 1, (unsigned)((kc + 255) / 256), 1, 1, 256, 1, 1, 0,
            wino_dropin_filter_kernel_ptr());
   if (use_xb)
@@ -303,6 +334,55 @@ extern "C" int wino_conv2d_fused(const void* x, const void* ucache, void* y, int
                                          dim3(wino_fused_threads()), args,
                                          (size_t)wino_fused_smem_bytes(), (cudaStream_t)stream);
   return e == cudaSuccess ? WINO_OK : WINO_ECUDA;
+}
+
+// ------------------------------------------------------ two-stage path ----
+// Workspace: the channel-blocked input (XB) then M16, each 256-byte aligned.
+extern "C" size_t wino_twostage_workspace_bytes(int n, int c, int h, int w, int k) {
+  if (wino_check_shape(n, c, h, w, k) != WINO_OK || !xb_items_ok(n, c, h, w)) return 0;
+  const size_t xb = (wino_xb_bytes(n, c, h, w) + 255) / 256 * 256;
+  return xb + wino_twostage_m_bytes(n, h, w, k);
+}
+
+// One stage of the two-stage path (0: input pre-pass, 1: tap GEMM, 2: output
+// transform) on the workspace layout of wino_conv2d_twostage, for callers
+// that time or overlap the stages.
+extern "C" int wino_twostage_stage(int stage, const void* x, const void* ucache2, void* workspace,
+                                   void* y, int n, int c, int h, int w, int k, void* stream) {
+  if (!x || !ucache2 || !y || !workspace || stage < 0 || stage > 2) return WINO_EINVAL;
+  if ((reinterpret_cast<uintptr_t>(workspace) & 255) != 0) return WINO_EINVAL;
+  const int st = wino_check_shape(n, c, h, w, k);
+  if (st != WINO_OK) return st;
+  if (!xb_items_ok(n, c, h, w)) return WINO_EUNSUPPORTED;
+  if (wino_twostage_prepare() != 0) return WINO_ECUDA;
+  const size_t xb = (wino_xb_bytes(n, c, h, w) + 255) / 256 * 256;
+  wino::KernelParam p = make_param(x, nullptr, y, workspace, const_cast<void*>(ucache2),
+                                   static_cast<uint8_t*>(workspace) + xb, n, c, h, w, k);
+  const cudaStream_t s = (cudaStream_t)stream;
+  void* args[] = {&p};
+  if (stage == 0) return wino_launch_xb_layout(&p, s) == 0 ? WINO_OK : WINO_ECUDA;
+  if (stage == 1)
+    return cudaLaunchKernel(wino_twostage_gemm_kernel_ptr(),
+                            dim3(wino_twostage_gemm_grid(n, h, w, k, sm_count())),
+                            dim3(wino_twostage_threads()), args, (size_t)wino_twostage_smem_bytes(),
+                            s) == cudaSuccess
+               ? WINO_OK
+               : WINO_ECUDA;
+  unsigned ox, oy;
+  wino_twostage_output_grid(n, h, w, k, &ox, &oy);
+  return cudaLaunchKernel(wino_twostage_output_kernel_ptr(), dim3(ox, oy), dim3(256), args, 0, s) ==
+                 cudaSuccess
+             ? WINO_OK
+             : WINO_ECUDA;
+}
+
+extern "C" int wino_conv2d_twostage(const void* x, const void* ucache2, void* workspace, void* y,
+                                    int n, int c, int h, int w, int k, void* stream) {
+  for (int stage = 0; stage < 3; ++stage) {
+    const int rc = wino_twostage_stage(stage, x, ucache2, workspace, y, n, c, h, w, k, stream);
+    if (rc != WINO_OK) return rc;
+  }
+  return WINO_OK;
 }
 
 extern "C" size_t wino_fused_workspace_bytes(int n, int c, int h, int w) {
@@ -484,6 +564,7 @@ extern "C" int wino_error_read_clear(uint32_t* code) {
   if (!code) return WINO_EINVAL;
   const uint32_t a = wino_fused_error_read_clear();
   const uint32_t b = wino_unfused_error_read_clear();
-  *code = a ? a : b;
+  const uint32_t c = wino_twostage_error_read_clear();
+  *code = a ? a : (b ? b : c);
   return WINO_OK;
 }

@@ -5,14 +5,16 @@ One step = one forward conv of the single-large-layer workload
 (N=128, C=K=256, H=W=28, 3x3, stride 1, pad 1; x = ReLU(N(0,1)),
 w ~ N(0, 2/(9C)), seed 0), run through the drop-in ABI exactly as the
 reference harness runs it: getkernelInfo once, then per step the four launch
-slots (filter transform, fused conv, two empty slots).
+slots (for this even-sized layer: filter transform, input re-layout,
+input-fused tap GEMM writing M to mid_result, output transform).
 
 Printed (rank 0, one JSON line):
   value      direct-conv-equivalent TFLOP/s (2*N*K*C*P*Q*9 / time), whole job,
              inputs resident in HBM, L2 flushed between steps
   e2e        the same metric through the C-ABI with host buffers: each step
              copies x host->device, runs the four slots, copies y back
-  roofline   the fused conv kernel against the tensor-pipe roofline: Winograd
+  roofline   the step's GEMM kernel (two-stage tap GEMM, or the fused kernel
+             on the other route) against the tensor-pipe roofline: Winograd
              GEMM FLOPs (2*16*K*C*N*ceil(P/2)*ceil(Q/2)) per launch over its
              CUDA-event time, peak from MEASURED_PEAKS.json
   cpu_baseline  the reference's own conv2dcpu (oracle/_ref) on this host's
@@ -77,11 +79,12 @@ def measured_peaks():
         return dict(hbm_gbs=6650.0, tflops=1590.0, tflops_sustained=1400.0, source="fallback")
 
 
-def committed_traffic():
-    """DRAM bytes per fused launch from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "fused_conv_n128_c256_h28.json")
+def committed_traffic(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summaries, if any."""
+    name = {"fused_wino_f16_kernel": "fused_conv_n128_c256_h28.json",
+            "twostage_gemm_kernel": "twostage_conv_n128_c256_h28.json"}[kernel]
     try:
-        with open(path) as f:
+        with open(os.path.join(ROOT, "profiles", name)) as f:
             return json.load(f).get("dram_bytes_per_launch")
     except (OSError, ValueError):
         return None
@@ -287,6 +290,13 @@ def run_ours(args, rank, world, local_rank):
         lambda: wino.conv2d_fused(x, ucache, k, out=yf, stream=stream, workspace=xbws), iters)
     layout_ms, _ = timed(lambda: wino.input_layout(x, xbws, stream), iters)
     u2 = wino.filter_transform_unfused(wt)
+    # two-stage path on cached U: pre-pass + input-fused tap GEMM + output transform
+    ts_ws = wino._aligned_ws(wino.twostage_workspace_bytes(n, c, h, w, k), dev)
+    yt = torch.empty_like(y)
+    ts_ms, _ = timed(lambda: wino.conv2d_twostage(x, u2, k, out=yt, workspace=ts_ws, stream=stream), iters)
+    ts_gemm_ms, _ = timed(lambda: wino.twostage_stage(1, x, u2, k, yt, ts_ws, stream), iters)
+    ts_out_ms, _ = timed(lambda: wino.twostage_stage(2, x, u2, k, yt, ts_ws, stream), iters)
+    del ts_ws
     ws = wino.UnfusedWorkspace(n, c, h, w, k, dev)
     yu = torch.empty_like(y)
     unf_ms, _ = timed(lambda: wino.conv2d_unfused(x, u2, k, ws=ws, out=yu, stream=stream), iters)
@@ -299,6 +309,10 @@ def run_ours(args, rank, world, local_rank):
     kernel_us = max(fused_us - layout_us, 1e-3)  # the fused kernel
     unfused_us = unf_ms / iters * 1e3
     ft_us = ft_ms / iters * 1e3
+    ts_us, ts_gemm_us, ts_out_us = (ts_ms / iters * 1e3, ts_gemm_ms / iters * 1e3,
+                                    ts_out_ms / iters * 1e3)
+    # the route getkernelInfo chose for the timed drop-in step
+    two_stage = ki.slot(3)["kernel"] == wino.lib().wino_twostage_gemm_kernel_ptr()
 
     # --- end to end through the C-ABI with host buffers.  Every step uploads
     # its input from pinned host memory, runs the drop-in slots and downloads
@@ -370,8 +384,10 @@ def run_ours(args, rank, world, local_rank):
         return 0
     peaks = measured_peaks()
     wflops = wino_flops(n, c, h, w, k)
-    achieved = wflops / (kernel_us * 1e-6) / 1e12
-    traffic = committed_traffic()
+    roof_kernel = "twostage_gemm_kernel" if two_stage else "fused_wino_f16_kernel"
+    roof_us = ts_gemm_us if two_stage else kernel_us
+    achieved = wflops / (roof_us * 1e-6) / 1e12
+    traffic = committed_traffic(roof_kernel)
     cpu = None
     if world == 1 and not args.no_cpu:
         try:
@@ -389,7 +405,9 @@ def run_ours(args, rank, world, local_rank):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f16",
         "data": "synthetic (seeded ReLU(N(0,1)) input, N(0,2/(9C)) weights)",
         "config": {"workload": WORKLOAD_NAME, **W, "parallelism": f"replicas x{world}",
-                   "step": "drop-in ABI: filter transform + input re-layout + fused conv + 1 empty slot",
+                   "step": ("drop-in ABI: filter transform + input re-layout + input-fused tap GEMM + "
+                            "output transform" if two_stage else
+                            "drop-in ABI: filter transform + input re-layout + fused conv + 1 empty slot"),
                    "l2": "flushed between steps (256 MB write)"},
         "us_per_layer": max_ms / args.steps * 1e3,
         "fused_us_cached_u": fused_us,
@@ -397,13 +415,16 @@ def run_ours(args, rank, world, local_rank):
         "fused_kernel_us": kernel_us,
         "fused_direct_equiv_tflops": dflops / (fused_us * 1e-6) / 1e12,
         "filter_transform_us": ft_us,
+        "two_stage_us_cached_u": ts_us,
+        "two_stage_gemm_us": ts_gemm_us,
+        "two_stage_output_us": ts_out_us,
         "unfused_us": unfused_us,
-        "speedup_vs_unfused": unfused_us / fused_us,
+        "speedup_vs_unfused": unfused_us / (ts_us if two_stage else fused_us),
         "rel_l2": rel_l2, "max_norm": max_norm, "unfused_rel_diff": unf_rel,
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peaks["tflops"],
                      "unit": "TFLOP/s", "frac": achieved / peaks["tflops"],
                      "traffic": traffic, "peak_source": peaks["source"],
-                     "kernel": "fused_wino_f16_kernel",
+                     "kernel": roof_kernel,
                      "algorithmic": "Winograd GEMM FLOPs 2*16*K*C*N*ceil(H/2)*ceil(W/2) per launch"},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": "TFLOP/s", "h2d_bytes_per_step": x.numel() * 2,
@@ -548,9 +569,20 @@ def extension_legs(wino, dev, flush, ev, peaks, steps):
                           "rel_l2": float(torch.linalg.vector_norm(d) / torch.linalg.vector_norm(y64)),
                           "max_norm": float(d.abs().max() / y64.abs().max()),
                           "direct_equiv_tflops": direct_flops(n, c, h, h, k) / (us * 1e-6) / 1e12}
+    u2 = wino.filter_transform_unfused(wt)
+    ws2 = wino._aligned_ws(wino.twostage_workspace_bytes(n, c, h, h, k), dev)
+    wino.conv2d_twostage(x, u2, k, out=y, workspace=ws2)
+    torch.cuda.synchronize()
+    d = y.double() - y64
+    us = timed(lambda: wino.conv2d_twostage(x, u2, k, out=y, workspace=ws2), steps)
+    f4["f2_two_stage_f16"] = {"us_per_call": us,
+                              "rel_l2": float(torch.linalg.vector_norm(d) / torch.linalg.vector_norm(y64)),
+                              "direct_equiv_tflops": direct_flops(n, c, h, h, k) / (us * 1e-6) / 1e12}
+    del u2, ws2
     out["winograd_f4"] = {"workload": "N128 C256 H28 K256, x = relu(N(0,1)); transformed filter cached; "
                                       "per call: input transform + 36-tap GEMM + output transform (F4), "
-                                      "pre-pass + fused kernel (F2)", **f4}
+                                      "pre-pass + fused kernel (F2), pre-pass + input-fused tap GEMM + "
+                                      "output transform (F2 two-stage)", **f4}
     del x, wt, y64, y, u, ws
 
     # --- fused epilogue (bias + residual + ReLU) vs the conv then separate elementwise ops

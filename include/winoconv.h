@@ -131,6 +131,23 @@ size_t wino_variant_workspace_bytes(int variant, int n, int c, int h, int w, int
 int wino_conv2d_variant(int variant, const void* x, const void* weight, void* y, void* workspace,
                         int n, int c, int h, int w, int k, void* stream);
 
+/* Two-stage F(2x2,3x3): the input transform runs inside full-rate tcgen05
+ * tap GEMMs (one tap x 128 tiles x 256 output channels per work unit, V formed
+ * in shared memory from the channel-blocked input), M is written as fp16
+ * (16 * k * tiles elements, tiles = n * ceil(h/2) * ceil(w/2)) and a second
+ * kernel applies the output transform.  ucache2: U in the unfused GEMM
+ * layout (wino_filter_transform_unfused).  workspace: 256-byte aligned,
+ * wino_twostage_workspace_bytes() bytes (channel-blocked input, then M).
+ * The output equals the unfused comparator's (same operands and rounding
+ * points) without V's HBM round trip; the reference's pipeline writes V and M
+ * to its workspaces (src/preprocessing.cuh:273-424, src/matrixmul.cuh:139-556). */
+size_t wino_twostage_workspace_bytes(int n, int c, int h, int w, int k);
+int wino_conv2d_twostage(const void* x, const void* ucache2, void* workspace, void* y, int n, int c,
+                         int h, int w, int k, void* stream);
+/* One stage of it: 0 input pre-pass, 1 tap GEMM, 2 output transform. */
+int wino_twostage_stage(int stage, const void* x, const void* ucache2, void* workspace, void* y,
+                        int n, int c, int h, int w, int k, void* stream);
+
 /* Winograd F(4x4,3x3) (36 taps, 4x4 output tiles; no counterpart in the
  * reference, which has F(2x2,3x3) only: src/preprocessing.cuh:75-424,
  * src/matrixmul.cuh:139-556, src/conv2d.cpp:17-250).  U and V are formed in

@@ -159,9 +159,34 @@ def test_dropin_slots_are_the_expected_kernels(wino, cuda, with_pin):
     for i in (1, 2, 3, 4):
         s = ki.slot(i)
         assert s["kernel"] and all(g >= 1 for g in s["grid"]) and all(b >= 1 for b in s["block"])
-    assert ki.slot(3)["lds"] > 48 * 1024  # the fused kernel's pipeline
-    # slot 2: the input re-layout pre-pass, or the same no-op kernel as slot 4
-    assert (ki.slot(2)["kernel"] != ki.slot(4)["kernel"]) == with_pin
+    assert ki.slot(3)["lds"] > 48 * 1024  # the GEMM pipeline's shared memory
+    L = wino.lib()
+    if with_pin:
+        # even H, W and a transform_pin: the two-stage route
+        assert ki.slot(1)["kernel"] == L.wino_dropin_filter_u2_kernel_ptr()
+        assert ki.slot(3)["kernel"] == L.wino_twostage_gemm_kernel_ptr()
+        assert ki.slot(4)["kernel"] == L.wino_twostage_output_kernel_ptr()
+    else:
+        # the fused kernel reads the NCHW input; slots 2 and 4 are the same no-op
+        assert ki.slot(3)["kernel"] == L.wino_fused_kernel_ptr()
+        assert ki.slot(2)["kernel"] == ki.slot(4)["kernel"]
+
+
+def test_dropin_odd_width_takes_the_fused_route(wino, cuda):
+    """Odd W: M would not fit the caller's mid_result, so slot 3 is the fused
+    kernel staging from the pre-pass records and slot 4 the no-op."""
+    import ctypes
+    import torch
+    x = torch.zeros((1, 16, 8, 7), dtype=torch.float16, device=cuda)
+    w = torch.zeros((16, 16, 3, 3), dtype=torch.float16, device=cuda)
+    y = torch.empty((1, 16, 8, 7), dtype=torch.float16, device=cuda)
+    ws = wino.DropinWorkspaces(1, 16, 8, 7, 16, cuda)
+    pr = wino.make_problem(x, w, y, ws.transform_pin, ws.transform_filter, ws.mid_result)
+    param = (ctypes.c_char * 80)()
+    rc, ki = wino.get_kernel_info(pr, param)
+    assert rc == 0
+    assert ki.slot(3)["kernel"] == wino.lib().wino_fused_kernel_ptr()
+    assert ki.slot(2)["kernel"] != ki.slot(4)["kernel"]
 
 
 @pytest.mark.parametrize("shape", [(2, 32, 9, 14), (1, 16, 1, 1), (3, 48, 8, 7)])
@@ -188,12 +213,13 @@ def test_input_layout_prepass_bit_exact(wino, cuda, oracle_mod, shape):
 
 
 def test_dropin_leaves_caller_mid_result_untouched(wino, cuda, oracle_mod):
-    """The drop-in kernels write only transform_filter (U), transform_pin
-    (the pre-pass records) and the output; the caller's mid_result workspace
-    keeps its contents."""
+    """On the fused route (odd W, where M would not fit mid_result) the
+    drop-in kernels write only transform_filter (U), transform_pin (the
+    pre-pass records) and the output; the caller's mid_result workspace keeps
+    its contents."""
     import torch
-    x, w = oracle_mod.make_inputs(2, 32, 12, 10, 32, seed=6, x_dist="normal")
-    ws = wino.DropinWorkspaces(2, 32, 12, 10, 32, cuda)
+    x, w = oracle_mod.make_inputs(2, 32, 12, 9, 32, seed=6, x_dist="normal")
+    ws = wino.DropinWorkspaces(2, 32, 12, 9, 32, cuda)
     ws.mid_result.fill_(1.25)
     y = wino.dropin_conv2d(_t(x, cuda), _t(w, cuda), ws=ws)
     torch.cuda.synchronize()

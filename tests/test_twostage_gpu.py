@@ -1,0 +1,154 @@
+"""Two-stage F(2x2,3x3) path (input transform fused into the tap GEMMs, fp16
+M, separate output transform) against the oracle.
+
+Bars: rel-L2 <= 2e-3 and max-normalised <= 1e-2 against FP64, the fp16 bar of
+the path.  The path's rounding points are those of the unfused comparator
+(U and V rounded to fp16 as in the fused kernel, fp32 accumulation, M rounded
+to fp16, fp32 output transform), so its output is also compared with the
+NumPy model of those steps and with the unfused comparator itself.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden_cases, load_golden
+
+pytestmark = pytest.mark.gpu
+
+REL_L2 = 2e-3
+MAX_NORM = 1e-2
+
+
+def _t(a, dev):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+
+def _twostage(wino, x16, w16, dev):
+    import torch
+    x, w = _t(x16, dev), _t(w16, dev)
+    u2 = wino.filter_transform_unfused(w)
+    y = wino.conv2d_twostage(x, u2, w.shape[0])
+    torch.cuda.synchronize()
+    assert wino.error_read_clear() == 0
+    return y.cpu().numpy()
+
+
+def _model(x16, w16):
+    """U rounded once, V in packed fp16 (oracle.winograd.input_transform_f16),
+    fp32 accumulation, M rounded to fp16, output transform, fp16 Y."""
+    from oracle import winograd as W
+    n, c, h, wd = x16.shape
+    k = w16.shape[0]
+    u = W._f16(W.filter_transform(w16))
+    v = W.input_transform_f16(x16)
+    m = W._f16(W.gemm(u, v).astype(np.float32))
+    return W.output_transform(m, n, k, h, wd).astype(np.float16)
+
+
+def _check(oracle_mod, y, y64, what):
+    rl2, mxn = oracle_mod.rel_l2(y, y64), oracle_mod.max_norm(y, y64)
+    assert np.isfinite(y.astype(np.float32)).all(), what
+    assert rl2 <= REL_L2, f"{what} rel_l2={rl2:.3e}"
+    assert mxn <= MAX_NORM, f"{what} max_norm={mxn:.3e}"
+
+
+@pytest.mark.parametrize("shape", [
+    (1, 16, 3, 5, 16),      # tiny, odd width
+    (2, 32, 12, 10, 32),
+    (3, 48, 9, 7, 144),     # C = 48 (3 K-steps), K = 128 + 16: a short second k-block
+    (1, 16, 1, 1, 16),      # one pixel
+    (2, 64, 14, 14, 256),   # two full k-blocks per unit
+    (1, 32, 30, 2, 16),     # tall and narrow
+    (5, 16, 40, 40, 48),    # several tile blocks, last one partial
+    (1, 80, 8, 8, 384),     # C = 80 (5 K-steps: a partial stage), three k-blocks
+])
+def test_twostage_shapes(wino, cuda, oracle_mod, shape):
+    n, c, h, w, k = shape
+    x, wt = oracle_mod.make_inputs(n, c, h, w, k, seed=sum(shape) + 1, x_dist="normal")
+    y = _twostage(wino, x, wt, cuda)
+    _check(oracle_mod, y, oracle_mod.conv2d_f64(x, wt), str(shape))
+    ym = _model(x, wt).astype(np.float64)
+    assert oracle_mod.rel_l2(y, ym) <= 2e-4, shape
+
+
+@pytest.mark.parametrize("path", golden_cases(), ids=lambda p: p.rsplit("/", 1)[-1])
+def test_twostage_vs_reference_golden(wino, cuda, oracle_mod, path):
+    x, w, y_ref = load_golden(path)
+    y = _twostage(wino, x, w, cuda)
+    _check(oracle_mod, y, oracle_mod.conv2d_f64(x, w), path)
+    assert oracle_mod.rel_l2(y, y_ref.astype(np.float64)) <= REL_L2
+
+
+def test_twostage_matches_unfused_comparator(wino, cuda, oracle_mod):
+    """Same operands (V formed with the same fp16 operations), the same
+    K-step accumulation order and the same rounding points as the unfused
+    comparator: the outputs are bit-identical."""
+    import torch
+    n, c, h, w, k = 4, 64, 14, 14, 128
+    x16, w16 = oracle_mod.make_inputs(n, c, h, w, k, seed=9, x_dist="relu_normal")
+    x, wt = _t(x16, cuda), _t(w16, cuda)
+    u2 = wino.filter_transform_unfused(wt)
+    ys = wino.conv2d_twostage(x, u2, k)
+    ws = wino.UnfusedWorkspace(n, c, h, w, k, cuda)
+    yu = wino.conv2d_unfused(x, u2, k, ws=ws)
+    torch.cuda.synchronize()
+    assert torch.equal(ys, yu)
+
+
+def test_twostage_large_layer(wino, cuda, oracle_mod):
+    """N=128 C=K=256 H=W=28, x = ReLU(N(0,1)), w ~ N(0, 2/(9C))."""
+    import torch
+    x16, w16 = oracle_mod.make_inputs(128, 256, 28, 28, 256, seed=0, x_dist="relu_normal",
+                                      w_std=np.sqrt(2.0 / (9 * 256)))
+    x, wt = _t(x16, cuda), _t(w16, cuda)
+    y = wino.conv2d_twostage(x, wino.filter_transform_unfused(wt), 256)
+    torch.cuda.synchronize()
+    assert wino.error_read_clear() == 0
+    y64 = torch.nn.functional.conv2d(x.double(), wt.double(), padding=1)
+    rl2 = float(torch.linalg.vector_norm(y.double() - y64) / torch.linalg.vector_norm(y64))
+    mxn = float((y.double() - y64).abs().max() / y64.abs().max())
+    assert rl2 <= REL_L2 and mxn <= MAX_NORM, (rl2, mxn)
+
+
+def test_dropin_large_layer_two_stage_route(wino, cuda, oracle_mod):
+    """N=128 C=K=256 H=W=28 through the drop-in ABI, which takes the
+    two-stage route for this shape."""
+    import torch
+    x16, w16 = oracle_mod.make_inputs(128, 256, 28, 28, 256, seed=1, x_dist="relu_normal",
+                                      w_std=np.sqrt(2.0 / (9 * 256)))
+    x, wt = _t(x16, cuda), _t(w16, cuda)
+    y = wino.dropin_conv2d(x, wt)
+    torch.cuda.synchronize()
+    assert wino.error_read_clear() == 0
+    y64 = torch.nn.functional.conv2d(x.double(), wt.double(), padding=1)
+    rl2 = float(torch.linalg.vector_norm(y.double() - y64) / torch.linalg.vector_norm(y64))
+    mxn = float((y.double() - y64).abs().max() / y64.abs().max())
+    assert rl2 <= REL_L2 and mxn <= MAX_NORM, (rl2, mxn)
+
+
+@pytest.mark.parametrize("shape", [(2, 32, 12, 10, 32), (1, 16, 2, 2, 16), (3, 48, 16, 6, 144)])
+def test_dropin_two_stage_route(wino, cuda, oracle_mod, shape):
+    """Even H and W: getkernelInfo fills the four slots with the U2 filter
+    transform, the pre-pass, the two-stage GEMM and the output transform
+    (M in the caller's mid_result), and the result equals the extension
+    entry point's."""
+    import ctypes
+    import torch
+    n, c, h, w, k = shape
+    x, wt = oracle_mod.make_inputs(n, c, h, w, k, seed=3, x_dist="uniform")
+    xt, wtt = _t(x, cuda), _t(wt, cuda)
+    ws = wino.DropinWorkspaces(n, c, h, w, k, cuda)
+    y = torch.empty((n, k, h, w), dtype=torch.float16, device=cuda)
+    pr = wino.make_problem(xt, wtt, y, ws.transform_pin, ws.transform_filter, ws.mid_result)
+    param = (ctypes.c_char * 80)()
+    rc, ki = wino.get_kernel_info(pr, param)
+    assert rc == 0
+    L = wino.lib()
+    assert ki.slot(3)["kernel"] == L.wino_twostage_gemm_kernel_ptr()
+    assert ki.slot(4)["kernel"] == L.wino_twostage_output_kernel_ptr()
+    y2 = wino.dropin_conv2d(xt, wtt, ws=ws)
+    y3 = wino.conv2d_twostage(xt, wino.filter_transform_unfused(wtt), k)
+    torch.cuda.synchronize()
+    assert wino.error_read_clear() == 0
+    assert torch.equal(y2, y3)
+    _check(oracle_mod, y2.cpu().numpy(), oracle_mod.conv2d_f64(x, wt), str(shape))
