@@ -356,38 +356,39 @@ __global__ void __launch_bounds__(ts::NTHREAD, 1) twostage_gemm_kernel(KernelPar
   }
 }
 
-// Output transform: thread = (4 consecutive tiles, k) reading the 16 taps of
-// M16 (tile stride = the number of tiles) as one 8-byte word each when the
-// tile count is a multiple of 4; Y tile = A^T m A in fp32, one fp16 rounding.
-// grid (ceil(tiles / 1024), K).
+// Output transform: thread = (2 consecutive tiles, k) reading the 16 taps of
+// M16 (tile stride = the number of tiles) as one fp16 pair each when the
+// tile count is even; Y tile = A^T m A in fp32, one fp16 rounding.
+// grid (ceil(tiles / 512), K).
+constexpr int OT_TILES = 2;
+
 __global__ void __launch_bounds__(256) twostage_output_kernel(KernelParam p) {
   const int K = p.k, P = p.Oh, Q = p.Ow;
   const int TP = (P + 1) >> 1, TQ = (Q + 1) >> 1;
   const long long NT = (long long)p.n * TP * TQ;
-  const long long tile0 = ((long long)blockIdx.x * 256 + threadIdx.x) * 4;
+  const long long tile0 = ((long long)blockIdx.x * 256 + threadIdx.x) * OT_TILES;
   const int k = blockIdx.y;
   if (tile0 >= NT) return;
-  const int nt = NT - tile0 < 4 ? (int)(NT - tile0) : 4;
+  const int nt = NT - tile0 < OT_TILES ? (int)(NT - tile0) : OT_TILES;
   const __half* m16 = static_cast<const __half*>(p.mid_result);
-  const bool vec = (NT & 3) == 0 && (reinterpret_cast<uintptr_t>(m16) & 7) == 0;
-  float m[16][4];
+  const bool vec = (NT & 1) == 0 && (reinterpret_cast<uintptr_t>(m16) & 3) == 0;
+  float m[16][OT_TILES];
 #pragma unroll
   for (int t = 0; t < 16; ++t) {
     const __half* src = m16 + ((size_t)t * K + k) * (size_t)NT + tile0;
     if (vec) {
-      const uint2 wd = *reinterpret_cast<const uint2*>(src);
-      const float2 lo = __half22float2(*reinterpret_cast<const __half2*>(&wd.x));
-      const float2 hi = __half22float2(*reinterpret_cast<const __half2*>(&wd.y));
-      m[t][0] = lo.x; m[t][1] = lo.y; m[t][2] = hi.x; m[t][3] = hi.y;
+      const float2 v = __half22float2(*reinterpret_cast<const __half2*>(src));
+      m[t][0] = v.x;
+      m[t][1] = v.y;
     } else {
-#pragma unroll
-      for (int j = 0; j < 4; ++j) m[t][j] = j < nt ? __half2float(src[j]) : 0.f;
+      m[t][0] = __half2float(src[0]);
+      m[t][1] = nt > 1 ? __half2float(src[1]) : 0.f;
     }
   }
   const long long per_img = (long long)TP * TQ;
   const bool pair_ok = (Q & 1) == 0 && (reinterpret_cast<uintptr_t>(p.pout) & 3) == 0;
 #pragma unroll
-  for (int j = 0; j < 4; ++j) {
+  for (int j = 0; j < OT_TILES; ++j) {
     if (j >= nt) break;
     float z[2][4];
 #pragma unroll
@@ -453,7 +454,7 @@ unsigned wino_twostage_gemm_grid(int n, int h, int w, int k, int sms) {
 }
 
 void wino_twostage_output_grid(int n, int h, int w, int k, unsigned* gx, unsigned* gy) {
-  *gx = (unsigned)((wino_twostage_tiles(n, h, w) + 1023) / 1024);
+  *gx = (unsigned)((wino_twostage_tiles(n, h, w) + 256 * OT_TILES - 1) / (256 * OT_TILES));
   *gy = (unsigned)k;
 }
 
