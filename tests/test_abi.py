@@ -246,3 +246,25 @@ def test_f4_entry_points_validate_and_size(wino):
     assert L.wino_conv2d_f4(d, d, 0, 16, 8, 8, 16, 1, d, full, None) == 1    # n = 0
     assert L.wino_conv2d_f4(d, d, 1, 16, 8, 8, 16, 1, d, full - 1, None) == 5
     assert L.wino_conv2d_f4(d, d, 1, 16, 8, 8, 16, 1, odd, full, None) == 1
+
+
+def test_twostage_entry_points_validate_and_size(wino):
+    """Two-stage path: workspace = blocked input (256-byte aligned) + 16*K*tiles
+    fp16 of M; argument checks return before any CUDA call."""
+    L = wino.lib()
+    d = ctypes.c_void_p(0x10000)
+    odd = ctypes.c_void_p(0x10010)
+    r256 = lambda b: (b + 255) // 256 * 256
+    # N128 C256 H28 K256: 25088 tiles; M = 16*256*25088*2 bytes = the reference's mid_result
+    m = 16 * 256 * 25088 * 2
+    assert m == 4 * 256 * 28 * 28 * 128 * 2
+    assert L.wino_twostage_workspace_bytes(128, 256, 28, 28, 256) == r256(L.wino_xb_bytes(128, 256, 28, 28)) + m
+    # odd sizes: tiles = n * ceil(h/2) * ceil(w/2)
+    assert (L.wino_twostage_workspace_bytes(3, 48, 9, 7, 144)
+            == r256(L.wino_xb_bytes(3, 48, 9, 7)) + 16 * 144 * (3 * 5 * 4) * 2)
+    assert L.wino_twostage_workspace_bytes(1, 24, 8, 8, 16) == 0          # C % 16
+    assert L.wino_conv2d_twostage(None, d, d, d, 1, 16, 8, 8, 16, None) == 1
+    assert L.wino_conv2d_twostage(d, d, odd, d, 1, 16, 8, 8, 16, None) == 1  # workspace alignment
+    assert L.wino_conv2d_twostage(d, d, d, d, 1, 16, 8, 8, 24, None) == 2    # K % 16
+    assert L.wino_twostage_stage(3, d, d, d, d, 1, 16, 8, 8, 16, None) == 1  # no such stage
+    assert L.wino_twostage_stage(-1, d, d, d, d, 1, 16, 8, 8, 16, None) == 1
