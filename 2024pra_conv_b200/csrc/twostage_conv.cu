@@ -29,9 +29,10 @@
 // Warp roles of the GEMM (448 threads, one CTA per SM): warp 0 lane 0 issues
 // the U bulk copies, warp 1 lane 0 the MMAs, warps 2-5 drain TMEM into M16,
 // warps 6-13 produce V (one thread per tile and 8-channel half; the 16
-// window loads of a stage are in flight together before any arithmetic).  Work units run tap-
-// fastest, so the 16 taps of a tile block are in flight on neighbouring CTAs
-// together and read the same XB rows from L2.  Every wait is bounded.
+// window loads of a stage are in flight together before any arithmetic).
+// Work units run tap-fastest, so the 16 taps of a tile block are in flight
+// on neighbouring CTAs together and read the same XB rows from L2.  Every
+// wait is bounded.
 //
 // The producers bound the GEMM: each stage's window loads (4 x 16 bytes per
 // tile, channel half and K-step, 64 KB per stage) come back from L2 after
