@@ -310,13 +310,9 @@ __global__ void __launch_bounds__(ts::NTHREAD, 1) twostage_gemm_kernel(KernelPar
       const ProdUnit pu = prod_unit(g, xb, t, tb, tl, hh);
       for (int j = 0; j < g.nst; ++j, ++it) {
         const int st = it % NSTAGE;
-        if (it >= NSTAGE &&
-            !mbar_wait_warp(&sh.empty[st], (it / NSTAGE - 1) & 1, abort_flag, err, ERR_WAIT_EMPTY,
-                            SLEEP_PROD_NS)) {
-          ok = false;
-          break;
-        }
         const int nk = min(SK, g.CS - j * SK);
+        // the window loads go out before the wait for a free stage: only the
+        // shared-memory stores below need it
         uint4 d[SK][4];
 #pragma unroll
         for (int kk = 0; kk < SK; ++kk) {
@@ -328,6 +324,12 @@ __global__ void __launch_bounds__(ts::NTHREAD, 1) twostage_gemm_kernel(KernelPar
 #pragma unroll
             for (int w = 0; w < 4; ++w) d[kk][w] = make_uint4(0u, 0u, 0u, 0u);
           }
+        }
+        if (it >= NSTAGE &&
+            !mbar_wait_warp(&sh.empty[st], (it / NSTAGE - 1) & 1, abort_flag, err, ERR_WAIT_EMPTY,
+                            SLEEP_PROD_NS)) {
+          ok = false;
+          break;
         }
         uint8_t* adst = smem + st * STAGE_BYTES + (tl >> 3) * 256 + hh * 128 + (tl & 7) * 16;
 #pragma unroll
