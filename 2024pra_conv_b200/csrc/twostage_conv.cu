@@ -390,6 +390,18 @@ __global__ void __launch_bounds__(256) twostage_output_kernel(KernelParam p) {
   }
   const long long per_img = (long long)TP * TQ;
   const bool pair_ok = (Q & 1) == 0 && (reinterpret_cast<uintptr_t>(p.pout) & 3) == 0;
+  // both tiles in one tile row with 8-byte aligned output rows: the four
+  // columns of each output row go out as one 8-byte store
+  float yy[OT_TILES][4];
+  int n0 = 0, ty0 = 0, tx0 = 0;
+  {
+    const int r0 = (int)(tile0 - (long long)(tile0 / per_img) * per_img);
+    n0 = (int)(tile0 / per_img);
+    ty0 = r0 / TQ;
+    tx0 = r0 - ty0 * TQ;
+  }
+  const bool row_pair = nt == 2 && tx0 + 1 < TQ && (Q & 3) == 0 && (tx0 & 1) == 0 &&
+                        (reinterpret_cast<uintptr_t>(p.pout) & 7) == 0;
 #pragma unroll
   for (int j = 0; j < OT_TILES; ++j) {
     if (j >= nt) break;
@@ -399,12 +411,13 @@ __global__ void __launch_bounds__(256) twostage_output_kernel(KernelParam p) {
       z[0][b] = m[b][j] + m[4 + b][j] + m[8 + b][j];
       z[1][b] = m[4 + b][j] - m[8 + b][j] - m[12 + b][j];
     }
-    float y[4];
+    float* y = yy[j];
 #pragma unroll
     for (int i = 0; i < 2; ++i) {
       y[2 * i + 0] = z[i][0] + z[i][1] + z[i][2];
       y[2 * i + 1] = z[i][1] - z[i][2] - z[i][3];
     }
+    if (row_pair) continue;
     const long long tile = tile0 + j;
     const int n = (int)(tile / per_img);
     const int r = (int)(tile - (long long)n * per_img);
@@ -422,6 +435,20 @@ __global__ void __launch_bounds__(256) twostage_output_kernel(KernelParam p) {
         o[Q] = __float2half_rn(y[2]);
         if (two_cols) o[Q + 1] = __float2half_rn(y[3]);
       }
+    }
+  }
+  if (row_pair) {
+    const int oy = 2 * ty0, ox = 2 * tx0;
+    __half* o = static_cast<__half*>(p.pout) + (((size_t)n0 * K + k) * P + oy) * (size_t)Q + ox;
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      if (oy + i >= P) break;
+      const __half2 a = __floats2half2_rn(yy[0][2 * i], yy[0][2 * i + 1]);
+      const __half2 b = __floats2half2_rn(yy[1][2 * i], yy[1][2 * i + 1]);
+      uint2 pk;
+      pk.x = *reinterpret_cast<const uint32_t*>(&a);
+      pk.y = *reinterpret_cast<const uint32_t*>(&b);
+      *reinterpret_cast<uint2*>(o + (size_t)i * Q) = pk;
     }
   }
 }
