@@ -137,6 +137,14 @@ wino::KernelParam make_param(const void* x, const void* w, void* y, void* vws, v
 // The pre-pass counts its items in 32 bits.
 bool xb_items_ok(int n, int c, int h, int w) { return wino_xb_items(n, c, h, w) < (1LL << 31); }
 
+// The two-stage producers address one (image, 16-channel) record block of the
+// blocked input with 32-bit byte offsets: (2*ceil(h/2) + 2) rows of
+// 64 * (ceil(w/2) + 1) bytes must stay below 2^31.
+bool twostage_ok(int n, int c, int h, int w) {
+  const long long rows = 2LL * ((h + 1) / 2) + 2, row_bytes = 64LL * ((w + 1) / 2 + 1);
+  return xb_items_ok(n, c, h, w) && rows * row_bytes < (1LL << 31);
+}
+
 unsigned fused_grid(int n, int h, int w, int k) {
   const long long nb = wino_fused_nblocks(n, h, w, k);
   const long long sms = sm_count();
@@ -243,6 +251,7 @@ int getkernelInfo(problem_t* problem, kernelInfo_t* kernelInfo, void* param) {
   // reference's mid_result size of 4*k*h*w*n fp16 elements (even H and W)
   // and the channel-blocked input fits transform_pin.
   const bool two_stage = use_xb && pr.mid_result != nullptr &&
+                         twostage_ok((int)pr.n, (int)pr.c, (int)pr.h, (int)pr.w) &&
                          wino_twostage_m_bytes((int)pr.n, (int)pr.h, (int)pr.w, (int)pr.k) <=
                              (size_t)4 * pr.k * pr.h * pr.w * pr.n * 2 &&
                          wino_twostage_prepare() == 0;
@@ -339,7 +348,7 @@ extern "C" int wino_conv2d_fused(const void* x, const void* ucache, void* y, int
 // ------------------------------------------------------ two-stage path ----
 // Workspace: the channel-blocked input (XB) then M16, each 256-byte aligned.
 extern "C" size_t wino_twostage_workspace_bytes(int n, int c, int h, int w, int k) {
-  if (wino_check_shape(n, c, h, w, k) != WINO_OK || !xb_items_ok(n, c, h, w)) return 0;
+  if (wino_check_shape(n, c, h, w, k) != WINO_OK || !twostage_ok(n, c, h, w)) return 0;
   const size_t xb = (wino_xb_bytes(n, c, h, w) + 255) / 256 * 256;
   return xb + wino_twostage_m_bytes(n, h, w, k);
 }
@@ -353,7 +362,7 @@ extern "C" int wino_twostage_stage(int stage, const void* x, const void* ucache2
   if ((reinterpret_cast<uintptr_t>(workspace) & 255) != 0) return WINO_EINVAL;
   const int st = wino_check_shape(n, c, h, w, k);
   if (st != WINO_OK) return st;
-  if (!xb_items_ok(n, c, h, w)) return WINO_EUNSUPPORTED;
+  if (!twostage_ok(n, c, h, w)) return WINO_EUNSUPPORTED;
   if (wino_twostage_prepare() != 0) return WINO_ECUDA;
   const size_t xb = (wino_xb_bytes(n, c, h, w) + 255) / 256 * 256;
   wino::KernelParam p = make_param(x, nullptr, y, workspace, const_cast<void*>(ucache2),

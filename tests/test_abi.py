@@ -268,3 +268,6 @@ def test_twostage_entry_points_validate_and_size(wino):
     assert L.wino_conv2d_twostage(d, d, d, d, 1, 16, 8, 8, 24, None) == 2    # K % 16
     assert L.wino_twostage_stage(3, d, d, d, d, 1, 16, 8, 8, 16, None) == 1  # no such stage
     assert L.wino_twostage_stage(-1, d, d, d, d, 1, 16, 8, 8, 16, None) == 1
+    # one 16384 x 16384 image: its blocked-input record block exceeds 2^31 bytes
+    assert L.wino_twostage_workspace_bytes(1, 16, 16384, 16384, 16) == 0
+    assert L.wino_conv2d_twostage(d, d, d, d, 1, 16, 16384, 16384, 16, None) == 2
