@@ -62,7 +62,7 @@ constexpr int SMEM_BYTES = NSTAGE * STAGE_BYTES + 1024;
 constexpr int WARP_U = 0, WARP_MMA = 1, WARP_E0 = 2, NWARP_E = 4, WARP_P0 = 6, NWARP_P = 8;
 // Back-off of the waiting warps (after 8 polls), so that spinning epilogue
 // and producer warps do not take issue slots from the working ones.
-constexpr uint32_t SLEEP_EPI_NS = 256, SLEEP_PROD_NS = 64;
+constexpr uint32_t SLEEP_EPI_NS = 32, SLEEP_PROD_NS = 32;
 constexpr int NTHREAD = (WARP_P0 + NWARP_P) * 32;
 
 struct Shared {
