@@ -131,7 +131,7 @@ size_t wino_variant_workspace_bytes(int variant, int n, int c, int h, int w, int
 int wino_conv2d_variant(int variant, const void* x, const void* weight, void* y, void* workspace,
                         int n, int c, int h, int w, int k, void* stream);
 
-/* Two-stage F(2x2,3x3): the input transform runs inside full-rate tcgen05
+/* Two-stage F(2x2,3x3): the input transform runs inside full-width tcgen05
  * tap GEMMs (one tap x 128 tiles x 256 output channels per work unit, V formed
  * in shared memory from the channel-blocked input), M is written as fp16
  * (16 * k * tiles elements, tiles = n * ceil(h/2) * ceil(w/2)) and a second
@@ -140,7 +140,11 @@ int wino_conv2d_variant(int variant, const void* x, const void* weight, void* y,
  * wino_twostage_workspace_bytes() bytes (channel-blocked input, then M).
  * The output equals the unfused comparator's (same operands and rounding
  * points) without V's HBM round trip; the reference's pipeline writes V and M
- * to its workspaces (src/preprocessing.cuh:273-424, src/matrixmul.cuh:139-556). */
+ * to its workspaces (src/preprocessing.cuh:273-424, src/matrixmul.cuh:139-556).
+ * getkernelInfo takes this route when M fits the caller's mid_result
+ * (4*k*h*w*n fp16: even h and w) and the blocked input fits transform_pin.
+ * Shapes whose blocked-input record block (one image, 16 channels) reaches
+ * 2^31 bytes return WINO_EUNSUPPORTED (workspace size 0). */
 size_t wino_twostage_workspace_bytes(int n, int c, int h, int w, int k);
 int wino_conv2d_twostage(const void* x, const void* ucache2, void* workspace, void* y, int n, int c,
                          int h, int w, int k, void* stream);
