@@ -113,6 +113,7 @@ def lib():
             "wino_conv2d_unfused": ([vp, vp, vp, vp, vp, i, i, i, i, i, vp], i),
             "wino_error_read_clear": ([ctypes.POINTER(ctypes.c_uint32)], i),
             "wino_twostage_workspace_bytes": ([i, i, i, i, i], sz),
+            "wino_dropin_route": ([vp], i),
             "wino_conv2d_twostage": ([vp, vp, vp, vp, i, i, i, i, i, vp], i),
             "wino_twostage_stage": ([i, vp, vp, vp, vp, i, i, i, i, i, vp], i),
             "wino_twostage_gemm_kernel_ptr": ([], vp),

@@ -196,6 +196,34 @@ int check_general(long long n, long long c, long long h, long long w, long long 
   return WINO_OK;
 }
 
+// Route of getkernelInfo for a validated problem (no CUDA calls).
+static int plan_route(const problem_t& pr) {
+  // Winograd F(2x2,3x3) for 3x3 / stride 1 / pad 1 with 16-channel multiples
+  // and a U-cache workspace; every other shape goes to the direct kernel.
+  const bool wino = pr.r == 3 && pr.s == 3 && pr.u == 1 && pr.v == 1 && pr.p == 1 && pr.q == 1 &&
+                    wino_check_shape((int)pr.n, (int)pr.c, (int)pr.h, (int)pr.w, (int)pr.k) == WINO_OK &&
+                    pr.transform_filter != nullptr;
+  if (!wino) return WINO_ROUTE_DIRECT;
+  // The caller's transform_pin workspace holds 4*h*h*n*c fp16 elements
+  // (reference src/main.cpp:36-38); when the channel-blocked input fits
+  // there (and is 16-byte aligned) slot 2 writes it, otherwise the fused
+  // kernel reads the NCHW input itself.
+  const size_t pin_ws_bytes = (size_t)4 * pr.h * pr.h * pr.n * pr.c * 2;
+  const bool use_xb = pr.transform_pin != nullptr &&
+                      (reinterpret_cast<uintptr_t>(pr.transform_pin) & 15) == 0 &&
+                      wino_xb_bytes((int)pr.n, (int)pr.c, (int)pr.h, (int)pr.w) <= pin_ws_bytes &&
+                      xb_items_ok((int)pr.n, (int)pr.c, (int)pr.h, (int)pr.w);
+  if (!use_xb) return WINO_ROUTE_FUSED;
+  // Two-stage route (input transform fused into full-width tap GEMMs, M in
+  // the caller's mid_result, output transform in slot 4) whenever M fits the
+  // reference's mid_result size of 4*k*h*w*n fp16 elements (even H and W).
+  const bool two_stage = pr.mid_result != nullptr &&
+                         twostage_ok((int)pr.n, (int)pr.c, (int)pr.h, (int)pr.w) &&
+                         wino_twostage_m_bytes((int)pr.n, (int)pr.h, (int)pr.w, (int)pr.k) <=
+                             (size_t)4 * pr.k * pr.h * pr.w * pr.n * 2;
+  return two_stage ? WINO_ROUTE_TWOSTAGE : WINO_ROUTE_FUSED_XB;
+}
+
 int getkernelInfo(problem_t* problem, kernelInfo_t* kernelInfo, void* param) {
   if (!problem || !kernelInfo || !param) return WINO_EINVAL;
   const problem_t& pr = *problem;
@@ -203,11 +231,8 @@ int getkernelInfo(problem_t* problem, kernelInfo_t* kernelInfo, void* param) {
   const int st = check_general(pr.n, pr.c, pr.h, pr.w, pr.k, pr.r, pr.s, pr.u, pr.v, pr.p, pr.q, &oh, &ow);
   if (st != WINO_OK) return st;
   if (!pr.in || !pr.weight || !pr.out) return WINO_EINVAL;
-  // Winograd F(2x2,3x3) for 3x3 / stride 1 / pad 1 with 16-channel multiples
-  // and a U-cache workspace; every other shape goes to the direct kernel.
-  const bool wino = pr.r == 3 && pr.s == 3 && pr.u == 1 && pr.v == 1 && pr.p == 1 && pr.q == 1 &&
-                    wino_check_shape((int)pr.n, (int)pr.c, (int)pr.h, (int)pr.w, (int)pr.k) == WINO_OK &&
-                    pr.transform_filter != nullptr;
+  int route = plan_route(pr);
+  const bool wino = route != WINO_ROUTE_DIRECT;
 
   mykernelParamType* a = static_cast<mykernelParamType*>(param);
   a->pin = pr.in;
@@ -233,29 +258,12 @@ int getkernelInfo(problem_t* problem, kernelInfo_t* kernelInfo, void* param) {
   }
 
   if (wino_fused_prepare() != 0) return WINO_ECUDA;
-
-  // The caller's transform_pin workspace holds 4*h*h*n*c fp16 elements
-  // (reference src/main.cpp:36-38); when the channel-blocked input fits
-  // there (and is 16-byte aligned) slot 2 writes it and the fused kernel
-  // stages from it, otherwise the fused kernel reads the NCHW input itself.
-  const size_t pin_ws_bytes = (size_t)4 * pr.h * pr.h * pr.n * pr.c * 2;
-  const bool use_xb = pr.transform_pin != nullptr &&
-                      (reinterpret_cast<uintptr_t>(pr.transform_pin) & 15) == 0 &&
-                      wino_xb_bytes((int)pr.n, (int)pr.c, (int)pr.h, (int)pr.w) <= pin_ws_bytes &&
-                      xb_items_ok((int)pr.n, (int)pr.c, (int)pr.h, (int)pr.w);
+  if (route == WINO_ROUTE_TWOSTAGE && wino_twostage_prepare() != 0) route = WINO_ROUTE_FUSED_XB;
+  const bool use_xb = route != WINO_ROUTE_FUSED;
   a->transform_pin = use_xb ? pr.transform_pin : nullptr;
 
   const long long kc = (long long)pr.k * pr.c;
-  // Two-stage route (input transform fused into full-width tap GEMMs, M in
-  // the caller's mid_result, output transform in slot 4) whenever M fits the
-  // reference's mid_result size of 4*k*h*w*n fp16 elements (even H and W)
-  // and the channel-blocked input fits transform_pin.
-  const bool two_stage = use_xb && pr.mid_result != nullptr &&
-                         twostage_ok((int)pr.n, (int)pr.c, (int)pr.h, (int)pr.w) &&
-                         wino_twostage_m_bytes((int)pr.n, (int)pr.h, (int)pr.w, (int)pr.k) <=
-                             (size_t)4 * pr.k * pr.h * pr.w * pr.n * 2 &&
-                         wino_twostage_prepare() == 0;
-  if (two_stage) {
+  if (route == WINO_ROUTE_TWOSTAGE) {
     set_slot(kernelInfo, 1, (unsigned)((kc + 255) / 256), 1, 1, 256, 1, 1, 0,
              wino_dropin_filter_u2_kernel_ptr());
     set_slot(kernelInfo, 2, wino_xb_layout_grid((int)pr.n, (int)pr.c, (int)pr.h, (int)pr.w), 1, 1, 256, 1, 1, 0,
@@ -280,6 +288,16 @@ int getkernelInfo(problem_t* problem, kernelInfo_t* kernelInfo, void* param) {
            wino_fused_kernel_ptr());
   set_slot(kernelInfo, 4, 1, 1, 1, 32, 1, 1, 0, wino_noop_kernel_ptr());
   return WINO_OK;
+}
+
+extern "C" int wino_dropin_route(const void* problem) {
+  if (!problem) return -WINO_EINVAL;
+  const problem_t& pr = *static_cast<const problem_t*>(problem);
+  int oh = 0, ow = 0;
+  const int st = check_general(pr.n, pr.c, pr.h, pr.w, pr.k, pr.r, pr.s, pr.u, pr.v, pr.p, pr.q, &oh, &ow);
+  if (st != WINO_OK) return -st;
+  if (!pr.in || !pr.weight || !pr.out) return -WINO_EINVAL;
+  return plan_route(pr);
 }
 
 extern "C" int wino_getParamsize(problem_t* problem, int* paramSize) {

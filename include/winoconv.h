@@ -47,6 +47,17 @@ enum {
 /* Validate a problem against the shape contract (no CUDA calls). */
 int wino_check_shape(int n, int c, int h, int w, int k);
 
+/* The route getkernelInfo takes for a problem_t (conv2d.h), without CUDA
+ * calls: the direct kernel (shapes outside the Winograd contract, or no
+ * transform_filter), the fused kernel reading the NCHW input (no usable
+ * transform_pin), the fused kernel after the input pre-pass, or the
+ * two-stage route (pre-pass, input-fused tap GEMM with M in mid_result,
+ * output transform: needs mid_result of 4*k*h*w*n fp16 to hold 16*k*tiles,
+ * i.e. even h and w).  Returns a WINO_ROUTE_* value, or minus a WINO_E* code
+ * for an invalid problem. */
+enum { WINO_ROUTE_DIRECT = 0, WINO_ROUTE_FUSED = 1, WINO_ROUTE_FUSED_XB = 2, WINO_ROUTE_TWOSTAGE = 3 };
+int wino_dropin_route(const void* problem);
+
 /* Bytes of the U cache for a variant (fp16: 16*k*c*2). */
 size_t wino_ucache_bytes(int k, int c, int variant);
 

@@ -271,3 +271,29 @@ def test_twostage_entry_points_validate_and_size(wino):
     # one 16384 x 16384 image: its blocked-input record block exceeds 2^31 bytes
     assert L.wino_twostage_workspace_bytes(1, 16, 16384, 16384, 16) == 0
     assert L.wino_conv2d_twostage(d, d, d, d, 1, 16, 16384, 16384, 16, None) == 2
+
+
+@pytest.mark.parametrize("kw,route", [
+    (dict(h=12, w=10, transform_pin=0x100000, mid_result=0x200000), 3),   # even H, W: two-stage
+    (dict(h=12, w=9, transform_pin=0x100000, mid_result=0x200000), 2),    # odd W: M would not fit
+    (dict(h=11, w=10, transform_pin=0x100000, mid_result=0x200000), 2),   # odd H
+    (dict(h=12, w=10, transform_pin=0x100000, mid_result=0), 2),          # no mid_result
+    (dict(h=12, w=10, transform_pin=0, mid_result=0x200000), 1),          # no transform_pin
+    (dict(h=12, w=10, transform_pin=0x100008, mid_result=0x200000), 1),   # misaligned transform_pin
+    (dict(h=12, w=10, transform_pin=0x100000, mid_result=0x200000, transform_filter=0), 0),
+    (dict(h=12, w=10, transform_pin=0x100000, mid_result=0x200000, r=5, s=5, p=2, q=2), 0),
+    (dict(h=12, w=10, transform_pin=0x100000, mid_result=0x200000, c=24), 0),
+    (dict(h=12, w=10, transform_pin=0x100000, mid_result=0x200000, u=2, v=2), 0),
+])
+def test_dropin_route_selection(wino, kw, route):
+    """Which kernels getkernelInfo will put in the slots (decided without CUDA
+    calls): 0 direct, 1 fused on the NCHW input, 2 fused after the pre-pass,
+    3 two-stage (M in the caller's mid_result)."""
+    pr = _problem(wino, **{"n": 2, "c": 32, "k": 32, **kw})
+    assert wino.lib().wino_dropin_route(ctypes.byref(pr)) == route
+
+
+def test_dropin_route_rejects_invalid(wino):
+    pr = _problem(wino, n=0)
+    assert wino.lib().wino_dropin_route(ctypes.byref(pr)) == -1
+    assert wino.lib().wino_dropin_route(None) == -1
