@@ -105,3 +105,37 @@ def test_winograd_f4_hilo_split():
     # lo's own rounding: half an fp16 step of |a - hi| <= 2^-12 |a|, or half
     # the fp16 subnormal step 2^-24 where lo is subnormal
     assert np.all(np.abs(hi + lo - a.astype(np.float32)) <= np.maximum(2.0 ** -22 * np.abs(a), 2.0 ** -25))
+
+
+@pytest.mark.parametrize("shape", [(1, 16, 6, 6), (2, 32, 5, 7), (1, 16, 9, 4)])
+def test_blocked_input_window_words_give_v(oracle_mod, shape):
+    """Layout contract of the two-stage producers: tap (a, b) of tile (n, ty,
+    tx) reads, from the blocked input XB[n][c/16][r][par][hh][e][8], the words
+    at rows 2ty + i (i in the tap row's pair) and columns 2tx - 1 + jc (jc in
+    the tap column's pair; parity (jc & 1) ^ 1, entry tx + (jc >> 1)), and
+    two fp16 +- steps (rows, then columns) give the fused kernel's V bit for
+    bit."""
+    from oracle import winograd as W
+    from test_fused_gpu import _xb_layout_np
+    n, c, h, w = shape
+    x, _ = oracle_mod.make_inputs(n, c, h, w, 16, seed=7, x_dist="normal")
+    xb = _xb_layout_np(x)                                      # [n][cb][r][par][hh][e][8]
+    tp, tq = (h + 1) // 2, (w + 1) // 2
+    pick = {0: (0, 2, 0), 1: (1, 2, 1), 2: (1, 2, 2), 3: (1, 3, 0)}   # (i0, i1, op)
+
+    def op(o, x0, x1):
+        r = x0 - x1 if o == 0 else (x0 + x1 if o == 1 else x1 - x0)
+        return r.astype(np.float16).astype(np.float32)
+
+    vref = W.input_transform_f16(x).astype(np.float16)        # [16][tiles][C]
+    for tile in range(n * tp * tq):
+        nn, r = divmod(tile, tp * tq)
+        ty, tx = divmod(r, tq)
+        for t in range(16):
+            i0, i1, opa = pick[t >> 2]
+            j0, j1, opb = pick[t & 3]
+            word = lambda i, jc: xb[nn, :, 2 * ty + i, (jc & 1) ^ 1, :, tx + (jc >> 1), :].astype(np.float32)
+            e0 = op(opa, word(i0, j0), word(i1, j0))
+            e1 = op(opa, word(i0, j1), word(i1, j1))
+            v = op(opb, e0, e1).astype(np.float16).reshape(-1)   # channel order cb, hh, 8
+            assert np.array_equal(v.view(np.uint16), vref[t, tile].view(np.uint16)), (tile, t)
