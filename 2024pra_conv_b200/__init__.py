@@ -341,7 +341,9 @@ def filter_transform_persistent(w, path, stream=None):
     if rc not in (WINO_ESTALE, WINO_EIO):
         raise WinoError(rc, "ucache_load")
     u = filter_transform(w, stream)
-    torch.cuda.current_stream().synchronize()
+    # wino_ucache_save reads U with a copy on the legacy stream, which is not
+    # ordered against `stream` when that is a non-blocking stream
+    (stream if stream is not None else torch.cuda.current_stream()).synchronize()
     _check(lib().wino_ucache_save(os.fsencode(path), ctypes.c_void_p(u.data_ptr()), k, c, tag), "ucache_save")
     return u, False
 

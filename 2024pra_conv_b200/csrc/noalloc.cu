@@ -14,16 +14,17 @@
 //     of fp16; every GPU that loads the library holds this array until the
 //     process exits.  Larger filters are rejected with WINO_ESCRATCH before
 //     anything is launched;
-//   * the first call on a device looks up the array's device address
-//     (cudaGetSymbolAddress, with that device current) and caches it; make that
-//     first call before any stream capture starts on that device;
+//   * every call looks up the array's device address on the current device
+//     (cudaGetSymbolAddress, with that device current) and checks the result;
+//     nothing is cached, so the address stays right after a cudaDeviceReset.
+//     The first call on a device may also load the library's kernels onto it:
+//     make that first call before any stream capture starts on that device;
 //   * every call, on every stream, uses the same array and leaves the last
 //     call's U in it.  Each call rewrites the whole part it reads, so nothing
 //     needs to start at zero, but calls whose kernels overlap on the GPU race
 //     on the array: serialise them (one stream, or events between streams);
 //   * no cudaMalloc, cudaFree or allocating library routine is called.
 #include <cuda_runtime.h>
-#include <mutex>
 
 #include "winoconv.h"
 #include "wino_param.h"
@@ -37,21 +38,13 @@ constexpr size_t kNoAllocElems = 16 * (size_t)kNoAllocMaxKC;  // fp16 elements
 // runtime; the device address comes from cudaGetSymbolAddress below.
 static __device__ __align__(256) unsigned short g_noalloc_ucache[kNoAllocElems];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_addr_mutex;
-void* g_addr[kMaxDevices] = {};
-
-// Device address of the scratch on the current device (looked up once).
+// Device address of the scratch on the current device.  Looked up on every
+// call (the lookup is a host-side table read): a cached address would go stale
+// when the caller resets the device.
 int scratch_address(void** out) {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return WINO_ECUDA;
-  std::lock_guard<std::mutex> lock(g_addr_mutex);
-  if (!g_addr[dev]) {
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_noalloc_ucache) != cudaSuccess || !p) return WINO_ECUDA;
-    g_addr[dev] = p;
-  }
-  *out = g_addr[dev];
+  void* p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_noalloc_ucache) != cudaSuccess || !p) return WINO_ECUDA;
+  *out = p;
   return WINO_OK;
 }
 

@@ -119,7 +119,11 @@ int wino_ucache_load(const char* path, void* ucache, int k, int c, unsigned long
   }
   std::fclose(f);
   if (rc != WINO_OK) return rc;
-  return cudaMemcpy(ucache, buf.data(), want, cudaMemcpyHostToDevice) == cudaSuccess ? WINO_OK : WINO_ECUDA;
+  // A copy from pageable memory may still be in flight when cudaMemcpy
+  // returns; waiting for the legacy stream makes the U cache complete before
+  // the caller's next launch on any stream.
+  if (cudaMemcpy(ucache, buf.data(), want, cudaMemcpyHostToDevice) != cudaSuccess) return WINO_ECUDA;
+  return cudaStreamSynchronize(cudaStreamLegacy) == cudaSuccess ? WINO_OK : WINO_ECUDA;
 }
 
 }  // extern "C"

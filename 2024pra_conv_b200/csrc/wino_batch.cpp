@@ -149,6 +149,29 @@ struct Batch {
   bool dirty = true;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  // Completion of the last run or graph launch, recorded on the caller's
+  // stream.  commit() and destroy wait for it before they rewrite or free
+  // the device table (or destroy the graph) that launch may still be reading:
+  // a caller's non-blocking stream is not ordered against the synchronous
+  // table copy on the legacy stream.
+  cudaEvent_t done = nullptr;
+  bool pending = false;
+
+  int mark(cudaStream_t s) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess) return WINO_ECUDA;
+    if (cs != cudaStreamCaptureStatusNone) return WINO_OK;  // recorded by the replay's owner
+    if (!done && cudaEventCreateWithFlags(&done, cudaEventDisableTiming) != cudaSuccess) return WINO_ECUDA;
+    if (cudaEventRecord(done, s) != cudaSuccess) return WINO_ECUDA;
+    pending = true;
+    return WINO_OK;
+  }
+
+  int settle() {
+    if (!pending) return WINO_OK;
+    pending = false;
+    return cudaEventSynchronize(done) == cudaSuccess ? WINO_OK : WINO_ECUDA;
+  }
 
   void drop_graph() {
     if (exec) cudaGraphExecDestroy(exec);
@@ -179,6 +202,7 @@ struct Batch {
     }
     t.total = begin;
     total = begin;
+    if (settle() != WINO_OK) return WINO_ECUDA;  // no launch still reads the old table
     if (cudaMemcpy(table_dev, &t, sizeof(t), cudaMemcpyHostToDevice) != cudaSuccess) return WINO_ECUDA;
     dirty = false;
     drop_graph();
@@ -268,8 +292,10 @@ int wino_batch_create(void** out) {
 int wino_batch_destroy(void* h) {
   Batch* b = as_batch(h);
   if (!b) return WINO_EINVAL;
+  b->settle();
   b->drop_graph();
   if (b->table_dev) cudaFree(b->table_dev);
+  if (b->done) cudaEventDestroy(b->done);
   delete b;
   return WINO_OK;
 }
@@ -342,9 +368,10 @@ int wino_batch_commit(void* h) {
 int wino_batch_run(void* h, void* stream) {
   Batch* b = as_batch(h);
   if (!b || b->layers.empty()) return WINO_EINVAL;
-  const int rc = b->commit();
+  int rc = b->commit();
   if (rc != WINO_OK) return rc;
-  return b->run((cudaStream_t)stream);
+  rc = b->run((cudaStream_t)stream);
+  return rc != WINO_OK ? rc : b->mark((cudaStream_t)stream);
 }
 
 // Autotune: per-layer configurations (exhaustive over CFG_*), then the layer
@@ -419,6 +446,7 @@ int wino_batch_graph_capture(void* h, void* stream) {
   int rc = b->commit();
   if (rc != WINO_OK) return rc;
   if (wino_fused_prepare_batch() != 0) return WINO_ECUDA;
+  if (b->settle() != WINO_OK) return WINO_ECUDA;  // the old graph may still be running
   b->drop_graph();
   cudaStream_t s = nullptr;
   if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return WINO_ECUDA;
@@ -445,7 +473,8 @@ int wino_batch_graph_capture(void* h, void* stream) {
 int wino_batch_graph_launch(void* h, void* stream) {
   Batch* b = as_batch(h);
   if (!b || !b->exec || b->dirty) return WINO_EINVAL;
-  return cudaGraphLaunch(b->exec, (cudaStream_t)stream) == cudaSuccess ? WINO_OK : WINO_ECUDA;
+  if (cudaGraphLaunch(b->exec, (cudaStream_t)stream) != cudaSuccess) return WINO_ECUDA;
+  return b->mark((cudaStream_t)stream);
 }
 
 }  // extern "C"

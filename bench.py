@@ -150,13 +150,34 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------- CPU legs -----
-def cpu_reference_sample(seed=0, images=None, threads=None):
+def cpu_info():
+    """CPU model string and logical CPU count of this host (lscpu / nproc)."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"cpu_model": model, "nproc": os.cpu_count()}
+
+
+BUILD_FLAGS = {"portable": "g++ -O3 -march=x86-64-v3 (fp16 products evaluated exactly in float)",
+               "avx512fp16": "g++ -O3 -march=x86-64-v4 -mavx512fp16 (products rounded to fp16)"}
+
+
+def cpu_reference_sample(seed=0, images=None, threads=None, variant=None):
     """Time the reference's conv2dcpu (oracle/_ref, unmodified verfiy.h) on
-    `images` images of the workload with all host threads."""
+    `images` images of the workload.  threads == 1 calls it once over all the
+    images, exactly as the reference harness does (src/main.cpp:138);
+    otherwise an OpenMP loop calls it once per image."""
     import numpy as np
     import oracle
     variants = oracle.ref_variants()
-    variant = "avx512fp16" if "avx512fp16" in variants else "portable"
+    if variant is None:
+        variant = "avx512fp16" if "avx512fp16" in variants else "portable"
     threads = threads or oracle.ref_max_threads(variant)
     images = images or max(2, threads)
     W = WORKLOAD
@@ -170,30 +191,63 @@ def cpu_reference_sample(seed=0, images=None, threads=None):
                 variant=variant)
 
 
+def cpu_baseline_modes():
+    """The reference CPU path in every mode this host offers: each build
+    (exact products; fp16-rounded products where the CPU has AVX512-FP16)
+    with one thread exactly as the reference calls it and with all host
+    threads.  Returns (modes, headline) where headline is the fastest mode."""
+    import oracle
+    modes = []
+    for variant in oracle.ref_variants():
+        allt = oracle.ref_max_threads(variant)
+        for threads, images in ((1, 2), (allt, 2 * allt)):
+            r = cpu_reference_sample(seed=0, images=images, threads=threads, variant=variant)
+            modes.append({"build": variant, "flags": BUILD_FLAGS.get(variant), "threads": threads,
+                          "images": images, "seconds": r["seconds"], "value": r["tflops"],
+                          "unit": "TFLOP/s"})
+    best = max(modes, key=lambda m: m["value"]) if modes else None
+    return modes, best
+
+
 def run_reference_arm(args, rank):
+    """The reference's own CPU implementation (conv2dcpu) on the host cores
+    with every thread, on the GPU arm's workload.  Each step runs as many of
+    the workload's 128 images as fit a budget of about 150 s for the whole
+    run (all 128 when the host is fast enough)."""
     if rank != 0:
         return 0
+    import oracle
+    variants = oracle.ref_variants()
+    variant = "avx512fp16" if "avx512fp16" in variants else "portable"
+    threads = oracle.ref_max_threads(variant)
+    cal = cpu_reference_sample(seed=0, images=threads, threads=threads, variant=variant)
+    per_image = cal["seconds"] / cal["images"]
+    budget = 150.0 / max(1, args.steps + args.warmup)
+    images = int(budget / per_image) // threads * threads
+    images = max(threads, min(WORKLOAD["n"], images))
     samples = []
     for i in range(args.warmup + args.steps):
-        r = cpu_reference_sample(seed=i)
+        r = cpu_reference_sample(seed=i, images=images, threads=threads, variant=variant)
         if i >= args.warmup:
             samples.append(r)
     secs = sum(s["seconds"] for s in samples)
     flops = sum(direct_flops(s["images"], WORKLOAD["c"], WORKLOAD["h"], WORKLOAD["w"],
                              WORKLOAD["k"]) for s in samples)
     value = flops / secs / 1e12
-    s0 = samples[0]
+    full = images == WORKLOAD["n"]
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "TFLOP/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": secs / len(samples) * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f16", "data": "synthetic (seeded)",
         "config": {"workload": WORKLOAD_NAME, **WORKLOAD,
-                   "step": f"{s0['images']} images of the workload on the host CPU"},
-        "cpu_baseline": {"value": value, "unit": "TFLOP/s", "cores": s0["threads"],
+                   "step": (f"all {images} images of the workload" if full else
+                            f"{images} of {WORKLOAD['n']} images of the workload") + " on the host CPU"},
+        "cpu_baseline": {"value": value, "unit": "TFLOP/s", "cores": threads,
                          "kind": "reference",
-                         "sample": f"{s0['images']} of {WORKLOAD['n']} images per step, "
-                                   f"conv2dcpu build '{s0['variant']}', OpenMP over images"},
+                         "sample": f"{images} of {WORKLOAD['n']} images per step, conv2dcpu build "
+                                   f"'{variant}' ({BUILD_FLAGS.get(variant)}), OpenMP over images",
+                         **cpu_info()},
         "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -391,14 +445,16 @@ def run_ours(args, rank, world, local_rank):
     cpu = None
     if world == 1 and not args.no_cpu:
         try:
-            r = cpu_reference_sample()
-            cpu = {"value": r["tflops"], "unit": "TFLOP/s", "cores": r["threads"],
+            modes, best = cpu_baseline_modes()
+            cpu = {"value": best["value"], "unit": "TFLOP/s", "cores": best["threads"],
                    "kind": "reference",
-                   "sample": f"{r['images']} of {n} images of the workload, reference conv2dcpu "
-                             f"build '{r['variant']}', {r['seconds']:.1f} s"}
+                   "sample": f"{best['images']} of {n} images of the workload, reference conv2dcpu "
+                             f"build '{best['build']}' on {best['threads']} threads, "
+                             f"{best['seconds']:.1f} s (fastest of the modes below)",
+                   "modes": modes, **cpu_info()}
         except Exception as e:  # noqa: BLE001 - report, do not fail the GPU numbers
             cpu = {"value": None, "unit": "TFLOP/s", "cores": None, "kind": "reference",
-                   "sample": f"unavailable: {e}"}
+                   "sample": f"unavailable: {e}", **cpu_info()}
     line = {
         "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world,
         "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": max_ms / args.steps,
@@ -502,13 +558,27 @@ def extension_legs(wino, dev, flush, ev, peaks, steps):
     for (x, wt, u, ws, y, c, k, h) in layers:
         y64 = torch.nn.functional.conv2d(x.double(), wt.double(), padding=1)
         worst = max(worst, float(torch.linalg.vector_norm(y.double() - y64) / torch.linalg.vector_norm(y64)))
+    # each layer alone with its tuned configuration (pre-pass + fused kernel),
+    # against its own roofline, to show which layer classes lose the time
+    per_layer = []
+    for i, (x, wt, u, ws, y, c, k, h) in enumerate(layers):
+        cfg = b.config(i)
+        cws = wino._aligned_ws(wino.cfg_workspace_bytes(n, c, h, h, k, cfg), dev)
+        us = timed(lambda: wino.conv2d_fused_cfg(x, u, k, cfg, workspace=cws, out=y), steps)
+        byt = 2.0 * (n * c * h * h + n * k * h * h + 16 * k * c)
+        t_hbm = byt / (peaks["hbm_gbs"] * 1e9) * 1e6
+        t_tc = wino_flops(n, c, h, h, k) / (peaks["tflops"] * 1e12) * 1e6
+        per_layer.append({"c": c, "k": k, "h": h, "cfg": cfg, "us": us, "bound_us": max(t_hbm, t_tc),
+                          "bound": "tensor" if t_tc > t_hbm else "hbm",
+                          "frac": max(t_hbm, t_tc) / us})
+        del cws
     out["layer_set"] = {
         "workload": "12 ResNet-style 3x3 s1 p1 layers at N=32, (C,K,H): " +
                     ", ".join(f"({c},{k},{h})" for (c, k, h) in wino.RESNET_LAYER_SET),
         "us_graph_tuned": graph_us, "us_persistent_untuned": untuned_us, "us_sequential_launches": seq_us,
         "direct_equiv_tflops": dfl / (graph_us * 1e-6) / 1e12,
         "configs": [b.config(i) for i in range(len(layers))], "order": b.order(),
-        "order_us": order_us, "worst_rel_l2": worst,
+        "order_us": order_us, "worst_rel_l2": worst, "per_layer_alone": per_layer,
         "roofline": {"per_layer_bound": f"{n_tc} of 12 layers tensor-bound, the rest HBM-bound",
                      "target_us": t_roof * 1e6, "frac": t_roof * 1e6 / graph_us,
                      "definition": "sum over layers of max(HBM bytes / hbm_gbs, Winograd FLOPs / "

@@ -11,20 +11,45 @@
  * Data layouts (reference readme.txt:21-24): input NCHW, weights KCRS,
  * output N K Oh Ow, all fp16.  Oh = (h - r + 2p)/u + 1, Ow = (w - s + 2q)/v + 1.
  *
- * Contract of this implementation (Winograd F(2x2,3x3) on sm_100a):
- *   - supported: r = s = 3, u = v = 1, p = q = 1, every dim <= 32767,
- *     c % 16 == 0, k % 16 == 0 (the reference silently misbehaves outside
- *     its six hard-coded shapes; this one returns an error instead);
+ * Contract of this implementation (sm_100a):
+ *   - every dim >= 1 and <= 32767 (the `short` fields of mykernelParamType),
+ *     a filter no larger than the padded input, non-null in / weight / out;
+ *     anything else returns an error code instead of the reference's silent
+ *     mis-dispatch outside its six hard-coded shapes;
  *   - the caller owns every buffer: in, weight, out and the three
  *     workspaces sized as the reference harness sizes them
- *     (src/main.cpp:36-38): transform_filter >= 16*k*c fp16 elements.
- *     The fused path writes the transformed filter (U) to transform_filter
- *     and leaves transform_pin and mid_result untouched;
+ *     (src/main.cpp:36-38): transform_pin >= 4*h*h*n*c, mid_result >=
+ *     4*k*h*w*n and transform_filter >= 16*k*c fp16 elements;
  *   - getkernelInfo fills four launch slots that the caller launches in
- *     order on one stream, each with args[0] pointing at `param`:
- *       slot 1  filter transform  weight -> transform_filter (U cache)
- *       slot 2  fused input transform + tensor-core GEMM + output transform
- *       slots 3, 4  empty kernels (the reference harness launches all four);
+ *     order on one stream, each with args[0] pointing at `param`.  Which
+ *     kernels go in the slots depends on the shape and on which workspaces
+ *     are usable (wino_dropin_route in winoconv.h reports the choice):
+ *
+ *     two-stage route: r = s = 3, u = v = 1, p = q = 1, c % 16 == k % 16
+ *       == 0, even h and w, all three workspaces present, transform_pin
+ *       16-byte aligned:
+ *         slot 1  filter transform   weight -> transform_filter (U)
+ *         slot 2  input re-layout    in -> transform_pin (channel-blocked)
+ *         slot 3  tap GEMMs          transform_pin, transform_filter ->
+ *                                    mid_result (M, 16*k*n*(h/2)*(w/2) fp16,
+ *                                    all of the caller's 4*k*h*w*n)
+ *         slot 4  output transform   mid_result -> out
+ *       All three workspaces are written, as the reference's own pipeline
+ *       writes them.
+ *     fused route with re-layout: the Winograd shape contract holds and
+ *       transform_pin is usable, but h or w is odd or mid_result is null:
+ *         slot 1  weight -> transform_filter (U); slot 2 in -> transform_pin;
+ *         slot 3  fused input transform + tensor-core GEMM + output
+ *                 transform -> out;  slot 4  empty kernel.
+ *       mid_result is left untouched.
+ *     fused route: as above without a usable transform_pin (null, not
+ *       16-byte aligned or too small): slot 2 is an empty kernel and the
+ *       fused kernel reads `in` directly; transform_pin and mid_result are
+ *       left untouched.
+ *     direct route: any other shape (filter size, stride, padding, channel
+ *       counts not multiples of 16) or a null transform_filter: slot 3 is a
+ *       direct convolution (fp32 accumulation), slots 1, 2, 4 empty kernels;
+ *       no workspace is touched.
  *   - return value 0 on success, non-zero (a WINO_E* code from winoconv.h)
  *     for unsupported shapes, null pointers or a CUDA attribute failure.
  */
@@ -40,9 +65,9 @@ typedef struct
     _Float16*       in;                 /* input,  NCHW, device memory            */
     _Float16*       weight;             /* weights, KCRS, device memory           */
     _Float16*       out;                /* output, N K Oh Ow, device memory       */
-    _Float16*       transform_pin;      /* workspace (unused by the fused path)   */
-    _Float16*       transform_filter;   /* workspace: receives the U cache        */
-    _Float16*       mid_result;         /* workspace (unused by the fused path)   */
+    _Float16*       transform_pin;      /* workspace: channel-blocked input       */
+    _Float16*       transform_filter;   /* workspace: transformed filter U        */
+    _Float16*       mid_result;         /* workspace: tap GEMM output M           */
     unsigned int    n;                  /* batch size                             */
     unsigned int    c;                  /* input channels                         */
     unsigned int    h;                  /* input height                           */

@@ -73,7 +73,11 @@ int wino_filter_transform(const void* weight, void* ucache, int k, int c, void* 
  * shape, layout version and that tag; wino_ucache_load fills a caller's U
  * buffer from such a file and returns WINO_ESTALE -- leaving the buffer
  * untouched -- when the file belongs to other weights (tag), another shape or
- * another layout version, so a caller re-runs wino_filter_transform then. */
+ * another layout version, so a caller re-runs wino_filter_transform then.
+ * wino_ucache_save copies U with a synchronous copy on the legacy default
+ * stream: the stream that wrote U must be synchronised first when it is a
+ * non-blocking stream.  wino_ucache_load returns once the U buffer is
+ * complete on the device. */
 int wino_weight_tag(const void* weight, int k, int c, unsigned long long* tag, void* stream);
 int wino_ucache_save(const char* path, const void* ucache, int k, int c, unsigned long long tag);
 int wino_ucache_load(const char* path, void* ucache, int k, int c, unsigned long long tag);
@@ -227,7 +231,11 @@ int wino_tune_layer(const void* x, const void* ucache, void* workspace, void* y,
  * fastest table order among {as added, longest first, longest/shortest
  * interleaved}; layer_us receives nlayers x WINO_NCFG timings, order_us the
  * three whole-batch timings (either may be NULL).  Configuration and order
- * changes invalidate a captured graph.  Each layer needs its own workspace
+ * changes invalidate a captured graph.  wino_batch_run and
+ * wino_batch_graph_launch record their completion on the caller's stream;
+ * the next commit (explicit, or the one a run or capture after a change
+ * makes) waits for it on the host before it rewrites the device layer table,
+ * so an earlier launch on any stream never reads a half-rewritten table.  Each layer needs its own workspace
  * (wino_fused_workspace_bytes of its shape, or NULL for direct reads): the
  * pre-passes of a run write all workspaces before the one launch reads
  * them, so layers sharing one would overwrite each other. */
@@ -259,8 +267,10 @@ int wino_launch_kernelinfo(const void* ki, void* param, void* stream);
  * points need; this one keeps U in a fixed array inside the library (8 MiB
  * held on every GPU that loads the library, for K*C <= wino_noalloc_max_kc())
  * and runs the filter transform and the fused conv on it.  Larger filters
- * return WINO_ESCRATCH.  The first call on a device looks the array up, so
- * make it before any stream capture on that device.  All calls share the
+ * return WINO_ESCRATCH.  Every call looks up the array's address on the
+ * current device (nothing cached, so a cudaDeviceReset does not leave a stale
+ * address); the first call on a device may also load the library's kernels,
+ * so make it before any stream capture on that device.  All calls share the
  * array: calls whose kernels overlap on the GPU race, so serialise them.
  * Allocates nothing.  x: NCHW fp16, weight: KCRS fp16, y: N K H W fp16. */
 int wino_conv2d_noalloc(const void* x, const void* weight, void* y, int n, int c, int h, int w,

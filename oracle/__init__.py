@@ -33,8 +33,10 @@ _ref = {}
 
 
 def build():
-    """Compile the C oracle (and the reference CPU path when its tree exists)."""
-    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    """Compile the C oracle (and the reference CPU path when the environment
+    variable WINO_REFERENCE_DIR names the reference tree)."""
+    ref = os.environ.get("WINO_REFERENCE_DIR")
+    subprocess.run(["make", "-s", "-C", HERE] + ([f"REF={ref}"] if ref else []), check=True)
 
 
 def _oracle_lib():
