@@ -1,43 +1,59 @@
-// Two-stage Winograd F(2x2,3x3): input transform fused into the tap GEMM,
+// Two-stage Winograd F(2x2,3x3): input transform fused into the tap GEMMs,
 // output transform as a second kernel.
 //
 // The single fused kernel (fused_conv.cu) keeps all 16 taps of a tile block
 // in TMEM until the output transform, which caps its MMAs at N = 32 tiles.
-// This path gives that up for full-width MMAs: a work unit is one tap x 128
-// tiles x 256 output channels (two M=128 N<=128 MMAs per K-step sharing the
-// tile operand); its V operand is formed in shared memory by producer warps
-// straight from the channel-blocked input (XB, written by the input
-// pre-pass, L2-resident), so V never reaches HBM; M goes out as fp16 (16 * K
-// * tiles elements, the size of the reference's mid_result for even H, W)
-// and a second kernel applies A^T m A.  Against the reference's pipeline
-// (src/preprocessing.cuh:273-424 writing V to transform_pin,
-// src/matrixmul.cuh:139-556 reading it back, src/conv2d.cpp:17-250 reading
-// M from mid_result) it drops the V round trip.
+// This path gives that up for full-width MMAs: the GEMM writes M once, in
+// fp16 (16 * K * tiles elements, the size of the reference's mid_result for
+// even H, W), and a second kernel applies A^T m A.  V never reaches HBM: it
+// is formed in shared memory by producer warps straight from the
+// channel-blocked input (XB, written by the input pre-pass).  Against the
+// reference's pipeline (src/preprocessing.cuh:273-424 writing V to
+// transform_pin, src/matrixmul.cuh:139-556 reading it back,
+// src/conv2d.cpp:17-250 reading M from mid_result) it drops the V round trip.
 //
 //   slot 1  dropin_filter_u2_kernel   W -> U2 (unfused GEMM layout), transform_filter
 //   slot 2  xb_layout_kernel          X -> XB, transform_pin
-//   slot 3  twostage_gemm_kernel      XB, U2 -> M16[t][k][tile], mid_result
-//   slot 4  twostage_output_kernel    M16 -> Y
+//   slot 3  twostage_pair_kernel      XB, U2 -> M (blocked, below), mid_result
+//           (twostage_stream_kernel when C > 256)
+//   slot 4  twostage_output_kernel    M -> Y
 // (the drop-in ABI's route when M fits mid_result, i.e. even H and W; the
 // extension entry point wino_conv2d_twostage runs slots 2-4 on any shape).
 //
-// V is formed with the fused kernel's packed-fp16 operations in the same
-// order (rows of B^T d first, then columns), so the GEMM operands are
-// bit-identical to the fused kernel's and to the unfused comparator's; with
-// M rounded once to fp16 the output equals the unfused comparator's.
+// M layout (blocked by 128-tile blocks): block tb holds M[t][k][i] for the
+// block's ntb = min(128, tiles - 128 tb) tiles, element
+//   tb * 16 * K * 128 + (t * K + k) * ntb + i,
+// 16 * K * tiles elements in all (no padding).  Rows of a full block are 256
+// bytes, so the GEMM epilogue writes and the output transform reads whole
+// 16- and 8-byte words.
 //
-// Warp roles of the GEMM (448 threads, one CTA per SM): warp 0 lane 0 issues
-// the U bulk copies, warp 1 lane 0 the MMAs, warps 2-5 drain TMEM into M16,
-// warps 6-13 produce V (one thread per tile and 8-channel half; the 16
-// window loads of a stage are in flight together before any arithmetic).
-// Work units run tap-fastest, so the 16 taps of a tile block are in flight
-// on neighbouring CTAs together and read the same XB rows from L2.  Every
-// wait is bounded.
+// V is formed with the fused kernel's packed-fp16 operations (rows of B^T d
+// first, then columns; every +- sum of two fp16 values rounded once), so the
+// GEMM operands are bit-identical to the fused kernel's and to the unfused
+// comparator's; with M rounded once to fp16 the output equals the unfused
+// comparator's.
 //
-// The producers bound the GEMM: each stage's window loads (4 x 16 bytes per
-// tile, channel half and K-step, 64 KB per stage) come back from L2 after
-// 1.5-2.5 k cycles under load, and each producer has one stage of loads in
-// flight.
+// twostage_pair_kernel (C <= 256): a cluster of two CTAs issues
+// tcgen05.mma.cta_group::2 of M = 256 output channels x N = 128 tiles x 16
+// channels.  A work unit is a PAIR of taps x 256 output channels x 128
+// tiles, all C.  The taps of a pair are chosen so that they read common
+// input-window words: (a,1)+(a,2) share all four words of their window rows
+// and columns, and (0,b)+(1,b), (3,b)+(2,b) for b in {0, 3} share three rows
+// and two columns (six words for two taps); over the 16 taps that is 40
+// words per tile and 8 channels against 64 for one tap per unit.  Each CTA
+// of the pair forms V for 64 of the unit's 128 tiles (the pair MMA reads
+// both halves) and keeps its 128 output channels of U for both taps and all
+// C resident in shared memory (128 KB, reloaded only when the pair's tap
+// pair or k-block changes), so the only L2 traffic of the main loop is the
+// window words.  Work units are dealt to the clusters in contiguous runs of
+// one (tap pair, k pair) each, weighted by the window words of the pair.
+//
+// twostage_stream_kernel (any C): one CTA per SM, a unit is one tap x 128
+// tiles x 256 output channels (two M = 128 MMAs per K-step sharing the tile
+// operand), U streamed per stage by bulk copy.
+//
+// Every wait is bounded; a timeout records an error code that
+// wino_twostage_error_read_clear returns.
 #include <cuda_runtime.h>
 #include <cuda_fp16.h>
 #include "tc_sm100.cuh"
@@ -50,8 +66,515 @@ static __device__ uint32_t g_twostage_err;
 
 namespace ts {
 
+// ---- shared geometry --------------------------------------------------------
+struct Geo {
+  int K, C, CS, HP, E, TP, TQ, nTB, nKB2, nKP;
+  long long NT;
+  uint32_t RB;
+  size_t cbs;   // bytes between 16-channel record blocks of XB
+};
+
+__device__ __forceinline__ Geo geo(const KernelParam& p) {
+  Geo g;
+  g.K = p.k;
+  g.C = p.c;
+  g.CS = p.c >> 4;
+  g.HP = xb_rows(p.h);
+  g.E = xb_entries(p.w);
+  g.RB = (uint32_t)xb_row_bytes(p.w);
+  g.cbs = (size_t)g.HP * g.RB;
+  g.TP = (p.Oh + 1) >> 1;
+  g.TQ = (p.Ow + 1) >> 1;
+  g.NT = (long long)p.n * g.TP * g.TQ;
+  g.nTB = (int)((g.NT + 127) / 128);
+  g.nKB2 = (g.K + KB2 - 1) / KB2;
+  g.nKP = (g.nKB2 + 1) / 2;
+  return g;
+}
+
+// Element offset of M[t][k][tile tb*128 + i] in the blocked layout.
+__host__ __device__ __forceinline__ size_t m_offset(int tb, int t, int k, int i, int K, long long NT) {
+  const long long rem = NT - (long long)tb * 128;
+  const int ntb = rem < 128 ? (int)rem : 128;
+  return (size_t)tb * 16 * (size_t)K * 128 + ((size_t)t * K + k) * (size_t)ntb + i;
+}
+
+// B^T row / column a of the 4-point transform (the fused kernel's bt_row /
+// bt_cols: d0-d2, d1+d2, d2-d1, d1-d3) as two indices and the signs s0, s1 of
+// s0*x[i0] + s1*x[i1], packed as fp16x2 (+1 = 0x3c00, -1 = 0xbc00).
+__host__ __device__ __forceinline__ void bt_pick(int a, int& i0, int& i1, uint32_t& s0, uint32_t& s1) {
+  i0 = a == 0 ? 0 : 1;
+  i1 = a == 3 ? 3 : 2;
+  s0 = a == 2 ? 0xbc00bc00u : 0x3c003c00u;
+  s1 = (a == 0 || a == 3) ? 0xbc00bc00u : 0x3c003c00u;
+}
+
+// s0*x0 + s1*x1 with one rounding: the product by +-1 is exact, so this is
+// bit-identical to the fused kernel's hadd2 / hsub2 whatever the operand order.
+__device__ __forceinline__ uint32_t bt_op(uint32_t s0, uint32_t s1, uint32_t x0, uint32_t x1) {
+  __half2 r = __hfma2(*reinterpret_cast<__half2*>(&x1), *reinterpret_cast<__half2*>(&s1),
+                      __hmul2(*reinterpret_cast<__half2*>(&x0), *reinterpret_cast<__half2*>(&s0)));
+  return *reinterpret_cast<uint32_t*>(&r);
+}
+
+__device__ __forceinline__ uint4 bt_op4(uint32_t s0, uint32_t s1, const uint4& x0, const uint4& x1) {
+  return make_uint4(bt_op(s0, s1, x0.x, x1.x), bt_op(s0, s1, x0.y, x1.y), bt_op(s0, s1, x0.z, x1.z),
+                    bt_op(s0, s1, x0.w, x1.w));
+}
+
+// Byte offset, inside one (image, 16-channel) XB record block, of the window
+// word at window row r (input row 2ty - 1 + r) and window column jc (input
+// column 2tx - 1 + jc) of channel half hh: column jc lies in parity
+// (jc & 1) ^ 1, entry tx + (jc >> 1).
+__device__ __forceinline__ uint32_t win_off(const Geo& g, int ty, int tx, int hh, int r, int jc) {
+  return (uint32_t)(2 * ty + r) * g.RB + (uint32_t)(((((jc & 1) ^ 1) * 2 + hh) * g.E + tx + (jc >> 1)) * 16);
+}
+
+__device__ __forceinline__ void tile_decode(const Geo& g, long long tile, int& n, int& ty, int& tx) {
+  const long long per = (long long)g.TP * g.TQ;
+  n = (int)(tile / per);
+  const int r = (int)(tile - (long long)n * per);
+  ty = r / g.TQ;
+  tx = r - ty * g.TQ;
+}
+
+}  // namespace ts
+
+// =============================================================================
+// Tap-pair GEMM on CTA pairs (C <= 256)
+// =============================================================================
+namespace tp {
+
+using namespace ts;
+
+constexpr int SK = 2;                         // K-steps (16 channels) per stage
+constexpr int NSTV = 8;                       // V stages
+constexpr int VT = 64;                        // tiles per CTA and unit (N / 2)
+constexpr int V_TAP = VT * 32;                // 2 KB: one tap, one K-step, 64 tiles x 16 channels
+constexpr int V_STAGE = SK * 2 * V_TAP;       // 8 KB
+constexpr int CS_MAX = 16;                    // resident U holds up to 16 K-steps (C <= 256)
+constexpr int U_STEP = 128 * 32;              // 4 KB: 128 k rows x 16 channels
+constexpr int U_TAP = CS_MAX * U_STEP;        // 64 KB
+constexpr int U_BYTES = 2 * U_TAP;
+constexpr int SMEM_BYTES = U_BYTES + NSTV * V_STAGE + 1024;
+// warps 0-3 epilogue (warp w reads TMEM lanes 32 (w % 4) ..), warp 4 lane 0
+// U loads (both CTAs) and MMA issue (rank 0), warps 5-12 V producers
+constexpr int WARP_E0 = 0, NWARP_E = 4, WARP_MMA = 4, WARP_P0 = 5, NWARP_P = 8;
+constexpr int NTHREAD = (WARP_P0 + NWARP_P) * 32;
+constexpr int NPAIR = 8;
+constexpr uint16_t BOTH = 3;                  // CTA mask of the pair
+constexpr uint32_t SLEEP_NS = 32;
+
+struct Shared {
+  uint64_t vfull[NSTV], vempty[NSTV];
+  uint64_t accfull[2], accempty[2];
+  uint64_t ufull, uempty, utx, mmadone;
+  uint32_t tmem_base;
+  int abort_flag;
+};
+
+// Tap pair q: the taps of accumulator slots 0 and 1.
+__device__ __forceinline__ void pair_taps(int q, int& t0, int& t1) {
+  switch (q) {
+    case 0: t0 = 1; t1 = 2; break;     // (0,1) (0,2)
+    case 1: t0 = 5; t1 = 6; break;     // (1,1) (1,2)
+    case 2: t0 = 9; t1 = 10; break;    // (2,1) (2,2)
+    case 3: t0 = 13; t1 = 14; break;   // (3,1) (3,2)
+    case 4: t0 = 0; t1 = 4; break;     // (0,0) (1,0)
+    case 5: t0 = 12; t1 = 8; break;    // (3,0) (2,0)
+    case 6: t0 = 3; t1 = 7; break;     // (0,3) (1,3)
+    default: t0 = 15; t1 = 11; break;  // (3,3) (2,3)
+  }
+}
+// Relative cost of a pair's unit: its window words per tile (4 or 6), halved.
+__host__ __device__ __forceinline__ int pair_weight(int q) { return q < 4 ? 2 : 3; }
+
+// Window words of a pair.  Four-word pairs (q < 4, tap row a = q, columns
+// 1 and 2): w0 = d(i0,1), w1 = d(i1,1), w2 = d(i0,2), w3 = d(i1,2).  Six-word
+// pairs (rows R0, R1, R2; columns j0, j1 of tap column b): w0..w2 = d(R*,j0),
+// w3..w5 = d(R*,j1); slot 0 combines rows R0 and R2, slot 1 rows R1 and R2.
+struct PairWords {
+  int nw;
+  int r[6], c[6];
+};
+
+__device__ __forceinline__ PairWords pair_words(int q) {
+  PairWords pw;
+  if (q < 4) {
+    int i0, i1;
+    uint32_t s0, s1;
+    bt_pick(q, i0, i1, s0, s1);
+    pw.nw = 4;
+    pw.r[0] = i0; pw.c[0] = 1;
+    pw.r[1] = i1; pw.c[1] = 1;
+    pw.r[2] = i0; pw.c[2] = 2;
+    pw.r[3] = i1; pw.c[3] = 2;
+    pw.r[4] = pw.r[5] = 0;
+    pw.c[4] = pw.c[5] = 0;
+  } else {
+    const bool top = (q & 1) == 0;           // q 4, 6: rows 0, 1, 2; q 5, 7: rows 3, 2, 1
+    const int b = q < 6 ? 0 : 3;
+    int j0, j1;
+    uint32_t s0, s1;
+    bt_pick(b, j0, j1, s0, s1);
+    const int R[3] = {top ? 0 : 3, top ? 1 : 2, top ? 2 : 1};
+    pw.nw = 6;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      pw.r[i] = R[i]; pw.c[i] = j0;
+      pw.r[3 + i] = R[i]; pw.c[3 + i] = j1;
+    }
+  }
+  return pw;
+}
+
+// Row signs of the window rows each slot combines, column signs of the pair.
+struct PairSigns {
+  uint32_t a0, a1;   // slot 0: rows (i0, i1) for q < 4, (R0, R2) otherwise
+  uint32_t c0, c1;   // slot 1: (R1, R2) (q >= 4)
+  uint32_t b0, b1;   // columns (q >= 4; q < 4 uses the fixed b = 1, 2 signs)
+};
+
+__device__ __forceinline__ PairSigns pair_signs(int q) {
+  PairSigns s;
+  int i0, i1;
+  if (q < 4) {
+    bt_pick(q, i0, i1, s.a0, s.a1);
+    s.c0 = s.c1 = s.b0 = s.b1 = 0;
+    return s;
+  }
+  int t0, t1;
+  pair_taps(q, t0, t1);
+  // top (rows 0,1,2): slot 0 a = 0 -> rows 0 (R0), 2 (R2); slot 1 a = 1 -> rows 1 (R1), 2 (R2)
+  // bottom (rows 3,2,1): slot 0 a = 3 -> rows 1 (R2), 3 (R0); slot 1 a = 2 -> rows 1 (R2), 2 (R1)
+  uint32_t x0, x1;
+  const bool top = (q & 1) == 0;
+  bt_pick(t0 >> 2, i0, i1, x0, x1);
+  if (top) { s.a0 = x0; s.a1 = x1; } else { s.a0 = x1; s.a1 = x0; }
+  bt_pick(t1 >> 2, i0, i1, x0, x1);
+  if (top) { s.c0 = x0; s.c1 = x1; } else { s.c0 = x1; s.c1 = x0; }
+  bt_pick(t0 & 3, i0, i1, s.b0, s.b1);
+  return s;
+}
+
+// Units: u = combo * nTB + tb, combo = q * nKP + kp.  Cluster g of G takes
+// the units whose weighted start position falls in its share.
+struct Range {
+  long long u0, u1;
+};
+
+__device__ __forceinline__ long long first_unit(const Geo& g, long long T) {
+  long long wc = 0;
+  const int ncombo = NPAIR * g.nKP;
+  for (int c = 0; c < ncombo; ++c) {
+    const int w = pair_weight(c / g.nKP);
+    const long long last = wc + (long long)(g.nTB - 1) * w;
+    if (T <= last) {
+      const long long d = T - wc;
+      const long long tb = d <= 0 ? 0 : (d + w - 1) / w;
+      return (long long)c * g.nTB + tb;
+    }
+    wc += (long long)g.nTB * w;
+  }
+  return (long long)ncombo * g.nTB;
+}
+
+__device__ __forceinline__ Range cluster_range(const Geo& g, int cl, int G) {
+  const long long W = (long long)g.nTB * g.nKP * (4 * 2 + 4 * 3);
+  Range r;
+  r.u0 = first_unit(g, ((long long)cl * W + G - 1) / G);
+  r.u1 = first_unit(g, ((long long)(cl + 1) * W + G - 1) / G);
+  return r;
+}
+
+struct Unit {
+  int q, kp, tb;
+};
+__device__ __forceinline__ Unit unit_of(const Geo& g, long long u) {
+  Unit x;
+  const long long combo = u / g.nTB;
+  x.tb = (int)(u - combo * g.nTB);
+  x.q = (int)(combo / g.nKP);
+  x.kp = (int)(combo - (long long)x.q * g.nKP);
+  return x;
+}
+
+// Load side of one unit for a producer thread (tile tl of this CTA's half,
+// channel half hh).
+struct ProdLoad {
+  const uint8_t* xn;   // XB of the tile's image, channel block 0
+  uint32_t off[6];
+  int nw;
+  bool live;
+};
+
+__device__ __forceinline__ ProdLoad prod_load(const Geo& g, const uint8_t* xb, const Unit& un, int rank,
+                                              int tl, int hh) {
+  ProdLoad pl;
+  const long long tile = (long long)un.tb * 128 + rank * VT + tl;
+  pl.live = tile < g.NT;
+  int n = 0, ty = 0, tx = 0;
+  if (pl.live) tile_decode(g, tile, n, ty, tx);
+  const PairWords pw = pair_words(un.q);
+  pl.nw = pw.nw;
+#pragma unroll
+  for (int w = 0; w < 6; ++w) pl.off[w] = win_off(g, ty, tx, hh, pw.r[w], pw.c[w]);
+  pl.xn = xb + (size_t)n * g.CS * g.cbs;
+  return pl;
+}
+
+}  // namespace tp
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tp::NTHREAD, 1)
+    twostage_pair_kernel(KernelParam p) {
+  using namespace tp;
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  __shared__ Shared sh;
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const Geo g = geo(p);
+  const int warp = warp_id(), lane = lane_id();
+  const int rank = (int)cluster_ctarank();
+  uint32_t* err = &g_twostage_err;
+  const Range rg = cluster_range(g, (int)cluster_id_x(), (int)cluster_count_x());
+  const int nst = (g.CS + SK - 1) / SK;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < NSTV; ++s) {
+      mbar_init(&sh.vfull[s], 2 * NWARP_P);
+      mbar_init(&sh.vempty[s], 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(&sh.accfull[a], 1);
+      mbar_init(&sh.accempty[a], 2 * NWARP_E);
+    }
+    mbar_init(&sh.ufull, 1);
+    mbar_init(&sh.uempty, 1);
+    mbar_init(&sh.utx, 1);
+    mbar_init(&sh.mmadone, 1);
+    sh.abort_flag = 0;
+    fence_barrier_init();
+  }
+  if (warp == WARP_MMA) { tmem_alloc_pair(&sh.tmem_base, 512); tmem_relinquish_pair(); }
+  tc_fence_before();
+  // both CTAs' barriers initialised and TMEM allocated before any remote use
+  cluster_sync();
+  tc_fence_after();
+  const uint32_t tmem = sh.tmem_base;
+  volatile int* abort_flag = &sh.abort_flag;
+  const uint32_t sbase = smem_u32(smem);
+  const uint32_t ubase = sbase, vbase = sbase + U_BYTES;
+  // rank 0's barriers, as shared::cluster addresses (the pair's MMA side)
+  const uint32_t lead_vfull = mapa_shared(smem_u32(&sh.vfull[0]), 0);
+  const uint32_t lead_accempty = mapa_shared(smem_u32(&sh.accempty[0]), 0);
+  const uint32_t lead_ufull = mapa_shared(smem_u32(&sh.ufull), 0);
+
+  if (warp == WARP_MMA) {
+    // ---- U loads and MMA issue.  Each CTA loads its 128 output channels of
+    // U for both taps and all C when the unit's (tap pair, k pair) changes;
+    // rank 0 also issues every MMA of the pair (per K-step both taps).
+    if (lane == 0) {
+      const uint8_t* u2 = static_cast<const uint8_t*>(p.transform_filter);
+      const uint32_t idesc = instr_desc(256, 128, 0, 0, 0, 0);
+      long long cur = -1;
+      uint32_t it = 0, ui = 0, nload = 0;
+      bool ok = true;
+      for (long long u = rg.u0; ok && u < rg.u1 && !*abort_flag; ++u, ++ui) {
+        const long long combo = u / g.nTB;
+        if (combo != cur) {
+          if (cur >= 0) {
+            // the old U is free once every MMA issued so far has finished
+            if (rank == 0) mma_commit_pair(&sh.uempty, BOTH);
+            if (!mbar_wait(&sh.uempty, (nload - 1) & 1, abort_flag, err, ERR_WAIT_EMPTY)) break;
+          }
+          cur = combo;
+          const Unit un = unit_of(g, u);
+          int t[2];
+          pair_taps(un.q, t[0], t[1]);
+          const int kb = 2 * un.kp + rank;
+          const int kbs = kb < g.nKB2 ? kblock2_rows(kb, g.K) : 0;
+          mbar_arrive_expect_tx(&sh.utx, (uint32_t)(2 * g.CS * kbs * 32));
+          for (int s = 0; s < 2 && kbs > 0; ++s) {
+            const uint8_t* src = u2 + u2_piece(t[s], kb, 0, g.K, g.C) * 2;
+            uint8_t* dst = smem + s * U_TAP;
+            if (kbs == 128) {
+              bulk_g2s(dst, src, (uint32_t)(g.CS * U_STEP), &sh.utx);
+            } else {
+              for (int cs = 0; cs < g.CS; ++cs)
+                bulk_g2s(dst + cs * U_STEP, src + (size_t)cs * kbs * 32, (uint32_t)(kbs * 32), &sh.utx);
+            }
+          }
+          if (!mbar_wait(&sh.utx, nload & 1, abort_flag, err, ERR_WAIT_FULL)) break;
+          if (rank == 1) {
+            mbar_arrive_remote(lead_ufull);
+          } else if (!mbar_wait_cluster(&sh.ufull, nload & 1, abort_flag, err, ERR_WAIT_FULL)) {
+            break;
+          }
+          ++nload;
+        }
+        if (rank != 0) continue;
+        const int ab = ui & 1;
+        if (ui >= 2 &&
+            !mbar_wait_cluster(&sh.accempty[ab], ((ui >> 1) - 1) & 1, abort_flag, err, ERR_WAIT_DRAIN))
+          break;
+        tc_fence_after();
+        const uint32_t d = tmem + ab * 256;
+        for (int j = 0; j < nst; ++j, ++it) {
+          const int st = it % NSTV;
+          if (!mbar_wait_cluster(&sh.vfull[st], (it / NSTV) & 1, abort_flag, err, ERR_WAIT_FULL)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const int nk = min(SK, g.CS - j * SK);
+          for (int kk = 0; kk < nk; ++kk) {
+            const int cs = j * SK + kk;
+#pragma unroll
+            for (int s = 0; s < 2; ++s)
+              mma_f16_pair(d + s * 128, smem_desc(ubase + s * U_TAP + cs * U_STEP, 128, 256),
+                           smem_desc(vbase + st * V_STAGE + (kk * 2 + s) * V_TAP, 128, 256), idesc,
+                           cs > 0 ? 1u : 0u);
+          }
+          mma_commit_pair(&sh.vempty[st], BOTH);
+        }
+        if (ok) mma_commit_pair(&sh.accfull[ab], BOTH);
+      }
+      if (rank == 0) {
+        // every MMA issued (also on an abort) has finished before TMEM is freed
+        mma_commit_pair(&sh.mmadone, 1);
+        mbar_wait(&sh.mmadone, 0, nullptr, err, ERR_WAIT_ACCUM);
+      }
+    }
+    __syncwarp();
+  } else if (warp < WARP_E0 + NWARP_E) {
+    // ---- epilogue: TMEM lane = output channel, columns = the unit's tiles
+    const int quarter = warp & 3;
+    __half* m16 = static_cast<__half*>(p.mid_result);
+    uint32_t ui = 0;
+    for (long long u = rg.u0; u < rg.u1; ++u, ++ui) {
+      const Unit un = unit_of(g, u);
+      const int ab = ui & 1;
+      if (!mbar_wait_warp(&sh.accfull[ab], (ui >> 1) & 1, abort_flag, err, ERR_WAIT_ACCUM, SLEEP_NS)) break;
+      tc_fence_after();
+      int t[2];
+      pair_taps(un.q, t[0], t[1]);
+      const int k = (2 * un.kp + rank) * 128 + quarter * 32 + lane;
+      const long long rem = g.NT - (long long)un.tb * 128;
+      const int ntb = rem < 128 ? (int)rem : 128;
+      const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + ab * 256;
+#pragma unroll 1
+      for (int s = 0; s < 2; ++s) {
+        __half* row = m16 + m_offset(un.tb, t[s], k < g.K ? k : 0, 0, g.K, g.NT);
+#pragma unroll 1
+        for (int c0 = 0; c0 < 128; c0 += 32) {
+          float v[32];
+          tmem_ld16(taddr + s * 128 + c0, v);
+          tmem_ld16(taddr + s * 128 + c0 + 16, v + 16);
+          tmem_ld_wait();
+          if (k >= g.K || c0 >= ntb) continue;
+          if (ntb == 128) {
+            uint32_t h[16];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+              const __half2 x = __floats2half2_rn(v[2 * i], v[2 * i + 1]);
+              h[i] = *reinterpret_cast<const uint32_t*>(&x);
+            }
+            uint4* dst = reinterpret_cast<uint4*>(row + c0);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) dst[i] = make_uint4(h[4 * i], h[4 * i + 1], h[4 * i + 2], h[4 * i + 3]);
+          } else {
+#pragma unroll
+            for (int i = 0; i < 32; ++i)
+              if (c0 + i < ntb) row[c0 + i] = __float2half_rn(v[i]);
+          }
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive_remote(lead_accempty + ab * 8);
+    }
+  } else {
+    // ---- V producers: thread = (tile tl of this CTA's 64, channel half hh,
+    // K-step kq of each stage)
+    const int pw = warp - WARP_P0;
+    const int tl = (pw & 1) * 32 + lane, hh = (pw >> 1) & 1, kq = pw >> 2;
+    const uint8_t* xb = static_cast<const uint8_t*>(p.transform_pin);
+    // the load cursor (lu, lj) runs one stage ahead of the consume cursor (cu, cj)
+    long long lu = rg.u0, cu = rg.u0;
+    int lj = 0, cj = 0;
+    ProdLoad pl;
+    uint4 wa[6], wb[6];
+    auto issue = [&](uint4 (&w)[6]) {
+      if (lj == 0) pl = prod_load(g, xb, unit_of(g, lu), rank, tl, hh);
+      const int cs = lj * SK + kq;
+      if (pl.live && cs < g.CS) {
+        const uint8_t* rec = pl.xn + (size_t)cs * g.cbs;
+#pragma unroll
+        for (int i = 0; i < 6; ++i)
+          if (i < pl.nw) w[i] = __ldg(reinterpret_cast<const uint4*>(rec + pl.off[i]));
+      }
+      if (++lj == nst) { lj = 0; ++lu; }
+    };
+    uint32_t it = 0;
+    auto consume = [&](const uint4 (&w)[6]) -> bool {
+      const int st = it % NSTV;
+      if (it >= NSTV &&
+          !mbar_wait_warp(&sh.vempty[st], (it / NSTV - 1) & 1, abort_flag, err, ERR_WAIT_EMPTY, SLEEP_NS))
+        return false;
+      const Unit un = unit_of(g, cu);
+      const bool live = (long long)un.tb * 128 + rank * VT + tl < g.NT;
+      if (live && cj * SK + kq < g.CS) {
+        const PairSigns sg = pair_signs(un.q);
+        uint4 v0, v1;
+        if (un.q < 4) {
+          const uint4 e1 = bt_op4(sg.a0, sg.a1, w[0], w[1]);
+          const uint4 e2 = bt_op4(sg.a0, sg.a1, w[2], w[3]);
+          v0 = bt_op4(0x3c003c00u, 0x3c003c00u, e1, e2);   // b = 1: d1 + d2
+          v1 = bt_op4(0xbc00bc00u, 0x3c003c00u, e1, e2);   // b = 2: d2 - d1
+        } else {
+          v0 = bt_op4(sg.b0, sg.b1, bt_op4(sg.a0, sg.a1, w[0], w[2]), bt_op4(sg.a0, sg.a1, w[3], w[5]));
+          v1 = bt_op4(sg.b0, sg.b1, bt_op4(sg.c0, sg.c1, w[1], w[2]), bt_op4(sg.c0, sg.c1, w[4], w[5]));
+        }
+        uint8_t* dst = smem + U_BYTES + st * V_STAGE + (kq * 2) * V_TAP + (tl >> 3) * 256 + hh * 128 +
+                       (tl & 7) * 16;
+        *reinterpret_cast<uint4*>(dst) = v0;
+        *reinterpret_cast<uint4*>(dst + V_TAP) = v1;
+      }
+      fence_proxy_async_shared();
+      __syncwarp();
+      if (lane == 0) mbar_arrive_remote(lead_vfull + st * 8);
+      ++it;
+      if (++cj == nst) { cj = 0; ++cu; }
+      return true;
+    };
+    if (lu < rg.u1) issue(wa);
+    while (cu < rg.u1 && !*abort_flag) {
+      if (lu < rg.u1) issue(wb);
+      if (!consume(wa)) break;
+      if (cu >= rg.u1 || *abort_flag) break;
+      if (lu < rg.u1) issue(wa);
+      if (!consume(wb)) break;
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  // the peer may still read this CTA's shared memory or arrive on its
+  // barriers until both CTAs get here
+  cluster_sync();
+  if (warp == WARP_MMA) {
+    tc_fence_after();
+    tmem_dealloc_pair(tmem, 512);
+  }
+}
+
+// =============================================================================
+// One-tap GEMM with streamed U (any C)
+// =============================================================================
+namespace tsk {
+
+using namespace ts;
+
 constexpr int NSTAGE = 4;
-constexpr int SK = 4;                         // K-steps (16 channels each) per stage
+constexpr int SK = 4;                         // K-steps (16 channels) per stage
 constexpr int KPU = 2;                        // 128-row k-blocks per unit
 constexpr int A_STEP = 128 * 16 * 2;          // 4 KB: V of 128 tiles x 16 channels (K-major)
 constexpr int B_STEP = KB2 * 16 * 2;          // 4 KB: U of one 128-row k-block
@@ -60,122 +583,69 @@ constexpr int STAGE_B = SK * B_STEP;
 constexpr int STAGE_BYTES = STAGE_A + KPU * STAGE_B;
 constexpr int SMEM_BYTES = NSTAGE * STAGE_BYTES + 1024;
 constexpr int WARP_U = 0, WARP_MMA = 1, WARP_E0 = 2, NWARP_E = 4, WARP_P0 = 6, NWARP_P = 8;
-// Back-off of the waiting warps (after 8 polls), so that spinning epilogue
-// and producer warps do not take issue slots from the working ones.
 constexpr uint32_t SLEEP_EPI_NS = 32, SLEEP_PROD_NS = 32;
 constexpr int NTHREAD = (WARP_P0 + NWARP_P) * 32;
 
 struct Shared {
   uint64_t full[NSTAGE], empty[NSTAGE];
   uint64_t accfull[2], accempty[2];
+  uint64_t mmadone;
   uint32_t tmem_base;
   int abort_flag;
 };
 
-struct Geo {
-  int K, CS, HP, E, TP, TQ, nTB, nKB2, nKP, nst;
-  long long NT, nunits;
-  uint32_t RB;
-};
-
-__device__ __forceinline__ Geo geo(const KernelParam& p) {
-  Geo g;
-  g.K = p.k;
-  g.CS = p.c >> 4;
-  g.HP = xb_rows(p.h);
-  g.E = xb_entries(p.w);
-  g.RB = (uint32_t)xb_row_bytes(p.w);
-  g.TP = (p.Oh + 1) >> 1;
-  g.TQ = (p.Ow + 1) >> 1;
-  g.NT = (long long)p.n * g.TP * g.TQ;
-  g.nTB = (int)((g.NT + 127) / 128);
-  g.nKB2 = (g.K + KB2 - 1) / KB2;
-  g.nKP = (g.nKB2 + KPU - 1) / KPU;
-  g.nunits = 16LL * g.nTB * g.nKP;
-  g.nst = (g.CS + SK - 1) / SK;
-  return g;
-}
+__device__ __forceinline__ long long nunits(const Geo& g) { return 16LL * g.nTB * ((g.nKB2 + KPU - 1) / KPU); }
 
 // Unit u -> tap t (fastest), k-block pair, tile block; kbs[i] = rows of the
 // pair's i-th k-block (0 when absent).
 __device__ __forceinline__ void unit_coords(const Geo& g, long long u, int& t, int& tb, int& kb,
                                             int (&kbs)[KPU]) {
+  const int nKP = (g.nKB2 + KPU - 1) / KPU;
   t = (int)(u & 15);
   const long long r = u >> 4;
-  const int kp = (int)(r % g.nKP);
-  tb = (int)(r / g.nKP);
+  const int kp = (int)(r % nKP);
+  tb = (int)(r / nKP);
   kb = kp * KPU;
 #pragma unroll
   for (int i = 0; i < KPU; ++i) kbs[i] = kb + i < g.nKB2 ? kblock2_rows(kb + i, g.K) : 0;
 }
 
-// B^T row / column a of the 4-point transform (the fused kernel's bt_row /
-// bt_cols: d0-d2, d1+d2, d2-d1, d1-d3) as two indices and the signs s0, s1 of
-// s0*x[i0] + s1*x[i1], packed as fp16x2 (+1 = 0x3c00, -1 = 0xbc00).
-__device__ __forceinline__ void bt_pick(int a, int& i0, int& i1, uint32_t& s0, uint32_t& s1) {
-  i0 = a == 0 ? 0 : 1;
-  i1 = a == 3 ? 3 : 2;
-  s0 = a == 2 ? 0xbc00bc00u : 0x3c003c00u;
-  s1 = (a == 0 || a == 3) ? 0xbc00bc00u : 0x3c003c00u;
-}
-
-// s0*x0 + s1*x1 with one rounding: the product by +-1 is exact, so this is
-// bit-identical to the fused kernel's hadd2 / hsub2.
-__device__ __forceinline__ uint32_t bt_op(uint32_t s0, uint32_t s1, uint32_t x0, uint32_t x1) {
-  __half2 r = __hfma2(*reinterpret_cast<__half2*>(&x1), *reinterpret_cast<__half2*>(&s1),
-                      __hmul2(*reinterpret_cast<__half2*>(&x0), *reinterpret_cast<__half2*>(&s0)));
-  return *reinterpret_cast<uint32_t*>(&r);
-}
-
-// Loading side of one work unit for a producer thread.
 struct ProdUnit {
-  const uint8_t* xn;          // XB of the tile's image, channel block 0
-  uint32_t o[4];              // window positions (i0,j0) (i0,j1) (i1,j0) (i1,j1)
+  const uint8_t* xn;
+  uint32_t o[4];
   uint32_t sa0, sa1, sb0, sb1;
   bool live;
 };
 
-__device__ __forceinline__ ProdUnit prod_unit(const Geo& g, const uint8_t* xb, int t, int tb, int tl,
-                                              int hh) {
+__device__ __forceinline__ ProdUnit prod_unit(const Geo& g, const uint8_t* xb, int t, int tb, int tl, int hh) {
   ProdUnit pu;
   const long long tile = (long long)tb * 128 + tl;
   pu.live = tile < g.NT;
   int n = 0, ty = 0, tx = 0;
-  if (pu.live) {
-    const long long per = (long long)g.TP * g.TQ;
-    n = (int)(tile / per);
-    const int r = (int)(tile - (long long)n * per);
-    ty = r / g.TQ;
-    tx = r - ty * g.TQ;
-  }
+  if (pu.live) tile_decode(g, tile, n, ty, tx);
   int i0, i1, j0, j1;
   bt_pick(t >> 2, i0, i1, pu.sa0, pu.sa1);
   bt_pick(t & 3, j0, j1, pu.sb0, pu.sb1);
-  // byte offsets in an XB record block (n, cb) of the window positions (row
-  // 2ty + i, column 2tx - 1 + jc) of channel half hh: column jc lies in
-  // parity (jc & 1) ^ 1, entry tx + (jc >> 1)
-  const uint32_t rbase = (uint32_t)(2 * ty) * g.RB;
-  auto col_off = [&](int jc) {
-    return (uint32_t)(((((jc & 1) ^ 1) * 2 + hh) * g.E + tx + (jc >> 1)) * 16);
-  };
-  pu.o[0] = rbase + i0 * g.RB + col_off(j0);
-  pu.o[1] = rbase + i0 * g.RB + col_off(j1);
-  pu.o[2] = rbase + i1 * g.RB + col_off(j0);
-  pu.o[3] = rbase + i1 * g.RB + col_off(j1);
-  pu.xn = xb + (size_t)n * g.CS * g.HP * g.RB;
+  pu.o[0] = win_off(g, ty, tx, hh, i0, j0);
+  pu.o[1] = win_off(g, ty, tx, hh, i0, j1);
+  pu.o[2] = win_off(g, ty, tx, hh, i1, j0);
+  pu.o[3] = win_off(g, ty, tx, hh, i1, j1);
+  pu.xn = xb + (size_t)n * g.CS * g.cbs;
   return pu;
 }
 
-}  // namespace ts
+}  // namespace tsk
 
-__global__ void __launch_bounds__(ts::NTHREAD, 1) twostage_gemm_kernel(KernelParam p) {
-  using namespace ts;
+__global__ void __launch_bounds__(tsk::NTHREAD, 1) twostage_stream_kernel(KernelParam p) {
+  using namespace tsk;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   __shared__ Shared sh;
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const Geo g = geo(p);
   const int warp = warp_id(), lane = lane_id();
   uint32_t* err = &g_twostage_err;
+  const long long NU = nunits(g);
+  const int nst = (g.CS + SK - 1) / SK;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < NSTAGE; ++s) {
@@ -186,6 +656,7 @@ __global__ void __launch_bounds__(ts::NTHREAD, 1) twostage_gemm_kernel(KernelPar
       mbar_init(&sh.accfull[a], 1);
       mbar_init(&sh.accempty[a], NWARP_E);
     }
+    mbar_init(&sh.mmadone, 1);
     sh.abort_flag = 0;
     fence_barrier_init();
   }
@@ -202,10 +673,10 @@ __global__ void __launch_bounds__(ts::NTHREAD, 1) twostage_gemm_kernel(KernelPar
       const uint8_t* u2 = static_cast<const uint8_t*>(p.transform_filter);
       uint32_t it = 0;
       bool ok = true;
-      for (long long u = blockIdx.x; ok && u < g.nunits && !*abort_flag; u += gridDim.x) {
+      for (long long u = blockIdx.x; ok && u < NU && !*abort_flag; u += gridDim.x) {
         int t, tb, kb, kbs[KPU];
         unit_coords(g, u, t, tb, kb, kbs);
-        for (int j = 0; j < g.nst; ++j, ++it) {
+        for (int j = 0; j < nst; ++j, ++it) {
           const int st = it % NSTAGE;
           if (it >= NSTAGE &&
               !mbar_wait(&sh.empty[st], (it / NSTAGE - 1) & 1, abort_flag, err, ERR_WAIT_EMPTY)) {
@@ -231,7 +702,7 @@ __global__ void __launch_bounds__(ts::NTHREAD, 1) twostage_gemm_kernel(KernelPar
     if (lane == 0) {
       uint32_t it = 0, ui = 0;
       bool ok = true;
-      for (long long u = blockIdx.x; ok && u < g.nunits && !*abort_flag; u += gridDim.x, ++ui) {
+      for (long long u = blockIdx.x; ok && u < NU && !*abort_flag; u += gridDim.x, ++ui) {
         int t, tb, kb, kbs[KPU];
         unit_coords(g, u, t, tb, kb, kbs);
         uint32_t idesc[KPU];
@@ -242,7 +713,7 @@ __global__ void __launch_bounds__(ts::NTHREAD, 1) twostage_gemm_kernel(KernelPar
           break;
         tc_fence_after();
         const uint32_t d = tmem + ab * (KPU * 128);
-        for (int j = 0; j < g.nst; ++j, ++it) {
+        for (int j = 0; j < nst; ++j, ++it) {
           const int st = it % NSTAGE;
           if (!mbar_wait(&sh.full[st], (it / NSTAGE) & 1, abort_flag, err, ERR_WAIT_FULL)) {
             ok = false;
@@ -263,33 +734,35 @@ __global__ void __launch_bounds__(ts::NTHREAD, 1) twostage_gemm_kernel(KernelPar
         }
         if (ok) mma_commit(&sh.accfull[ab]);
       }
+      // every MMA issued (also on an abort) has finished before TMEM is freed
+      mma_commit(&sh.mmadone);
+      mbar_wait(&sh.mmadone, 0, nullptr, err, ERR_WAIT_ACCUM);
     }
     __syncwarp();
   } else if (warp < WARP_E0 + NWARP_E) {
     // epilogue: TMEM lanes 32*quarter .. +31 = tiles of the block
     const int quarter = warp & 3;
     __half* m16 = static_cast<__half*>(p.mid_result);
-    const size_t NT = (size_t)g.NT;
     uint32_t ui = 0;
-    for (long long u = blockIdx.x; u < g.nunits; u += gridDim.x, ++ui) {
+    for (long long u = blockIdx.x; u < NU; u += gridDim.x, ++ui) {
       int t, tb, kb, kbs[KPU];
       unit_coords(g, u, t, tb, kb, kbs);
       const int ab = ui & 1;
       if (!mbar_wait_warp(&sh.accfull[ab], (ui >> 1) & 1, abort_flag, err, ERR_WAIT_ACCUM, SLEEP_EPI_NS)) break;
       tc_fence_after();
-      const size_t tile = (size_t)tb * 128 + quarter * 32 + lane;
-      const bool live = tile < NT;
+      const int i = quarter * 32 + lane;   // tile within the block
+      const bool live = (long long)tb * 128 + i < g.NT;
       const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + ab * (KPU * 128);
       for (int cc = 0; cc < KPU * 128; cc += 16) {
-        const int i = cc >> 7, c0 = cc & 127;
-        if (c0 >= kbs[i]) continue;
+        const int kbi = cc >> 7, c0 = cc & 127;
+        if (c0 >= kbs[kbi]) continue;
         float v[16];
         tmem_ld16(taddr + cc, v);
         tmem_ld_wait();
         if (live) {
-          __half* dst = m16 + ((size_t)t * g.K + (size_t)(kb + i) * KB2 + c0) * NT + tile;
+          const int k0 = (kb + kbi) * KB2 + c0;
 #pragma unroll
-          for (int jj = 0; jj < 16; ++jj) dst[(size_t)jj * NT] = __float2half_rn(v[jj]);
+          for (int jj = 0; jj < 16; ++jj) m16[m_offset(tb, t, k0 + jj, i, g.K, g.NT)] = __float2half_rn(v[jj]);
         }
       }
       tc_fence_before();
@@ -301,14 +774,13 @@ __global__ void __launch_bounds__(ts::NTHREAD, 1) twostage_gemm_kernel(KernelPar
     const int pw = warp - WARP_P0;
     const int tl = (pw & 3) * 32 + lane, hh = pw >> 2;
     const uint8_t* xb = static_cast<const uint8_t*>(p.transform_pin);
-    const size_t cb_stride = (size_t)g.HP * g.RB;
     uint32_t it = 0;
     bool ok = true;
-    for (long long u = blockIdx.x; ok && u < g.nunits && !*abort_flag; u += gridDim.x) {
+    for (long long u = blockIdx.x; ok && u < NU && !*abort_flag; u += gridDim.x) {
       int t, tb, kb, kbs[KPU];
       unit_coords(g, u, t, tb, kb, kbs);
       const ProdUnit pu = prod_unit(g, xb, t, tb, tl, hh);
-      for (int j = 0; j < g.nst; ++j, ++it) {
+      for (int j = 0; j < nst; ++j, ++it) {
         const int st = it % NSTAGE;
         const int nk = min(SK, g.CS - j * SK);
         // the window loads go out before the wait for a free stage: only the
@@ -317,7 +789,7 @@ __global__ void __launch_bounds__(ts::NTHREAD, 1) twostage_gemm_kernel(KernelPar
 #pragma unroll
         for (int kk = 0; kk < SK; ++kk) {
           if (pu.live && kk < nk) {
-            const uint8_t* rec = pu.xn + (size_t)(j * SK + kk) * cb_stride;
+            const uint8_t* rec = pu.xn + (size_t)(j * SK + kk) * g.cbs;
 #pragma unroll
             for (int w = 0; w < 4; ++w) d[kk][w] = __ldg(reinterpret_cast<const uint4*>(rec + pu.o[w]));
           } else {
@@ -336,13 +808,9 @@ __global__ void __launch_bounds__(ts::NTHREAD, 1) twostage_gemm_kernel(KernelPar
         for (int kk = 0; kk < SK; ++kk) {
           if (kk < nk) {
             // rows first (e_jc = sa0*d[i0][jc] + sa1*d[i1][jc]), then columns
-            const uint4 a0 = d[kk][0], a1 = d[kk][1], b0 = d[kk][2], b1 = d[kk][3];
-            uint4 v;
-            v.x = bt_op(pu.sb0, pu.sb1, bt_op(pu.sa0, pu.sa1, a0.x, b0.x), bt_op(pu.sa0, pu.sa1, a1.x, b1.x));
-            v.y = bt_op(pu.sb0, pu.sb1, bt_op(pu.sa0, pu.sa1, a0.y, b0.y), bt_op(pu.sa0, pu.sa1, a1.y, b1.y));
-            v.z = bt_op(pu.sb0, pu.sb1, bt_op(pu.sa0, pu.sa1, a0.z, b0.z), bt_op(pu.sa0, pu.sa1, a1.z, b1.z));
-            v.w = bt_op(pu.sb0, pu.sb1, bt_op(pu.sa0, pu.sa1, a0.w, b0.w), bt_op(pu.sa0, pu.sa1, a1.w, b1.w));
-            *reinterpret_cast<uint4*>(adst + kk * A_STEP) = v;
+            *reinterpret_cast<uint4*>(adst + kk * A_STEP) =
+                bt_op4(pu.sb0, pu.sb1, bt_op4(pu.sa0, pu.sa1, d[kk][0], d[kk][2]),
+                       bt_op4(pu.sa0, pu.sa1, d[kk][1], d[kk][3]));
           }
         }
         fence_proxy_async_shared();
@@ -359,71 +827,69 @@ __global__ void __launch_bounds__(ts::NTHREAD, 1) twostage_gemm_kernel(KernelPar
   }
 }
 
-// Output transform: thread = (2 consecutive tiles, k) reading the 16 taps of
-// M16 (tile stride = the number of tiles) as one fp16 pair each when the
-// tile count is even; Y tile = A^T m A in fp32, one fp16 rounding.
-// grid (ceil(tiles / 512), K).
-constexpr int OT_TILES = 2;
+// =============================================================================
+// Output transform
+// =============================================================================
+// CTA = (tile block tb, 8 output channels); thread = (channel kl, 4 tiles
+// g4 .. g4+3 of the block): 16 taps x one 8-byte word of the blocked M (a
+// warp reads 256 contiguous bytes per tap), Y tile = A^T m A in fp32, one
+// fp16 rounding.  grid (tile blocks, ceil(K/8)).
+constexpr int OT_TILES = 4;
 
 __global__ void __launch_bounds__(256) twostage_output_kernel(KernelParam p) {
+  using namespace ts;
   const int K = p.k, P = p.Oh, Q = p.Ow;
   const int TP = (P + 1) >> 1, TQ = (Q + 1) >> 1;
   const long long NT = (long long)p.n * TP * TQ;
-  const long long tile0 = ((long long)blockIdx.x * 256 + threadIdx.x) * OT_TILES;
-  const int k = blockIdx.y;
-  if (tile0 >= NT) return;
-  const int nt = NT - tile0 < OT_TILES ? (int)(NT - tile0) : OT_TILES;
+  const int tb = blockIdx.x;
+  const int k = blockIdx.y * 8 + (threadIdx.x >> 5);
+  const int g4 = (threadIdx.x & 31) * OT_TILES;
+  if (k >= K) return;
+  const long long rem = NT - (long long)tb * 128;
+  const int ntb = rem < 128 ? (int)rem : 128;
+  if (g4 >= ntb) return;
   const __half* m16 = static_cast<const __half*>(p.mid_result);
-  const bool vec = (NT & 1) == 0 && (reinterpret_cast<uintptr_t>(m16) & 3) == 0;
   float m[16][OT_TILES];
+  if (ntb == 128) {
 #pragma unroll
-  for (int t = 0; t < 16; ++t) {
-    const __half* src = m16 + ((size_t)t * K + k) * (size_t)NT + tile0;
-    if (vec) {
-      const float2 v = __half22float2(*reinterpret_cast<const __half2*>(src));
-      m[t][0] = v.x;
-      m[t][1] = v.y;
-    } else {
-      m[t][0] = __half2float(src[0]);
-      m[t][1] = nt > 1 ? __half2float(src[1]) : 0.f;
+    for (int t = 0; t < 16; ++t) {
+      const uint2 w = *reinterpret_cast<const uint2*>(m16 + m_offset(tb, t, k, g4, K, NT));
+      const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&w.x));
+      const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&w.y));
+      m[t][0] = a.x; m[t][1] = a.y; m[t][2] = b.x; m[t][3] = b.y;
+    }
+  } else {
+#pragma unroll
+    for (int t = 0; t < 16; ++t) {
+      const __half* src = m16 + m_offset(tb, t, k, g4, K, NT);
+#pragma unroll
+      for (int i = 0; i < OT_TILES; ++i) m[t][i] = g4 + i < ntb ? __half2float(src[i]) : 0.f;
     }
   }
   const long long per_img = (long long)TP * TQ;
   const bool pair_ok = (Q & 1) == 0 && (reinterpret_cast<uintptr_t>(p.pout) & 3) == 0;
-  // both tiles in one tile row with 8-byte aligned output rows: the four
-  // columns of each output row go out as one 8-byte store
-  float yy[OT_TILES][4];
-  int n0 = 0, ty0 = 0, tx0 = 0;
-  {
-    const int r0 = (int)(tile0 - (long long)(tile0 / per_img) * per_img);
-    n0 = (int)(tile0 / per_img);
-    ty0 = r0 / TQ;
-    tx0 = r0 - ty0 * TQ;
-  }
-  const bool row_pair = nt == 2 && tx0 + 1 < TQ && (Q & 3) == 0 && (tx0 & 1) == 0 &&
-                        (reinterpret_cast<uintptr_t>(p.pout) & 7) == 0;
+  __half* out = static_cast<__half*>(p.pout);
 #pragma unroll
-  for (int j = 0; j < OT_TILES; ++j) {
-    if (j >= nt) break;
+  for (int i = 0; i < OT_TILES; ++i) {
+    if (g4 + i >= ntb) break;
     float z[2][4];
 #pragma unroll
     for (int b = 0; b < 4; ++b) {
-      z[0][b] = m[b][j] + m[4 + b][j] + m[8 + b][j];
-      z[1][b] = m[4 + b][j] - m[8 + b][j] - m[12 + b][j];
+      z[0][b] = m[b][i] + m[4 + b][i] + m[8 + b][i];
+      z[1][b] = m[4 + b][i] - m[8 + b][i] - m[12 + b][i];
     }
-    float* y = yy[j];
+    float y[4];
 #pragma unroll
-    for (int i = 0; i < 2; ++i) {
-      y[2 * i + 0] = z[i][0] + z[i][1] + z[i][2];
-      y[2 * i + 1] = z[i][1] - z[i][2] - z[i][3];
+    for (int r = 0; r < 2; ++r) {
+      y[2 * r + 0] = z[r][0] + z[r][1] + z[r][2];
+      y[2 * r + 1] = z[r][1] - z[r][2] - z[r][3];
     }
-    if (row_pair) continue;
-    const long long tile = tile0 + j;
+    const long long tile = (long long)tb * 128 + g4 + i;
     const int n = (int)(tile / per_img);
-    const int r = (int)(tile - (long long)n * per_img);
-    const int ty = r / TQ, tx = r - ty * TQ;
+    const int rr = (int)(tile - (long long)n * per_img);
+    const int ty = rr / TQ, tx = rr - ty * TQ;
     const int oy = 2 * ty, ox = 2 * tx;
-    __half* o = static_cast<__half*>(p.pout) + (((size_t)n * K + k) * P + oy) * (size_t)Q + ox;
+    __half* o = out + (((size_t)n * K + k) * P + oy) * (size_t)Q + ox;
     const bool two_cols = ox + 1 < Q, two_rows = oy + 1 < P;
     if (two_cols && pair_ok) {
       *reinterpret_cast<__half2*>(o) = __floats2half2_rn(y[0], y[1]);
@@ -437,20 +903,6 @@ __global__ void __launch_bounds__(256) twostage_output_kernel(KernelParam p) {
       }
     }
   }
-  if (row_pair) {
-    const int oy = 2 * ty0, ox = 2 * tx0;
-    __half* o = static_cast<__half*>(p.pout) + (((size_t)n0 * K + k) * P + oy) * (size_t)Q + ox;
-#pragma unroll
-    for (int i = 0; i < 2; ++i) {
-      if (oy + i >= P) break;
-      const __half2 a = __floats2half2_rn(yy[0][2 * i], yy[0][2 * i + 1]);
-      const __half2 b = __floats2half2_rn(yy[1][2 * i], yy[1][2 * i + 1]);
-      uint2 pk;
-      pk.x = *reinterpret_cast<const uint32_t*>(&a);
-      pk.y = *reinterpret_cast<const uint32_t*>(&b);
-      *reinterpret_cast<uint2*>(o + (size_t)i * Q) = pk;
-    }
-  }
 }
 
 }  // namespace wino
@@ -459,33 +911,57 @@ using namespace wino;
 
 extern "C" {
 
-void* wino_twostage_gemm_kernel_ptr() { return (void*)twostage_gemm_kernel; }
+// The GEMM kernel for C input channels: the tap-pair kernel keeps U resident
+// for up to 256 channels, the streamed-U kernel takes any C.
+static bool use_pair(int c) { return c <= 16 * tp::CS_MAX; }
+
+void* wino_twostage_gemm_kernel_ptr_for(int c) {
+  return use_pair(c) ? (void*)twostage_pair_kernel : (void*)twostage_stream_kernel;
+}
+void* wino_twostage_pair_kernel_ptr() { return (void*)twostage_pair_kernel; }
+void* wino_twostage_stream_kernel_ptr() { return (void*)twostage_stream_kernel; }
 void* wino_twostage_output_kernel_ptr() { return (void*)twostage_output_kernel; }
-int wino_twostage_threads() { return ts::NTHREAD; }
-int wino_twostage_smem_bytes() { return ts::SMEM_BYTES; }
+int wino_twostage_threads_for(int c) { return use_pair(c) ? tp::NTHREAD : tsk::NTHREAD; }
+int wino_twostage_smem_bytes_for(int c) { return use_pair(c) ? tp::SMEM_BYTES : tsk::SMEM_BYTES; }
 
 int wino_twostage_prepare() {
-  return (int)cudaFuncSetAttribute(twostage_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   ts::SMEM_BYTES);
+  if (cudaFuncSetAttribute(twostage_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           tsk::SMEM_BYTES) != cudaSuccess)
+    return 1;
+  return (int)cudaFuncSetAttribute(twostage_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   tp::SMEM_BYTES);
 }
 
-// Tiles and the M16 bytes of a shape (tile stride = tiles, no padding).
+// Tiles and the M16 bytes of a shape (no padding).
 long long wino_twostage_tiles(int n, int h, int w) { return (long long)n * ((h + 1) / 2) * ((w + 1) / 2); }
 size_t wino_twostage_m_bytes(int n, int h, int w, int k) {
   return (size_t)16 * (size_t)k * (size_t)wino_twostage_tiles(n, h, w) * 2;
 }
 
-// GEMM grid: one CTA per SM up to the number of work units.
-unsigned wino_twostage_gemm_grid(int n, int h, int w, int k, int sms) {
+// Element offset of M[t][kk][tile] in the blocked M layout (for callers that
+// read mid_result).
+size_t wino_twostage_m_offset(int n, int h, int w, int k, int t, int kk, long long tile) {
+  const long long NT = wino_twostage_tiles(n, h, w);
+  return ts::m_offset((int)(tile / 128), t, kk, (int)(tile % 128), k, NT);
+}
+
+// GEMM grid: one CTA per SM up to the work available; the tap-pair kernel
+// runs clusters of two CTAs (an even grid).
+unsigned wino_twostage_gemm_grid(int n, int c, int h, int w, int k, int sms) {
   const long long ntb = (wino_twostage_tiles(n, h, w) + 127) / 128;
-  const long long nkp = ((k + KB2 - 1) / KB2 + ts::KPU - 1) / ts::KPU;
-  const long long units = 16LL * ntb * nkp;
+  const long long nkb = (k + KB2 - 1) / KB2;
+  if (use_pair(c)) {
+    const long long units = (long long)tp::NPAIR * ntb * ((nkb + 1) / 2);
+    const long long clusters = sms / 2;
+    return (unsigned)(2 * (units < clusters ? units : clusters));
+  }
+  const long long units = 16LL * ntb * ((nkb + tsk::KPU - 1) / tsk::KPU);
   return (unsigned)(units < sms ? units : sms);
 }
 
 void wino_twostage_output_grid(int n, int h, int w, int k, unsigned* gx, unsigned* gy) {
-  *gx = (unsigned)((wino_twostage_tiles(n, h, w) + 256 * OT_TILES - 1) / (256 * OT_TILES));
-  *gy = (unsigned)k;
+  *gx = (unsigned)((wino_twostage_tiles(n, h, w) + 127) / 128);
+  *gy = (unsigned)((k + 7) / 8);
 }
 
 uint32_t wino_twostage_error_read_clear() {

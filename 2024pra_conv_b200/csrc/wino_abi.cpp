@@ -80,13 +80,13 @@ uint32_t wino_unfused_error_read_clear();
 int wino_launch_filter_transform(const void* weight, void* ucache, void* ucache_lo, int K, int C,
                                  int bf16, int layout, cudaStream_t stream);
 void* wino_dropin_filter_u2_kernel_ptr();
-void* wino_twostage_gemm_kernel_ptr();
+void* wino_twostage_gemm_kernel_ptr_for(int c);
 void* wino_twostage_output_kernel_ptr();
-int wino_twostage_threads();
-int wino_twostage_smem_bytes();
+int wino_twostage_threads_for(int c);
+int wino_twostage_smem_bytes_for(int c);
 int wino_twostage_prepare();
 size_t wino_twostage_m_bytes(int n, int h, int w, int k);
-unsigned wino_twostage_gemm_grid(int n, int h, int w, int k, int sms);
+unsigned wino_twostage_gemm_grid(int n, int c, int h, int w, int k, int sms);
 void wino_twostage_output_grid(int n, int h, int w, int k, unsigned* gx, unsigned* gy);
 uint32_t wino_twostage_error_read_clear();
 }
@@ -218,6 +218,7 @@ static int plan_route(const problem_t& pr) {
   // the caller's mid_result, output transform in slot 4) whenever M fits the
   // reference's mid_result size of 4*k*h*w*n fp16 elements (even H and W).
   const bool two_stage = pr.mid_result != nullptr &&
+                         (reinterpret_cast<uintptr_t>(pr.mid_result) & 15) == 0 &&
                          twostage_ok((int)pr.n, (int)pr.c, (int)pr.h, (int)pr.w) &&
                          wino_twostage_m_bytes((int)pr.n, (int)pr.h, (int)pr.w, (int)pr.k) <=
                              (size_t)4 * pr.k * pr.h * pr.w * pr.n * 2;
@@ -268,9 +269,10 @@ int getkernelInfo(problem_t* problem, kernelInfo_t* kernelInfo, void* param) {
              wino_dropin_filter_u2_kernel_ptr());
     set_slot(kernelInfo, 2, wino_xb_layout_grid((int)pr.n, (int)pr.c, (int)pr.h, (int)pr.w), 1, 1, 256, 1, 1, 0,
              wino_xb_layout_kernel_ptr());
-    set_slot(kernelInfo, 3, wino_twostage_gemm_grid((int)pr.n, (int)pr.h, (int)pr.w, (int)pr.k, sm_count()), 1, 1,
-             (unsigned)wino_twostage_threads(), 1, 1, (unsigned)wino_twostage_smem_bytes(),
-             wino_twostage_gemm_kernel_ptr());
+    const int c = (int)pr.c;
+    set_slot(kernelInfo, 3, wino_twostage_gemm_grid((int)pr.n, c, (int)pr.h, (int)pr.w, (int)pr.k, sm_count()), 1,
+             1, (unsigned)wino_twostage_threads_for(c), 1, 1, (unsigned)wino_twostage_smem_bytes_for(c),
+             wino_twostage_gemm_kernel_ptr_for(c));
     unsigned ox, oy;
     wino_twostage_output_grid((int)pr.n, (int)pr.h, (int)pr.w, (int)pr.k, &ox, &oy);
     set_slot(kernelInfo, 4, ox, oy, 1, 256, 1, 1, 0, wino_twostage_output_kernel_ptr());
@@ -389,10 +391,10 @@ extern "C" int wino_twostage_stage(int stage, const void* x, const void* ucache2
   void* args[] = {&p};
   if (stage == 0) return wino_launch_xb_layout(&p, s) == 0 ? WINO_OK : WINO_ECUDA;
   if (stage == 1)
-    return cudaLaunchKernel(wino_twostage_gemm_kernel_ptr(),
-                            dim3(wino_twostage_gemm_grid(n, h, w, k, sm_count())),
-                            dim3(wino_twostage_threads()), args, (size_t)wino_twostage_smem_bytes(),
-                            s) == cudaSuccess
+    return cudaLaunchKernel(wino_twostage_gemm_kernel_ptr_for(c),
+                            dim3(wino_twostage_gemm_grid(n, c, h, w, k, sm_count())),
+                            dim3(wino_twostage_threads_for(c)), args,
+                            (size_t)wino_twostage_smem_bytes_for(c), s) == cudaSuccess
                ? WINO_OK
                : WINO_ECUDA;
   unsigned ox, oy;

@@ -366,7 +366,7 @@ def run_ours(args, rank, world, local_rank):
     ts_us, ts_gemm_us, ts_out_us = (ts_ms / iters * 1e3, ts_gemm_ms / iters * 1e3,
                                     ts_out_ms / iters * 1e3)
     # the route getkernelInfo chose for the timed drop-in step
-    two_stage = ki.slot(3)["kernel"] == wino.lib().wino_twostage_gemm_kernel_ptr()
+    two_stage = ki.slot(3)["kernel"] == wino.lib().wino_twostage_gemm_kernel_ptr_for(c)
 
     # --- end to end through the C-ABI with host buffers.  Every step uploads
     # its input from pinned host memory, runs the drop-in slots and downloads

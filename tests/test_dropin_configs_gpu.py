@@ -36,7 +36,7 @@ def _dropin(wino, cuda, x16, w16):
     rc, ki = wino.get_kernel_info(pr, param)
     assert rc == 0
     L = wino.lib()
-    assert ki.slot(3)["kernel"] == L.wino_twostage_gemm_kernel_ptr()
+    assert ki.slot(3)["kernel"] == L.wino_twostage_gemm_kernel_ptr_for(c)
     assert ki.slot(4)["kernel"] == L.wino_twostage_output_kernel_ptr()
     wino.launch_kernel_info(ki, param)
     torch.cuda.synchronize()

@@ -164,7 +164,7 @@ def test_dropin_slots_are_the_expected_kernels(wino, cuda, with_pin):
     if with_pin:
         # even H, W and a transform_pin: the two-stage route
         assert ki.slot(1)["kernel"] == L.wino_dropin_filter_u2_kernel_ptr()
-        assert ki.slot(3)["kernel"] == L.wino_twostage_gemm_kernel_ptr()
+        assert ki.slot(3)["kernel"] == L.wino_twostage_gemm_kernel_ptr_for(16)
         assert ki.slot(4)["kernel"] == L.wino_twostage_output_kernel_ptr()
     else:
         # the fused kernel reads the NCHW input; slots 2 and 4 are the same no-op

@@ -61,6 +61,9 @@ def _check(oracle_mod, y, y64, what):
     (1, 32, 30, 2, 16),     # tall and narrow
     (5, 16, 40, 40, 48),    # several tile blocks, last one partial
     (1, 80, 8, 8, 384),     # C = 80 (5 K-steps: a partial stage), three k-blocks
+    (2, 256, 10, 6, 64),    # C = 256: the largest U the tap-pair kernel keeps resident
+    (2, 272, 6, 8, 48),     # C = 272: the streamed-U kernel
+    (1, 512, 5, 4, 272),    # C = 512, K = 272 on the streamed-U kernel
 ])
 def test_twostage_shapes(wino, cuda, oracle_mod, shape):
     n, c, h, w, k = shape
@@ -79,12 +82,14 @@ def test_twostage_vs_reference_golden(wino, cuda, oracle_mod, path):
     assert oracle_mod.rel_l2(y, y_ref.astype(np.float64)) <= REL_L2
 
 
-def test_twostage_matches_unfused_comparator(wino, cuda, oracle_mod):
+@pytest.mark.parametrize("c", [64, 288])
+def test_twostage_matches_unfused_comparator(wino, cuda, oracle_mod, c):
     """Same operands (V formed with the same fp16 operations), the same
     K-step accumulation order and the same rounding points as the unfused
-    comparator: the outputs are bit-identical."""
+    comparator: the outputs are bit-identical, on the tap-pair kernel (C = 64)
+    and on the streamed-U kernel (C = 288)."""
     import torch
-    n, c, h, w, k = 4, 64, 14, 14, 128
+    n, h, w, k = 4, 14, 14, 128
     x16, w16 = oracle_mod.make_inputs(n, c, h, w, k, seed=9, x_dist="relu_normal")
     x, wt = _t(x16, cuda), _t(w16, cuda)
     u2 = wino.filter_transform_unfused(wt)
@@ -144,7 +149,7 @@ def test_dropin_two_stage_route(wino, cuda, oracle_mod, shape):
     rc, ki = wino.get_kernel_info(pr, param)
     assert rc == 0
     L = wino.lib()
-    assert ki.slot(3)["kernel"] == L.wino_twostage_gemm_kernel_ptr()
+    assert ki.slot(3)["kernel"] == L.wino_twostage_gemm_kernel_ptr_for(c)
     assert ki.slot(4)["kernel"] == L.wino_twostage_output_kernel_ptr()
     y2 = wino.dropin_conv2d(xt, wtt, ws=ws)
     y3 = wino.conv2d_twostage(xt, wino.filter_transform_unfused(wtt), k)
