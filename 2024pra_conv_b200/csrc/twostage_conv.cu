@@ -45,8 +45,9 @@
 // both halves) and keeps its 128 output channels of U for both taps and all
 // C resident in shared memory (128 KB, reloaded only when the pair's tap
 // pair or k-block changes), so the only L2 traffic of the main loop is the
-// window words.  Work units are dealt to the clusters in contiguous runs of
-// one (tap pair, k pair) each, weighted by the window words of the pair.
+// window words.  Each (tap pair, k pair) has its own clusters, in number
+// proportional to the pair's window words, which take its tile blocks
+// round-robin (make_sched below).
 //
 // twostage_stream_kernel (any C): one CTA per SM, a unit is one tap x 128
 // tiles x 256 output channels (two M = 128 MMAs per K-step sharing the tile
@@ -257,34 +258,72 @@ __device__ __forceinline__ PairSigns pair_signs(int q) {
   return s;
 }
 
-// Units: u = combo * nTB + tb, combo = q * nKP + kp.  Cluster g of G takes
-// the units whose weighted start position falls in its share.
-struct Range {
-  long long u0, u1;
+// Units: u = combo * nTB + tb, combo = q * nKP + kp.  With at least as many
+// clusters G as combos, each combo gets a fixed set of n_c >= 1 clusters (one
+// each, then the rest in proportion to the pair weights, leftovers by
+// largest remainder) and the j-th of them takes the tile blocks j, j + n_c,
+// j + 2 n_c, ...: every combo then sweeps the tile blocks at about the same
+// pace, so the 8 tap pairs of a tile block read its input rows from L2
+// within a short window, and each cluster keeps one U resident throughout.
+// With fewer clusters than combos, cluster g takes the combos g, g + G, ...
+// whole, one after another.
+struct Sched {
+  int combo;   // the cluster's combo (G >= combos), else its first combo
+  int j, s;    // first tile block and tile-block stride (G >= combos)
+  int G;
+  long long cnt;  // units of this cluster
 };
 
-__device__ __forceinline__ long long first_unit(const Geo& g, long long T) {
-  long long wc = 0;
+__device__ __forceinline__ Sched make_sched(const Geo& g, int cl, int G) {
+  Sched sc;
+  sc.G = G;
   const int ncombo = NPAIR * g.nKP;
-  for (int c = 0; c < ncombo; ++c) {
-    const int w = pair_weight(c / g.nKP);
-    const long long last = wc + (long long)(g.nTB - 1) * w;
-    if (T <= last) {
-      const long long d = T - wc;
-      const long long tb = d <= 0 ? 0 : (d + w - 1) / w;
-      return (long long)c * g.nTB + tb;
-    }
-    wc += (long long)g.nTB * w;
+  if (G < ncombo) {
+    const int mc = cl < ncombo ? (ncombo - cl + G - 1) / G : 0;
+    sc.combo = cl;
+    sc.j = 0;
+    sc.s = 1;
+    sc.cnt = (long long)mc * g.nTB;
+    return sc;
   }
-  return (long long)ncombo * g.nTB;
+  const long long wsum = (long long)g.nKP * (4 * pair_weight(0) + 4 * pair_weight(4));
+  const long long extra = G - ncombo;  // clusters after one per combo
+  // per weight class: floor share and remainder
+  const long long fa = extra * pair_weight(0) / wsum, ra = extra * pair_weight(0) % wsum;
+  const long long fb = extra * pair_weight(4) / wsum, rb = extra * pair_weight(4) % wsum;
+  const long long half = 4LL * g.nKP;  // combos per class
+  long long left = extra - half * (fa + fb);
+  // leftovers: the class with the larger remainder first, in combo order
+  const bool b_first = rb >= ra;
+  long long start = 0;
+  sc.combo = 0;
+  sc.s = 1;
+  for (int c = 0; c < ncombo; ++c) {
+    const bool isb = (c / g.nKP) >= 4;
+    const long long rank_in = isb ? c - half : c;   // index within its class
+    long long n = 1 + (isb ? fb : fa);
+    const long long first_class_left = left < half ? left : half;
+    const long long second_class_left = left - first_class_left;
+    if (isb == b_first ? rank_in < first_class_left : rank_in < second_class_left) ++n;
+    if (cl < start + n) {
+      sc.combo = c;
+      sc.j = (int)(cl - start);
+      sc.s = (int)n;
+      break;
+    }
+    start += n;
+  }
+  sc.cnt = sc.j < g.nTB ? (g.nTB - sc.j + sc.s - 1) / sc.s : 0;
+  return sc;
 }
 
-__device__ __forceinline__ Range cluster_range(const Geo& g, int cl, int G) {
-  const long long W = (long long)g.nTB * g.nKP * (4 * 2 + 4 * 3);
-  Range r;
-  r.u0 = first_unit(g, ((long long)cl * W + G - 1) / G);
-  r.u1 = first_unit(g, ((long long)(cl + 1) * W + G - 1) / G);
-  return r;
+// The i-th unit of a cluster.
+__device__ __forceinline__ long long sched_unit(const Geo& g, const Sched& sc, long long i) {
+  if (sc.G < NPAIR * g.nKP) {
+    const long long m = i / g.nTB;
+    return (sc.combo + m * sc.G) * g.nTB + (i - m * g.nTB);
+  }
+  return (long long)sc.combo * g.nTB + sc.j + i * sc.s;
 }
 
 struct Unit {
@@ -335,7 +374,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tp::NTHREAD, 1)
   const int warp = warp_id(), lane = lane_id();
   const int rank = (int)cluster_ctarank();
   uint32_t* err = &g_twostage_err;
-  const Range rg = cluster_range(g, (int)cluster_id_x(), (int)cluster_count_x());
+  const Sched sc = make_sched(g, (int)cluster_id_x(), (int)cluster_count_x());
   const int nst = (g.CS + SK - 1) / SK;
 
   if (threadIdx.x == 0) {
@@ -378,7 +417,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tp::NTHREAD, 1)
       long long cur = -1;
       uint32_t it = 0, ui = 0, nload = 0;
       bool ok = true;
-      for (long long u = rg.u0; ok && u < rg.u1 && !*abort_flag; ++u, ++ui) {
+      for (long long i = 0; ok && i < sc.cnt && !*abort_flag; ++i, ++ui) {
+        const long long u = sched_unit(g, sc, i);
         const long long combo = u / g.nTB;
         if (combo != cur) {
           if (cur >= 0) {
@@ -450,8 +490,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tp::NTHREAD, 1)
     const int quarter = warp & 3;
     __half* m16 = static_cast<__half*>(p.mid_result);
     uint32_t ui = 0;
-    for (long long u = rg.u0; u < rg.u1; ++u, ++ui) {
-      const Unit un = unit_of(g, u);
+    for (long long i = 0; i < sc.cnt; ++i, ++ui) {
+      const Unit un = unit_of(g, sched_unit(g, sc, i));
       const int ab = ui & 1;
       if (!mbar_wait_warp(&sh.accfull[ab], (ui >> 1) & 1, abort_flag, err, ERR_WAIT_ACCUM, SLEEP_NS)) break;
       tc_fence_after();
@@ -499,12 +539,12 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tp::NTHREAD, 1)
     const int tl = (pw & 1) * 32 + lane, hh = (pw >> 1) & 1, kq = pw >> 2;
     const uint8_t* xb = static_cast<const uint8_t*>(p.transform_pin);
     // the load cursor (lu, lj) runs one stage ahead of the consume cursor (cu, cj)
-    long long lu = rg.u0, cu = rg.u0;
+    long long lu = 0, cu = 0;   // unit indices of this cluster
     int lj = 0, cj = 0;
     ProdLoad pl;
     uint4 wa[6], wb[6];
     auto issue = [&](uint4 (&w)[6]) {
-      if (lj == 0) pl = prod_load(g, xb, unit_of(g, lu), rank, tl, hh);
+      if (lj == 0) pl = prod_load(g, xb, unit_of(g, sched_unit(g, sc, lu)), rank, tl, hh);
       const int cs = lj * SK + kq;
       if (pl.live && cs < g.CS) {
         const uint8_t* rec = pl.xn + (size_t)cs * g.cbs;
@@ -520,7 +560,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tp::NTHREAD, 1)
       if (it >= NSTV &&
           !mbar_wait_warp(&sh.vempty[st], (it / NSTV - 1) & 1, abort_flag, err, ERR_WAIT_EMPTY, SLEEP_NS))
         return false;
-      const Unit un = unit_of(g, cu);
+      const Unit un = unit_of(g, sched_unit(g, sc, cu));
       const bool live = (long long)un.tb * 128 + rank * VT + tl < g.NT;
       if (live && cj * SK + kq < g.CS) {
         const PairSigns sg = pair_signs(un.q);
@@ -546,12 +586,12 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tp::NTHREAD, 1)
       if (++cj == nst) { cj = 0; ++cu; }
       return true;
     };
-    if (lu < rg.u1) issue(wa);
-    while (cu < rg.u1 && !*abort_flag) {
-      if (lu < rg.u1) issue(wb);
+    if (lu < sc.cnt) issue(wa);
+    while (cu < sc.cnt && !*abort_flag) {
+      if (lu < sc.cnt) issue(wb);
       if (!consume(wa)) break;
-      if (cu >= rg.u1 || *abort_flag) break;
-      if (lu < rg.u1) issue(wa);
+      if (cu >= sc.cnt || *abort_flag) break;
+      if (lu < sc.cnt) issue(wa);
       if (!consume(wb)) break;
     }
   }
