@@ -717,6 +717,12 @@ def run_only(args):
         ws = wino.UnfusedWorkspace(n, c, h, w, k, dev)
         for _ in range(args.steps):
             wino.conv2d_unfused(x, u2, k, ws=ws)
+    elif args.only == "twostage":
+        u2 = wino.filter_transform_unfused(wt)
+        ws = wino._aligned_ws(wino.twostage_workspace_bytes(n, c, h, w, k), dev)
+        y = torch.empty((n, k, h, w), dtype=torch.float16, device=dev)
+        for _ in range(args.steps):
+            wino.conv2d_twostage(x, u2, k, out=y, workspace=ws)
     elif args.only == "f4":
         conv = wino.ConvF4(wt, n, h, w, hilo=True)
         for _ in range(args.steps):
@@ -740,7 +746,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the layer-set / variants / cost-model legs")
-    ap.add_argument("--only", choices=["fused", "unfused", "dropin", "f4"],
+    ap.add_argument("--only", choices=["fused", "unfused", "dropin", "f4", "twostage"],
                     help="only launch this path (profiler captures)")
     ap.add_argument("--n", type=int, default=0, help="batch size for --only")
     args = ap.parse_args()
