@@ -70,6 +70,16 @@ __device__ __forceinline__ void mbar_arrive_remote(uint32_t cluster_addr) {
                : "memory");
 }
 
+// Arrive on an mbarrier of the cluster (own CTA or peer, address from mapa)
+// with CTA-scope release: it orders this thread's shared-memory and tensor
+// memory accesses before the arrival without waiting for its outstanding
+// global loads and stores, which a cluster-scope release would.  Used where
+// the data handed over is in shared memory (operands for the pair MMA, made
+// visible to it by fence.proxy.async) or in TMEM (drained accumulators).
+__device__ __forceinline__ void mbar_arrive_peer(uint32_t cluster_addr) {
+  asm volatile("mbarrier.arrive.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(

@@ -445,7 +445,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tp::NTHREAD, 1)
           }
           if (!mbar_wait(&sh.utx, nload & 1, abort_flag, err, ERR_WAIT_FULL)) break;
           if (rank == 1) {
-            mbar_arrive_remote(lead_ufull);
+            mbar_arrive_peer(lead_ufull);
           } else if (!mbar_wait_cluster(&sh.ufull, nload & 1, abort_flag, err, ERR_WAIT_FULL)) {
             break;
           }
@@ -530,7 +530,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tp::NTHREAD, 1)
       }
       tc_fence_before();
       __syncwarp();
-      if (lane == 0) mbar_arrive_remote(lead_accempty + ab * 8);
+      if (lane == 0) mbar_arrive_peer(lead_accempty + ab * 8);
     }
   } else {
     // ---- V producers: thread = (tile tl of this CTA's 64, channel half hh,
@@ -581,7 +581,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tp::NTHREAD, 1)
       }
       fence_proxy_async_shared();
       __syncwarp();
-      if (lane == 0) mbar_arrive_remote(lead_vfull + st * 8);
+      if (lane == 0) mbar_arrive_peer(lead_vfull + st * 8);
       ++it;
       if (++cj == nst) { cj = 0; ++cu; }
       return true;
