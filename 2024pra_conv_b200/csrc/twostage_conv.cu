@@ -258,6 +258,30 @@ __device__ __forceinline__ PairSigns pair_signs(int q) {
   return s;
 }
 
+// pair_signs(q) as a table (a0, a1, c0, c1, b0, b1), read by the producers
+// with a warp-uniform index.
+#define WINO_P 0x3c003c00u
+#define WINO_M 0xbc00bc00u
+__constant__ uint32_t c_pair_signs[NPAIR][6] = {
+    {WINO_P, WINO_M, 0, 0, 0, 0},                     // a = 0: d0 - d2
+    {WINO_P, WINO_P, 0, 0, 0, 0},                     // a = 1: d1 + d2
+    {WINO_M, WINO_P, 0, 0, 0, 0},                     // a = 2: d2 - d1
+    {WINO_P, WINO_M, 0, 0, 0, 0},                     // a = 3: d1 - d3
+    {WINO_P, WINO_M, WINO_P, WINO_P, WINO_P, WINO_M}, // rows 0,1,2; b = 0
+    {WINO_M, WINO_P, WINO_P, WINO_M, WINO_P, WINO_M}, // rows 3,2,1; b = 0
+    {WINO_P, WINO_M, WINO_P, WINO_P, WINO_P, WINO_M}, // rows 0,1,2; b = 3
+    {WINO_M, WINO_P, WINO_P, WINO_M, WINO_P, WINO_M}, // rows 3,2,1; b = 3
+};
+#undef WINO_P
+#undef WINO_M
+
+__device__ __forceinline__ uint4 hadd4(const uint4& a, const uint4& b) {
+  return make_uint4(hadd2(a.x, b.x), hadd2(a.y, b.y), hadd2(a.z, b.z), hadd2(a.w, b.w));
+}
+__device__ __forceinline__ uint4 hsub4(const uint4& a, const uint4& b) {
+  return make_uint4(hsub2(a.x, b.x), hsub2(a.y, b.y), hsub2(a.z, b.z), hsub2(a.w, b.w));
+}
+
 // Units: u = combo * nTB + tb, combo = q * nKP + kp.  With at least as many
 // clusters G as combos, each combo gets a fixed set of n_c >= 1 clusters (one
 // each, then the rest in proportion to the pair weights, leftovers by
@@ -538,20 +562,46 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tp::NTHREAD, 1)
     const int pw = warp - WARP_P0;
     const int tl = (pw & 1) * 32 + lane, hh = (pw >> 1) & 1, kq = pw >> 2;
     const uint8_t* xb = static_cast<const uint8_t*>(p.transform_pin);
-    // the load cursor (lu, lj) runs one stage ahead of the consume cursor (cu, cj)
+    // The load cursor (lu, lj) runs one stage ahead of the consume cursor
+    // (cu, cj).  Everything a unit needs is worked out when the load cursor
+    // enters it: the window offsets and record pointer for the loads, and
+    // for the consume side the tap pair and whether the tile exists, kept per
+    // unit parity (4 bits each) since the two cursors are at most one unit
+    // apart.
     long long lu = 0, cu = 0;   // unit indices of this cluster
     int lj = 0, cj = 0;
-    ProdLoad pl;
+    uint32_t info = 0;
+    const uint8_t* rec = xb;
+    uint32_t off[6];
+    int nw = 4;
+    bool llive = false;
+    const size_t step_bytes = (size_t)SK * g.cbs;
     uint4 wa[6], wb[6];
     auto issue = [&](uint4 (&w)[6]) {
-      if (lj == 0) pl = prod_load(g, xb, unit_of(g, sched_unit(g, sc, lu)), rank, tl, hh);
-      const int cs = lj * SK + kq;
-      if (pl.live && cs < g.CS) {
-        const uint8_t* rec = pl.xn + (size_t)cs * g.cbs;
+      if (lj == 0) {
+        const Unit un = unit_of(g, sched_unit(g, sc, lu));
+        const ProdLoad pl = prod_load(g, xb, un, rank, tl, hh);
+#pragma unroll
+        for (int i = 0; i < 6; ++i) off[i] = pl.off[i];
+        nw = pl.nw;
+        llive = pl.live;
+        rec = pl.xn + (size_t)kq * g.cbs;
+        const uint32_t sh4 = (uint32_t)(lu & 1) * 4;
+        info = (info & ~(15u << sh4)) | ((uint32_t)(un.q | (pl.live ? 8 : 0)) << sh4);
+      }
+      if (llive && lj * SK + kq < g.CS) {
 #pragma unroll
         for (int i = 0; i < 6; ++i)
-          if (i < pl.nw) w[i] = __ldg(reinterpret_cast<const uint4*>(rec + pl.off[i]));
+          if (i < nw) w[i] = __ldg(reinterpret_cast<const uint4*>(rec + off[i]));
+        // the next stage's words of this unit into L1, so that its register
+        // loads (issued a stage from now) find them on the SM
+        if ((lj + 1) * SK + kq < g.CS) {
+#pragma unroll
+          for (int i = 0; i < 6; ++i)
+            if (i < nw) prefetch_l1(rec + step_bytes + off[i]);
+        }
       }
+      rec += step_bytes;
       if (++lj == nst) { lj = 0; ++lu; }
     };
     uint32_t it = 0;
@@ -560,19 +610,19 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tp::NTHREAD, 1)
       if (it >= NSTV &&
           !mbar_wait_warp(&sh.vempty[st], (it / NSTV - 1) & 1, abort_flag, err, ERR_WAIT_EMPTY, SLEEP_NS))
         return false;
-      const Unit un = unit_of(g, sched_unit(g, sc, cu));
-      const bool live = (long long)un.tb * 128 + rank * VT + tl < g.NT;
-      if (live && cj * SK + kq < g.CS) {
-        const PairSigns sg = pair_signs(un.q);
+      const uint32_t inf = (info >> ((uint32_t)(cu & 1) * 4)) & 15u;
+      const int q = (int)(inf & 7u);
+      if ((inf & 8u) && cj * SK + kq < g.CS) {
+        const uint32_t* sg = c_pair_signs[q];
         uint4 v0, v1;
-        if (un.q < 4) {
-          const uint4 e1 = bt_op4(sg.a0, sg.a1, w[0], w[1]);
-          const uint4 e2 = bt_op4(sg.a0, sg.a1, w[2], w[3]);
-          v0 = bt_op4(0x3c003c00u, 0x3c003c00u, e1, e2);   // b = 1: d1 + d2
-          v1 = bt_op4(0xbc00bc00u, 0x3c003c00u, e1, e2);   // b = 2: d2 - d1
+        if (q < 4) {
+          const uint4 e1 = bt_op4(sg[0], sg[1], w[0], w[1]);
+          const uint4 e2 = bt_op4(sg[0], sg[1], w[2], w[3]);
+          v0 = hadd4(e1, e2);   // b = 1: d1 + d2
+          v1 = hsub4(e2, e1);   // b = 2: d2 - d1
         } else {
-          v0 = bt_op4(sg.b0, sg.b1, bt_op4(sg.a0, sg.a1, w[0], w[2]), bt_op4(sg.a0, sg.a1, w[3], w[5]));
-          v1 = bt_op4(sg.b0, sg.b1, bt_op4(sg.c0, sg.c1, w[1], w[2]), bt_op4(sg.c0, sg.c1, w[4], w[5]));
+          v0 = bt_op4(sg[4], sg[5], bt_op4(sg[0], sg[1], w[0], w[2]), bt_op4(sg[0], sg[1], w[3], w[5]));
+          v1 = bt_op4(sg[4], sg[5], bt_op4(sg[2], sg[3], w[1], w[2]), bt_op4(sg[2], sg[3], w[4], w[5]));
         }
         uint8_t* dst = smem + U_BYTES + st * V_STAGE + (kq * 2) * V_TAP + (tl >> 3) * 256 + hh * 128 +
                        (tl & 7) * 16;
@@ -870,59 +920,90 @@ __global__ void __launch_bounds__(tsk::NTHREAD, 1) twostage_stream_kernel(Kernel
 // =============================================================================
 // Output transform
 // =============================================================================
-// CTA = (tile block tb, 8 output channels); thread = (channel kl, 4 tiles
-// g4 .. g4+3 of the block): 16 taps x one 8-byte word of the blocked M (a
-// warp reads 256 contiguous bytes per tap), Y tile = A^T m A in fp32, one
-// fp16 rounding.  grid (tile blocks, ceil(K/8)).
-constexpr int OT_TILES = 4;
+// CTA = (tile block tb, 8 output channels).  The CTA's 16 taps x 8 channels
+// of the blocked M (16 contiguous runs of 8 * ntb fp16) come in by bulk
+// copy, so the bytes in flight do not depend on registers; thread =
+// (channel kl, 4 tiles g4 .. g4+3 of the block) then reads its 16 taps from
+// shared memory (a warp's 8-byte reads are contiguous), accumulates
+// z = A^T m in fp32 tap by tap in the order of the comparator's output
+// transform (so the result is bit-identical to it), forms y = z A and
+// stores it with one fp16 rounding.  grid (tile blocks, K/8); K is a
+// multiple of 16 and mid_result 16-byte aligned, so every copy starts on a
+// 16-byte boundary and moves a multiple of 16 bytes.
+namespace ot {
+constexpr int KG = 8;                         // output channels per CTA
+constexpr int TT = 4;                         // tiles per thread
+constexpr int SMEM_BYTES = 16 * KG * 128 * 2 + 128;
+}
 
 __global__ void __launch_bounds__(256) twostage_output_kernel(KernelParam p) {
   using namespace ts;
+  extern __shared__ __align__(128) uint8_t osm[];
+  __shared__ uint64_t full;
   const int K = p.k, P = p.Oh, Q = p.Ow;
   const int TP = (P + 1) >> 1, TQ = (Q + 1) >> 1;
   const long long NT = (long long)p.n * TP * TQ;
   const int tb = blockIdx.x;
-  const int k = blockIdx.y * 8 + (threadIdx.x >> 5);
-  const int g4 = (threadIdx.x & 31) * OT_TILES;
-  if (k >= K) return;
+  const int k0 = blockIdx.y * ot::KG;
   const long long rem = NT - (long long)tb * 128;
   const int ntb = rem < 128 ? (int)rem : 128;
-  if (g4 >= ntb) return;
+  const uint32_t run = (uint32_t)(ot::KG * ntb * 2);   // bytes of one tap's KG rows
   const __half* m16 = static_cast<const __half*>(p.mid_result);
-  float m[16][OT_TILES];
-  if (ntb == 128) {
-#pragma unroll
-    for (int t = 0; t < 16; ++t) {
-      const uint2 w = *reinterpret_cast<const uint2*>(m16 + m_offset(tb, t, k, g4, K, NT));
-      const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&w.x));
-      const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&w.y));
-      m[t][0] = a.x; m[t][1] = a.y; m[t][2] = b.x; m[t][3] = b.y;
+  const __half* ms = reinterpret_cast<const __half*>(osm);   // [t][kl][ntb]
+  if (threadIdx.x == 0) {
+    mbar_init(&full, 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    if (threadIdx.x == 0) mbar_arrive_expect_tx(&full, 16 * run);
+    __syncwarp();
+    if (threadIdx.x < 16) {
+      const int t = threadIdx.x;
+      bulk_g2s(osm + t * run, m16 + m_offset(tb, t, k0, 0, K, NT), run, &full);
     }
-  } else {
+  }
+  const int kl = threadIdx.x >> 5, g4 = (threadIdx.x & 31) * ot::TT;
+  const int k = k0 + kl;
+  // the copies complete within microseconds; a wait past the bound leaves
+  // the error word set and the output unwritten
+  if (!mbar_wait(&full, 0, nullptr, &g_twostage_err, ERR_WAIT_FULL)) return;
+  if (g4 >= ntb) return;
+  // z[r][b] = sum_a At[r][a] m[4a+b], accumulated in tap order a = 0..3
+  float z[ot::TT][2][4];
 #pragma unroll
-    for (int t = 0; t < 16; ++t) {
-      const __half* src = m16 + m_offset(tb, t, k, g4, K, NT);
+  for (int t = 0; t < 16; ++t) {
+    const int a = t >> 2, b = t & 3;
+    const __half* src = ms + (size_t)t * (run / 2) + kl * ntb + g4;
+    float v[ot::TT];
+    if (ntb == 128) {
+      const uint2 w = *reinterpret_cast<const uint2*>(src);
+      const float2 f0 = __half22float2(*reinterpret_cast<const __half2*>(&w.x));
+      const float2 f1 = __half22float2(*reinterpret_cast<const __half2*>(&w.y));
+      v[0] = f0.x; v[1] = f0.y; v[2] = f1.x; v[3] = f1.y;
+    } else {
 #pragma unroll
-      for (int i = 0; i < OT_TILES; ++i) m[t][i] = g4 + i < ntb ? __half2float(src[i]) : 0.f;
+      for (int i = 0; i < ot::TT; ++i) v[i] = g4 + i < ntb ? __half2float(src[i]) : 0.f;
+    }
+#pragma unroll
+    for (int i = 0; i < ot::TT; ++i) {
+      if (a == 0) z[i][0][b] = v[i];
+      if (a == 1) { z[i][0][b] = z[i][0][b] + v[i]; z[i][1][b] = v[i]; }
+      if (a == 2) { z[i][0][b] = z[i][0][b] + v[i]; z[i][1][b] = z[i][1][b] - v[i]; }
+      if (a == 3) z[i][1][b] = z[i][1][b] - v[i];
     }
   }
   const long long per_img = (long long)TP * TQ;
   const bool pair_ok = (Q & 1) == 0 && (reinterpret_cast<uintptr_t>(p.pout) & 3) == 0;
   __half* out = static_cast<__half*>(p.pout);
 #pragma unroll
-  for (int i = 0; i < OT_TILES; ++i) {
+  for (int i = 0; i < ot::TT; ++i) {
     if (g4 + i >= ntb) break;
-    float z[2][4];
-#pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      z[0][b] = m[b][i] + m[4 + b][i] + m[8 + b][i];
-      z[1][b] = m[4 + b][i] - m[8 + b][i] - m[12 + b][i];
-    }
     float y[4];
 #pragma unroll
     for (int r = 0; r < 2; ++r) {
-      y[2 * r + 0] = z[r][0] + z[r][1] + z[r][2];
-      y[2 * r + 1] = z[r][1] - z[r][2] - z[r][3];
+      y[2 * r + 0] = z[i][r][0] + z[i][r][1] + z[i][r][2];
+      y[2 * r + 1] = z[i][r][1] - z[i][r][2] - z[i][r][3];
     }
     const long long tile = (long long)tb * 128 + g4 + i;
     const int n = (int)(tile / per_img);
@@ -964,7 +1045,12 @@ void* wino_twostage_output_kernel_ptr() { return (void*)twostage_output_kernel; 
 int wino_twostage_threads_for(int c) { return use_pair(c) ? tp::NTHREAD : tsk::NTHREAD; }
 int wino_twostage_smem_bytes_for(int c) { return use_pair(c) ? tp::SMEM_BYTES : tsk::SMEM_BYTES; }
 
+int wino_twostage_output_smem_bytes() { return ot::SMEM_BYTES; }
+
 int wino_twostage_prepare() {
+  if (cudaFuncSetAttribute(twostage_output_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           ot::SMEM_BYTES) != cudaSuccess)
+    return 1;
   if (cudaFuncSetAttribute(twostage_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            tsk::SMEM_BYTES) != cudaSuccess)
     return 1;
@@ -1001,7 +1087,7 @@ unsigned wino_twostage_gemm_grid(int n, int c, int h, int w, int k, int sms) {
 
 void wino_twostage_output_grid(int n, int h, int w, int k, unsigned* gx, unsigned* gy) {
   *gx = (unsigned)((wino_twostage_tiles(n, h, w) + 127) / 128);
-  *gy = (unsigned)((k + 7) / 8);
+  *gy = (unsigned)((k + ot::KG - 1) / ot::KG);
 }
 
 uint32_t wino_twostage_error_read_clear() {

@@ -88,6 +88,7 @@ int wino_twostage_prepare();
 size_t wino_twostage_m_bytes(int n, int h, int w, int k);
 unsigned wino_twostage_gemm_grid(int n, int c, int h, int w, int k, int sms);
 void wino_twostage_output_grid(int n, int h, int w, int k, unsigned* gx, unsigned* gy);
+int wino_twostage_output_smem_bytes();
 uint32_t wino_twostage_error_read_clear();
 }
 
@@ -275,7 +276,8 @@ int getkernelInfo(problem_t* problem, kernelInfo_t* kernelInfo, void* param) {
              wino_twostage_gemm_kernel_ptr_for(c));
     unsigned ox, oy;
     wino_twostage_output_grid((int)pr.n, (int)pr.h, (int)pr.w, (int)pr.k, &ox, &oy);
-    set_slot(kernelInfo, 4, ox, oy, 1, 256, 1, 1, 0, wino_twostage_output_kernel_ptr());
+    set_slot(kernelInfo, 4, ox, oy, 1, 256, 1, 1, (unsigned)wino_twostage_output_smem_bytes(),
+             wino_twostage_output_kernel_ptr());
     return WINO_OK;
   }
   set_slot(kernelInfo, 1, (unsigned)((kc + 255) / 256), 1, 1, 256, 1, 1, 0,
@@ -399,7 +401,8 @@ extern "C" int wino_twostage_stage(int stage, const void* x, const void* ucache2
                : WINO_ECUDA;
   unsigned ox, oy;
   wino_twostage_output_grid(n, h, w, k, &ox, &oy);
-  return cudaLaunchKernel(wino_twostage_output_kernel_ptr(), dim3(ox, oy), dim3(256), args, 0, s) ==
+  return cudaLaunchKernel(wino_twostage_output_kernel_ptr(), dim3(ox, oy), dim3(256), args,
+                          (size_t)wino_twostage_output_smem_bytes(), s) ==
                  cudaSuccess
              ? WINO_OK
              : WINO_ECUDA;
