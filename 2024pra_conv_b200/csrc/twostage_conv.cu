@@ -142,6 +142,86 @@ __device__ __forceinline__ void tile_decode(const Geo& g, long long tile, int& n
 }  // namespace ts
 
 // =============================================================================
+// Row-transformed input (the tap-pair kernel's pre-pass)
+// =============================================================================
+// XR: per (image, 16-channel block) the rows rho = 4 ty + a, ty < ceil(H/2),
+// a < 4, each row in XB's record format ([parity][channel half][entry][8
+// channels], par 0 entry e = column 2e, par 1 entry e = column 2e - 1): row
+// (ty, a) holds, per column x in [-1, 2 ceil(W/2)], the tap-row combination
+// of the tile row's window,
+//   R_a(ty, x) = s0 * X(2ty - 1 + i0, x) + s1 * X(2ty - 1 + i1, x)
+// ((i0, i1, s0, s1) = B^T row a), zero rows / columns outside the image, each
+// rounded once to fp16: exactly the first (row) step of B^T d B in the fused
+// kernel's producers, so V formed from XR by the column step is bit for bit
+// the same.  Size N * C/16 * 4 ceil(H/2) * 64 (ceil(W/2) + 1) bytes, about
+// twice the input.  One thread per (row, entry e): columns 2e and 2e + 1 of
+// 16 channels (par 0 entry e, par 1 entry e + 1; the last entry's thread
+// also writes the zero column -1).
+namespace xr {
+__host__ __device__ __forceinline__ int rows(int H) { return 4 * ((H + 1) >> 1); }
+__host__ __device__ __forceinline__ size_t bytes(int N, int C, int H, int W) {
+  return (size_t)N * (size_t)(C >> 4) * (size_t)rows(H) * (size_t)xb_row_bytes(W);
+}
+}  // namespace xr
+
+__global__ void __launch_bounds__(256) xr_layout_kernel(KernelParam p) {
+  const int C = p.c, H = p.h, W = p.w;
+  const int CB = C >> 4, TP = (H + 1) >> 1, E = xb_entries(W);
+  const uint32_t items = (uint32_t)p.n * CB * TP * 4 * E;
+  const unsigned short* X = static_cast<const unsigned short*>(p.pin);
+  uint4* XR = static_cast<uint4*>(p.transform_pin);
+  const size_t plane = (size_t)H * W;
+  const bool w_even = (W & 1) == 0;
+  for (uint32_t it = blockIdx.x * blockDim.x + threadIdx.x; it < items; it += gridDim.x * blockDim.x) {
+    const uint32_t rec = it / E;                  // ((n * CB + cb) * TP + ty) * 4 + a
+    const int e = (int)(it - rec * E);
+    const int a = (int)(rec & 3);
+    const uint32_t r2 = rec >> 2;
+    const int ty = (int)(r2 % TP);
+    const uint32_t ncb = r2 / TP;
+    const int cb = (int)(ncb % CB), n = (int)(ncb / CB);
+    int i0, i1;
+    uint32_t s0, s1;
+    ts::bt_pick(a, i0, i1, s0, s1);
+    const int x0 = 2 * e;
+    uint32_t r[16];                               // (column x0, column x0 + 1) of channel 16 cb + i
+#pragma unroll
+    for (int i = 0; i < 16; ++i) r[i] = 0u;
+    const unsigned short* base = X + ((size_t)n * C + 16 * cb) * plane;
+    uint32_t v[2][16];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int y = 2 * ty - 1 + (k == 0 ? i0 : i1);
+      const bool rok = y >= 0 && y < H;
+      const bool ok0 = rok && x0 < W, ok1 = rok && x0 + 1 < W;
+      const unsigned short* src = base + (size_t)(rok ? y : 0) * W + x0;
+      if (w_even && ok1) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) v[k][i] = *reinterpret_cast<const uint32_t*>(src + i * plane);
+      } else {
+#pragma unroll
+        for (int i = 0; i < 16; ++i)
+          v[k][i] = (ok0 ? (uint32_t)src[i * plane] : 0u) | ((ok1 ? (uint32_t)src[i * plane + 1] : 0u) << 16);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 16; ++i) r[i] = ts::bt_op(s0, s1, v[0][i], v[1][i]);
+    uint4* out = XR + (size_t)rec * (4 * E);
+#pragma unroll
+    for (int hh = 0; hh < 2; ++hh) {
+      const uint32_t* q = r + 8 * hh;
+      out[hh * E + e] = make_uint4(__byte_perm(q[0], q[1], 0x5410), __byte_perm(q[2], q[3], 0x5410),
+                                   __byte_perm(q[4], q[5], 0x5410), __byte_perm(q[6], q[7], 0x5410));
+      if (e + 1 < E)
+        out[(2 + hh) * E + e + 1] = make_uint4(__byte_perm(q[0], q[1], 0x7632), __byte_perm(q[2], q[3], 0x7632),
+                                               __byte_perm(q[4], q[5], 0x7632), __byte_perm(q[6], q[7], 0x7632));
+      else
+        out[(2 + hh) * E] = make_uint4(0u, 0u, 0u, 0u);
+    }
+  }
+}
+
+// =============================================================================
 // Tap-pair GEMM on CTA pairs (C <= 256)
 // =============================================================================
 namespace tp {
@@ -159,8 +239,8 @@ constexpr int U_TAP = CS_MAX * U_STEP;        // 64 KB
 constexpr int U_BYTES = 2 * U_TAP;
 constexpr int SMEM_BYTES = U_BYTES + NSTV * V_STAGE + 1024;
 // warps 0-3 epilogue (warp w reads TMEM lanes 32 (w % 4) ..), warp 4 lane 0
-// U loads (both CTAs) and MMA issue (rank 0), warps 5-12 V producers
-constexpr int WARP_E0 = 0, NWARP_E = 4, WARP_MMA = 4, WARP_P0 = 5, NWARP_P = 8;
+// U loads (both CTAs) and MMA issue (rank 0), warps 5-20 V producers
+constexpr int WARP_E0 = 0, NWARP_E = 4, WARP_MMA = 4, WARP_P0 = 5, NWARP_P = 16;
 constexpr int NTHREAD = (WARP_P0 + NWARP_P) * 32;
 constexpr int NPAIR = 8;
 constexpr uint16_t BOTH = 3;                  // CTA mask of the pair
@@ -174,8 +254,9 @@ struct Shared {
   int abort_flag;
 };
 
-// Tap pair q: the taps of accumulator slots 0 and 1.
-__device__ __forceinline__ void pair_taps(int q, int& t0, int& t1) {
+// Tap pair q: the taps of accumulator slots 0 and 1.  q < 4: (a, 1) and
+// (a, 2) of tap row a = q; q >= 4: two tap rows (a0, a1) of tap column b.
+__host__ __device__ __forceinline__ void pair_taps(int q, int& t0, int& t1) {
   switch (q) {
     case 0: t0 = 1; t1 = 2; break;     // (0,1) (0,2)
     case 1: t0 = 5; t1 = 6; break;     // (1,1) (1,2)
@@ -187,100 +268,9 @@ __device__ __forceinline__ void pair_taps(int q, int& t0, int& t1) {
     default: t0 = 15; t1 = 11; break;  // (3,3) (2,3)
   }
 }
-// Relative cost of a pair's unit: its window words per tile (4 or 6), halved.
+// Relative cost of a pair's unit (it reads 2 or 4 XR words per tile and
+// K-step; the MMA work is the same).
 __host__ __device__ __forceinline__ int pair_weight(int q) { return q < 4 ? 2 : 3; }
-
-// Window words of a pair.  Four-word pairs (q < 4, tap row a = q, columns
-// 1 and 2): w0 = d(i0,1), w1 = d(i1,1), w2 = d(i0,2), w3 = d(i1,2).  Six-word
-// pairs (rows R0, R1, R2; columns j0, j1 of tap column b): w0..w2 = d(R*,j0),
-// w3..w5 = d(R*,j1); slot 0 combines rows R0 and R2, slot 1 rows R1 and R2.
-struct PairWords {
-  int nw;
-  int r[6], c[6];
-};
-
-__device__ __forceinline__ PairWords pair_words(int q) {
-  PairWords pw;
-  if (q < 4) {
-    int i0, i1;
-    uint32_t s0, s1;
-    bt_pick(q, i0, i1, s0, s1);
-    pw.nw = 4;
-    pw.r[0] = i0; pw.c[0] = 1;
-    pw.r[1] = i1; pw.c[1] = 1;
-    pw.r[2] = i0; pw.c[2] = 2;
-    pw.r[3] = i1; pw.c[3] = 2;
-    pw.r[4] = pw.r[5] = 0;
-    pw.c[4] = pw.c[5] = 0;
-  } else {
-    const bool top = (q & 1) == 0;           // q 4, 6: rows 0, 1, 2; q 5, 7: rows 3, 2, 1
-    const int b = q < 6 ? 0 : 3;
-    int j0, j1;
-    uint32_t s0, s1;
-    bt_pick(b, j0, j1, s0, s1);
-    const int R[3] = {top ? 0 : 3, top ? 1 : 2, top ? 2 : 1};
-    pw.nw = 6;
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-      pw.r[i] = R[i]; pw.c[i] = j0;
-      pw.r[3 + i] = R[i]; pw.c[3 + i] = j1;
-    }
-  }
-  return pw;
-}
-
-// Row signs of the window rows each slot combines, column signs of the pair.
-struct PairSigns {
-  uint32_t a0, a1;   // slot 0: rows (i0, i1) for q < 4, (R0, R2) otherwise
-  uint32_t c0, c1;   // slot 1: (R1, R2) (q >= 4)
-  uint32_t b0, b1;   // columns (q >= 4; q < 4 uses the fixed b = 1, 2 signs)
-};
-
-__device__ __forceinline__ PairSigns pair_signs(int q) {
-  PairSigns s;
-  int i0, i1;
-  if (q < 4) {
-    bt_pick(q, i0, i1, s.a0, s.a1);
-    s.c0 = s.c1 = s.b0 = s.b1 = 0;
-    return s;
-  }
-  int t0, t1;
-  pair_taps(q, t0, t1);
-  // top (rows 0,1,2): slot 0 a = 0 -> rows 0 (R0), 2 (R2); slot 1 a = 1 -> rows 1 (R1), 2 (R2)
-  // bottom (rows 3,2,1): slot 0 a = 3 -> rows 1 (R2), 3 (R0); slot 1 a = 2 -> rows 1 (R2), 2 (R1)
-  uint32_t x0, x1;
-  const bool top = (q & 1) == 0;
-  bt_pick(t0 >> 2, i0, i1, x0, x1);
-  if (top) { s.a0 = x0; s.a1 = x1; } else { s.a0 = x1; s.a1 = x0; }
-  bt_pick(t1 >> 2, i0, i1, x0, x1);
-  if (top) { s.c0 = x0; s.c1 = x1; } else { s.c0 = x1; s.c1 = x0; }
-  bt_pick(t0 & 3, i0, i1, s.b0, s.b1);
-  return s;
-}
-
-// pair_signs(q) as a table (a0, a1, c0, c1, b0, b1), read by the producers
-// with a warp-uniform index.
-#define WINO_P 0x3c003c00u
-#define WINO_M 0xbc00bc00u
-__constant__ uint32_t c_pair_signs[NPAIR][6] = {
-    {WINO_P, WINO_M, 0, 0, 0, 0},                     // a = 0: d0 - d2
-    {WINO_P, WINO_P, 0, 0, 0, 0},                     // a = 1: d1 + d2
-    {WINO_M, WINO_P, 0, 0, 0, 0},                     // a = 2: d2 - d1
-    {WINO_P, WINO_M, 0, 0, 0, 0},                     // a = 3: d1 - d3
-    {WINO_P, WINO_M, WINO_P, WINO_P, WINO_P, WINO_M}, // rows 0,1,2; b = 0
-    {WINO_M, WINO_P, WINO_P, WINO_M, WINO_P, WINO_M}, // rows 3,2,1; b = 0
-    {WINO_P, WINO_M, WINO_P, WINO_P, WINO_P, WINO_M}, // rows 0,1,2; b = 3
-    {WINO_M, WINO_P, WINO_P, WINO_M, WINO_P, WINO_M}, // rows 3,2,1; b = 3
-};
-#undef WINO_P
-#undef WINO_M
-
-__device__ __forceinline__ uint4 hadd4(const uint4& a, const uint4& b) {
-  return make_uint4(hadd2(a.x, b.x), hadd2(a.y, b.y), hadd2(a.z, b.z), hadd2(a.w, b.w));
-}
-__device__ __forceinline__ uint4 hsub4(const uint4& a, const uint4& b) {
-  return make_uint4(hsub2(a.x, b.x), hsub2(a.y, b.y), hsub2(a.z, b.z), hsub2(a.w, b.w));
-}
 
 // Units: u = combo * nTB + tb, combo = q * nKP + kp.  With at least as many
 // clusters G as combos, each combo gets a fixed set of n_c >= 1 clusters (one
@@ -290,12 +280,13 @@ __device__ __forceinline__ uint4 hsub4(const uint4& a, const uint4& b) {
 // pace, so the 8 tap pairs of a tile block read its input rows from L2
 // within a short window, and each cluster keeps one U resident throughout.
 // With fewer clusters than combos, cluster g takes the combos g, g + G, ...
-// whole, one after another.
+// whole, one after another.  Unit indices fit 32 bits (the host bounds the
+// tile count).
 struct Sched {
   int combo;   // the cluster's combo (G >= combos), else its first combo
   int j, s;    // first tile block and tile-block stride (G >= combos)
   int G;
-  long long cnt;  // units of this cluster
+  int cnt;     // units of this cluster
 };
 
 __device__ __forceinline__ Sched make_sched(const Geo& g, int cl, int G) {
@@ -307,32 +298,33 @@ __device__ __forceinline__ Sched make_sched(const Geo& g, int cl, int G) {
     sc.combo = cl;
     sc.j = 0;
     sc.s = 1;
-    sc.cnt = (long long)mc * g.nTB;
+    sc.cnt = mc * g.nTB;
     return sc;
   }
-  const long long wsum = (long long)g.nKP * (4 * pair_weight(0) + 4 * pair_weight(4));
-  const long long extra = G - ncombo;  // clusters after one per combo
+  const int wsum = g.nKP * (4 * pair_weight(0) + 4 * pair_weight(4));
+  const int extra = G - ncombo;  // clusters after one per combo
   // per weight class: floor share and remainder
-  const long long fa = extra * pair_weight(0) / wsum, ra = extra * pair_weight(0) % wsum;
-  const long long fb = extra * pair_weight(4) / wsum, rb = extra * pair_weight(4) % wsum;
-  const long long half = 4LL * g.nKP;  // combos per class
-  long long left = extra - half * (fa + fb);
+  const int fa = extra * pair_weight(0) / wsum, ra = extra * pair_weight(0) % wsum;
+  const int fb = extra * pair_weight(4) / wsum, rb = extra * pair_weight(4) % wsum;
+  const int half = 4 * g.nKP;    // combos per class
+  const int left = extra - half * (fa + fb);
   // leftovers: the class with the larger remainder first, in combo order
   const bool b_first = rb >= ra;
-  long long start = 0;
+  const int first_class_left = left < half ? left : half;
+  const int second_class_left = left - first_class_left;
+  int start = 0;
   sc.combo = 0;
+  sc.j = 0;
   sc.s = 1;
   for (int c = 0; c < ncombo; ++c) {
     const bool isb = (c / g.nKP) >= 4;
-    const long long rank_in = isb ? c - half : c;   // index within its class
-    long long n = 1 + (isb ? fb : fa);
-    const long long first_class_left = left < half ? left : half;
-    const long long second_class_left = left - first_class_left;
+    const int rank_in = isb ? c - half : c;   // index within its class
+    int n = 1 + (isb ? fb : fa);
     if (isb == b_first ? rank_in < first_class_left : rank_in < second_class_left) ++n;
     if (cl < start + n) {
       sc.combo = c;
-      sc.j = (int)(cl - start);
-      sc.s = (int)n;
+      sc.j = cl - start;
+      sc.s = n;
       break;
     }
     start += n;
@@ -341,49 +333,80 @@ __device__ __forceinline__ Sched make_sched(const Geo& g, int cl, int G) {
   return sc;
 }
 
-// The i-th unit of a cluster.
-__device__ __forceinline__ long long sched_unit(const Geo& g, const Sched& sc, long long i) {
-  if (sc.G < NPAIR * g.nKP) {
-    const long long m = i / g.nTB;
-    return (sc.combo + m * sc.G) * g.nTB + (i - m * g.nTB);
-  }
-  return (long long)sc.combo * g.nTB + sc.j + i * sc.s;
-}
-
 struct Unit {
   int q, kp, tb;
 };
-__device__ __forceinline__ Unit unit_of(const Geo& g, long long u) {
+
+// The i-th unit of a cluster.
+__device__ __forceinline__ Unit sched_unit(const Geo& g, const Sched& sc, int i) {
+  int combo, tb;
+  if (sc.G < NPAIR * g.nKP) {
+    const int m = i / g.nTB;
+    combo = sc.combo + m * sc.G;
+    tb = i - m * g.nTB;
+  } else {
+    combo = sc.combo;
+    tb = sc.j + i * sc.s;
+  }
   Unit x;
-  const long long combo = u / g.nTB;
-  x.tb = (int)(u - combo * g.nTB);
-  x.q = (int)(combo / g.nKP);
-  x.kp = (int)(combo - (long long)x.q * g.nKP);
+  x.tb = tb;
+  x.q = combo / g.nKP;
+  x.kp = combo - x.q * g.nKP;
   return x;
 }
 
 // Load side of one unit for a producer thread (tile tl of this CTA's half,
-// channel half hh).
+// channel half hh, 8-byte half hw of each 16-byte word): the XR words its
+// taps' column step reads.  q < 4: row (ty, a) at columns 2tx (par 0 entry
+// tx) and 2tx + 1 (par 1 entry tx + 1); q >= 4: rows (ty, a0), (ty, a1) at
+// the two columns of tap column b (b = 0: 2tx - 1, 2tx + 1, par 1 entries
+// tx, tx + 1; b = 3: 2tx, 2tx + 2, par 0 entries tx, tx + 1).
 struct ProdLoad {
-  const uint8_t* xn;   // XB of the tile's image, channel block 0
-  uint32_t off[6];
-  int nw;
-  bool live;
+  const uint8_t* rec;  // XR of the tile's image, channel block 0
+  uint32_t off[4];
+  bool live, four;
 };
 
-__device__ __forceinline__ ProdLoad prod_load(const Geo& g, const uint8_t* xb, const Unit& un, int rank,
-                                              int tl, int hh) {
+__device__ __forceinline__ ProdLoad prod_load(const Geo& g, const uint8_t* xr, const Unit& un, int rank,
+                                              int tl, int hh, int hw) {
   ProdLoad pl;
-  const long long tile = (long long)un.tb * 128 + rank * VT + tl;
-  pl.live = tile < g.NT;
+  const int tile = un.tb * 128 + rank * VT + tl;
+  pl.live = tile < (int)g.NT;
+  pl.four = un.q >= 4;
   int n = 0, ty = 0, tx = 0;
-  if (pl.live) tile_decode(g, tile, n, ty, tx);
-  const PairWords pw = pair_words(un.q);
-  pl.nw = pw.nw;
-#pragma unroll
-  for (int w = 0; w < 6; ++w) pl.off[w] = win_off(g, ty, tx, hh, pw.r[w], pw.c[w]);
-  pl.xn = xb + (size_t)n * g.CS * g.cbs;
+  if (pl.live) {
+    const int per = g.TP * g.TQ;
+    n = tile / per;
+    const int r = tile - n * per;
+    ty = r / g.TQ;
+    tx = r - ty * g.TQ;
+  }
+  int t0, t1;
+  pair_taps(un.q, t0, t1);
+  const uint32_t RB = g.RB, E = (uint32_t)g.E;
+  const uint32_t row0 = (uint32_t)(4 * ty + (t0 >> 2)) * RB, row1 = (uint32_t)(4 * ty + (t1 >> 2)) * RB;
+  const uint32_t hb = (uint32_t)(hh * E) * 16 + (uint32_t)hw * 8;
+  if (!pl.four) {
+    pl.off[0] = row0 + hb + (uint32_t)tx * 16;                    // column 2tx
+    pl.off[1] = row0 + hb + (2 * E + (uint32_t)tx + 1) * 16;      // column 2tx + 1
+    pl.off[2] = pl.off[3] = 0;
+  } else {
+    const uint32_t par = (t0 & 3) == 0 ? 2 * E : 0;              // b = 0: odd columns
+    const uint32_t c0 = (par + (uint32_t)tx) * 16, c1 = (par + (uint32_t)tx + 1) * 16;
+    pl.off[0] = row0 + hb + c0;
+    pl.off[1] = row0 + hb + c1;
+    pl.off[2] = row1 + hb + c0;
+    pl.off[3] = row1 + hb + c1;
+  }
+  pl.rec = xr + (size_t)n * g.CS * g.cbs;
   return pl;
+}
+
+__device__ __forceinline__ uint2 hadd_2(const uint2& a, const uint2& b) {
+  return make_uint2(hadd2(a.x, b.x), hadd2(a.y, b.y));
+}
+__device__ __forceinline__ uint2 hsub_2(const uint2& a, const uint2& b) {
+  return make_uint2(hsub2(a.x, b.x), hsub2(a.y, b.y));
 }
 
 }  // namespace tp
@@ -394,7 +417,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tp::NTHREAD, 1)
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   __shared__ Shared sh;
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  const Geo g = geo(p);
+  Geo g = geo(p);
+  g.cbs = (size_t)xr::rows(p.h) * g.RB;           // XR record blocks
   const int warp = warp_id(), lane = lane_id();
   const int rank = (int)cluster_ctarank();
   uint32_t* err = &g_twostage_err;
@@ -438,20 +462,19 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tp::NTHREAD, 1)
     if (lane == 0) {
       const uint8_t* u2 = static_cast<const uint8_t*>(p.transform_filter);
       const uint32_t idesc = instr_desc(256, 128, 0, 0, 0, 0);
-      long long cur = -1;
+      int cq = -1, ckp = -1;
       uint32_t it = 0, ui = 0, nload = 0;
       bool ok = true;
-      for (long long i = 0; ok && i < sc.cnt && !*abort_flag; ++i, ++ui) {
-        const long long u = sched_unit(g, sc, i);
-        const long long combo = u / g.nTB;
-        if (combo != cur) {
-          if (cur >= 0) {
+      for (int i = 0; ok && i < sc.cnt && !*abort_flag; ++i, ++ui) {
+        const Unit un = sched_unit(g, sc, i);
+        if (un.q != cq || un.kp != ckp) {
+          if (cq >= 0) {
             // the old U is free once every MMA issued so far has finished
             if (rank == 0) mma_commit_pair(&sh.uempty, BOTH);
             if (!mbar_wait(&sh.uempty, (nload - 1) & 1, abort_flag, err, ERR_WAIT_EMPTY)) break;
           }
-          cur = combo;
-          const Unit un = unit_of(g, u);
+          cq = un.q;
+          ckp = un.kp;
           int t[2];
           pair_taps(un.q, t[0], t[1]);
           const int kb = 2 * un.kp + rank;
@@ -514,8 +537,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tp::NTHREAD, 1)
     const int quarter = warp & 3;
     __half* m16 = static_cast<__half*>(p.mid_result);
     uint32_t ui = 0;
-    for (long long i = 0; i < sc.cnt; ++i, ++ui) {
-      const Unit un = unit_of(g, sched_unit(g, sc, i));
+    for (int i = 0; i < sc.cnt; ++i, ++ui) {
+      const Unit un = sched_unit(g, sc, i);
       const int ab = ui & 1;
       if (!mbar_wait_warp(&sh.accfull[ab], (ui >> 1) & 1, abort_flag, err, ERR_WAIT_ACCUM, SLEEP_NS)) break;
       tc_fence_after();
@@ -538,17 +561,17 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tp::NTHREAD, 1)
           if (ntb == 128) {
             uint32_t h[16];
 #pragma unroll
-            for (int i = 0; i < 16; ++i) {
-              const __half2 x = __floats2half2_rn(v[2 * i], v[2 * i + 1]);
-              h[i] = *reinterpret_cast<const uint32_t*>(&x);
+            for (int i2 = 0; i2 < 16; ++i2) {
+              const __half2 x = __floats2half2_rn(v[2 * i2], v[2 * i2 + 1]);
+              h[i2] = *reinterpret_cast<const uint32_t*>(&x);
             }
             uint4* dst = reinterpret_cast<uint4*>(row + c0);
 #pragma unroll
-            for (int i = 0; i < 4; ++i) dst[i] = make_uint4(h[4 * i], h[4 * i + 1], h[4 * i + 2], h[4 * i + 3]);
+            for (int i2 = 0; i2 < 4; ++i2) dst[i2] = make_uint4(h[4 * i2], h[4 * i2 + 1], h[4 * i2 + 2], h[4 * i2 + 3]);
           } else {
 #pragma unroll
-            for (int i = 0; i < 32; ++i)
-              if (c0 + i < ntb) row[c0 + i] = __float2half_rn(v[i]);
+            for (int i2 = 0; i2 < 32; ++i2)
+              if (c0 + i2 < ntb) row[c0 + i2] = __float2half_rn(v[i2]);
           }
         }
       }
@@ -557,77 +580,66 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tp::NTHREAD, 1)
       if (lane == 0) mbar_arrive_peer(lead_accempty + ab * 8);
     }
   } else {
-    // ---- V producers: thread = (tile tl of this CTA's 64, channel half hh,
-    // K-step kq of each stage)
+    // ---- V producers.  Warp pw = (tile group tg of 16, channel half hh,
+    // K-step kq of each stage); lane = (tile tl of the group, 8-byte half hw
+    // of each 16-byte word), so a warp's loads of one word cover 16 tiles'
+    // 256 contiguous bytes.  V of (a, 1), (a, 2) is R(col 2tx) + R(2tx + 1)
+    // and R(2tx + 1) - R(2tx); V of (a, b) for b = 0, 3 is R(first column of
+    // b) - R(second), one fp16 rounding each.
     const int pw = warp - WARP_P0;
-    const int tl = (pw & 1) * 32 + lane, hh = (pw >> 1) & 1, kq = pw >> 2;
-    const uint8_t* xb = static_cast<const uint8_t*>(p.transform_pin);
+    const int tl = (pw & 3) * 16 + (lane >> 1), hw = lane & 1, hh = (pw >> 2) & 1, kq = pw >> 3;
+    const uint8_t* xr = static_cast<const uint8_t*>(p.transform_pin);
     // The load cursor (lu, lj) runs one stage ahead of the consume cursor
-    // (cu, cj).  Everything a unit needs is worked out when the load cursor
-    // enters it: the window offsets and record pointer for the loads, and
-    // for the consume side the tap pair and whether the tile exists, kept per
-    // unit parity (4 bits each) since the two cursors are at most one unit
-    // apart.
-    long long lu = 0, cu = 0;   // unit indices of this cluster
-    int lj = 0, cj = 0;
+    // (cu, cj); everything a unit needs is worked out when the load cursor
+    // enters it.  The consume side keeps, per unit parity (4 bits each, the
+    // two cursors are at most one unit apart), whether the tile exists and
+    // whether the pair reads four words.
+    int lu = 0, cu = 0, lj = 0, cj = 0;
     uint32_t info = 0;
-    const uint8_t* rec = xb;
-    uint32_t off[6];
-    int nw = 4;
-    bool llive = false;
+    ProdLoad pl;
+    pl.rec = xr;
+    pl.live = false;
+    pl.four = false;
     const size_t step_bytes = (size_t)SK * g.cbs;
-    uint4 wa[6], wb[6];
-    auto issue = [&](uint4 (&w)[6]) {
+    uint2 wa[4], wb[4];
+    auto issue = [&](uint2 (&w)[4]) {
       if (lj == 0) {
-        const Unit un = unit_of(g, sched_unit(g, sc, lu));
-        const ProdLoad pl = prod_load(g, xb, un, rank, tl, hh);
-#pragma unroll
-        for (int i = 0; i < 6; ++i) off[i] = pl.off[i];
-        nw = pl.nw;
-        llive = pl.live;
-        rec = pl.xn + (size_t)kq * g.cbs;
+        pl = prod_load(g, xr, sched_unit(g, sc, lu), rank, tl, hh, hw);
+        pl.rec += (size_t)kq * g.cbs;
         const uint32_t sh4 = (uint32_t)(lu & 1) * 4;
-        info = (info & ~(15u << sh4)) | ((uint32_t)(un.q | (pl.live ? 8 : 0)) << sh4);
+        info = (info & ~(15u << sh4)) | ((uint32_t)((pl.live ? 1 : 0) | (pl.four ? 2 : 0)) << sh4);
       }
-      if (llive && lj * SK + kq < g.CS) {
-#pragma unroll
-        for (int i = 0; i < 6; ++i)
-          if (i < nw) w[i] = __ldg(reinterpret_cast<const uint4*>(rec + off[i]));
-        // the next stage's words of this unit into L1, so that its register
-        // loads (issued a stage from now) find them on the SM
-        if ((lj + 1) * SK + kq < g.CS) {
-#pragma unroll
-          for (int i = 0; i < 6; ++i)
-            if (i < nw) prefetch_l1(rec + step_bytes + off[i]);
+      if (pl.live && lj * SK + kq < g.CS) {
+        w[0] = __ldg(reinterpret_cast<const uint2*>(pl.rec + pl.off[0]));
+        w[1] = __ldg(reinterpret_cast<const uint2*>(pl.rec + pl.off[1]));
+        if (pl.four) {
+          w[2] = __ldg(reinterpret_cast<const uint2*>(pl.rec + pl.off[2]));
+          w[3] = __ldg(reinterpret_cast<const uint2*>(pl.rec + pl.off[3]));
         }
       }
-      rec += step_bytes;
+      pl.rec += step_bytes;
       if (++lj == nst) { lj = 0; ++lu; }
     };
     uint32_t it = 0;
-    auto consume = [&](const uint4 (&w)[6]) -> bool {
+    auto consume = [&](const uint2 (&w)[4]) -> bool {
       const int st = it % NSTV;
       if (it >= NSTV &&
           !mbar_wait_warp(&sh.vempty[st], (it / NSTV - 1) & 1, abort_flag, err, ERR_WAIT_EMPTY, SLEEP_NS))
         return false;
       const uint32_t inf = (info >> ((uint32_t)(cu & 1) * 4)) & 15u;
-      const int q = (int)(inf & 7u);
-      if ((inf & 8u) && cj * SK + kq < g.CS) {
-        const uint32_t* sg = c_pair_signs[q];
-        uint4 v0, v1;
-        if (q < 4) {
-          const uint4 e1 = bt_op4(sg[0], sg[1], w[0], w[1]);
-          const uint4 e2 = bt_op4(sg[0], sg[1], w[2], w[3]);
-          v0 = hadd4(e1, e2);   // b = 1: d1 + d2
-          v1 = hsub4(e2, e1);   // b = 2: d2 - d1
+      if ((inf & 1u) && cj * SK + kq < g.CS) {
+        uint2 v0, v1;
+        if (inf & 2u) {
+          v0 = hsub_2(w[0], w[1]);
+          v1 = hsub_2(w[2], w[3]);
         } else {
-          v0 = bt_op4(sg[4], sg[5], bt_op4(sg[0], sg[1], w[0], w[2]), bt_op4(sg[0], sg[1], w[3], w[5]));
-          v1 = bt_op4(sg[4], sg[5], bt_op4(sg[2], sg[3], w[1], w[2]), bt_op4(sg[2], sg[3], w[4], w[5]));
+          v0 = hadd_2(w[0], w[1]);   // b = 1: d1 + d2
+          v1 = hsub_2(w[1], w[0]);   // b = 2: d2 - d1
         }
         uint8_t* dst = smem + U_BYTES + st * V_STAGE + (kq * 2) * V_TAP + (tl >> 3) * 256 + hh * 128 +
-                       (tl & 7) * 16;
-        *reinterpret_cast<uint4*>(dst) = v0;
-        *reinterpret_cast<uint4*>(dst + V_TAP) = v1;
+                       (tl & 7) * 16 + hw * 8;
+        *reinterpret_cast<uint2*>(dst) = v0;
+        *reinterpret_cast<uint2*>(dst + V_TAP) = v1;
       }
       fence_proxy_async_shared();
       __syncwarp();
@@ -920,109 +932,129 @@ __global__ void __launch_bounds__(tsk::NTHREAD, 1) twostage_stream_kernel(Kernel
 // =============================================================================
 // Output transform
 // =============================================================================
-// CTA = (tile block tb, 8 output channels).  The CTA's 16 taps x 8 channels
-// of the blocked M (16 contiguous runs of 8 * ntb fp16) come in by bulk
-// copy, so the bytes in flight do not depend on registers; thread =
-// (channel kl, 4 tiles g4 .. g4+3 of the block) then reads its 16 taps from
-// shared memory (a warp's 8-byte reads are contiguous), accumulates
-// z = A^T m in fp32 tap by tap in the order of the comparator's output
-// transform (so the result is bit-identical to it), forms y = z A and
-// stores it with one fp16 rounding.  grid (tile blocks, K/8); K is a
-// multiple of 16 and mid_result 16-byte aligned, so every copy starts on a
-// 16-byte boundary and moves a multiple of 16 bytes.
+// Persistent: work item = (tile block tb, 8 output channels kg), item i =
+// kg * tile blocks + tb, CTA b takes items b, b + grid, ...  An item's 16
+// taps x 8 channels of the blocked M (16 contiguous runs of 8 * ntb fp16)
+// come in by bulk copy into one of three shared-memory buffers, issued as
+// soon as a buffer is free, so two items per CTA are in flight while the
+// third is transformed and the bytes in flight do not depend on registers.
+// Thread = (channel kl, 4 tiles g4 .. g4+3 of the block): it reads its 16
+// taps from shared memory (a warp's 8-byte reads are contiguous),
+// accumulates z = A^T m in fp32 tap by tap in the order of the comparator's
+// output transform (so the result is bit-identical to it), forms y = z A and
+// stores it with one fp16 rounding.  K is a multiple of 16 and mid_result
+// 16-byte aligned, so every copy starts on a 16-byte boundary and moves a
+// multiple of 16 bytes.
 namespace ot {
-constexpr int KG = 8;                         // output channels per CTA
+constexpr int KG = 8;                         // output channels per item
 constexpr int TT = 4;                         // tiles per thread
-constexpr int SMEM_BYTES = 16 * KG * 128 * 2 + 128;
+constexpr int NBUF = 3;
+constexpr int BUF_BYTES = 16 * KG * 128 * 2;  // 32 KB
+constexpr int SMEM_BYTES = NBUF * BUF_BYTES + 128;
 }
 
-__global__ void __launch_bounds__(256) twostage_output_kernel(KernelParam p) {
+__global__ void __launch_bounds__(256, 2) twostage_output_kernel(KernelParam p) {
   using namespace ts;
   extern __shared__ __align__(128) uint8_t osm[];
-  __shared__ uint64_t full;
+  __shared__ uint64_t full[ot::NBUF];
   const int K = p.k, P = p.Oh, Q = p.Ow;
   const int TP = (P + 1) >> 1, TQ = (Q + 1) >> 1;
   const long long NT = (long long)p.n * TP * TQ;
-  const int tb = blockIdx.x;
-  const int k0 = blockIdx.y * ot::KG;
-  const long long rem = NT - (long long)tb * 128;
-  const int ntb = rem < 128 ? (int)rem : 128;
-  const uint32_t run = (uint32_t)(ot::KG * ntb * 2);   // bytes of one tap's KG rows
+  const int nTB = (int)((NT + 127) / 128);
+  const int nitems = nTB * (K / ot::KG);
   const __half* m16 = static_cast<const __half*>(p.mid_result);
-  const __half* ms = reinterpret_cast<const __half*>(osm);   // [t][kl][ntb]
   if (threadIdx.x == 0) {
-    mbar_init(&full, 1);
+    for (int b = 0; b < ot::NBUF; ++b) mbar_init(&full[b], 1);
     fence_barrier_init();
   }
   __syncthreads();
-  if (threadIdx.x < 32) {
-    if (threadIdx.x == 0) mbar_arrive_expect_tx(&full, 16 * run);
+  // issue the copies of `item` into buffer `buf` (warp 0)
+  auto fetch = [&](int item, int buf) {
+    const int tb = item % nTB, k0 = (item / nTB) * ot::KG;
+    const long long rem = NT - (long long)tb * 128;
+    const int ntb = rem < 128 ? (int)rem : 128;
+    const uint32_t run = (uint32_t)(ot::KG * ntb * 2);
+    if (threadIdx.x == 0) mbar_arrive_expect_tx(&full[buf], 16 * run);
     __syncwarp();
-    if (threadIdx.x < 16) {
-      const int t = threadIdx.x;
-      bulk_g2s(osm + t * run, m16 + m_offset(tb, t, k0, 0, K, NT), run, &full);
-    }
-  }
+    if (threadIdx.x < 16)
+      bulk_g2s(osm + buf * ot::BUF_BYTES + threadIdx.x * run,
+               m16 + m_offset(tb, threadIdx.x, k0, 0, K, NT), run, &full[buf]);
+  };
+  if (threadIdx.x < 32)
+    for (int b = 0; b < ot::NBUF; ++b)
+      if ((int)blockIdx.x + b * (int)gridDim.x < nitems) fetch(blockIdx.x + b * gridDim.x, b);
   const int kl = threadIdx.x >> 5, g4 = (threadIdx.x & 31) * ot::TT;
-  const int k = k0 + kl;
-  // the copies complete within microseconds; a wait past the bound leaves
-  // the error word set and the output unwritten
-  if (!mbar_wait(&full, 0, nullptr, &g_twostage_err, ERR_WAIT_FULL)) return;
-  if (g4 >= ntb) return;
-  // z[r][b] = sum_a At[r][a] m[4a+b], accumulated in tap order a = 0..3
-  float z[ot::TT][2][4];
-#pragma unroll
-  for (int t = 0; t < 16; ++t) {
-    const int a = t >> 2, b = t & 3;
-    const __half* src = ms + (size_t)t * (run / 2) + kl * ntb + g4;
-    float v[ot::TT];
-    if (ntb == 128) {
-      const uint2 w = *reinterpret_cast<const uint2*>(src);
-      const float2 f0 = __half22float2(*reinterpret_cast<const __half2*>(&w.x));
-      const float2 f1 = __half22float2(*reinterpret_cast<const __half2*>(&w.y));
-      v[0] = f0.x; v[1] = f0.y; v[2] = f1.x; v[3] = f1.y;
-    } else {
-#pragma unroll
-      for (int i = 0; i < ot::TT; ++i) v[i] = g4 + i < ntb ? __half2float(src[i]) : 0.f;
-    }
-#pragma unroll
-    for (int i = 0; i < ot::TT; ++i) {
-      if (a == 0) z[i][0][b] = v[i];
-      if (a == 1) { z[i][0][b] = z[i][0][b] + v[i]; z[i][1][b] = v[i]; }
-      if (a == 2) { z[i][0][b] = z[i][0][b] + v[i]; z[i][1][b] = z[i][1][b] - v[i]; }
-      if (a == 3) z[i][1][b] = z[i][1][b] - v[i];
-    }
-  }
   const long long per_img = (long long)TP * TQ;
   const bool pair_ok = (Q & 1) == 0 && (reinterpret_cast<uintptr_t>(p.pout) & 3) == 0;
   __half* out = static_cast<__half*>(p.pout);
+  int j = 0;
+  for (int item = blockIdx.x; item < nitems; item += gridDim.x, ++j) {
+    const int buf = j % ot::NBUF;
+    const int tb = item % nTB, k = (item / nTB) * ot::KG + kl;
+    const long long rem = NT - (long long)tb * 128;
+    const int ntb = rem < 128 ? (int)rem : 128;
+    const uint32_t run = (uint32_t)(ot::KG * ntb * 2);
+    // the copies complete within microseconds; a wait past the bound leaves
+    // the error word set and the rest of the output unwritten
+    if (!mbar_wait(&full[buf], (j / ot::NBUF) & 1, nullptr, &g_twostage_err, ERR_WAIT_FULL)) break;
+    if (g4 < ntb) {
+      const __half* ms = reinterpret_cast<const __half*>(osm + buf * ot::BUF_BYTES);
+      // z[r][b] = sum_a At[r][a] m[4a+b], accumulated in tap order a = 0..3
+      float z[ot::TT][2][4];
 #pragma unroll
-  for (int i = 0; i < ot::TT; ++i) {
-    if (g4 + i >= ntb) break;
-    float y[4];
+      for (int t = 0; t < 16; ++t) {
+        const int a = t >> 2, b = t & 3;
+        const __half* src = ms + (size_t)t * (run / 2) + kl * ntb + g4;
+        float v[ot::TT];
+        if (ntb == 128) {
+          const uint2 w = *reinterpret_cast<const uint2*>(src);
+          const float2 f0 = __half22float2(*reinterpret_cast<const __half2*>(&w.x));
+          const float2 f1 = __half22float2(*reinterpret_cast<const __half2*>(&w.y));
+          v[0] = f0.x; v[1] = f0.y; v[2] = f1.x; v[3] = f1.y;
+        } else {
 #pragma unroll
-    for (int r = 0; r < 2; ++r) {
-      y[2 * r + 0] = z[i][r][0] + z[i][r][1] + z[i][r][2];
-      y[2 * r + 1] = z[i][r][1] - z[i][r][2] - z[i][r][3];
-    }
-    const long long tile = (long long)tb * 128 + g4 + i;
-    const int n = (int)(tile / per_img);
-    const int rr = (int)(tile - (long long)n * per_img);
-    const int ty = rr / TQ, tx = rr - ty * TQ;
-    const int oy = 2 * ty, ox = 2 * tx;
-    __half* o = out + (((size_t)n * K + k) * P + oy) * (size_t)Q + ox;
-    const bool two_cols = ox + 1 < Q, two_rows = oy + 1 < P;
-    if (two_cols && pair_ok) {
-      *reinterpret_cast<__half2*>(o) = __floats2half2_rn(y[0], y[1]);
-      if (two_rows) *reinterpret_cast<__half2*>(o + Q) = __floats2half2_rn(y[2], y[3]);
-    } else {
-      o[0] = __float2half_rn(y[0]);
-      if (two_cols) o[1] = __float2half_rn(y[1]);
-      if (two_rows) {
-        o[Q] = __float2half_rn(y[2]);
-        if (two_cols) o[Q + 1] = __float2half_rn(y[3]);
+          for (int i = 0; i < ot::TT; ++i) v[i] = g4 + i < ntb ? __half2float(src[i]) : 0.f;
+        }
+#pragma unroll
+        for (int i = 0; i < ot::TT; ++i) {
+          if (a == 0) z[i][0][b] = v[i];
+          if (a == 1) { z[i][0][b] = z[i][0][b] + v[i]; z[i][1][b] = v[i]; }
+          if (a == 2) { z[i][0][b] = z[i][0][b] + v[i]; z[i][1][b] = z[i][1][b] - v[i]; }
+          if (a == 3) z[i][1][b] = z[i][1][b] - v[i];
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < ot::TT; ++i) {
+        if (g4 + i >= ntb) break;
+        float y[4];
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+          y[2 * r + 0] = z[i][r][0] + z[i][r][1] + z[i][r][2];
+          y[2 * r + 1] = z[i][r][1] - z[i][r][2] - z[i][r][3];
+        }
+        const long long tile = (long long)tb * 128 + g4 + i;
+        const int n = (int)(tile / per_img);
+        const int rr = (int)(tile - (long long)n * per_img);
+        const int ty = rr / TQ, tx = rr - ty * TQ;
+        const int oy = 2 * ty, ox = 2 * tx;
+        __half* o = out + (((size_t)n * K + k) * P + oy) * (size_t)Q + ox;
+        const bool two_cols = ox + 1 < Q, two_rows = oy + 1 < P;
+        if (two_cols && pair_ok) {
+          *reinterpret_cast<__half2*>(o) = __floats2half2_rn(y[0], y[1]);
+          if (two_rows) *reinterpret_cast<__half2*>(o + Q) = __floats2half2_rn(y[2], y[3]);
+        } else {
+          o[0] = __float2half_rn(y[0]);
+          if (two_cols) o[1] = __float2half_rn(y[1]);
+          if (two_rows) {
+            o[Q] = __float2half_rn(y[2]);
+            if (two_cols) o[Q + 1] = __float2half_rn(y[3]);
+          }
+        }
       }
     }
+    __syncthreads();   // every thread is done with the buffer
+    const int next = item + ot::NBUF * (int)gridDim.x;
+    if (threadIdx.x < 32 && next < nitems) fetch(next, buf);
   }
 }
 
@@ -1058,6 +1090,35 @@ int wino_twostage_prepare() {
                                    tp::SMEM_BYTES);
 }
 
+// The two-stage pre-pass: row-transformed records (XR) for the tap-pair
+// kernel, channel-blocked records (XB) for the streamed-U kernel.
+size_t wino_xb_bytes(int n, int c, int h, int w);
+unsigned wino_xb_layout_grid(int n, int c, int h, int w);
+void* wino_xb_layout_kernel_ptr();
+
+size_t wino_twostage_prepass_bytes(int n, int c, int h, int w) {
+  return use_pair(c) ? xr::bytes(n, c, h, w) : wino_xb_bytes(n, c, h, w);
+}
+long long wino_twostage_prepass_items(int n, int c, int h, int w) {
+  const long long rows = use_pair(c) ? xr::rows(h) : xb_rows(h);
+  return (long long)n * (c >> 4) * rows * xb_entries(w);
+}
+void* wino_twostage_prepass_kernel_ptr_for(int c) {
+  return use_pair(c) ? (void*)xr_layout_kernel : wino_xb_layout_kernel_ptr();
+}
+unsigned wino_twostage_prepass_grid(int n, int c, int h, int w) {
+  if (!use_pair(c)) return wino_xb_layout_grid(n, c, h, w);
+  const long long blocks = (wino_twostage_prepass_items(n, c, h, w) + 255) / 256;
+  const long long cap = 148LL * 64;
+  return (unsigned)(blocks < cap ? (blocks > 0 ? blocks : 1) : cap);
+}
+int wino_launch_twostage_prepass(const KernelParam* p, cudaStream_t stream) {
+  void* args[] = {const_cast<KernelParam*>(p)};
+  return (int)cudaLaunchKernel(wino_twostage_prepass_kernel_ptr_for(p->c),
+                               dim3(wino_twostage_prepass_grid(p->n, p->c, p->h, p->w)), dim3(256), args, 0,
+                               stream);
+}
+
 // Tiles and the M16 bytes of a shape (no padding).
 long long wino_twostage_tiles(int n, int h, int w) { return (long long)n * ((h + 1) / 2) * ((w + 1) / 2); }
 size_t wino_twostage_m_bytes(int n, int h, int w, int k) {
@@ -1085,9 +1146,12 @@ unsigned wino_twostage_gemm_grid(int n, int c, int h, int w, int k, int sms) {
   return (unsigned)(units < sms ? units : sms);
 }
 
-void wino_twostage_output_grid(int n, int h, int w, int k, unsigned* gx, unsigned* gy) {
-  *gx = (unsigned)((wino_twostage_tiles(n, h, w) + 127) / 128);
-  *gy = (unsigned)((k + ot::KG - 1) / ot::KG);
+// Output transform grid: two persistent CTAs per SM up to the work items.
+void wino_twostage_output_grid(int n, int h, int w, int k, int sms, unsigned* gx, unsigned* gy) {
+  const long long items = (wino_twostage_tiles(n, h, w) + 127) / 128 * (k / ot::KG);
+  const long long cap = 2LL * sms;
+  *gx = (unsigned)(items < cap ? items : cap);
+  *gy = 1;
 }
 
 uint32_t wino_twostage_error_read_clear() {

@@ -87,7 +87,12 @@ int wino_twostage_smem_bytes_for(int c);
 int wino_twostage_prepare();
 size_t wino_twostage_m_bytes(int n, int h, int w, int k);
 unsigned wino_twostage_gemm_grid(int n, int c, int h, int w, int k, int sms);
-void wino_twostage_output_grid(int n, int h, int w, int k, unsigned* gx, unsigned* gy);
+size_t wino_twostage_prepass_bytes(int n, int c, int h, int w);
+long long wino_twostage_prepass_items(int n, int c, int h, int w);
+void* wino_twostage_prepass_kernel_ptr_for(int c);
+unsigned wino_twostage_prepass_grid(int n, int c, int h, int w);
+int wino_launch_twostage_prepass(const wino::KernelParam* p, cudaStream_t stream);
+void wino_twostage_output_grid(int n, int h, int w, int k, int sms, unsigned* gx, unsigned* gy);
 int wino_twostage_output_smem_bytes();
 uint32_t wino_twostage_error_read_clear();
 }
@@ -138,12 +143,15 @@ wino::KernelParam make_param(const void* x, const void* w, void* y, void* vws, v
 // The pre-pass counts its items in 32 bits.
 bool xb_items_ok(int n, int c, int h, int w) { return wino_xb_items(n, c, h, w) < (1LL << 31); }
 
-// The two-stage producers address one (image, 16-channel) record block of the
-// blocked input with 32-bit byte offsets: (2*ceil(h/2) + 2) rows of
-// 64 * (ceil(w/2) + 1) bytes must stay below 2^31.
+// The two-stage producers address one (image, 16-channel) record block of
+// their pre-pass records with 32-bit byte offsets: up to 4*ceil(h/2) + 2 rows
+// of 64 * (ceil(w/2) + 1) bytes must stay below 2^31; the pre-pass counts its
+// items and the GEMM its tiles in 32 bits.
 bool twostage_ok(int n, int c, int h, int w) {
-  const long long rows = 2LL * ((h + 1) / 2) + 2, row_bytes = 64LL * ((w + 1) / 2 + 1);
-  return xb_items_ok(n, c, h, w) && rows * row_bytes < (1LL << 31);
+  const long long rows = 4LL * ((h + 1) / 2) + 2, row_bytes = 64LL * ((w + 1) / 2 + 1);
+  const long long tiles = (long long)n * ((h + 1) / 2) * ((w + 1) / 2);
+  return xb_items_ok(n, c, h, w) && wino_twostage_prepass_items(n, c, h, w) < (1LL << 31) &&
+         rows * row_bytes < (1LL << 31) && tiles < (1LL << 30);
 }
 
 unsigned fused_grid(int n, int h, int w, int k) {
@@ -214,16 +222,21 @@ static int plan_route(const problem_t& pr) {
                       (reinterpret_cast<uintptr_t>(pr.transform_pin) & 15) == 0 &&
                       wino_xb_bytes((int)pr.n, (int)pr.c, (int)pr.h, (int)pr.w) <= pin_ws_bytes &&
                       xb_items_ok((int)pr.n, (int)pr.c, (int)pr.h, (int)pr.w);
-  if (!use_xb) return WINO_ROUTE_FUSED;
   // Two-stage route (input transform fused into full-width tap GEMMs, M in
   // the caller's mid_result, output transform in slot 4) whenever M fits the
-  // reference's mid_result size of 4*k*h*w*n fp16 elements (even H and W).
-  const bool two_stage = pr.mid_result != nullptr &&
+  // reference's mid_result size of 4*k*h*w*n fp16 elements (even H and W) and
+  // the pre-pass records fit transform_pin.
+  const bool two_stage = pr.transform_pin != nullptr &&
+                         (reinterpret_cast<uintptr_t>(pr.transform_pin) & 15) == 0 &&
+                         pr.mid_result != nullptr &&
                          (reinterpret_cast<uintptr_t>(pr.mid_result) & 15) == 0 &&
                          twostage_ok((int)pr.n, (int)pr.c, (int)pr.h, (int)pr.w) &&
+                         wino_twostage_prepass_bytes((int)pr.n, (int)pr.c, (int)pr.h, (int)pr.w) <=
+                             pin_ws_bytes &&
                          wino_twostage_m_bytes((int)pr.n, (int)pr.h, (int)pr.w, (int)pr.k) <=
                              (size_t)4 * pr.k * pr.h * pr.w * pr.n * 2;
-  return two_stage ? WINO_ROUTE_TWOSTAGE : WINO_ROUTE_FUSED_XB;
+  if (two_stage) return WINO_ROUTE_TWOSTAGE;
+  return use_xb ? WINO_ROUTE_FUSED_XB : WINO_ROUTE_FUSED;
 }
 
 int getkernelInfo(problem_t* problem, kernelInfo_t* kernelInfo, void* param) {
@@ -268,14 +281,14 @@ int getkernelInfo(problem_t* problem, kernelInfo_t* kernelInfo, void* param) {
   if (route == WINO_ROUTE_TWOSTAGE) {
     set_slot(kernelInfo, 1, (unsigned)((kc + 255) / 256), 1, 1, 256, 1, 1, 0,
              wino_dropin_filter_u2_kernel_ptr());
-    set_slot(kernelInfo, 2, wino_xb_layout_grid((int)pr.n, (int)pr.c, (int)pr.h, (int)pr.w), 1, 1, 256, 1, 1, 0,
-             wino_xb_layout_kernel_ptr());
     const int c = (int)pr.c;
+    set_slot(kernelInfo, 2, wino_twostage_prepass_grid((int)pr.n, c, (int)pr.h, (int)pr.w), 1, 1, 256, 1, 1, 0,
+             wino_twostage_prepass_kernel_ptr_for(c));
     set_slot(kernelInfo, 3, wino_twostage_gemm_grid((int)pr.n, c, (int)pr.h, (int)pr.w, (int)pr.k, sm_count()), 1,
              1, (unsigned)wino_twostage_threads_for(c), 1, 1, (unsigned)wino_twostage_smem_bytes_for(c),
              wino_twostage_gemm_kernel_ptr_for(c));
     unsigned ox, oy;
-    wino_twostage_output_grid((int)pr.n, (int)pr.h, (int)pr.w, (int)pr.k, &ox, &oy);
+    wino_twostage_output_grid((int)pr.n, (int)pr.h, (int)pr.w, (int)pr.k, sm_count(), &ox, &oy);
     set_slot(kernelInfo, 4, ox, oy, 1, 256, 1, 1, (unsigned)wino_twostage_output_smem_bytes(),
              wino_twostage_output_kernel_ptr());
     return WINO_OK;
@@ -368,10 +381,11 @@ extern "C" int wino_conv2d_fused(const void* x, const void* ucache, void* y, int
 }
 
 // ------------------------------------------------------ two-stage path ----
-// Workspace: the channel-blocked input (XB) then M16, each 256-byte aligned.
+// Workspace: the pre-pass records (row-transformed XR when C <= 256, else the
+// channel-blocked XB) then M16, each 256-byte aligned.
 extern "C" size_t wino_twostage_workspace_bytes(int n, int c, int h, int w, int k) {
   if (wino_check_shape(n, c, h, w, k) != WINO_OK || !twostage_ok(n, c, h, w)) return 0;
-  const size_t xb = (wino_xb_bytes(n, c, h, w) + 255) / 256 * 256;
+  const size_t xb = (wino_twostage_prepass_bytes(n, c, h, w) + 255) / 256 * 256;
   return xb + wino_twostage_m_bytes(n, h, w, k);
 }
 
@@ -386,12 +400,12 @@ extern "C" int wino_twostage_stage(int stage, const void* x, const void* ucache2
   if (st != WINO_OK) return st;
   if (!twostage_ok(n, c, h, w)) return WINO_EUNSUPPORTED;
   if (wino_twostage_prepare() != 0) return WINO_ECUDA;
-  const size_t xb = (wino_xb_bytes(n, c, h, w) + 255) / 256 * 256;
+  const size_t xb = (wino_twostage_prepass_bytes(n, c, h, w) + 255) / 256 * 256;
   wino::KernelParam p = make_param(x, nullptr, y, workspace, const_cast<void*>(ucache2),
                                    static_cast<uint8_t*>(workspace) + xb, n, c, h, w, k);
   const cudaStream_t s = (cudaStream_t)stream;
   void* args[] = {&p};
-  if (stage == 0) return wino_launch_xb_layout(&p, s) == 0 ? WINO_OK : WINO_ECUDA;
+  if (stage == 0) return wino_launch_twostage_prepass(&p, s) == 0 ? WINO_OK : WINO_ECUDA;
   if (stage == 1)
     return cudaLaunchKernel(wino_twostage_gemm_kernel_ptr_for(c),
                             dim3(wino_twostage_gemm_grid(n, c, h, w, k, sm_count())),
@@ -400,7 +414,7 @@ extern "C" int wino_twostage_stage(int stage, const void* x, const void* ucache2
                ? WINO_OK
                : WINO_ECUDA;
   unsigned ox, oy;
-  wino_twostage_output_grid(n, h, w, k, &ox, &oy);
+  wino_twostage_output_grid(n, h, w, k, sm_count(), &ox, &oy);
   return cudaLaunchKernel(wino_twostage_output_kernel_ptr(), dim3(ox, oy), dim3(256), args,
                           (size_t)wino_twostage_output_smem_bytes(), s) ==
                  cudaSuccess

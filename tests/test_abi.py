@@ -248,9 +248,16 @@ def test_f4_entry_points_validate_and_size(wino):
     assert L.wino_conv2d_f4(d, d, 1, 16, 8, 8, 16, 1, odd, full, None) == 1
 
 
+def _xr_bytes(n, c, h, w):
+    """Row-transformed pre-pass records of the tap-pair route: per image and
+    16-channel block 4*ceil(h/2) rows of 64*(ceil(w/2) + 1) bytes."""
+    return n * (c // 16) * 4 * ((h + 1) // 2) * 64 * ((w + 1) // 2 + 1)
+
+
 def test_twostage_entry_points_validate_and_size(wino):
-    """Two-stage path: workspace = blocked input (256-byte aligned) + 16*K*tiles
-    fp16 of M; argument checks return before any CUDA call."""
+    """Two-stage path: workspace = pre-pass records (row-transformed for
+    C <= 256, channel-blocked above; 256-byte aligned) + 16*K*tiles fp16 of M;
+    argument checks return before any CUDA call."""
     L = wino.lib()
     d = ctypes.c_void_p(0x10000)
     odd = ctypes.c_void_p(0x10010)
@@ -258,10 +265,15 @@ def test_twostage_entry_points_validate_and_size(wino):
     # N128 C256 H28 K256: 25088 tiles; M = 16*256*25088*2 bytes = the reference's mid_result
     m = 16 * 256 * 25088 * 2
     assert m == 4 * 256 * 28 * 28 * 128 * 2
-    assert L.wino_twostage_workspace_bytes(128, 256, 28, 28, 256) == r256(L.wino_xb_bytes(128, 256, 28, 28)) + m
+    assert L.wino_twostage_workspace_bytes(128, 256, 28, 28, 256) == r256(_xr_bytes(128, 256, 28, 28)) + m
+    # the records fit the reference harness's transform_pin (4*h*h*n*c fp16)
+    assert _xr_bytes(128, 256, 28, 28) <= 4 * 28 * 28 * 128 * 256 * 2
     # odd sizes: tiles = n * ceil(h/2) * ceil(w/2)
     assert (L.wino_twostage_workspace_bytes(3, 48, 9, 7, 144)
-            == r256(L.wino_xb_bytes(3, 48, 9, 7)) + 16 * 144 * (3 * 5 * 4) * 2)
+            == r256(_xr_bytes(3, 48, 9, 7)) + 16 * 144 * (3 * 5 * 4) * 2)
+    # C > 256: the streamed-U kernel reads the channel-blocked records
+    assert (L.wino_twostage_workspace_bytes(2, 272, 6, 8, 48)
+            == r256(L.wino_xb_bytes(2, 272, 6, 8)) + 16 * 48 * (2 * 3 * 4) * 2)
     assert L.wino_twostage_workspace_bytes(1, 24, 8, 8, 16) == 0          # C % 16
     assert L.wino_conv2d_twostage(None, d, d, d, 1, 16, 8, 8, 16, None) == 1
     assert L.wino_conv2d_twostage(d, d, odd, d, 1, 16, 8, 8, 16, None) == 1  # workspace alignment

@@ -157,3 +157,46 @@ def test_dropin_two_stage_route(wino, cuda, oracle_mod, shape):
     assert wino.error_read_clear() == 0
     assert torch.equal(y2, y3)
     _check(oracle_mod, y2.cpu().numpy(), oracle_mod.conv2d_f64(x, wt), str(shape))
+
+
+def _xr_layout_np(x16):
+    """NumPy statement of the row-transformed records the tap-pair route's
+    pre-pass writes: XR[n][c/16][ty][a][par][hh][e][8] with
+    R_a(ty, x) = fp16(s0 * X(2ty - 1 + i0, x) + s1 * X(2ty - 1 + i1, x)) for
+    B^T row a = s0 * d_i0 + s1 * d_i1 (one rounding of the exact two-term
+    sum), par 0 entry e = column 2e, par 1 entry e = column 2e - 1, zero
+    outside the image."""
+    from oracle import winograd as W
+    n, c, h, w = x16.shape
+    tp, tq = (h + 1) // 2, (w + 1) // 2
+    e = tq + 1
+    pad = np.zeros((n, c, 2 * tp + 2, 2 * e + 1), np.float64)   # rows -1 .. 2tp, cols -1 .. 2e-1
+    pad[:, :, 1:h + 1, 1:w + 1] = x16.astype(np.float64)
+    win = np.stack([pad[:, :, 2 * t:2 * t + 4] for t in range(tp)], axis=2)   # n c ty i col
+    r = np.einsum("ai,nctix->nctax", W.BT, win).astype(np.float16)            # n c ty a col
+    out = np.zeros((n, c // 16, tp, 4, 2, 2, e, 8), np.float16)
+    v = r.reshape(n, c // 16, 2, 8, tp, 4, 2 * e + 1)                         # n cb hh ci ty a col
+    out[:, :, :, :, 0] = v[..., 2 * np.arange(e) + 1].transpose(0, 1, 4, 5, 2, 6, 3)
+    out[:, :, :, :, 1] = v[..., 2 * np.arange(e)].transpose(0, 1, 4, 5, 2, 6, 3)
+    return out
+
+
+@pytest.mark.parametrize("shape", [(2, 32, 12, 10), (1, 16, 9, 7), (3, 48, 1, 1), (1, 16, 28, 28)])
+def test_twostage_row_prepass_bit_exact(wino, cuda, oracle_mod, shape):
+    """The tap-pair route's pre-pass (stage 0 of conv2d_twostage for
+    C <= 256) writes exactly the NumPy statement of its records."""
+    import torch
+    n, c, h, w = shape
+    k = 16
+    x16, _ = oracle_mod.make_inputs(n, c, h, w, k, seed=5, x_dist="normal")
+    ref = _xr_layout_np(x16)
+    nb = wino.twostage_workspace_bytes(n, c, h, w, k)
+    ws = wino._aligned_ws(nb, cuda)
+    ws.fill_(0xA5)                                                 # poison
+    x = _t(x16, cuda)
+    u2 = torch.zeros(16 * k * c, dtype=torch.float16, device=cuda)
+    y = torch.empty((n, k, h, w), dtype=torch.float16, device=cuda)
+    wino.twostage_stage(0, x, u2, k, y, ws)
+    torch.cuda.synchronize()
+    got = ws[:ref.nbytes].cpu().numpy().view(np.uint16)
+    assert np.array_equal(got, ref.view(np.uint16).reshape(-1))
