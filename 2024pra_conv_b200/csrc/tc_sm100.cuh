@@ -182,6 +182,12 @@ __device__ __forceinline__ void bulk_g2s_hint(void* dst_smem, const void* src_gm
       : "memory");
 }
 
+// Bring [src, src + bytes) from device memory into L2 without a destination
+// (16-byte aligned, bytes % 16 == 0); completes on its own.
+__device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
 __device__ __forceinline__ uint64_t policy_evict_last() {
   uint64_t p;
   asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));

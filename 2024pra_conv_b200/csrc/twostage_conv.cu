@@ -154,8 +154,9 @@ __device__ __forceinline__ void tile_decode(const Geo& g, long long tile, int& n
 // rounded once to fp16: exactly the first (row) step of B^T d B in the fused
 // kernel's producers, so V formed from XR by the column step is bit for bit
 // the same.  Size N * C/16 * 4 ceil(H/2) * 64 (ceil(W/2) + 1) bytes, about
-// twice the input.  One thread per (row, entry e): columns 2e and 2e + 1 of
-// 16 channels (par 0 entry e, par 1 entry e + 1; the last entry's thread
+// twice the input.  One thread per (tile row, entry e): the four window rows
+// at columns 2e and 2e + 1 of 16 channels, read once, give the entries of
+// all four rows (par 0 entry e, par 1 entry e + 1; the last entry's thread
 // also writes the zero column -1).
 namespace xr {
 __host__ __device__ __forceinline__ int rows(int H) { return 4 * ((H + 1) >> 1); }
@@ -167,56 +168,57 @@ __host__ __device__ __forceinline__ size_t bytes(int N, int C, int H, int W) {
 __global__ void __launch_bounds__(256) xr_layout_kernel(KernelParam p) {
   const int C = p.c, H = p.h, W = p.w;
   const int CB = C >> 4, TP = (H + 1) >> 1, E = xb_entries(W);
-  const uint32_t items = (uint32_t)p.n * CB * TP * 4 * E;
+  const uint32_t items = (uint32_t)p.n * CB * TP * E;
   const unsigned short* X = static_cast<const unsigned short*>(p.pin);
   uint4* XR = static_cast<uint4*>(p.transform_pin);
   const size_t plane = (size_t)H * W;
   const bool w_even = (W & 1) == 0;
   for (uint32_t it = blockIdx.x * blockDim.x + threadIdx.x; it < items; it += gridDim.x * blockDim.x) {
-    const uint32_t rec = it / E;                  // ((n * CB + cb) * TP + ty) * 4 + a
-    const int e = (int)(it - rec * E);
-    const int a = (int)(rec & 3);
-    const uint32_t r2 = rec >> 2;
-    const int ty = (int)(r2 % TP);
-    const uint32_t ncb = r2 / TP;
+    const uint32_t trow = it / E;                 // (n * CB + cb) * TP + ty
+    const int e = (int)(it - trow * E);
+    const int ty = (int)(trow % TP);
+    const uint32_t ncb = trow / TP;
     const int cb = (int)(ncb % CB), n = (int)(ncb / CB);
-    int i0, i1;
-    uint32_t s0, s1;
-    ts::bt_pick(a, i0, i1, s0, s1);
     const int x0 = 2 * e;
-    uint32_t r[16];                               // (column x0, column x0 + 1) of channel 16 cb + i
-#pragma unroll
-    for (int i = 0; i < 16; ++i) r[i] = 0u;
     const unsigned short* base = X + ((size_t)n * C + 16 * cb) * plane;
-    uint32_t v[2][16];
+    // window rows 0..3 (input rows 2ty - 1 ..), columns (x0, x0 + 1), 16 channels
+    uint32_t d[4][16];
 #pragma unroll
-    for (int k = 0; k < 2; ++k) {
-      const int y = 2 * ty - 1 + (k == 0 ? i0 : i1);
+    for (int r = 0; r < 4; ++r) {
+      const int y = 2 * ty - 1 + r;
       const bool rok = y >= 0 && y < H;
       const bool ok0 = rok && x0 < W, ok1 = rok && x0 + 1 < W;
       const unsigned short* src = base + (size_t)(rok ? y : 0) * W + x0;
       if (w_even && ok1) {
 #pragma unroll
-        for (int i = 0; i < 16; ++i) v[k][i] = *reinterpret_cast<const uint32_t*>(src + i * plane);
+        for (int i = 0; i < 16; ++i) d[r][i] = *reinterpret_cast<const uint32_t*>(src + i * plane);
       } else {
 #pragma unroll
         for (int i = 0; i < 16; ++i)
-          v[k][i] = (ok0 ? (uint32_t)src[i * plane] : 0u) | ((ok1 ? (uint32_t)src[i * plane + 1] : 0u) << 16);
+          d[r][i] = (ok0 ? (uint32_t)src[i * plane] : 0u) | ((ok1 ? (uint32_t)src[i * plane + 1] : 0u) << 16);
       }
     }
+    uint4* out = XR + (size_t)trow * 4 * (4 * E);
 #pragma unroll
-    for (int i = 0; i < 16; ++i) r[i] = ts::bt_op(s0, s1, v[0][i], v[1][i]);
-    uint4* out = XR + (size_t)rec * (4 * E);
+    for (int a = 0; a < 4; ++a) {
+      // B^T row a: d0 - d2, d1 + d2, d2 - d1, d1 - d3 (one rounding each)
+      uint32_t r[16];
 #pragma unroll
-    for (int hh = 0; hh < 2; ++hh) {
-      const uint32_t* q = r + 8 * hh;
-      out[hh * E + e] = make_uint4(__byte_perm(q[0], q[1], 0x5410), __byte_perm(q[2], q[3], 0x5410),
-                                   __byte_perm(q[4], q[5], 0x5410), __byte_perm(q[6], q[7], 0x5410));
-      if (e + 1 < E)
-        out[(2 + hh) * E + e + 1] = make_uint4(__byte_perm(q[0], q[1], 0x7632), __byte_perm(q[2], q[3], 0x7632),
-                                               __byte_perm(q[4], q[5], 0x7632), __byte_perm(q[6], q[7], 0x7632));
-      else
-        out[(2 + hh) * E] = make_uint4(0u, 0u, 0u, 0u);
+      for (int i = 0; i < 16; ++i)
+        r[i] = a == 0 ? hsub2(d[0][i], d[2][i]) : a == 1 ? hadd2(d[1][i], d[2][i])
+             : a == 2 ? hsub2(d[2][i], d[1][i]) : hsub2(d[1][i], d[3][i]);
+      uint4* row = out + a * (4 * E);
+#pragma unroll
+      for (int hh = 0; hh < 2; ++hh) {
+        const uint32_t* q = r + 8 * hh;
+        row[hh * E + e] = make_uint4(__byte_perm(q[0], q[1], 0x5410), __byte_perm(q[2], q[3], 0x5410),
+                                     __byte_perm(q[4], q[5], 0x5410), __byte_perm(q[6], q[7], 0x5410));
+        if (e + 1 < E)
+          row[(2 + hh) * E + e + 1] = make_uint4(__byte_perm(q[0], q[1], 0x7632), __byte_perm(q[2], q[3], 0x7632),
+                                                 __byte_perm(q[4], q[5], 0x7632), __byte_perm(q[6], q[7], 0x7632));
+        else
+          row[(2 + hh) * E] = make_uint4(0u, 0u, 0u, 0u);
+      }
     }
   }
 }
@@ -400,6 +402,26 @@ __device__ __forceinline__ ProdLoad prod_load(const Geo& g, const uint8_t* xr, c
   }
   pl.rec = xr + (size_t)n * g.CS * g.cbs;
   return pl;
+}
+
+// L2 prefetch of the XR rows (all four tap rows of each tile row, every
+// channel block) that this CTA's half of unit `un` reads, one bulk prefetch
+// per (image, channel block).  The records were written by the pre-pass and
+// mostly left L2 again; the producers, a stage of loads ahead at most, would
+// otherwise wait for device memory.
+__device__ __forceinline__ void prefetch_unit(const Geo& g, const uint8_t* xr, const Unit& un, int rank) {
+  const int per = g.TP * g.TQ;
+  const int t0 = un.tb * 128 + rank * VT;
+  if (t0 >= (int)g.NT) return;
+  const int t1 = min(t0 + VT, (int)g.NT) - 1;
+  const int n0 = t0 / per, n1 = t1 / per;
+  for (int n = n0; n <= n1; ++n) {
+    const int ya = n == n0 ? (t0 - n0 * per) / g.TQ : 0;
+    const int yb = n == n1 ? (t1 - n1 * per) / g.TQ : g.TP - 1;
+    const uint32_t bytes = (uint32_t)(4 * (yb - ya + 1)) * g.RB;
+    for (int cb = 0; cb < g.CS; ++cb)
+      bulk_prefetch_l2(xr + ((size_t)n * g.CS + cb) * g.cbs + (size_t)(4 * ya) * g.RB, bytes);
+  }
 }
 
 __device__ __forceinline__ uint2 hadd_2(const uint2& a, const uint2& b) {
@@ -604,6 +626,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tp::NTHREAD, 1)
     uint2 wa[4], wb[4];
     auto issue = [&](uint2 (&w)[4]) {
       if (lj == 0) {
+        // one thread keeps the XR rows of the next two units on their way to L2
+        if (pw == 0 && lane == 0) {
+          if (lu == 0 && sc.cnt > 1) prefetch_unit(g, xr, sched_unit(g, sc, 1), rank);
+          if (lu + 2 < sc.cnt) prefetch_unit(g, xr, sched_unit(g, sc, lu + 2), rank);
+        }
         pl = prod_load(g, xr, sched_unit(g, sc, lu), rank, tl, hh, hw);
         pl.rec += (size_t)kq * g.cbs;
         const uint32_t sh4 = (uint32_t)(lu & 1) * 4;
@@ -984,7 +1011,7 @@ __global__ void __launch_bounds__(256, 2) twostage_output_kernel(KernelParam p) 
     for (int b = 0; b < ot::NBUF; ++b)
       if ((int)blockIdx.x + b * (int)gridDim.x < nitems) fetch(blockIdx.x + b * gridDim.x, b);
   const int kl = threadIdx.x >> 5, g4 = (threadIdx.x & 31) * ot::TT;
-  const long long per_img = (long long)TP * TQ;
+  const int per_img = TP * TQ;
   const bool pair_ok = (Q & 1) == 0 && (reinterpret_cast<uintptr_t>(p.pout) & 3) == 0;
   __half* out = static_cast<__half*>(p.pout);
   int j = 0;
@@ -1032,9 +1059,9 @@ __global__ void __launch_bounds__(256, 2) twostage_output_kernel(KernelParam p) 
           y[2 * r + 0] = z[i][r][0] + z[i][r][1] + z[i][r][2];
           y[2 * r + 1] = z[i][r][1] - z[i][r][2] - z[i][r][3];
         }
-        const long long tile = (long long)tb * 128 + g4 + i;
-        const int n = (int)(tile / per_img);
-        const int rr = (int)(tile - (long long)n * per_img);
+        const int tile = tb * 128 + g4 + i;       // tiles < 2^30 (host check)
+        const int n = tile / per_img;
+        const int rr = tile - n * per_img;
         const int ty = rr / TQ, tx = rr - ty * TQ;
         const int oy = 2 * ty, ox = 2 * tx;
         __half* o = out + (((size_t)n * K + k) * P + oy) * (size_t)Q + ox;
@@ -1108,7 +1135,7 @@ void* wino_twostage_prepass_kernel_ptr_for(int c) {
 }
 unsigned wino_twostage_prepass_grid(int n, int c, int h, int w) {
   if (!use_pair(c)) return wino_xb_layout_grid(n, c, h, w);
-  const long long blocks = (wino_twostage_prepass_items(n, c, h, w) + 255) / 256;
+  const long long blocks = (wino_twostage_prepass_items(n, c, h, w) / 4 + 255) / 256;
   const long long cap = 148LL * 64;
   return (unsigned)(blocks < cap ? (blocks > 0 ? blocks : 1) : cap);
 }
