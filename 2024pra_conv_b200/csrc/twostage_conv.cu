@@ -241,8 +241,9 @@ constexpr int U_TAP = CS_MAX * U_STEP;        // 64 KB
 constexpr int U_BYTES = 2 * U_TAP;
 constexpr int SMEM_BYTES = U_BYTES + NSTV * V_STAGE + 1024;
 // warps 0-3 epilogue (warp w reads TMEM lanes 32 (w % 4) ..), warp 4 lane 0
-// U loads (both CTAs) and MMA issue (rank 0), warps 5-20 V producers
-constexpr int WARP_E0 = 0, NWARP_E = 4, WARP_MMA = 4, WARP_P0 = 5, NWARP_P = 16;
+// U loads (both CTAs) and MMA issue (rank 0), warps 5-12 V producers
+constexpr int WARP_E0 = 0, NWARP_E = 4, WARP_MMA = 4, WARP_P0 = 5, NWARP_P = 8;
+constexpr int RING = 4;                       // producer register ring (stages of loads)
 constexpr int NTHREAD = (WARP_P0 + NWARP_P) * 32;
 constexpr int NPAIR = 8;
 constexpr uint16_t BOTH = 3;                  // CTA mask of the pair
@@ -358,7 +359,7 @@ __device__ __forceinline__ Unit sched_unit(const Geo& g, const Sched& sc, int i)
 }
 
 // Load side of one unit for a producer thread (tile tl of this CTA's half,
-// channel half hh, 8-byte half hw of each 16-byte word): the XR words its
+// channel half hh): the 16-byte XR words its
 // taps' column step reads.  q < 4: row (ty, a) at columns 2tx (par 0 entry
 // tx) and 2tx + 1 (par 1 entry tx + 1); q >= 4: rows (ty, a0), (ty, a1) at
 // the two columns of tap column b (b = 0: 2tx - 1, 2tx + 1, par 1 entries
@@ -370,7 +371,7 @@ struct ProdLoad {
 };
 
 __device__ __forceinline__ ProdLoad prod_load(const Geo& g, const uint8_t* xr, const Unit& un, int rank,
-                                              int tl, int hh, int hw) {
+                                              int tl, int hh) {
   ProdLoad pl;
   const int tile = un.tb * 128 + rank * VT + tl;
   pl.live = tile < (int)g.NT;
@@ -387,7 +388,7 @@ __device__ __forceinline__ ProdLoad prod_load(const Geo& g, const uint8_t* xr, c
   pair_taps(un.q, t0, t1);
   const uint32_t RB = g.RB, E = (uint32_t)g.E;
   const uint32_t row0 = (uint32_t)(4 * ty + (t0 >> 2)) * RB, row1 = (uint32_t)(4 * ty + (t1 >> 2)) * RB;
-  const uint32_t hb = (uint32_t)(hh * E) * 16 + (uint32_t)hw * 8;
+  const uint32_t hb = (uint32_t)(hh * E) * 16;
   if (!pl.four) {
     pl.off[0] = row0 + hb + (uint32_t)tx * 16;                    // column 2tx
     pl.off[1] = row0 + hb + (2 * E + (uint32_t)tx + 1) * 16;      // column 2tx + 1
@@ -404,31 +405,11 @@ __device__ __forceinline__ ProdLoad prod_load(const Geo& g, const uint8_t* xr, c
   return pl;
 }
 
-// L2 prefetch of the XR rows (all four tap rows of each tile row, every
-// channel block) that this CTA's half of unit `un` reads, one bulk prefetch
-// per (image, channel block).  The records were written by the pre-pass and
-// mostly left L2 again; the producers, a stage of loads ahead at most, would
-// otherwise wait for device memory.
-__device__ __forceinline__ void prefetch_unit(const Geo& g, const uint8_t* xr, const Unit& un, int rank) {
-  const int per = g.TP * g.TQ;
-  const int t0 = un.tb * 128 + rank * VT;
-  if (t0 >= (int)g.NT) return;
-  const int t1 = min(t0 + VT, (int)g.NT) - 1;
-  const int n0 = t0 / per, n1 = t1 / per;
-  for (int n = n0; n <= n1; ++n) {
-    const int ya = n == n0 ? (t0 - n0 * per) / g.TQ : 0;
-    const int yb = n == n1 ? (t1 - n1 * per) / g.TQ : g.TP - 1;
-    const uint32_t bytes = (uint32_t)(4 * (yb - ya + 1)) * g.RB;
-    for (int cb = 0; cb < g.CS; ++cb)
-      bulk_prefetch_l2(xr + ((size_t)n * g.CS + cb) * g.cbs + (size_t)(4 * ya) * g.RB, bytes);
-  }
+__device__ __forceinline__ uint4 hadd_4(const uint4& a, const uint4& b) {
+  return make_uint4(hadd2(a.x, b.x), hadd2(a.y, b.y), hadd2(a.z, b.z), hadd2(a.w, b.w));
 }
-
-__device__ __forceinline__ uint2 hadd_2(const uint2& a, const uint2& b) {
-  return make_uint2(hadd2(a.x, b.x), hadd2(a.y, b.y));
-}
-__device__ __forceinline__ uint2 hsub_2(const uint2& a, const uint2& b) {
-  return make_uint2(hsub2(a.x, b.x), hsub2(a.y, b.y));
+__device__ __forceinline__ uint4 hsub_4(const uint4& a, const uint4& b) {
+  return make_uint4(hsub2(a.x, b.x), hsub2(a.y, b.y), hsub2(a.z, b.z), hsub2(a.w, b.w));
 }
 
 }  // namespace tp
@@ -602,19 +583,19 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tp::NTHREAD, 1)
       if (lane == 0) mbar_arrive_peer(lead_accempty + ab * 8);
     }
   } else {
-    // ---- V producers.  Warp pw = (tile group tg of 16, channel half hh,
-    // K-step kq of each stage); lane = (tile tl of the group, 8-byte half hw
-    // of each 16-byte word), so a warp's loads of one word cover 16 tiles'
-    // 256 contiguous bytes.  V of (a, 1), (a, 2) is R(col 2tx) + R(2tx + 1)
-    // and R(2tx + 1) - R(2tx); V of (a, b) for b = 0, 3 is R(first column of
-    // b) - R(second), one fp16 rounding each.
+    // ---- V producers: thread = (tile tl of this CTA's 64, channel half hh,
+    // K-step kq of each stage); a warp's loads of one word cover 32 tiles'
+    // consecutive 16-byte entries.  V of (a, 1), (a, 2) is R(col 2tx) +
+    // R(2tx + 1) and R(2tx + 1) - R(2tx); V of (a, b) for b = 0, 3 is R(first
+    // column of b) - R(second), one fp16 rounding each.
     const int pw = warp - WARP_P0;
-    const int tl = (pw & 3) * 16 + (lane >> 1), hw = lane & 1, hh = (pw >> 2) & 1, kq = pw >> 3;
+    const int tl = (pw & 1) * 32 + lane, hh = (pw >> 1) & 1, kq = pw >> 2;
     const uint8_t* xr = static_cast<const uint8_t*>(p.transform_pin);
-    // The load cursor (lu, lj) runs one stage ahead of the consume cursor
-    // (cu, cj); everything a unit needs is worked out when the load cursor
-    // enters it.  The consume side keeps, per unit parity (4 bits each, the
-    // two cursors are at most one unit apart), whether the tile exists and
+    // The load cursor (lu, lj) runs RING - 1 stages ahead of the consume
+    // cursor (cu, cj), the loads of those stages in flight in a register
+    // ring; everything a unit needs is worked out when the load cursor enters
+    // it.  The consume side keeps, per unit index mod 4 (4 bits each; the
+    // cursors are at most RING - 1 units apart), whether the tile exists and
     // whether the pair reads four words.
     int lu = 0, cu = 0, lj = 0, cj = 0;
     uint32_t info = 0;
@@ -623,65 +604,67 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tp::NTHREAD, 1)
     pl.live = false;
     pl.four = false;
     const size_t step_bytes = (size_t)SK * g.cbs;
-    uint2 wa[4], wb[4];
-    auto issue = [&](uint2 (&w)[4]) {
+    uint4 w0[4], w1[4], w2[4], w3[4];
+    auto issue = [&](uint4 (&w)[4]) {
+      if (lu >= sc.cnt) return;
       if (lj == 0) {
-        // one thread keeps the XR rows of the next two units on their way to L2
-        if (pw == 0 && lane == 0) {
-          if (lu == 0 && sc.cnt > 1) prefetch_unit(g, xr, sched_unit(g, sc, 1), rank);
-          if (lu + 2 < sc.cnt) prefetch_unit(g, xr, sched_unit(g, sc, lu + 2), rank);
-        }
-        pl = prod_load(g, xr, sched_unit(g, sc, lu), rank, tl, hh, hw);
+        pl = prod_load(g, xr, sched_unit(g, sc, lu), rank, tl, hh);
         pl.rec += (size_t)kq * g.cbs;
-        const uint32_t sh4 = (uint32_t)(lu & 1) * 4;
+        const uint32_t sh4 = (uint32_t)(lu & 3) * 4;
         info = (info & ~(15u << sh4)) | ((uint32_t)((pl.live ? 1 : 0) | (pl.four ? 2 : 0)) << sh4);
       }
       if (pl.live && lj * SK + kq < g.CS) {
-        w[0] = __ldg(reinterpret_cast<const uint2*>(pl.rec + pl.off[0]));
-        w[1] = __ldg(reinterpret_cast<const uint2*>(pl.rec + pl.off[1]));
+        w[0] = __ldg(reinterpret_cast<const uint4*>(pl.rec + pl.off[0]));
+        w[1] = __ldg(reinterpret_cast<const uint4*>(pl.rec + pl.off[1]));
         if (pl.four) {
-          w[2] = __ldg(reinterpret_cast<const uint2*>(pl.rec + pl.off[2]));
-          w[3] = __ldg(reinterpret_cast<const uint2*>(pl.rec + pl.off[3]));
+          w[2] = __ldg(reinterpret_cast<const uint4*>(pl.rec + pl.off[2]));
+          w[3] = __ldg(reinterpret_cast<const uint4*>(pl.rec + pl.off[3]));
         }
       }
       pl.rec += step_bytes;
       if (++lj == nst) { lj = 0; ++lu; }
     };
     uint32_t it = 0;
-    auto consume = [&](const uint2 (&w)[4]) -> bool {
+    auto consume = [&](const uint4 (&w)[4]) -> bool {
       const int st = it % NSTV;
       if (it >= NSTV &&
           !mbar_wait_warp(&sh.vempty[st], (it / NSTV - 1) & 1, abort_flag, err, ERR_WAIT_EMPTY, SLEEP_NS))
         return false;
-      const uint32_t inf = (info >> ((uint32_t)(cu & 1) * 4)) & 15u;
+      const uint32_t inf = (info >> ((uint32_t)(cu & 3) * 4)) & 15u;
       if ((inf & 1u) && cj * SK + kq < g.CS) {
-        uint2 v0, v1;
+        uint4 v0, v1;
         if (inf & 2u) {
-          v0 = hsub_2(w[0], w[1]);
-          v1 = hsub_2(w[2], w[3]);
+          v0 = hsub_4(w[0], w[1]);
+          v1 = hsub_4(w[2], w[3]);
         } else {
-          v0 = hadd_2(w[0], w[1]);   // b = 1: d1 + d2
-          v1 = hsub_2(w[1], w[0]);   // b = 2: d2 - d1
+          v0 = hadd_4(w[0], w[1]);   // b = 1: d1 + d2
+          v1 = hsub_4(w[1], w[0]);   // b = 2: d2 - d1
         }
         uint8_t* dst = smem + U_BYTES + st * V_STAGE + (kq * 2) * V_TAP + (tl >> 3) * 256 + hh * 128 +
-                       (tl & 7) * 16 + hw * 8;
-        *reinterpret_cast<uint2*>(dst) = v0;
-        *reinterpret_cast<uint2*>(dst + V_TAP) = v1;
+                       (tl & 7) * 16;
+        *reinterpret_cast<uint4*>(dst) = v0;
+        *reinterpret_cast<uint4*>(dst + V_TAP) = v1;
       }
       fence_proxy_async_shared();
       __syncwarp();
       if (lane == 0) mbar_arrive_peer(lead_vfull + st * 8);
       ++it;
       if (++cj == nst) { cj = 0; ++cu; }
-      return true;
+      return cu < sc.cnt && !*abort_flag;
     };
-    if (lu < sc.cnt) issue(wa);
+    static_assert(RING == 4, "the ring below is written out for four slots");
+    issue(w0);
+    issue(w1);
+    issue(w2);
     while (cu < sc.cnt && !*abort_flag) {
-      if (lu < sc.cnt) issue(wb);
-      if (!consume(wa)) break;
-      if (cu >= sc.cnt || *abort_flag) break;
-      if (lu < sc.cnt) issue(wa);
-      if (!consume(wb)) break;
+      issue(w3);
+      if (!consume(w0)) break;
+      issue(w0);
+      if (!consume(w1)) break;
+      issue(w1);
+      if (!consume(w2)) break;
+      issue(w2);
+      if (!consume(w3)) break;
     }
   }
   tc_fence_before();
