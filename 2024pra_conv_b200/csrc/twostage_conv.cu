@@ -1033,19 +1033,24 @@ __global__ void __launch_bounds__(256, 2) twostage_output_kernel(KernelParam p) 
           if (a == 3) z[i][1][b] = z[i][1][b] - v[i];
         }
       }
+      // the first tile's (n, ty, tx), then step along the tile row
+      const int tile0 = tb * 128 + g4;            // tiles < 2^30 (host check)
+      int n = tile0 / per_img;
+      int ty = (tile0 - n * per_img) / TQ;
+      int tx = tile0 - n * per_img - ty * TQ;
 #pragma unroll
       for (int i = 0; i < ot::TT; ++i) {
         if (g4 + i >= ntb) break;
+        if (i > 0 && ++tx == TQ) {
+          tx = 0;
+          if (++ty == TP) { ty = 0; ++n; }
+        }
         float y[4];
 #pragma unroll
         for (int r = 0; r < 2; ++r) {
           y[2 * r + 0] = z[i][r][0] + z[i][r][1] + z[i][r][2];
           y[2 * r + 1] = z[i][r][1] - z[i][r][2] - z[i][r][3];
         }
-        const int tile = tb * 128 + g4 + i;       // tiles < 2^30 (host check)
-        const int n = tile / per_img;
-        const int rr = tile - n * per_img;
-        const int ty = rr / TQ, tx = rr - ty * TQ;
         const int oy = 2 * ty, ox = 2 * tx;
         __half* o = out + (((size_t)n * K + k) * P + oy) * (size_t)Q + ox;
         const bool two_cols = ox + 1 < Q, two_rows = oy + 1 < P;
