@@ -33,6 +33,9 @@ CXX = shutil.which("g++") or "g++"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
                      "-ccbin", CXX, "-I", INCLUDE, "-I", CSRC]
+# Extra nvcc flags for tuning builds (e.g. -DWINO_PAIR_LOAD=__ldcg); the
+# default build uses none.
+NVCC_FLAGS += os.environ.get("WINO_NVCC_EXTRA", "").split()
 CXX_FLAGS = ["-O2", "-fPIC", "-std=c++17", "-I", INCLUDE, "-I", CSRC,
              "-I", os.path.join(CUDA_HOME, "include")]
 

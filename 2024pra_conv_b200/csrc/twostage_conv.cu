@@ -20,12 +20,13 @@
 // (the drop-in ABI's route when M fits mid_result, i.e. even H and W; the
 // extension entry point wino_conv2d_twostage runs slots 2-4 on any shape).
 //
-// M layout (blocked by 128-tile blocks): block tb holds M[t][k][i] for the
-// block's ntb = min(128, tiles - 128 tb) tiles, element
-//   tb * 16 * K * 128 + (t * K + k) * ntb + i,
-// 16 * K * tiles elements in all (no padding).  Rows of a full block are 256
-// bytes, so the GEMM epilogue writes and the output transform reads whole
-// 16- and 8-byte words.
+// M layout (blocked by 128-tile blocks, 16 * K * tiles elements in all, no
+// padding): a full block tb holds M[t][k][i] as [t][i / 8][k][i % 8] at
+// tb * 16 * K * 128, so 8 consecutive tiles of one output channel are one
+// 16-byte word and consecutive channels' words are adjacent; the last,
+// partial block holds [t][k][i] for its ntb tiles.  The GEMM epilogue (lane =
+// output channel) stores, and the output transform (lane = output channel)
+// loads, one contiguous 512-byte run per warp instruction.
 //
 // V is formed with the fused kernel's packed-fp16 operations (rows of B^T d
 // first, then columns; every +- sum of two fp16 values rounded once), so the
@@ -61,6 +62,12 @@
 #include "wino_common.cuh"
 #include "vgen.cuh"
 
+// Load instruction of the tap-pair producers' window words: through L1
+// (ld.global.nc) by default, or cached in L2 only (ld.global.cg).
+#ifndef WINO_PAIR_LOAD
+#define WINO_PAIR_LOAD __ldg
+#endif
+
 namespace wino {
 
 static __device__ uint32_t g_twostage_err;
@@ -93,11 +100,17 @@ __device__ __forceinline__ Geo geo(const KernelParam& p) {
   return g;
 }
 
-// Element offset of M[t][k][tile tb*128 + i] in the blocked layout.
+// Element offset of M[t][k][tile tb*128 + i].  Full blocks interleave by
+// octets of tiles, [t][i / 8][k][i % 8], so the 16 bytes of 8 consecutive
+// tiles of consecutive output channels are consecutive (a warp over 32
+// channels stores or loads one 512-byte run); the last, partial block is
+// [t][k][i] with its ntb tiles.
 __host__ __device__ __forceinline__ size_t m_offset(int tb, int t, int k, int i, int K, long long NT) {
   const long long rem = NT - (long long)tb * 128;
-  const int ntb = rem < 128 ? (int)rem : 128;
-  return (size_t)tb * 16 * (size_t)K * 128 + ((size_t)t * K + k) * (size_t)ntb + i;
+  const size_t base = (size_t)tb * 16 * (size_t)K * 128;
+  if (rem >= 128)
+    return base + ((size_t)t * 16 + (i >> 3)) * (size_t)K * 8 + (size_t)k * 8 + (i & 7);
+  return base + ((size_t)t * K + k) * (size_t)rem + i;
 }
 
 // B^T row / column a of the 4-point transform (the fused kernel's bt_row /
@@ -553,7 +566,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tp::NTHREAD, 1)
       const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + ab * 256;
 #pragma unroll 1
       for (int s = 0; s < 2; ++s) {
-        __half* row = m16 + m_offset(un.tb, t[s], k < g.K ? k : 0, 0, g.K, g.NT);
+        const int kk = k < g.K ? k : 0;
 #pragma unroll 1
         for (int c0 = 0; c0 < 128; c0 += 32) {
           float v[32];
@@ -568,10 +581,12 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tp::NTHREAD, 1)
               const __half2 x = __floats2half2_rn(v[2 * i2], v[2 * i2 + 1]);
               h[i2] = *reinterpret_cast<const uint32_t*>(&x);
             }
-            uint4* dst = reinterpret_cast<uint4*>(row + c0);
 #pragma unroll
-            for (int i2 = 0; i2 < 4; ++i2) dst[i2] = make_uint4(h[4 * i2], h[4 * i2 + 1], h[4 * i2 + 2], h[4 * i2 + 3]);
+            for (int o = 0; o < 4; ++o)
+              *reinterpret_cast<uint4*>(m16 + m_offset(un.tb, t[s], kk, c0 + 8 * o, g.K, g.NT)) =
+                  make_uint4(h[4 * o], h[4 * o + 1], h[4 * o + 2], h[4 * o + 3]);
           } else {
+            __half* row = m16 + m_offset(un.tb, t[s], kk, 0, g.K, g.NT);
 #pragma unroll
             for (int i2 = 0; i2 < 32; ++i2)
               if (c0 + i2 < ntb) row[c0 + i2] = __float2half_rn(v[i2]);
@@ -614,11 +629,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tp::NTHREAD, 1)
         info = (info & ~(15u << sh4)) | ((uint32_t)((pl.live ? 1 : 0) | (pl.four ? 2 : 0)) << sh4);
       }
       if (pl.live && lj * SK + kq < g.CS) {
-        w[0] = __ldg(reinterpret_cast<const uint4*>(pl.rec + pl.off[0]));
-        w[1] = __ldg(reinterpret_cast<const uint4*>(pl.rec + pl.off[1]));
+        w[0] = WINO_PAIR_LOAD(reinterpret_cast<const uint4*>(pl.rec + pl.off[0]));
+        w[1] = WINO_PAIR_LOAD(reinterpret_cast<const uint4*>(pl.rec + pl.off[1]));
         if (pl.four) {
-          w[2] = __ldg(reinterpret_cast<const uint4*>(pl.rec + pl.off[2]));
-          w[3] = __ldg(reinterpret_cast<const uint4*>(pl.rec + pl.off[3]));
+          w[2] = WINO_PAIR_LOAD(reinterpret_cast<const uint4*>(pl.rec + pl.off[2]));
+          w[3] = WINO_PAIR_LOAD(reinterpret_cast<const uint4*>(pl.rec + pl.off[3]));
         }
       }
       pl.rec += step_bytes;
@@ -942,134 +957,95 @@ __global__ void __launch_bounds__(tsk::NTHREAD, 1) twostage_stream_kernel(Kernel
 // =============================================================================
 // Output transform
 // =============================================================================
-// Persistent: work item = (tile block tb, 8 output channels kg), item i =
-// kg * tile blocks + tb, CTA b takes items b, b + grid, ...  An item's 16
-// taps x 8 channels of the blocked M (16 contiguous runs of 8 * ntb fp16)
-// come in by bulk copy into one of three shared-memory buffers, issued as
-// soon as a buffer is free, so two items per CTA are in flight while the
-// third is transformed and the bytes in flight do not depend on registers.
-// Thread = (channel kl, 4 tiles g4 .. g4+3 of the block): it reads its 16
-// taps from shared memory (a warp's 8-byte reads are contiguous),
-// accumulates z = A^T m in fp32 tap by tap in the order of the comparator's
-// output transform (so the result is bit-identical to it), forms y = z A and
-// stores it with one fp16 rounding.  K is a multiple of 16 and mid_result
-// 16-byte aligned, so every copy starts on a 16-byte boundary and moves a
-// multiple of 16 bytes.
+// CTA = (tile block tb, half of its 16 tile octets, 32 output channels);
+// thread = (channel k = lane, octet o = warp): 16 taps x one 16-byte word of
+// M (8 tiles), a warp's loads of one tap one contiguous 512-byte run of the
+// octet-interleaved block.  z = A^T m is accumulated in fp32 tap by tap in
+// the order of the comparator's output transform (so the result is
+// bit-identical to it), then y = z A with one fp16 rounding per output.  The
+// partial last block (plain [t][k][i] layout) is read element by element.
+// grid (2 * tile blocks, ceil(K/32)).
 namespace ot {
-constexpr int KG = 8;                         // output channels per item
-constexpr int TT = 4;                         // tiles per thread
-constexpr int NBUF = 3;
-constexpr int BUF_BYTES = 16 * KG * 128 * 2;  // 32 KB
-constexpr int SMEM_BYTES = NBUF * BUF_BYTES + 128;
+constexpr int TT = 8;                         // tiles per thread (one octet)
 }
 
-__global__ void __launch_bounds__(256, 2) twostage_output_kernel(KernelParam p) {
+__global__ void __launch_bounds__(256) twostage_output_kernel(KernelParam p) {
   using namespace ts;
-  extern __shared__ __align__(128) uint8_t osm[];
-  __shared__ uint64_t full[ot::NBUF];
   const int K = p.k, P = p.Oh, Q = p.Ow;
   const int TP = (P + 1) >> 1, TQ = (Q + 1) >> 1;
   const long long NT = (long long)p.n * TP * TQ;
-  const int nTB = (int)((NT + 127) / 128);
-  const int nitems = nTB * (K / ot::KG);
+  const int tb = blockIdx.x >> 1;
+  const int o = (blockIdx.x & 1) * 8 + (threadIdx.x >> 5);
+  const int k = blockIdx.y * 32 + (threadIdx.x & 31);
+  if (k >= K) return;
+  const long long rem = NT - (long long)tb * 128;
+  const int ntb = rem < 128 ? (int)rem : 128;
+  const int i0 = o * 8;
+  if (i0 >= ntb) return;
   const __half* m16 = static_cast<const __half*>(p.mid_result);
-  if (threadIdx.x == 0) {
-    for (int b = 0; b < ot::NBUF; ++b) mbar_init(&full[b], 1);
-    fence_barrier_init();
+  // z[r][b] = sum_a At[r][a] m[4a+b], accumulated in tap order a = 0..3
+  float z[ot::TT][2][4];
+#pragma unroll
+  for (int t = 0; t < 16; ++t) {
+    const int a = t >> 2, b = t & 3;
+    float v[ot::TT];
+    if (ntb == 128) {
+      const uint4 w = *reinterpret_cast<const uint4*>(m16 + m_offset(tb, t, k, i0, K, NT));
+      const uint32_t h[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&h[i]));
+        v[2 * i] = f.x;
+        v[2 * i + 1] = f.y;
+      }
+    } else {
+      const __half* src = m16 + m_offset(tb, t, k, i0, K, NT);
+#pragma unroll
+      for (int i = 0; i < ot::TT; ++i) v[i] = i0 + i < ntb ? __half2float(src[i]) : 0.f;
+    }
+#pragma unroll
+    for (int i = 0; i < ot::TT; ++i) {
+      if (a == 0) z[i][0][b] = v[i];
+      if (a == 1) { z[i][0][b] = z[i][0][b] + v[i]; z[i][1][b] = v[i]; }
+      if (a == 2) { z[i][0][b] = z[i][0][b] + v[i]; z[i][1][b] = z[i][1][b] - v[i]; }
+      if (a == 3) z[i][1][b] = z[i][1][b] - v[i];
+    }
   }
-  __syncthreads();
-  // issue the copies of `item` into buffer `buf` (warp 0)
-  auto fetch = [&](int item, int buf) {
-    const int tb = item % nTB, k0 = (item / nTB) * ot::KG;
-    const long long rem = NT - (long long)tb * 128;
-    const int ntb = rem < 128 ? (int)rem : 128;
-    const uint32_t run = (uint32_t)(ot::KG * ntb * 2);
-    if (threadIdx.x == 0) mbar_arrive_expect_tx(&full[buf], 16 * run);
-    __syncwarp();
-    if (threadIdx.x < 16)
-      bulk_g2s(osm + buf * ot::BUF_BYTES + threadIdx.x * run,
-               m16 + m_offset(tb, threadIdx.x, k0, 0, K, NT), run, &full[buf]);
-  };
-  if (threadIdx.x < 32)
-    for (int b = 0; b < ot::NBUF; ++b)
-      if ((int)blockIdx.x + b * (int)gridDim.x < nitems) fetch(blockIdx.x + b * gridDim.x, b);
-  const int kl = threadIdx.x >> 5, g4 = (threadIdx.x & 31) * ot::TT;
   const int per_img = TP * TQ;
   const bool pair_ok = (Q & 1) == 0 && (reinterpret_cast<uintptr_t>(p.pout) & 3) == 0;
   __half* out = static_cast<__half*>(p.pout);
-  int j = 0;
-  for (int item = blockIdx.x; item < nitems; item += gridDim.x, ++j) {
-    const int buf = j % ot::NBUF;
-    const int tb = item % nTB, k = (item / nTB) * ot::KG + kl;
-    const long long rem = NT - (long long)tb * 128;
-    const int ntb = rem < 128 ? (int)rem : 128;
-    const uint32_t run = (uint32_t)(ot::KG * ntb * 2);
-    // the copies complete within microseconds; a wait past the bound leaves
-    // the error word set and the rest of the output unwritten
-    if (!mbar_wait(&full[buf], (j / ot::NBUF) & 1, nullptr, &g_twostage_err, ERR_WAIT_FULL)) break;
-    if (g4 < ntb) {
-      const __half* ms = reinterpret_cast<const __half*>(osm + buf * ot::BUF_BYTES);
-      // z[r][b] = sum_a At[r][a] m[4a+b], accumulated in tap order a = 0..3
-      float z[ot::TT][2][4];
+  // the first tile's (n, ty, tx), then step along the tile row
+  const int tile0 = tb * 128 + i0;               // tiles < 2^30 (host check)
+  int n = tile0 / per_img;
+  int ty = (tile0 - n * per_img) / TQ;
+  int tx = tile0 - n * per_img - ty * TQ;
 #pragma unroll
-      for (int t = 0; t < 16; ++t) {
-        const int a = t >> 2, b = t & 3;
-        const __half* src = ms + (size_t)t * (run / 2) + kl * ntb + g4;
-        float v[ot::TT];
-        if (ntb == 128) {
-          const uint2 w = *reinterpret_cast<const uint2*>(src);
-          const float2 f0 = __half22float2(*reinterpret_cast<const __half2*>(&w.x));
-          const float2 f1 = __half22float2(*reinterpret_cast<const __half2*>(&w.y));
-          v[0] = f0.x; v[1] = f0.y; v[2] = f1.x; v[3] = f1.y;
-        } else {
+  for (int i = 0; i < ot::TT; ++i) {
+    if (i0 + i >= ntb) break;
+    if (i > 0 && ++tx == TQ) {
+      tx = 0;
+      if (++ty == TP) { ty = 0; ++n; }
+    }
+    float y[4];
 #pragma unroll
-          for (int i = 0; i < ot::TT; ++i) v[i] = g4 + i < ntb ? __half2float(src[i]) : 0.f;
-        }
-#pragma unroll
-        for (int i = 0; i < ot::TT; ++i) {
-          if (a == 0) z[i][0][b] = v[i];
-          if (a == 1) { z[i][0][b] = z[i][0][b] + v[i]; z[i][1][b] = v[i]; }
-          if (a == 2) { z[i][0][b] = z[i][0][b] + v[i]; z[i][1][b] = z[i][1][b] - v[i]; }
-          if (a == 3) z[i][1][b] = z[i][1][b] - v[i];
-        }
-      }
-      // the first tile's (n, ty, tx), then step along the tile row
-      const int tile0 = tb * 128 + g4;            // tiles < 2^30 (host check)
-      int n = tile0 / per_img;
-      int ty = (tile0 - n * per_img) / TQ;
-      int tx = tile0 - n * per_img - ty * TQ;
-#pragma unroll
-      for (int i = 0; i < ot::TT; ++i) {
-        if (g4 + i >= ntb) break;
-        if (i > 0 && ++tx == TQ) {
-          tx = 0;
-          if (++ty == TP) { ty = 0; ++n; }
-        }
-        float y[4];
-#pragma unroll
-        for (int r = 0; r < 2; ++r) {
-          y[2 * r + 0] = z[i][r][0] + z[i][r][1] + z[i][r][2];
-          y[2 * r + 1] = z[i][r][1] - z[i][r][2] - z[i][r][3];
-        }
-        const int oy = 2 * ty, ox = 2 * tx;
-        __half* o = out + (((size_t)n * K + k) * P + oy) * (size_t)Q + ox;
-        const bool two_cols = ox + 1 < Q, two_rows = oy + 1 < P;
-        if (two_cols && pair_ok) {
-          *reinterpret_cast<__half2*>(o) = __floats2half2_rn(y[0], y[1]);
-          if (two_rows) *reinterpret_cast<__half2*>(o + Q) = __floats2half2_rn(y[2], y[3]);
-        } else {
-          o[0] = __float2half_rn(y[0]);
-          if (two_cols) o[1] = __float2half_rn(y[1]);
-          if (two_rows) {
-            o[Q] = __float2half_rn(y[2]);
-            if (two_cols) o[Q + 1] = __float2half_rn(y[3]);
-          }
-        }
+    for (int r = 0; r < 2; ++r) {
+      y[2 * r + 0] = z[i][r][0] + z[i][r][1] + z[i][r][2];
+      y[2 * r + 1] = z[i][r][1] - z[i][r][2] - z[i][r][3];
+    }
+    const int oy = 2 * ty, ox = 2 * tx;
+    __half* op = out + (((size_t)n * K + k) * P + oy) * (size_t)Q + ox;
+    const bool two_cols = ox + 1 < Q, two_rows = oy + 1 < P;
+    if (two_cols && pair_ok) {
+      *reinterpret_cast<__half2*>(op) = __floats2half2_rn(y[0], y[1]);
+      if (two_rows) *reinterpret_cast<__half2*>(op + Q) = __floats2half2_rn(y[2], y[3]);
+    } else {
+      op[0] = __float2half_rn(y[0]);
+      if (two_cols) op[1] = __float2half_rn(y[1]);
+      if (two_rows) {
+        op[Q] = __float2half_rn(y[2]);
+        if (two_cols) op[Q + 1] = __float2half_rn(y[3]);
       }
     }
-    __syncthreads();   // every thread is done with the buffer
-    const int next = item + ot::NBUF * (int)gridDim.x;
-    if (threadIdx.x < 32 && next < nitems) fetch(next, buf);
   }
 }
 
@@ -1092,12 +1068,9 @@ void* wino_twostage_output_kernel_ptr() { return (void*)twostage_output_kernel; 
 int wino_twostage_threads_for(int c) { return use_pair(c) ? tp::NTHREAD : tsk::NTHREAD; }
 int wino_twostage_smem_bytes_for(int c) { return use_pair(c) ? tp::SMEM_BYTES : tsk::SMEM_BYTES; }
 
-int wino_twostage_output_smem_bytes() { return ot::SMEM_BYTES; }
+int wino_twostage_output_smem_bytes() { return 0; }
 
 int wino_twostage_prepare() {
-  if (cudaFuncSetAttribute(twostage_output_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           ot::SMEM_BYTES) != cudaSuccess)
-    return 1;
   if (cudaFuncSetAttribute(twostage_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            tsk::SMEM_BYTES) != cudaSuccess)
     return 1;
@@ -1161,12 +1134,10 @@ unsigned wino_twostage_gemm_grid(int n, int c, int h, int w, int k, int sms) {
   return (unsigned)(units < sms ? units : sms);
 }
 
-// Output transform grid: two persistent CTAs per SM up to the work items.
 void wino_twostage_output_grid(int n, int h, int w, int k, int sms, unsigned* gx, unsigned* gy) {
-  const long long items = (wino_twostage_tiles(n, h, w) + 127) / 128 * (k / ot::KG);
-  const long long cap = 2LL * sms;
-  *gx = (unsigned)(items < cap ? items : cap);
-  *gy = 1;
+  (void)sms;
+  *gx = (unsigned)(2 * ((wino_twostage_tiles(n, h, w) + 127) / 128));
+  *gy = (unsigned)((k + 31) / 32);
 }
 
 uint32_t wino_twostage_error_read_clear() {
