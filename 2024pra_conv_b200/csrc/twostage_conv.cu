@@ -957,93 +957,110 @@ __global__ void __launch_bounds__(tsk::NTHREAD, 1) twostage_stream_kernel(Kernel
 // =============================================================================
 // Output transform
 // =============================================================================
-// CTA = (tile block tb, half of its 16 tile octets, 32 output channels);
-// thread = (channel k = lane, octet o = warp): 16 taps x one 16-byte word of
-// M (8 tiles), a warp's loads of one tap one contiguous 512-byte run of the
-// octet-interleaved block.  z = A^T m is accumulated in fp32 tap by tap in
-// the order of the comparator's output transform (so the result is
-// bit-identical to it), then y = z A with one fp16 rounding per output.  The
-// partial last block (plain [t][k][i] layout) is read element by element.
-// grid (2 * tile blocks, ceil(K/32)).
+// CTA = (tile block tb, 16 output channels), two phases through shared
+// memory.  Phase 1, thread = (channel k = lane % 16, tile octet o): 16 taps x
+// one 16-byte word of M (8 tiles; two octets' 256-byte runs per warp
+// instruction of the octet-interleaved block), z = A^T m accumulated in fp32
+// tap by tap in the order of the comparator's output transform (so the
+// result is bit-identical to it), y = z A rounded once to fp16, the tile's
+// 2 x 2 outputs to shared memory.  Phase 2, thread = (channel, tile) with
+// consecutive lanes on consecutive tiles: the outputs go to Y in runs along
+// the output rows.  The partial last block (plain [t][k][i] layout) is read
+// element by element.  grid (tile blocks, K/16).
 namespace ot {
-constexpr int TT = 8;                         // tiles per thread (one octet)
+constexpr int TT = 8;                         // tiles per phase-1 thread (one octet)
+constexpr int KG = 16;                        // output channels per CTA
+constexpr int ROW = 128 * 8 + 16;             // bytes per channel of the staged outputs (padded)
 }
 
 __global__ void __launch_bounds__(256) twostage_output_kernel(KernelParam p) {
   using namespace ts;
+  __shared__ __align__(16) uint8_t ys[ot::KG * ot::ROW];
   const int K = p.k, P = p.Oh, Q = p.Ow;
   const int TP = (P + 1) >> 1, TQ = (Q + 1) >> 1;
   const long long NT = (long long)p.n * TP * TQ;
-  const int tb = blockIdx.x >> 1;
-  const int o = (blockIdx.x & 1) * 8 + (threadIdx.x >> 5);
-  const int k = blockIdx.y * 32 + (threadIdx.x & 31);
-  if (k >= K) return;
+  const int tb = blockIdx.x;
+  const int k0 = blockIdx.y * ot::KG;
   const long long rem = NT - (long long)tb * 128;
   const int ntb = rem < 128 ? (int)rem : 128;
-  const int i0 = o * 8;
-  if (i0 >= ntb) return;
   const __half* m16 = static_cast<const __half*>(p.mid_result);
-  // z[r][b] = sum_a At[r][a] m[4a+b], accumulated in tap order a = 0..3
-  float z[ot::TT][2][4];
+  {
+    const int kl = threadIdx.x & 15, o = threadIdx.x >> 4;
+    const int k = k0 + kl, i0 = o * ot::TT;
+    if (i0 < ntb) {
+      // z[r][b] = sum_a At[r][a] m[4a+b], accumulated in tap order a = 0..3
+      float z[ot::TT][2][4];
 #pragma unroll
-  for (int t = 0; t < 16; ++t) {
-    const int a = t >> 2, b = t & 3;
-    float v[ot::TT];
-    if (ntb == 128) {
-      const uint4 w = *reinterpret_cast<const uint4*>(m16 + m_offset(tb, t, k, i0, K, NT));
-      const uint32_t h[4] = {w.x, w.y, w.z, w.w};
+      for (int t = 0; t < 16; ++t) {
+        const int a = t >> 2, b = t & 3;
+        float v[ot::TT];
+        if (ntb == 128) {
+          const uint4 w = *reinterpret_cast<const uint4*>(m16 + m_offset(tb, t, k, i0, K, NT));
+          const uint32_t h[4] = {w.x, w.y, w.z, w.w};
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&h[i]));
-        v[2 * i] = f.x;
-        v[2 * i + 1] = f.y;
+          for (int i = 0; i < 4; ++i) {
+            const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&h[i]));
+            v[2 * i] = f.x;
+            v[2 * i + 1] = f.y;
+          }
+        } else {
+          const __half* src = m16 + m_offset(tb, t, k, i0, K, NT);
+#pragma unroll
+          for (int i = 0; i < ot::TT; ++i) v[i] = i0 + i < ntb ? __half2float(src[i]) : 0.f;
+        }
+#pragma unroll
+        for (int i = 0; i < ot::TT; ++i) {
+          if (a == 0) z[i][0][b] = v[i];
+          if (a == 1) { z[i][0][b] = z[i][0][b] + v[i]; z[i][1][b] = v[i]; }
+          if (a == 2) { z[i][0][b] = z[i][0][b] + v[i]; z[i][1][b] = z[i][1][b] - v[i]; }
+          if (a == 3) z[i][1][b] = z[i][1][b] - v[i];
+        }
       }
-    } else {
-      const __half* src = m16 + m_offset(tb, t, k, i0, K, NT);
+      uint4* dst = reinterpret_cast<uint4*>(ys + kl * ot::ROW + i0 * 8);
 #pragma unroll
-      for (int i = 0; i < ot::TT; ++i) v[i] = i0 + i < ntb ? __half2float(src[i]) : 0.f;
-    }
+      for (int i = 0; i < ot::TT; i += 2) {
+        uint32_t q[4];
 #pragma unroll
-    for (int i = 0; i < ot::TT; ++i) {
-      if (a == 0) z[i][0][b] = v[i];
-      if (a == 1) { z[i][0][b] = z[i][0][b] + v[i]; z[i][1][b] = v[i]; }
-      if (a == 2) { z[i][0][b] = z[i][0][b] + v[i]; z[i][1][b] = z[i][1][b] - v[i]; }
-      if (a == 3) z[i][1][b] = z[i][1][b] - v[i];
+        for (int j = 0; j < 2; ++j) {
+          const float y0 = z[i + j][0][0] + z[i + j][0][1] + z[i + j][0][2];
+          const float y1 = z[i + j][0][1] - z[i + j][0][2] - z[i + j][0][3];
+          const float y2 = z[i + j][1][0] + z[i + j][1][1] + z[i + j][1][2];
+          const float y3 = z[i + j][1][1] - z[i + j][1][2] - z[i + j][1][3];
+          const __half2 r0 = __floats2half2_rn(y0, y1), r1 = __floats2half2_rn(y2, y3);
+          q[2 * j] = *reinterpret_cast<const uint32_t*>(&r0);
+          q[2 * j + 1] = *reinterpret_cast<const uint32_t*>(&r1);
+        }
+        dst[i / 2] = make_uint4(q[0], q[1], q[2], q[3]);
+      }
     }
   }
+  __syncthreads();
   const int per_img = TP * TQ;
   const bool pair_ok = (Q & 1) == 0 && (reinterpret_cast<uintptr_t>(p.pout) & 3) == 0;
   __half* out = static_cast<__half*>(p.pout);
-  // the first tile's (n, ty, tx), then step along the tile row
-  const int tile0 = tb * 128 + i0;               // tiles < 2^30 (host check)
-  int n = tile0 / per_img;
-  int ty = (tile0 - n * per_img) / TQ;
-  int tx = tile0 - n * per_img - ty * TQ;
-#pragma unroll
-  for (int i = 0; i < ot::TT; ++i) {
-    if (i0 + i >= ntb) break;
-    if (i > 0 && ++tx == TQ) {
-      tx = 0;
-      if (++ty == TP) { ty = 0; ++n; }
-    }
-    float y[4];
-#pragma unroll
-    for (int r = 0; r < 2; ++r) {
-      y[2 * r + 0] = z[i][r][0] + z[i][r][1] + z[i][r][2];
-      y[2 * r + 1] = z[i][r][1] - z[i][r][2] - z[i][r][3];
-    }
+#pragma unroll 1
+  for (int idx = threadIdx.x; idx < ot::KG * 128; idx += 256) {
+    const int kl = idx >> 7, i = idx & 127;
+    if (i >= ntb) continue;
+    const int k = k0 + kl;
+    const uint2 yy = *reinterpret_cast<const uint2*>(ys + kl * ot::ROW + i * 8);
+    const int tile = tb * 128 + i;                // tiles < 2^30 (host check)
+    const int n = tile / per_img;
+    const int rr = tile - n * per_img;
+    const int ty = rr / TQ, tx = rr - ty * TQ;
     const int oy = 2 * ty, ox = 2 * tx;
     __half* op = out + (((size_t)n * K + k) * P + oy) * (size_t)Q + ox;
     const bool two_cols = ox + 1 < Q, two_rows = oy + 1 < P;
     if (two_cols && pair_ok) {
-      *reinterpret_cast<__half2*>(op) = __floats2half2_rn(y[0], y[1]);
-      if (two_rows) *reinterpret_cast<__half2*>(op + Q) = __floats2half2_rn(y[2], y[3]);
+      *reinterpret_cast<uint32_t*>(op) = yy.x;
+      if (two_rows) *reinterpret_cast<uint32_t*>(op + Q) = yy.y;
     } else {
-      op[0] = __float2half_rn(y[0]);
-      if (two_cols) op[1] = __float2half_rn(y[1]);
+      const __half* h = reinterpret_cast<const __half*>(&yy);
+      op[0] = h[0];
+      if (two_cols) op[1] = h[1];
       if (two_rows) {
-        op[Q] = __float2half_rn(y[2]);
-        if (two_cols) op[Q + 1] = __float2half_rn(y[3]);
+        op[Q] = h[2];
+        if (two_cols) op[Q + 1] = h[3];
       }
     }
   }
@@ -1136,8 +1153,8 @@ unsigned wino_twostage_gemm_grid(int n, int c, int h, int w, int k, int sms) {
 
 void wino_twostage_output_grid(int n, int h, int w, int k, int sms, unsigned* gx, unsigned* gy) {
   (void)sms;
-  *gx = (unsigned)(2 * ((wino_twostage_tiles(n, h, w) + 127) / 128));
-  *gy = (unsigned)((k + 31) / 32);
+  *gx = (unsigned)((wino_twostage_tiles(n, h, w) + 127) / 128);
+  *gy = (unsigned)(k / ot::KG);
 }
 
 uint32_t wino_twostage_error_read_clear() {
