@@ -957,37 +957,47 @@ __global__ void __launch_bounds__(tsk::NTHREAD, 1) twostage_stream_kernel(Kernel
 // =============================================================================
 // Output transform
 // =============================================================================
-// CTA = (tile block tb, 16 output channels), two phases through shared
-// memory.  Phase 1, thread = (channel k = lane % 16, tile octet o): 16 taps x
-// one 16-byte word of M (8 tiles; two octets' 256-byte runs per warp
-// instruction of the octet-interleaved block), z = A^T m accumulated in fp32
-// tap by tap in the order of the comparator's output transform (so the
-// result is bit-identical to it), y = z A rounded once to fp16, the tile's
-// 2 x 2 outputs to shared memory.  Phase 2, thread = (channel, tile) with
-// consecutive lanes on consecutive tiles: the outputs go to Y in runs along
-// the output rows.  The partial last block (plain [t][k][i] layout) is read
-// element by element.  grid (tile blocks, K/16).
+// CTA = (tile block tb, tile octet pair op: tiles 16 op .. 16 op + 15), all
+// output channels in chunks of 128, two phases through shared memory per
+// chunk.  In the octet-interleaved block the CTA's words of one tap are one
+// contiguous run of 2 x K x 16 bytes.  Phase 1, thread = (channel k = lane +
+// 32 (warp % 4), octet o = op * 2 + warp / 4): 16 taps x one 16-byte word
+// (8 tiles; a warp's loads of one tap one 512-byte run), z = A^T m
+// accumulated in fp32 tap by tap in the order of the comparator's output
+// transform (so the result is bit-identical to it), y = z A rounded once to
+// fp16, each tile's 2 x 2 outputs to shared memory.  Phase 2, thread =
+// (channel, tile) with consecutive lanes on consecutive tiles: the outputs
+// go to Y in runs along the output rows.  The partial last block (plain
+// [t][k][i] layout) is read element by element.  grid (tile blocks, 8).
 namespace ot {
 constexpr int TT = 8;                         // tiles per phase-1 thread (one octet)
-constexpr int KG = 16;                        // output channels per CTA
-constexpr int ROW = 128 * 8 + 16;             // bytes per channel of the staged outputs (padded)
+constexpr int KC = 128;                       // output channels per chunk
+constexpr int ROW = 16 * 8 + 16;              // bytes per channel of the staged outputs (padded)
 }
 
 __global__ void __launch_bounds__(256) twostage_output_kernel(KernelParam p) {
   using namespace ts;
-  __shared__ __align__(16) uint8_t ys[ot::KG * ot::ROW];
+  __shared__ __align__(16) uint8_t ys[ot::KC * ot::ROW];
   const int K = p.k, P = p.Oh, Q = p.Ow;
   const int TP = (P + 1) >> 1, TQ = (Q + 1) >> 1;
   const long long NT = (long long)p.n * TP * TQ;
-  const int tb = blockIdx.x;
-  const int k0 = blockIdx.y * ot::KG;
+  const int tb = blockIdx.x, op = blockIdx.y;
   const long long rem = NT - (long long)tb * 128;
   const int ntb = rem < 128 ? (int)rem : 128;
+  const int t16 = op * 16;                       // first tile of the pair
+  if (t16 >= ntb) return;
   const __half* m16 = static_cast<const __half*>(p.mid_result);
-  {
-    const int kl = threadIdx.x & 15, o = threadIdx.x >> 4;
-    const int k = k0 + kl, i0 = o * ot::TT;
-    if (i0 < ntb) {
+  const int per_img = TP * TQ;
+  const bool pair_ok = (Q & 1) == 0 && (reinterpret_cast<uintptr_t>(p.pout) & 3) == 0;
+  __half* out = static_cast<__half*>(p.pout);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ol = warp >> 2;                      // octet of the pair
+  const int i0 = t16 + ol * ot::TT;              // first tile of this thread's octet
+#pragma unroll 1
+  for (int kc = 0; kc < K; kc += ot::KC) {
+    const int kl = lane + 32 * (warp & 3);
+    const int k = kc + kl;
+    if (k < K && i0 < ntb) {
       // z[r][b] = sum_a At[r][a] m[4a+b], accumulated in tap order a = 0..3
       float z[ot::TT][2][4];
 #pragma unroll
@@ -1016,7 +1026,7 @@ __global__ void __launch_bounds__(256) twostage_output_kernel(KernelParam p) {
           if (a == 3) z[i][1][b] = z[i][1][b] - v[i];
         }
       }
-      uint4* dst = reinterpret_cast<uint4*>(ys + kl * ot::ROW + i0 * 8);
+      uint4* dst = reinterpret_cast<uint4*>(ys + kl * ot::ROW + ol * ot::TT * 8);
 #pragma unroll
       for (int i = 0; i < ot::TT; i += 2) {
         uint32_t q[4];
@@ -1033,36 +1043,34 @@ __global__ void __launch_bounds__(256) twostage_output_kernel(KernelParam p) {
         dst[i / 2] = make_uint4(q[0], q[1], q[2], q[3]);
       }
     }
-  }
-  __syncthreads();
-  const int per_img = TP * TQ;
-  const bool pair_ok = (Q & 1) == 0 && (reinterpret_cast<uintptr_t>(p.pout) & 3) == 0;
-  __half* out = static_cast<__half*>(p.pout);
+    __syncthreads();
 #pragma unroll 1
-  for (int idx = threadIdx.x; idx < ot::KG * 128; idx += 256) {
-    const int kl = idx >> 7, i = idx & 127;
-    if (i >= ntb) continue;
-    const int k = k0 + kl;
-    const uint2 yy = *reinterpret_cast<const uint2*>(ys + kl * ot::ROW + i * 8);
-    const int tile = tb * 128 + i;                // tiles < 2^30 (host check)
-    const int n = tile / per_img;
-    const int rr = tile - n * per_img;
-    const int ty = rr / TQ, tx = rr - ty * TQ;
-    const int oy = 2 * ty, ox = 2 * tx;
-    __half* op = out + (((size_t)n * K + k) * P + oy) * (size_t)Q + ox;
-    const bool two_cols = ox + 1 < Q, two_rows = oy + 1 < P;
-    if (two_cols && pair_ok) {
-      *reinterpret_cast<uint32_t*>(op) = yy.x;
-      if (two_rows) *reinterpret_cast<uint32_t*>(op + Q) = yy.y;
-    } else {
-      const __half* h = reinterpret_cast<const __half*>(&yy);
-      op[0] = h[0];
-      if (two_cols) op[1] = h[1];
-      if (two_rows) {
-        op[Q] = h[2];
-        if (two_cols) op[Q + 1] = h[3];
+    for (int idx = threadIdx.x; idx < ot::KC * 16; idx += 256) {
+      const int kl2 = idx >> 4, i = t16 + (idx & 15);
+      const int k2 = kc + kl2;
+      if (k2 >= K || i >= ntb) continue;
+      const uint2 yy = *reinterpret_cast<const uint2*>(ys + kl2 * ot::ROW + (idx & 15) * 8);
+      const int tile = tb * 128 + i;             // tiles < 2^30 (host check)
+      const int n = tile / per_img;
+      const int rr = tile - n * per_img;
+      const int ty = rr / TQ, tx = rr - ty * TQ;
+      const int oy = 2 * ty, ox = 2 * tx;
+      __half* o = out + (((size_t)n * K + k2) * P + oy) * (size_t)Q + ox;
+      const bool two_cols = ox + 1 < Q, two_rows = oy + 1 < P;
+      if (two_cols && pair_ok) {
+        *reinterpret_cast<uint32_t*>(o) = yy.x;
+        if (two_rows) *reinterpret_cast<uint32_t*>(o + Q) = yy.y;
+      } else {
+        const __half* h = reinterpret_cast<const __half*>(&yy);
+        o[0] = h[0];
+        if (two_cols) o[1] = h[1];
+        if (two_rows) {
+          o[Q] = h[2];
+          if (two_cols) o[Q + 1] = h[3];
+        }
       }
     }
+    __syncthreads();
   }
 }
 
@@ -1153,8 +1161,9 @@ unsigned wino_twostage_gemm_grid(int n, int c, int h, int w, int k, int sms) {
 
 void wino_twostage_output_grid(int n, int h, int w, int k, int sms, unsigned* gx, unsigned* gy) {
   (void)sms;
+  (void)k;
   *gx = (unsigned)((wino_twostage_tiles(n, h, w) + 127) / 128);
-  *gy = (unsigned)(k / ot::KG);
+  *gy = 8;
 }
 
 uint32_t wino_twostage_error_read_clear() {
