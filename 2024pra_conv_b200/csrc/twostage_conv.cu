@@ -20,13 +20,12 @@
 // (the drop-in ABI's route when M fits mid_result, i.e. even H and W; the
 // extension entry point wino_conv2d_twostage runs slots 2-4 on any shape).
 //
-// M layout (blocked by 128-tile blocks, 16 * K * tiles elements in all, no
-// padding): a full block tb holds M[t][k][i] as [t][i / 8][k][i % 8] at
-// tb * 16 * K * 128, so 8 consecutive tiles of one output channel are one
-// 16-byte word and consecutive channels' words are adjacent; the last,
-// partial block holds [t][k][i] for its ntb tiles.  The GEMM epilogue (lane =
-// output channel) stores, and the output transform (lane = output channel)
-// loads, one contiguous 512-byte run per warp instruction.
+// M layout (blocked by 128-tile blocks): block tb holds M[t][k][i] for the
+// block's ntb = min(128, tiles - 128 tb) tiles, element
+//   tb * 16 * K * 128 + (t * K + k) * ntb + i,
+// 16 * K * tiles elements in all (no padding).  Rows of a full block are 256
+// bytes, so the GEMM epilogue writes and the output transform reads whole
+// 16- and 8-byte words.
 //
 // V is formed with the fused kernel's packed-fp16 operations (rows of B^T d
 // first, then columns; every +- sum of two fp16 values rounded once), so the
@@ -100,17 +99,11 @@ __device__ __forceinline__ Geo geo(const KernelParam& p) {
   return g;
 }
 
-// Element offset of M[t][k][tile tb*128 + i].  Full blocks interleave by
-// octets of tiles, [t][i / 8][k][i % 8], so the 16 bytes of 8 consecutive
-// tiles of consecutive output channels are consecutive (a warp over 32
-// channels stores or loads one 512-byte run); the last, partial block is
-// [t][k][i] with its ntb tiles.
+// Element offset of M[t][k][tile tb*128 + i] in the blocked layout.
 __host__ __device__ __forceinline__ size_t m_offset(int tb, int t, int k, int i, int K, long long NT) {
   const long long rem = NT - (long long)tb * 128;
-  const size_t base = (size_t)tb * 16 * (size_t)K * 128;
-  if (rem >= 128)
-    return base + ((size_t)t * 16 + (i >> 3)) * (size_t)K * 8 + (size_t)k * 8 + (i & 7);
-  return base + ((size_t)t * K + k) * (size_t)rem + i;
+  const int ntb = rem < 128 ? (int)rem : 128;
+  return (size_t)tb * 16 * (size_t)K * 128 + ((size_t)t * K + k) * (size_t)ntb + i;
 }
 
 // B^T row / column a of the 4-point transform (the fused kernel's bt_row /
@@ -552,6 +545,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tp::NTHREAD, 1)
     // ---- epilogue: TMEM lane = output channel, columns = the unit's tiles
     const int quarter = warp & 3;
     __half* m16 = static_cast<__half*>(p.mid_result);
+    const bool m_aligned32 = (reinterpret_cast<uintptr_t>(m16) & 31) == 0;
     uint32_t ui = 0;
     for (int i = 0; i < sc.cnt; ++i, ++ui) {
       const Unit un = sched_unit(g, sc, i);
@@ -581,10 +575,17 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(tp::NTHREAD, 1)
               const __half2 x = __floats2half2_rn(v[2 * i2], v[2 * i2 + 1]);
               h[i2] = *reinterpret_cast<const uint32_t*>(&x);
             }
+            // 32 bytes per lane and store, whole sectors (a full block's rows
+            // are 256-byte multiples from a 32-byte aligned mid_result)
+            __half* dst = m16 + m_offset(un.tb, t[s], kk, c0, g.K, g.NT);
+            if (m_aligned32) {
 #pragma unroll
-            for (int o = 0; o < 4; ++o)
-              *reinterpret_cast<uint4*>(m16 + m_offset(un.tb, t[s], kk, c0 + 8 * o, g.K, g.NT)) =
-                  make_uint4(h[4 * o], h[4 * o + 1], h[4 * o + 2], h[4 * o + 3]);
+              for (int o = 0; o < 2; ++o) st_global_v8(dst + 16 * o, h + 8 * o);
+            } else {
+#pragma unroll
+              for (int o = 0; o < 4; ++o)
+                reinterpret_cast<uint4*>(dst)[o] = make_uint4(h[4 * o], h[4 * o + 1], h[4 * o + 2], h[4 * o + 3]);
+            }
           } else {
             __half* row = m16 + m_offset(un.tb, t[s], kk, 0, g.K, g.NT);
 #pragma unroll
@@ -957,66 +958,88 @@ __global__ void __launch_bounds__(tsk::NTHREAD, 1) twostage_stream_kernel(Kernel
 // =============================================================================
 // Output transform
 // =============================================================================
-// CTA = (tile block tb, tile octet pair op: tiles 16 op .. 16 op + 15), all
-// output channels in chunks of 128, two phases through shared memory per
-// chunk.  In the octet-interleaved block the CTA's words of one tap are one
-// contiguous run of 2 x K x 16 bytes.  Phase 1, thread = (channel k = lane +
-// 32 (warp % 4), octet o = op * 2 + warp / 4): 16 taps x one 16-byte word
-// (8 tiles; a warp's loads of one tap one 512-byte run), z = A^T m
-// accumulated in fp32 tap by tap in the order of the comparator's output
-// transform (so the result is bit-identical to it), y = z A rounded once to
-// fp16, each tile's 2 x 2 outputs to shared memory.  Phase 2, thread =
-// (channel, tile) with consecutive lanes on consecutive tiles: the outputs
-// go to Y in runs along the output rows.  The partial last block (plain
-// [t][k][i] layout) is read element by element.  grid (tile blocks, 8).
+// Persistent: work item = (tile block tb, 8 output channels kg), item i =
+// kg * tile blocks + tb, CTA b takes items b, b + grid, ...  An item's 16
+// taps x 8 channels of the blocked M (16 contiguous runs of 8 * ntb fp16)
+// come in by bulk copy into one of three shared-memory buffers, issued as
+// soon as a buffer is free, so two items per CTA are in flight while the
+// third is transformed and the bytes in flight do not depend on registers.
+// Thread = (channel kl, 4 tiles g4 .. g4+3 of the block): it reads its 16
+// taps from shared memory (a warp's 8-byte reads are contiguous),
+// accumulates z = A^T m in fp32 tap by tap in the order of the comparator's
+// output transform (so the result is bit-identical to it), forms y = z A and
+// stores it with one fp16 rounding.  K is a multiple of 16 and mid_result
+// 16-byte aligned, so every copy starts on a 16-byte boundary and moves a
+// multiple of 16 bytes.
 namespace ot {
-constexpr int TT = 8;                         // tiles per phase-1 thread (one octet)
-constexpr int KC = 128;                       // output channels per chunk
-constexpr int ROW = 16 * 8 + 16;              // bytes per channel of the staged outputs (padded)
+constexpr int KG = 8;                         // output channels per item
+constexpr int TT = 4;                         // tiles per thread
+constexpr int NBUF = 3;
+constexpr int BUF_BYTES = 16 * KG * 128 * 2;  // 32 KB
+constexpr int SMEM_BYTES = NBUF * BUF_BYTES + 128;
 }
 
-__global__ void __launch_bounds__(256) twostage_output_kernel(KernelParam p) {
+__global__ void __launch_bounds__(256, 2) twostage_output_kernel(KernelParam p) {
   using namespace ts;
-  __shared__ __align__(16) uint8_t ys[ot::KC * ot::ROW];
+  extern __shared__ __align__(128) uint8_t osm[];
+  __shared__ uint64_t full[ot::NBUF];
   const int K = p.k, P = p.Oh, Q = p.Ow;
   const int TP = (P + 1) >> 1, TQ = (Q + 1) >> 1;
   const long long NT = (long long)p.n * TP * TQ;
-  const int tb = blockIdx.x, op = blockIdx.y;
-  const long long rem = NT - (long long)tb * 128;
-  const int ntb = rem < 128 ? (int)rem : 128;
-  const int t16 = op * 16;                       // first tile of the pair
-  if (t16 >= ntb) return;
+  const int nTB = (int)((NT + 127) / 128);
+  const int nitems = nTB * (K / ot::KG);
   const __half* m16 = static_cast<const __half*>(p.mid_result);
+  if (threadIdx.x == 0) {
+    for (int b = 0; b < ot::NBUF; ++b) mbar_init(&full[b], 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  // issue the copies of `item` into buffer `buf` (warp 0)
+  auto fetch = [&](int item, int buf) {
+    const int tb = item % nTB, k0 = (item / nTB) * ot::KG;
+    const long long rem = NT - (long long)tb * 128;
+    const int ntb = rem < 128 ? (int)rem : 128;
+    const uint32_t run = (uint32_t)(ot::KG * ntb * 2);
+    if (threadIdx.x == 0) mbar_arrive_expect_tx(&full[buf], 16 * run);
+    __syncwarp();
+    if (threadIdx.x < 16)
+      bulk_g2s(osm + buf * ot::BUF_BYTES + threadIdx.x * run,
+               m16 + m_offset(tb, threadIdx.x, k0, 0, K, NT), run, &full[buf]);
+  };
+  if (threadIdx.x < 32)
+    for (int b = 0; b < ot::NBUF; ++b)
+      if ((int)blockIdx.x + b * (int)gridDim.x < nitems) fetch(blockIdx.x + b * gridDim.x, b);
+  const int kl = threadIdx.x >> 5, g4 = (threadIdx.x & 31) * ot::TT;
   const int per_img = TP * TQ;
   const bool pair_ok = (Q & 1) == 0 && (reinterpret_cast<uintptr_t>(p.pout) & 3) == 0;
   __half* out = static_cast<__half*>(p.pout);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int ol = warp >> 2;                      // octet of the pair
-  const int i0 = t16 + ol * ot::TT;              // first tile of this thread's octet
-#pragma unroll 1
-  for (int kc = 0; kc < K; kc += ot::KC) {
-    const int kl = lane + 32 * (warp & 3);
-    const int k = kc + kl;
-    if (k < K && i0 < ntb) {
+  int j = 0;
+  for (int item = blockIdx.x; item < nitems; item += gridDim.x, ++j) {
+    const int buf = j % ot::NBUF;
+    const int tb = item % nTB, k = (item / nTB) * ot::KG + kl;
+    const long long rem = NT - (long long)tb * 128;
+    const int ntb = rem < 128 ? (int)rem : 128;
+    const uint32_t run = (uint32_t)(ot::KG * ntb * 2);
+    // the copies complete within microseconds; a wait past the bound leaves
+    // the error word set and the rest of the output unwritten
+    if (!mbar_wait(&full[buf], (j / ot::NBUF) & 1, nullptr, &g_twostage_err, ERR_WAIT_FULL)) break;
+    if (g4 < ntb) {
+      const __half* ms = reinterpret_cast<const __half*>(osm + buf * ot::BUF_BYTES);
       // z[r][b] = sum_a At[r][a] m[4a+b], accumulated in tap order a = 0..3
       float z[ot::TT][2][4];
 #pragma unroll
       for (int t = 0; t < 16; ++t) {
         const int a = t >> 2, b = t & 3;
+        const __half* src = ms + (size_t)t * (run / 2) + kl * ntb + g4;
         float v[ot::TT];
         if (ntb == 128) {
-          const uint4 w = *reinterpret_cast<const uint4*>(m16 + m_offset(tb, t, k, i0, K, NT));
-          const uint32_t h[4] = {w.x, w.y, w.z, w.w};
-#pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&h[i]));
-            v[2 * i] = f.x;
-            v[2 * i + 1] = f.y;
-          }
+          const uint2 w = *reinterpret_cast<const uint2*>(src);
+          const float2 f0 = __half22float2(*reinterpret_cast<const __half2*>(&w.x));
+          const float2 f1 = __half22float2(*reinterpret_cast<const __half2*>(&w.y));
+          v[0] = f0.x; v[1] = f0.y; v[2] = f1.x; v[3] = f1.y;
         } else {
-          const __half* src = m16 + m_offset(tb, t, k, i0, K, NT);
 #pragma unroll
-          for (int i = 0; i < ot::TT; ++i) v[i] = i0 + i < ntb ? __half2float(src[i]) : 0.f;
+          for (int i = 0; i < ot::TT; ++i) v[i] = g4 + i < ntb ? __half2float(src[i]) : 0.f;
         }
 #pragma unroll
         for (int i = 0; i < ot::TT; ++i) {
@@ -1026,51 +1049,43 @@ __global__ void __launch_bounds__(256) twostage_output_kernel(KernelParam p) {
           if (a == 3) z[i][1][b] = z[i][1][b] - v[i];
         }
       }
-      uint4* dst = reinterpret_cast<uint4*>(ys + kl * ot::ROW + ol * ot::TT * 8);
+      // the first tile's (n, ty, tx), then step along the tile row
+      const int tile0 = tb * 128 + g4;            // tiles < 2^30 (host check)
+      int n = tile0 / per_img;
+      int ty = (tile0 - n * per_img) / TQ;
+      int tx = tile0 - n * per_img - ty * TQ;
 #pragma unroll
-      for (int i = 0; i < ot::TT; i += 2) {
-        uint32_t q[4];
-#pragma unroll
-        for (int j = 0; j < 2; ++j) {
-          const float y0 = z[i + j][0][0] + z[i + j][0][1] + z[i + j][0][2];
-          const float y1 = z[i + j][0][1] - z[i + j][0][2] - z[i + j][0][3];
-          const float y2 = z[i + j][1][0] + z[i + j][1][1] + z[i + j][1][2];
-          const float y3 = z[i + j][1][1] - z[i + j][1][2] - z[i + j][1][3];
-          const __half2 r0 = __floats2half2_rn(y0, y1), r1 = __floats2half2_rn(y2, y3);
-          q[2 * j] = *reinterpret_cast<const uint32_t*>(&r0);
-          q[2 * j + 1] = *reinterpret_cast<const uint32_t*>(&r1);
+      for (int i = 0; i < ot::TT; ++i) {
+        if (g4 + i >= ntb) break;
+        if (i > 0 && ++tx == TQ) {
+          tx = 0;
+          if (++ty == TP) { ty = 0; ++n; }
         }
-        dst[i / 2] = make_uint4(q[0], q[1], q[2], q[3]);
-      }
-    }
-    __syncthreads();
-#pragma unroll 1
-    for (int idx = threadIdx.x; idx < ot::KC * 16; idx += 256) {
-      const int kl2 = idx >> 4, i = t16 + (idx & 15);
-      const int k2 = kc + kl2;
-      if (k2 >= K || i >= ntb) continue;
-      const uint2 yy = *reinterpret_cast<const uint2*>(ys + kl2 * ot::ROW + (idx & 15) * 8);
-      const int tile = tb * 128 + i;             // tiles < 2^30 (host check)
-      const int n = tile / per_img;
-      const int rr = tile - n * per_img;
-      const int ty = rr / TQ, tx = rr - ty * TQ;
-      const int oy = 2 * ty, ox = 2 * tx;
-      __half* o = out + (((size_t)n * K + k2) * P + oy) * (size_t)Q + ox;
-      const bool two_cols = ox + 1 < Q, two_rows = oy + 1 < P;
-      if (two_cols && pair_ok) {
-        *reinterpret_cast<uint32_t*>(o) = yy.x;
-        if (two_rows) *reinterpret_cast<uint32_t*>(o + Q) = yy.y;
-      } else {
-        const __half* h = reinterpret_cast<const __half*>(&yy);
-        o[0] = h[0];
-        if (two_cols) o[1] = h[1];
-        if (two_rows) {
-          o[Q] = h[2];
-          if (two_cols) o[Q + 1] = h[3];
+        float y[4];
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+          y[2 * r + 0] = z[i][r][0] + z[i][r][1] + z[i][r][2];
+          y[2 * r + 1] = z[i][r][1] - z[i][r][2] - z[i][r][3];
+        }
+        const int oy = 2 * ty, ox = 2 * tx;
+        __half* o = out + (((size_t)n * K + k) * P + oy) * (size_t)Q + ox;
+        const bool two_cols = ox + 1 < Q, two_rows = oy + 1 < P;
+        if (two_cols && pair_ok) {
+          *reinterpret_cast<__half2*>(o) = __floats2half2_rn(y[0], y[1]);
+          if (two_rows) *reinterpret_cast<__half2*>(o + Q) = __floats2half2_rn(y[2], y[3]);
+        } else {
+          o[0] = __float2half_rn(y[0]);
+          if (two_cols) o[1] = __float2half_rn(y[1]);
+          if (two_rows) {
+            o[Q] = __float2half_rn(y[2]);
+            if (two_cols) o[Q + 1] = __float2half_rn(y[3]);
+          }
         }
       }
     }
-    __syncthreads();
+    __syncthreads();   // every thread is done with the buffer
+    const int next = item + ot::NBUF * (int)gridDim.x;
+    if (threadIdx.x < 32 && next < nitems) fetch(next, buf);
   }
 }
 
@@ -1093,9 +1108,12 @@ void* wino_twostage_output_kernel_ptr() { return (void*)twostage_output_kernel; 
 int wino_twostage_threads_for(int c) { return use_pair(c) ? tp::NTHREAD : tsk::NTHREAD; }
 int wino_twostage_smem_bytes_for(int c) { return use_pair(c) ? tp::SMEM_BYTES : tsk::SMEM_BYTES; }
 
-int wino_twostage_output_smem_bytes() { return 0; }
+int wino_twostage_output_smem_bytes() { return ot::SMEM_BYTES; }
 
 int wino_twostage_prepare() {
+  if (cudaFuncSetAttribute(twostage_output_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           ot::SMEM_BYTES) != cudaSuccess)
+    return 1;
   if (cudaFuncSetAttribute(twostage_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            tsk::SMEM_BYTES) != cudaSuccess)
     return 1;
@@ -1159,11 +1177,12 @@ unsigned wino_twostage_gemm_grid(int n, int c, int h, int w, int k, int sms) {
   return (unsigned)(units < sms ? units : sms);
 }
 
+// Output transform grid: two persistent CTAs per SM up to the work items.
 void wino_twostage_output_grid(int n, int h, int w, int k, int sms, unsigned* gx, unsigned* gy) {
-  (void)sms;
-  (void)k;
-  *gx = (unsigned)((wino_twostage_tiles(n, h, w) + 127) / 128);
-  *gy = 8;
+  const long long items = (wino_twostage_tiles(n, h, w) + 127) / 128 * (k / ot::KG);
+  const long long cap = 2LL * sms;
+  *gx = (unsigned)(items < cap ? items : cap);
+  *gy = 1;
 }
 
 uint32_t wino_twostage_error_read_clear() {
