@@ -14,8 +14,8 @@
 //
 //   slot 1  dropin_filter_u2_kernel   W -> U2 (unfused GEMM layout), transform_filter
 //   slot 2  xb_layout_kernel          X -> XB, transform_pin
-//   slot 3  twostage_pair_kernel      XB, U2 -> M (blocked, below), mid_result
-//           (twostage_stream_kernel when C > 256)
+//   slot 3  twostage_stream_kernel    XB, U2 -> M (blocked, below), mid_result
+//           (twostage_pair_kernel on XR when C <= WINO_PAIR_MAX_C)
 //   slot 4  twostage_output_kernel    M -> Y
 // (the drop-in ABI's route when M fits mid_result, i.e. even H and W; the
 // extension entry point wino_conv2d_twostage runs slots 2-4 on any shape).
@@ -65,6 +65,15 @@
 // (ld.global.nc) by default, or cached in L2 only (ld.global.cg).
 #ifndef WINO_PAIR_LOAD
 #define WINO_PAIR_LOAD __ldg
+#endif
+
+// Largest C routed to the tap-pair kernel (0: every C takes the streamed-U
+// kernel).  The default build routes none: on N128 C256 H=W28 K256 the
+// streamed-U kernel's pre-pass + GEMM measure 26.8 + 147.6 us against the
+// tap-pair route's 41.0 + 187.6 us.  Tuning builds set
+// -DWINO_PAIR_MAX_C=256 (at most 16 * tp::CS_MAX).
+#ifndef WINO_PAIR_MAX_C
+#define WINO_PAIR_MAX_C 0
 #endif
 
 namespace wino {
@@ -881,16 +890,27 @@ __global__ void __launch_bounds__(tsk::NTHREAD, 1) twostage_stream_kernel(Kernel
       const int i = quarter * 32 + lane;   // tile within the block
       const bool live = (long long)tb * 128 + i < g.NT;
       const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + ab * (KPU * 128);
-      for (int cc = 0; cc < KPU * 128; cc += 16) {
+      // rows of the block are ntb elements apart: one base pointer per unit
+      const long long rem = g.NT - (long long)tb * 128;
+      const int ntb = rem < 128 ? (int)rem : 128;
+      __half* mrow = m16 + m_offset(tb, t, kb * KB2, i, g.K, g.NT);
+      for (int cc = 0; cc < KPU * 128; cc += 32) {
         const int kbi = cc >> 7, c0 = cc & 127;
         if (c0 >= kbs[kbi]) continue;
-        float v[16];
+        // K is a multiple of 16: the second half exists when c0 + 16 < rows
+        const bool two = c0 + 16 < kbs[kbi];
+        float v[32];
         tmem_ld16(taddr + cc, v);
+        if (two) tmem_ld16(taddr + cc + 16, v + 16);
         tmem_ld_wait();
         if (live) {
-          const int k0 = (kb + kbi) * KB2 + c0;
+          __half* dst = mrow + (size_t)cc * ntb;
 #pragma unroll
-          for (int jj = 0; jj < 16; ++jj) m16[m_offset(tb, t, k0 + jj, i, g.K, g.NT)] = __float2half_rn(v[jj]);
+          for (int jj = 0; jj < 16; ++jj) dst[(size_t)jj * ntb] = __float2half_rn(v[jj]);
+          if (two) {
+#pragma unroll
+            for (int jj = 16; jj < 32; ++jj) dst[(size_t)jj * ntb] = __float2half_rn(v[jj]);
+          }
         }
       }
       tc_fence_before();
@@ -1097,7 +1117,8 @@ extern "C" {
 
 // The GEMM kernel for C input channels: the tap-pair kernel keeps U resident
 // for up to 256 channels, the streamed-U kernel takes any C.
-static bool use_pair(int c) { return c <= 16 * tp::CS_MAX; }
+static_assert(WINO_PAIR_MAX_C <= 16 * tp::CS_MAX, "the tap-pair kernel keeps U for at most 256 channels");
+static bool use_pair(int c) { return c <= WINO_PAIR_MAX_C; }
 
 void* wino_twostage_gemm_kernel_ptr_for(int c) {
   return use_pair(c) ? (void*)twostage_pair_kernel : (void*)twostage_stream_kernel;

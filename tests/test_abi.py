@@ -254,10 +254,19 @@ def _xr_bytes(n, c, h, w):
     return n * (c // 16) * 4 * ((h + 1) // 2) * 64 * ((w + 1) // 2 + 1)
 
 
+def _pre_bytes(L, n, c, h, w):
+    """Pre-pass records of the kernel the build routes C to: row-transformed
+    for the tap-pair kernel, channel-blocked for the streamed-U kernel."""
+    if L.wino_twostage_gemm_kernel_ptr_for(c) == L.wino_twostage_pair_kernel_ptr():
+        return _xr_bytes(n, c, h, w)
+    return L.wino_xb_bytes(n, c, h, w)
+
+
 def test_twostage_entry_points_validate_and_size(wino):
-    """Two-stage path: workspace = pre-pass records (row-transformed for
-    C <= 256, channel-blocked above; 256-byte aligned) + 16*K*tiles fp16 of M;
-    argument checks return before any CUDA call."""
+    """Two-stage path: workspace = pre-pass records (row-transformed for the
+    tap-pair kernel, channel-blocked for the streamed-U kernel; 256-byte
+    aligned) + 16*K*tiles fp16 of M; argument checks return before any CUDA
+    call."""
     L = wino.lib()
     d = ctypes.c_void_p(0x10000)
     odd = ctypes.c_void_p(0x10010)
@@ -265,13 +274,15 @@ def test_twostage_entry_points_validate_and_size(wino):
     # N128 C256 H28 K256: 25088 tiles; M = 16*256*25088*2 bytes = the reference's mid_result
     m = 16 * 256 * 25088 * 2
     assert m == 4 * 256 * 28 * 28 * 128 * 2
-    assert L.wino_twostage_workspace_bytes(128, 256, 28, 28, 256) == r256(_xr_bytes(128, 256, 28, 28)) + m
-    # the records fit the reference harness's transform_pin (4*h*h*n*c fp16)
+    assert L.wino_twostage_workspace_bytes(128, 256, 28, 28, 256) == r256(_pre_bytes(L, 128, 256, 28, 28)) + m
+    # either kind of record fits the reference harness's transform_pin (4*h*h*n*c fp16)
     assert _xr_bytes(128, 256, 28, 28) <= 4 * 28 * 28 * 128 * 256 * 2
+    assert L.wino_xb_bytes(128, 256, 28, 28) <= 4 * 28 * 28 * 128 * 256 * 2
     # odd sizes: tiles = n * ceil(h/2) * ceil(w/2)
     assert (L.wino_twostage_workspace_bytes(3, 48, 9, 7, 144)
-            == r256(_xr_bytes(3, 48, 9, 7)) + 16 * 144 * (3 * 5 * 4) * 2)
-    # C > 256: the streamed-U kernel reads the channel-blocked records
+            == r256(_pre_bytes(L, 3, 48, 9, 7)) + 16 * 144 * (3 * 5 * 4) * 2)
+    # C > 256: always the streamed-U kernel on the channel-blocked records
+    assert L.wino_twostage_gemm_kernel_ptr_for(272) == L.wino_twostage_stream_kernel_ptr()
     assert (L.wino_twostage_workspace_bytes(2, 272, 6, 8, 48)
             == r256(L.wino_xb_bytes(2, 272, 6, 8)) + 16 * 48 * (2 * 3 * 4) * 2)
     assert L.wino_twostage_workspace_bytes(1, 24, 8, 8, 16) == 0          # C % 16

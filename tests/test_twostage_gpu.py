@@ -86,8 +86,8 @@ def test_twostage_vs_reference_golden(wino, cuda, oracle_mod, path):
 def test_twostage_matches_unfused_comparator(wino, cuda, oracle_mod, c):
     """Same operands (V formed with the same fp16 operations), the same
     K-step accumulation order and the same rounding points as the unfused
-    comparator: the outputs are bit-identical, on the tap-pair kernel (C = 64)
-    and on the streamed-U kernel (C = 288)."""
+    comparator: the outputs are bit-identical, on the GEMM the build routes
+    C = 64 to and on the streamed-U kernel (C = 288)."""
     import torch
     n, h, w, k = 4, 14, 14, 128
     x16, w16 = oracle_mod.make_inputs(n, c, h, w, k, seed=9, x_dist="relu_normal")
@@ -183,10 +183,14 @@ def _xr_layout_np(x16):
 
 @pytest.mark.parametrize("shape", [(2, 32, 12, 10), (1, 16, 9, 7), (3, 48, 1, 1), (1, 16, 28, 28)])
 def test_twostage_row_prepass_bit_exact(wino, cuda, oracle_mod, shape):
-    """The tap-pair route's pre-pass (stage 0 of conv2d_twostage for
-    C <= 256) writes exactly the NumPy statement of its records."""
+    """The tap-pair route's pre-pass (stage 0 of conv2d_twostage when the
+    build routes C to the tap-pair kernel) writes exactly the NumPy statement
+    of its records."""
     import torch
     n, c, h, w = shape
+    L = wino.lib()
+    if L.wino_twostage_gemm_kernel_ptr_for(c) != L.wino_twostage_pair_kernel_ptr():
+        pytest.skip("this build routes no C to the tap-pair kernel (WINO_PAIR_MAX_C)")
     k = 16
     x16, _ = oracle_mod.make_inputs(n, c, h, w, k, seed=5, x_dist="normal")
     ref = _xr_layout_np(x16)
