@@ -75,6 +75,11 @@
 #ifndef WINO_PAIR_MAX_C
 #define WINO_PAIR_MAX_C 0
 #endif
+// Largest C routed to the resident-U kernel (C above it, and above
+// WINO_PAIR_MAX_C, takes the streamed-U kernel).
+#ifndef WINO_RES_MAX_C
+#define WINO_RES_MAX_C 256
+#endif
 
 namespace wino {
 
@@ -976,6 +981,405 @@ __global__ void __launch_bounds__(tsk::NTHREAD, 1) twostage_stream_kernel(Kernel
 }
 
 // =============================================================================
+// One-tap GEMM with resident U on row-transformed input (C <= 256)
+// =============================================================================
+// The streamed-U kernel's unit (one tap x 128 tiles x two 128-row k-blocks,
+// two M = 128 MMAs per K-step sharing the tile operand), with the two
+// per-unit streams it pays for removed:
+//  - U: each CTA serves one (tap, k pair) "combo" and keeps that combo's U
+//    (both k-blocks, all C: at most 128 KB) in shared memory, loaded once;
+//    the CTAs of a combo take its tile blocks round-robin (j, j + s, ...),
+//    so all combos sweep the tile blocks at the same pace and the input rows
+//    of a tile block are read by its 16 taps from L2 within a short window.
+//  - input words: V of tap (a, b) is one fp16 add / subtract of two XR words
+//    (the row step already applied by the pre-pass), 2 loads per V word
+//    instead of the 4 window words of XB.
+// Each producer thread keeps RING - 1 stages of window loads in flight in a
+// register ring while it stores one.
+namespace trs {
+
+using namespace ts;
+
+constexpr int NSTAGE = 5;
+constexpr int SK = 4;                         // K-steps (16 channels) per stage
+constexpr int KPU = 2;                        // 128-row k-blocks per unit
+constexpr int CS_MAX = 16;                    // resident U holds up to 16 K-steps (C <= 256)
+constexpr int A_STEP = 128 * 16 * 2;          // 4 KB: V of 128 tiles x 16 channels
+constexpr int STAGE_A = SK * A_STEP;          // 16 KB
+// U of the unit's k pair, K-step major: K-step cs holds its 256 k rows (the
+// two k-blocks' row groups back to back) at cs * U_CS, so one N = 256 MMA
+// reads both k-blocks
+constexpr int U_CS = KPU * KB2 * 16 * 2;      // 8 KB
+constexpr int U_BYTES = CS_MAX * U_CS;        // 128 KB
+constexpr int SMEM_BYTES = U_BYTES + NSTAGE * STAGE_A + 1024;
+// warp 0 lane 0 U loads and MMA issue, warps 1-4 epilogue (warp w reads
+// TMEM lanes 32 (w % 4) ..), warps 5-12 V producers
+constexpr int WARP_MMA = 0, WARP_E0 = 1, NWARP_E = 4, WARP_P0 = 5, NWARP_P = 8;
+constexpr int NTHREAD = (WARP_P0 + NWARP_P) * 32;
+constexpr uint32_t SLEEP_NS = 32;
+// producer register ring: stages of window loads held in registers (the
+// loads of RING - 1 stages are in flight while one stage is stored)
+#ifndef WINO_RES_RING
+#define WINO_RES_RING 2
+#endif
+constexpr int RING = WINO_RES_RING;
+static_assert(RING == 2 || RING == 3, "ring of two or three stages");
+
+struct Shared {
+  uint64_t full[NSTAGE], empty[NSTAGE];
+  uint64_t accfull[2], accempty[2];
+  uint64_t ufull, uempty, mmadone;
+  uint32_t tmem_base;
+  int abort_flag;
+};
+
+// Combos: c = t * nKP + kp.  With at least as many CTAs G as combos, combo c
+// gets s = G / ncombo CTAs (one more for the first G % ncombo combos) and its
+// j-th CTA takes the tile blocks j, j + s, ...; with fewer, CTA g takes the
+// combos g, g + G, ... whole, one after another.  Unit indices fit 32 bits
+// (the host bounds the tile count).
+struct Sched {
+  int combo, j, s, G, cnt;
+};
+
+__device__ __forceinline__ Sched make_sched(int ncombo, int nTB, int cl, int G) {
+  Sched sc;
+  sc.G = G;
+  if (G < ncombo) {
+    const int mc = cl < ncombo ? (ncombo - cl + G - 1) / G : 0;
+    sc.combo = cl;
+    sc.j = 0;
+    sc.s = 1;
+    sc.cnt = mc * nTB;
+    return sc;
+  }
+  const int base = G / ncombo, extra = G - base * ncombo;
+  const int big = extra * (base + 1);
+  if (cl < big) {
+    sc.combo = cl / (base + 1);
+    sc.j = cl - sc.combo * (base + 1);
+    sc.s = base + 1;
+  } else {
+    const int r = cl - big;
+    sc.combo = extra + r / base;
+    sc.j = r - (r / base) * base;
+    sc.s = base;
+  }
+  sc.cnt = sc.j < nTB ? (nTB - sc.j + sc.s - 1) / sc.s : 0;
+  return sc;
+}
+
+struct Unit {
+  int combo, t, kp, tb;
+};
+
+__device__ __forceinline__ Unit sched_unit(const Geo& g, const Sched& sc, int i) {
+  Unit x;
+  const int ncombo = 16 * g.nKP;
+  if (sc.G < ncombo) {
+    const int m = i / g.nTB;
+    x.combo = sc.combo + m * sc.G;
+    x.tb = i - m * g.nTB;
+  } else {
+    x.combo = sc.combo;
+    x.tb = sc.j + i * sc.s;
+  }
+  x.t = x.combo / g.nKP;
+  x.kp = x.combo - x.t * g.nKP;
+  return x;
+}
+
+// Producer side of one unit for thread (tile tl, channel half hh): V of tap
+// (a, b) is x op y of the XR words at byte offsets ox, oy of row (ty, a):
+//   b = 0: R(2tx - 1) - R(2tx + 1)    (par 1 entries tx, tx + 1)
+//   b = 1: R(2tx) + R(2tx + 1)        (par 0 entry tx, par 1 entry tx + 1)
+//   b = 2: R(2tx + 1) - R(2tx)
+//   b = 3: R(2tx) - R(2tx + 2)        (par 0 entries tx, tx + 1)
+// (the B^T columns d0 - d2, d1 + d2, d2 - d1, d1 - d3 over the window
+// columns 2tx - 1 ..), one fp16 rounding as in the fused kernel.
+struct Prod {
+  const uint8_t* rec;  // XR of the tile's image, channel block 0
+  uint32_t ox, oy;
+  bool live, add;
+};
+
+__device__ __forceinline__ Prod prod(const Geo& g, const uint8_t* xr, int t, int tb, int tl, int hh) {
+  Prod pr;
+  const int tile = tb * 128 + tl;
+  pr.live = tile < (int)g.NT;
+  int n = 0, ty = 0, tx = 0;
+  if (pr.live) {
+    const int per = g.TP * g.TQ;
+    n = tile / per;
+    const int r = tile - n * per;
+    ty = r / g.TQ;
+    tx = r - ty * g.TQ;
+  }
+  const int a = t >> 2, b = t & 3;
+  const uint32_t E = (uint32_t)g.E;
+  const uint32_t row = (uint32_t)(4 * ty + a) * g.RB + (uint32_t)(hh * E) * 16;
+  const uint32_t p0 = row + (uint32_t)tx * 16, p1 = row + (2 * E + (uint32_t)tx) * 16;
+  switch (b) {
+    case 0: pr.ox = p1; pr.oy = p1 + 16; break;
+    case 1: pr.ox = p0; pr.oy = p1 + 16; break;
+    case 2: pr.ox = p1 + 16; pr.oy = p0; break;
+    default: pr.ox = p0; pr.oy = p0 + 16; break;
+  }
+  pr.add = b == 1;
+  pr.rec = xr + (size_t)n * g.CS * g.cbs;
+  return pr;
+}
+
+}  // namespace trs
+
+__global__ void __launch_bounds__(trs::NTHREAD, 1) twostage_res_kernel(KernelParam p) {
+  using namespace trs;
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  __shared__ Shared sh;
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  Geo g = geo(p);
+  g.cbs = (size_t)xr::rows(p.h) * g.RB;           // XR record blocks
+  const int warp = warp_id(), lane = lane_id();
+  uint32_t* err = &g_twostage_err;
+  const Sched sc = make_sched(16 * g.nKP, g.nTB, (int)blockIdx.x, (int)gridDim.x);
+  const int nst = (g.CS + SK - 1) / SK;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < NSTAGE; ++s) {
+      mbar_init(&sh.full[s], NWARP_P);
+      mbar_init(&sh.empty[s], 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(&sh.accfull[a], 1);
+      mbar_init(&sh.accempty[a], NWARP_E);
+    }
+    mbar_init(&sh.ufull, 1);
+    mbar_init(&sh.uempty, 1);
+    mbar_init(&sh.mmadone, 1);
+    sh.abort_flag = 0;
+    fence_barrier_init();
+  }
+  if (warp == WARP_MMA) { tmem_alloc(&sh.tmem_base, 512); tmem_relinquish(); }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = sh.tmem_base;
+  volatile int* abort_flag = &sh.abort_flag;
+  const uint32_t sbase = smem_u32(smem);
+
+  if (warp == WARP_MMA) {
+    if (lane == 0) {
+      const uint8_t* u2 = static_cast<const uint8_t*>(p.transform_filter);
+      int cur = -1;
+      uint32_t it = 0, nload = 0;
+      bool ok = true;
+      for (int i = 0; ok && i < sc.cnt && !*abort_flag; ++i) {
+        const Unit un = sched_unit(g, sc, i);
+        const int kb = un.kp * KPU;
+        int kbs[KPU];
+#pragma unroll
+        for (int q = 0; q < KPU; ++q) kbs[q] = kb + q < g.nKB2 ? kblock2_rows(kb + q, g.K) : 0;
+        if (un.combo != cur) {
+          if (cur >= 0) {
+            // the old U is free once every MMA issued so far has finished
+            mma_commit(&sh.uempty);
+            if (!mbar_wait(&sh.uempty, (nload - 1) & 1, abort_flag, err, ERR_WAIT_EMPTY)) break;
+          }
+          cur = un.combo;
+          uint32_t bytes = 0;
+#pragma unroll
+          for (int q = 0; q < KPU; ++q) bytes += (uint32_t)(kbs[q] * g.C * 2);
+          mbar_arrive_expect_tx(&sh.ufull, bytes);
+          for (int cs = 0; cs < g.CS; ++cs)
+#pragma unroll
+            for (int q = 0; q < KPU; ++q)
+              if (kbs[q])
+                bulk_g2s(smem + cs * U_CS + q * (KB2 * 32), u2 + u2_piece(un.t, kb + q, cs, g.K, g.C) * 2,
+                         (uint32_t)(kbs[q] * 32), &sh.ufull);
+          if (!mbar_wait(&sh.ufull, nload & 1, abort_flag, err, ERR_WAIT_FULL)) break;
+          ++nload;
+        }
+        // one MMA per K-step: M = 128 tiles, N = the k pair's rows (<= 256)
+        const uint32_t idesc = instr_desc(128, (uint32_t)(kbs[0] + kbs[1]), 0, 0, 0, 0);
+        const int ab = i & 1;
+        if (i >= 2 && !mbar_wait(&sh.accempty[ab], ((i >> 1) - 1) & 1, abort_flag, err, ERR_WAIT_DRAIN)) break;
+        tc_fence_after();
+        const uint32_t d = tmem + ab * (KPU * 128);
+        // descriptors advance by adding the byte step >> 4 to the address field
+        const uint64_t bdesc0 = smem_desc(sbase, 128, 256);
+        for (int j = 0; j < nst; ++j, ++it) {
+          const int st = it % NSTAGE;
+          if (!mbar_wait(&sh.full[st], (it / NSTAGE) & 1, abort_flag, err, ERR_WAIT_FULL)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const int nk = min(SK, g.CS - j * SK);
+          const uint64_t adesc = smem_desc(sbase + U_BYTES + st * STAGE_A, 128, 256);
+          const uint64_t bdesc = bdesc0 + (uint64_t)(j * SK * (U_CS >> 4));
+          if (nk == SK) {
+#pragma unroll
+            for (int kk = 0; kk < SK; ++kk)
+              mma_f16(d, adesc + (uint64_t)(kk * (A_STEP >> 4)), bdesc + (uint64_t)(kk * (U_CS >> 4)), idesc,
+                      (j > 0 || kk > 0) ? 1u : 0u);
+          } else {
+            for (int kk = 0; kk < nk; ++kk)
+              mma_f16(d, adesc + (uint64_t)(kk * (A_STEP >> 4)), bdesc + (uint64_t)(kk * (U_CS >> 4)), idesc,
+                      (j > 0 || kk > 0) ? 1u : 0u);
+          }
+          mma_commit(&sh.empty[st]);
+        }
+        if (ok) mma_commit(&sh.accfull[ab]);
+      }
+      // every MMA issued (also on an abort) has finished before TMEM is freed
+      mma_commit(&sh.mmadone);
+      mbar_wait(&sh.mmadone, 0, nullptr, err, ERR_WAIT_ACCUM);
+    }
+    __syncwarp();
+  } else if (warp < WARP_E0 + NWARP_E) {
+    // epilogue: TMEM lanes 32*quarter .. +31 = tiles of the block
+    const int quarter = warp & 3;
+    __half* m16 = static_cast<__half*>(p.mid_result);
+    for (int ui = 0; ui < sc.cnt; ++ui) {
+      const Unit un = sched_unit(g, sc, ui);
+      const int kb = un.kp * KPU;
+      const int ab = ui & 1;
+      if (!mbar_wait_warp(&sh.accfull[ab], (ui >> 1) & 1, abort_flag, err, ERR_WAIT_ACCUM, SLEEP_NS)) break;
+      tc_fence_after();
+      const int i = quarter * 32 + lane;   // tile within the block
+      const bool live = (long long)un.tb * 128 + i < g.NT;
+      const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + ab * (KPU * 128);
+      const long long rem = g.NT - (long long)un.tb * 128;
+      const int ntb = rem < 128 ? (int)rem : 128;
+      __half* mrow = m16 + m_offset(un.tb, un.t, kb * KB2, i, g.K, g.NT);
+      // the unit's k rows (columns of D): a multiple of 16, at most 256
+      int nrows = 0;
+#pragma unroll
+      for (int q = 0; q < KPU; ++q) nrows += kb + q < g.nKB2 ? kblock2_rows(kb + q, g.K) : 0;
+      // 32-column chunks, the TMEM load of the next chunk in flight while
+      // the current one is converted and stored
+      auto ld = [&](int cc, float* v) {
+        tmem_ld16(taddr + cc, v);
+        if (cc + 16 < nrows) tmem_ld16(taddr + cc + 16, v + 16);
+      };
+      auto st = [&](int cc, const float* v) {
+        if (!live) return;
+        __half* dst = mrow + (size_t)cc * ntb;
+#pragma unroll
+        for (int jj = 0; jj < 16; ++jj) dst[(size_t)jj * ntb] = __float2half_rn(v[jj]);
+        if (cc + 16 < nrows) {
+#pragma unroll
+          for (int jj = 16; jj < 32; ++jj) dst[(size_t)jj * ntb] = __float2half_rn(v[jj]);
+        }
+      };
+      float va[32], vb[32];
+      ld(0, va);
+      tmem_ld_wait();
+      for (int cc = 0; cc < nrows; cc += 64) {
+        if (cc + 32 < nrows) ld(cc + 32, vb);
+        st(cc, va);
+        tmem_ld_wait();
+        if (cc + 32 >= nrows) break;
+        if (cc + 64 < nrows) ld(cc + 64, va);
+        st(cc + 32, vb);
+        tmem_ld_wait();
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&sh.accempty[ab]);
+    }
+  } else {
+    // V producers: thread = (tile tl of the unit's 128-tile block, channel
+    // half hh).  The load cursor (lu, lj) runs up to RING stages ahead of
+    // the consume cursor (cu, cj); the consume side keeps per unit index
+    // mod 4 (2 bits each) whether the tile exists and whether its tap adds.
+    const int pw = warp - WARP_P0;
+    const int tl = (pw & 3) * 32 + lane, hh = pw >> 2;
+    const uint8_t* xr = static_cast<const uint8_t*>(p.transform_pin);
+    int lu = 0, lj = 0, cu = 0, cj = 0;
+    uint32_t info = 0;
+    Prod pr;
+    pr.rec = xr;
+    pr.ox = pr.oy = 0;
+    pr.live = pr.add = false;
+    const size_t step_bytes = (size_t)SK * g.cbs;
+    const uint8_t* rec = xr;
+    uint4 w0[SK][2], w1[SK][2], w2[SK][2];
+    auto issue = [&](uint4 (&w)[SK][2]) {
+      if (lu >= sc.cnt) return;
+      if (lj == 0) {
+        const Unit un = sched_unit(g, sc, lu);
+        pr = prod(g, xr, un.t, un.tb, tl, hh);
+        rec = pr.rec;
+        const uint32_t sh2 = (uint32_t)(lu & 3) * 2;
+        info = (info & ~(3u << sh2)) | ((uint32_t)((pr.live ? 1 : 0) | (pr.add ? 2 : 0)) << sh2);
+      }
+#pragma unroll
+      for (int kk = 0; kk < SK; ++kk) {
+        if (pr.live && lj * SK + kk < g.CS) {
+          const uint8_t* r = rec + (size_t)kk * g.cbs;
+          w[kk][0] = __ldg(reinterpret_cast<const uint4*>(r + pr.ox));
+          w[kk][1] = __ldg(reinterpret_cast<const uint4*>(r + pr.oy));
+        }
+      }
+      rec += step_bytes;
+      if (++lj == nst) { lj = 0; ++lu; }
+    };
+    uint32_t it = 0;
+    auto consume = [&](const uint4 (&w)[SK][2]) -> bool {
+      const int st = it % NSTAGE;
+      if (it >= NSTAGE &&
+          !mbar_wait_warp(&sh.empty[st], (it / NSTAGE - 1) & 1, abort_flag, err, ERR_WAIT_EMPTY, SLEEP_NS))
+        return false;
+      const uint32_t inf = (info >> ((uint32_t)(cu & 3) * 2)) & 3u;
+      uint8_t* adst = smem + U_BYTES + st * STAGE_A + (tl >> 3) * 256 + hh * 128 + (tl & 7) * 16;
+#pragma unroll
+      for (int kk = 0; kk < SK; ++kk) {
+        if (cj * SK + kk < g.CS) {
+          uint4 v = make_uint4(0u, 0u, 0u, 0u);
+          if (inf & 1u) v = (inf & 2u) ? tp::hadd_4(w[kk][0], w[kk][1]) : tp::hsub_4(w[kk][0], w[kk][1]);
+          *reinterpret_cast<uint4*>(adst + kk * A_STEP) = v;
+        }
+      }
+      fence_proxy_async_shared();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&sh.full[st]);
+      ++it;
+      if (++cj == nst) { cj = 0; ++cu; }
+      return cu < sc.cnt && !*abort_flag;
+    };
+    if (sc.cnt > 0) {
+      if constexpr (RING == 3) {
+        issue(w0);
+        issue(w1);
+        while (true) {
+          issue(w2);
+          if (!consume(w0)) break;
+          issue(w0);
+          if (!consume(w1)) break;
+          issue(w1);
+          if (!consume(w2)) break;
+        }
+      } else {
+        issue(w0);
+        while (true) {
+          issue(w1);
+          if (!consume(w0)) break;
+          issue(w0);
+          if (!consume(w1)) break;
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == WARP_MMA) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 512);
+  }
+}
+
+// =============================================================================
 // Output transform
 // =============================================================================
 // Persistent: work item = (tile block tb, 8 output channels kg), item i =
@@ -1118,16 +1522,40 @@ extern "C" {
 // The GEMM kernel for C input channels: the tap-pair kernel keeps U resident
 // for up to 256 channels, the streamed-U kernel takes any C.
 static_assert(WINO_PAIR_MAX_C <= 16 * tp::CS_MAX, "the tap-pair kernel keeps U for at most 256 channels");
-static bool use_pair(int c) { return c <= WINO_PAIR_MAX_C; }
+static_assert(WINO_RES_MAX_C <= 16 * trs::CS_MAX, "the resident-U kernel keeps U for at most 256 channels");
+enum GemmKind { GEMM_STREAM = 0, GEMM_RES = 1, GEMM_PAIR = 2 };
+static GemmKind gemm_kind(int c) {
+  if (c <= WINO_PAIR_MAX_C) return GEMM_PAIR;
+  if (c <= WINO_RES_MAX_C) return GEMM_RES;
+  return GEMM_STREAM;
+}
+static bool use_xr(int c) { return gemm_kind(c) != GEMM_STREAM; }
 
 void* wino_twostage_gemm_kernel_ptr_for(int c) {
-  return use_pair(c) ? (void*)twostage_pair_kernel : (void*)twostage_stream_kernel;
+  switch (gemm_kind(c)) {
+    case GEMM_PAIR: return (void*)twostage_pair_kernel;
+    case GEMM_RES: return (void*)twostage_res_kernel;
+    default: return (void*)twostage_stream_kernel;
+  }
 }
 void* wino_twostage_pair_kernel_ptr() { return (void*)twostage_pair_kernel; }
+void* wino_twostage_res_kernel_ptr() { return (void*)twostage_res_kernel; }
 void* wino_twostage_stream_kernel_ptr() { return (void*)twostage_stream_kernel; }
 void* wino_twostage_output_kernel_ptr() { return (void*)twostage_output_kernel; }
-int wino_twostage_threads_for(int c) { return use_pair(c) ? tp::NTHREAD : tsk::NTHREAD; }
-int wino_twostage_smem_bytes_for(int c) { return use_pair(c) ? tp::SMEM_BYTES : tsk::SMEM_BYTES; }
+int wino_twostage_threads_for(int c) {
+  switch (gemm_kind(c)) {
+    case GEMM_PAIR: return tp::NTHREAD;
+    case GEMM_RES: return trs::NTHREAD;
+    default: return tsk::NTHREAD;
+  }
+}
+int wino_twostage_smem_bytes_for(int c) {
+  switch (gemm_kind(c)) {
+    case GEMM_PAIR: return tp::SMEM_BYTES;
+    case GEMM_RES: return trs::SMEM_BYTES;
+    default: return tsk::SMEM_BYTES;
+  }
+}
 
 int wino_twostage_output_smem_bytes() { return ot::SMEM_BYTES; }
 
@@ -1138,28 +1566,32 @@ int wino_twostage_prepare() {
   if (cudaFuncSetAttribute(twostage_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            tsk::SMEM_BYTES) != cudaSuccess)
     return 1;
+  if (cudaFuncSetAttribute(twostage_res_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           trs::SMEM_BYTES) != cudaSuccess)
+    return 1;
   return (int)cudaFuncSetAttribute(twostage_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    tp::SMEM_BYTES);
 }
 
-// The two-stage pre-pass: row-transformed records (XR) for the tap-pair
-// kernel, channel-blocked records (XB) for the streamed-U kernel.
+// The two-stage pre-pass: row-transformed records (XR) for the resident-U
+// and tap-pair kernels, channel-blocked records (XB) for the streamed-U
+// kernel.
 size_t wino_xb_bytes(int n, int c, int h, int w);
 unsigned wino_xb_layout_grid(int n, int c, int h, int w);
 void* wino_xb_layout_kernel_ptr();
 
 size_t wino_twostage_prepass_bytes(int n, int c, int h, int w) {
-  return use_pair(c) ? xr::bytes(n, c, h, w) : wino_xb_bytes(n, c, h, w);
+  return use_xr(c) ? xr::bytes(n, c, h, w) : wino_xb_bytes(n, c, h, w);
 }
 long long wino_twostage_prepass_items(int n, int c, int h, int w) {
-  const long long rows = use_pair(c) ? xr::rows(h) : xb_rows(h);
+  const long long rows = use_xr(c) ? xr::rows(h) : xb_rows(h);
   return (long long)n * (c >> 4) * rows * xb_entries(w);
 }
 void* wino_twostage_prepass_kernel_ptr_for(int c) {
-  return use_pair(c) ? (void*)xr_layout_kernel : wino_xb_layout_kernel_ptr();
+  return use_xr(c) ? (void*)xr_layout_kernel : wino_xb_layout_kernel_ptr();
 }
 unsigned wino_twostage_prepass_grid(int n, int c, int h, int w) {
-  if (!use_pair(c)) return wino_xb_layout_grid(n, c, h, w);
+  if (!use_xr(c)) return wino_xb_layout_grid(n, c, h, w);
   const long long blocks = (wino_twostage_prepass_items(n, c, h, w) / 4 + 255) / 256;
   const long long cap = 148LL * 64;
   return (unsigned)(blocks < cap ? (blocks > 0 ? blocks : 1) : cap);
@@ -1189,11 +1621,12 @@ size_t wino_twostage_m_offset(int n, int h, int w, int k, int t, int kk, long lo
 unsigned wino_twostage_gemm_grid(int n, int c, int h, int w, int k, int sms) {
   const long long ntb = (wino_twostage_tiles(n, h, w) + 127) / 128;
   const long long nkb = (k + KB2 - 1) / KB2;
-  if (use_pair(c)) {
+  if (gemm_kind(c) == GEMM_PAIR) {
     const long long units = (long long)tp::NPAIR * ntb * ((nkb + 1) / 2);
     const long long clusters = sms / 2;
     return (unsigned)(2 * (units < clusters ? units : clusters));
   }
+  static_assert(tsk::KPU == trs::KPU, "both one-tap kernels take two k-blocks per unit");
   const long long units = 16LL * ntb * ((nkb + tsk::KPU - 1) / tsk::KPU);
   return (unsigned)(units < sms ? units : sms);
 }

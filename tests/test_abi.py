@@ -256,17 +256,19 @@ def _xr_bytes(n, c, h, w):
 
 def _pre_bytes(L, n, c, h, w):
     """Pre-pass records of the kernel the build routes C to: row-transformed
-    for the tap-pair kernel, channel-blocked for the streamed-U kernel."""
-    if L.wino_twostage_gemm_kernel_ptr_for(c) == L.wino_twostage_pair_kernel_ptr():
+    for the resident-U and tap-pair kernels, channel-blocked for the
+    streamed-U kernel."""
+    if L.wino_twostage_gemm_kernel_ptr_for(c) in (L.wino_twostage_pair_kernel_ptr(),
+                                                  L.wino_twostage_res_kernel_ptr()):
         return _xr_bytes(n, c, h, w)
     return L.wino_xb_bytes(n, c, h, w)
 
 
 def test_twostage_entry_points_validate_and_size(wino):
     """Two-stage path: workspace = pre-pass records (row-transformed for the
-    tap-pair kernel, channel-blocked for the streamed-U kernel; 256-byte
-    aligned) + 16*K*tiles fp16 of M; argument checks return before any CUDA
-    call."""
+    resident-U and tap-pair kernels, channel-blocked for the streamed-U
+    kernel; 256-byte aligned) + 16*K*tiles fp16 of M; argument checks return
+    before any CUDA call."""
     L = wino.lib()
     d = ctypes.c_void_p(0x10000)
     odd = ctypes.c_void_p(0x10010)

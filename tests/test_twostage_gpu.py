@@ -160,8 +160,8 @@ def test_dropin_two_stage_route(wino, cuda, oracle_mod, shape):
 
 
 def _xr_layout_np(x16):
-    """NumPy statement of the row-transformed records the tap-pair route's
-    pre-pass writes: XR[n][c/16][ty][a][par][hh][e][8] with
+    """NumPy statement of the row-transformed records the pre-pass of the
+    resident-U and tap-pair kernels writes: XR[n][c/16][ty][a][par][hh][e][8] with
     R_a(ty, x) = fp16(s0 * X(2ty - 1 + i0, x) + s1 * X(2ty - 1 + i1, x)) for
     B^T row a = s0 * d_i0 + s1 * d_i1 (one rounding of the exact two-term
     sum), par 0 entry e = column 2e, par 1 entry e = column 2e - 1, zero
@@ -183,14 +183,15 @@ def _xr_layout_np(x16):
 
 @pytest.mark.parametrize("shape", [(2, 32, 12, 10), (1, 16, 9, 7), (3, 48, 1, 1), (1, 16, 28, 28)])
 def test_twostage_row_prepass_bit_exact(wino, cuda, oracle_mod, shape):
-    """The tap-pair route's pre-pass (stage 0 of conv2d_twostage when the
-    build routes C to the tap-pair kernel) writes exactly the NumPy statement
-    of its records."""
+    """The row-transformed pre-pass (stage 0 of conv2d_twostage when the
+    build routes C to the resident-U or tap-pair kernel) writes exactly the
+    NumPy statement of its records."""
     import torch
     n, c, h, w = shape
     L = wino.lib()
-    if L.wino_twostage_gemm_kernel_ptr_for(c) != L.wino_twostage_pair_kernel_ptr():
-        pytest.skip("this build routes no C to the tap-pair kernel (WINO_PAIR_MAX_C)")
+    if L.wino_twostage_gemm_kernel_ptr_for(c) not in (L.wino_twostage_pair_kernel_ptr(),
+                                                      L.wino_twostage_res_kernel_ptr()):
+        pytest.skip("this build routes C to the streamed-U kernel")
     k = 16
     x16, _ = oracle_mod.make_inputs(n, c, h, w, k, seed=5, x_dist="normal")
     ref = _xr_layout_np(x16)
