@@ -119,6 +119,8 @@ def lib():
             "wino_twostage_gemm_kernel_ptr_for": ([i], vp),
             "wino_twostage_pair_kernel_ptr": ([], vp),
             "wino_twostage_res_kernel_ptr": ([], vp),
+            "wino_twostage_resv_kernel_ptr": ([], vp),
+            "wino_twostage_prepass_bytes": ([i, i, i, i], sz),
             "wino_twostage_stream_kernel_ptr": ([], vp),
             "wino_dropin_filter_u2_kernel_ptr": ([], vp),
             "wino_twostage_output_kernel_ptr": ([], vp),

@@ -433,4 +433,19 @@ __device__ __forceinline__ void fence_proxy_async_shared() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
+// Per-warpgroup register limits (all 128 threads of the warpgroup execute
+// it).  An increase waits until other warpgroups have released enough of
+// the registers the block was launched with, so the limits of all
+// warpgroups must add up to no more than that.
+template <uint32_t N>
+__device__ __forceinline__ void regs_inc() {
+  static_assert(N % 8 == 0 && N >= 24 && N <= 256, "register limit");
+  asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(N));
+}
+template <uint32_t N>
+__device__ __forceinline__ void regs_dec() {
+  static_assert(N % 8 == 0 && N >= 24 && N <= 256, "register limit");
+  asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(N));
+}
+
 }  // namespace wino

@@ -80,6 +80,11 @@
 #ifndef WINO_RES_MAX_C
 #define WINO_RES_MAX_C 256
 #endif
+// Largest C whose resident-U kernel forms V from row-transformed input
+// (XR) in producer warps instead of reading V2 by bulk copy (0: none).
+#ifndef WINO_RES_XR_MAX_C
+#define WINO_RES_XR_MAX_C 0
+#endif
 
 namespace wino {
 
@@ -1000,7 +1005,14 @@ namespace trs {
 
 using namespace ts;
 
-constexpr int NSTAGE = 5;
+#ifndef WINO_RES_NSTAGE
+#define WINO_RES_NSTAGE 5
+#endif
+// Load instruction of the producers' window words (__ldg: through L1).
+#ifndef WINO_RES_LOAD
+#define WINO_RES_LOAD __ldg
+#endif
+constexpr int NSTAGE = WINO_RES_NSTAGE;
 constexpr int SK = 4;                         // K-steps (16 channels) per stage
 constexpr int KPU = 2;                        // 128-row k-blocks per unit
 constexpr int CS_MAX = 16;                    // resident U holds up to 16 K-steps (C <= 256)
@@ -1012,18 +1024,27 @@ constexpr int STAGE_A = SK * A_STEP;          // 16 KB
 constexpr int U_CS = KPU * KB2 * 16 * 2;      // 8 KB
 constexpr int U_BYTES = CS_MAX * U_CS;        // 128 KB
 constexpr int SMEM_BYTES = U_BYTES + NSTAGE * STAGE_A + 1024;
-// warp 0 lane 0 U loads and MMA issue, warps 1-4 epilogue (warp w reads
-// TMEM lanes 32 (w % 4) ..), warps 5-12 V producers
-constexpr int WARP_MMA = 0, WARP_E0 = 1, NWARP_E = 4, WARP_P0 = 5, NWARP_P = 8;
+// Four warpgroups: warps 0-3 epilogue (warp w reads TMEM lanes 32 w ..),
+// warp 4 lane 0 U loads and MMA issue (warps 5-7 idle), warps 8-15 V
+// producers.  The block launches with 128 registers a thread (512 threads,
+// the whole register file); the epilogue and MMA warpgroups then give
+// registers up to the producers, whose window-load ring they hold:
+// 128 x 104 + 128 x 56 + 256 x 176 = 65536.
+constexpr int WARP_E0 = 0, NWARP_E = 4, WARP_MMA = 4, WARP_LOAD = 5, WARP_P0 = 8, NWARP_P = 8;
 constexpr int NTHREAD = (WARP_P0 + NWARP_P) * 32;
+constexpr int NTHREAD_V = WARP_P0 * 32;       // bulk-copy-fed variant: no producer warps
+constexpr int REGS_LAUNCH = 128, REGS_EPI = 104, REGS_MMA = 56, REGS_PROD = 176;
+static_assert(128 * REGS_EPI + 128 * REGS_MMA + 256 * REGS_PROD == NTHREAD * REGS_LAUNCH,
+              "the warpgroups' register limits add up to the launch allocation");
+static_assert(NTHREAD * REGS_LAUNCH == 65536, "the block holds the whole register file");
 constexpr uint32_t SLEEP_NS = 32;
 // producer register ring: stages of window loads held in registers (the
 // loads of RING - 1 stages are in flight while one stage is stored)
 #ifndef WINO_RES_RING
-#define WINO_RES_RING 2
+#define WINO_RES_RING 4
 #endif
 constexpr int RING = WINO_RES_RING;
-static_assert(RING == 2 || RING == 3, "ring of two or three stages");
+static_assert(RING >= 2 && RING <= 4, "ring of two to four stages");
 
 struct Shared {
   uint64_t full[NSTAGE], empty[NSTAGE];
@@ -1132,7 +1153,12 @@ __device__ __forceinline__ Prod prod(const Geo& g, const uint8_t* xr, int t, int
 
 }  // namespace trs
 
-__global__ void __launch_bounds__(trs::NTHREAD, 1) twostage_res_kernel(KernelParam p) {
+// TMAV false: V formed by the producer warps from XR (transform_pin).
+// TMAV true: V read by bulk copy from the transformed tiles V2 in
+// transform_pin (v2_layout_kernel); warp 5 lane 0 issues the copies and no
+// producer warps run.
+template <bool TMAV>
+__global__ void __launch_bounds__(TMAV ? trs::NTHREAD_V : trs::NTHREAD, 1) twostage_res_kernel_t(KernelParam p) {
   using namespace trs;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   __shared__ Shared sh;
@@ -1146,7 +1172,7 @@ __global__ void __launch_bounds__(trs::NTHREAD, 1) twostage_res_kernel(KernelPar
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < NSTAGE; ++s) {
-      mbar_init(&sh.full[s], NWARP_P);
+      mbar_init(&sh.full[s], TMAV ? 1 : NWARP_P);
       mbar_init(&sh.empty[s], 1);
     }
     for (int a = 0; a < 2; ++a) {
@@ -1166,9 +1192,48 @@ __global__ void __launch_bounds__(trs::NTHREAD, 1) twostage_res_kernel(KernelPar
   const uint32_t tmem = sh.tmem_base;
   volatile int* abort_flag = &sh.abort_flag;
   const uint32_t sbase = smem_u32(smem);
-
-  if (warp == WARP_MMA) {
-    if (lane == 0) {
+  // each role sets its warpgroup's register limit first thing in its branch
+  if (warp >= WARP_MMA && warp < WARP_P0) {
+    if constexpr (!TMAV) regs_dec<REGS_MMA>();
+    if (TMAV && warp == WARP_LOAD && lane == 0) {
+      // V2 loader: stage j of a unit is K-steps j*SK .. of the unit's tile
+      // block and tap; a full block's pieces (4 KB each) are contiguous, a
+      // partial block's pieces (rows * 32 bytes) go one by one to their
+      // 4 KB slots
+      const uint8_t* v2 = static_cast<const uint8_t*>(p.transform_pin);
+      const int NT8 = ((int)g.NT + 7) & ~7;
+      uint32_t it = 0;
+      for (int i = 0; i < sc.cnt && !*abort_flag; ++i) {
+        const Unit un = sched_unit(g, sc, i);
+        const int rows = min(128, NT8 - un.tb * 128);
+        const uint8_t* src = v2 + ((size_t)un.t * NT8 + (size_t)un.tb * 128) * g.C * 2;
+        bool ok = true;
+        for (int j = 0; j < nst; ++j, ++it) {
+          const int st = it % NSTAGE;
+          if (it >= NSTAGE &&
+              !mbar_wait(&sh.empty[st], (it / NSTAGE - 1) & 1, abort_flag, err, ERR_WAIT_EMPTY)) {
+            ok = false;
+            break;
+          }
+          const int nk = min(SK, g.CS - j * SK);
+          const uint32_t piece = (uint32_t)(rows * 32);
+          mbar_arrive_expect_tx(&sh.full[st], (uint32_t)nk * piece);
+          uint8_t* dst = smem + U_BYTES + st * STAGE_A;
+          const uint8_t* sp = src + (size_t)j * SK * piece;
+          if (rows == 128) {
+            bulk_g2s(dst, sp, (uint32_t)nk * piece, &sh.full[st]);
+          } else {
+            for (int kk = 0; kk < nk; ++kk) bulk_g2s(dst + kk * A_STEP, sp + (size_t)kk * piece, piece, &sh.full[st]);
+          }
+        }
+        if (!ok) break;
+      }
+      // copies still in flight land before the CTA leaves (on an abort the
+      // MMA side may not have waited for them)
+      for (uint32_t s2 = it > (uint32_t)NSTAGE ? it - NSTAGE : 0; s2 < it; ++s2)
+        mbar_wait(&sh.full[s2 % NSTAGE], (s2 / NSTAGE) & 1, nullptr, err, ERR_WAIT_FULL);
+    }
+    if (warp == WARP_MMA && lane == 0) {
       const uint8_t* u2 = static_cast<const uint8_t*>(p.transform_filter);
       int cur = -1;
       uint32_t it = 0, nload = 0;
@@ -1199,8 +1264,9 @@ __global__ void __launch_bounds__(trs::NTHREAD, 1) twostage_res_kernel(KernelPar
           if (!mbar_wait(&sh.ufull, nload & 1, abort_flag, err, ERR_WAIT_FULL)) break;
           ++nload;
         }
-        // one MMA per K-step: M = 128 tiles, N = the k pair's rows (<= 256)
-        const uint32_t idesc = instr_desc(128, (uint32_t)(kbs[0] + kbs[1]), 0, 0, 0, 0);
+        // one MMA per K-step: M = 128 tiles, N = the k pair's rows (<= 256);
+        // V2 is tile-major (MN-major A), the producers' V channel-major
+        const uint32_t idesc = instr_desc(128, (uint32_t)(kbs[0] + kbs[1]), 0, 0, TMAV ? 1 : 0, 0);
         const int ab = i & 1;
         if (i >= 2 && !mbar_wait(&sh.accempty[ab], ((i >> 1) - 1) & 1, abort_flag, err, ERR_WAIT_DRAIN)) break;
         tc_fence_after();
@@ -1237,6 +1303,7 @@ __global__ void __launch_bounds__(trs::NTHREAD, 1) twostage_res_kernel(KernelPar
     }
     __syncwarp();
   } else if (warp < WARP_E0 + NWARP_E) {
+    if constexpr (!TMAV) regs_dec<REGS_EPI>();
     // epilogue: TMEM lanes 32*quarter .. +31 = tiles of the block
     const int quarter = warp & 3;
     __half* m16 = static_cast<__half*>(p.mid_result);
@@ -1288,11 +1355,12 @@ __global__ void __launch_bounds__(trs::NTHREAD, 1) twostage_res_kernel(KernelPar
       __syncwarp();
       if (lane == 0) mbar_arrive(&sh.accempty[ab]);
     }
-  } else {
+  } else if constexpr (!TMAV) {
+    regs_inc<REGS_PROD>();
     // V producers: thread = (tile tl of the unit's 128-tile block, channel
     // half hh).  The load cursor (lu, lj) runs up to RING stages ahead of
     // the consume cursor (cu, cj); the consume side keeps per unit index
-    // mod 4 (2 bits each) whether the tile exists and whether its tap adds.
+    // mod 8 (2 bits each) whether the tile exists and whether its tap adds.
     const int pw = warp - WARP_P0;
     const int tl = (pw & 3) * 32 + lane, hh = pw >> 2;
     const uint8_t* xr = static_cast<const uint8_t*>(p.transform_pin);
@@ -1304,22 +1372,22 @@ __global__ void __launch_bounds__(trs::NTHREAD, 1) twostage_res_kernel(KernelPar
     pr.live = pr.add = false;
     const size_t step_bytes = (size_t)SK * g.cbs;
     const uint8_t* rec = xr;
-    uint4 w0[SK][2], w1[SK][2], w2[SK][2];
+    uint4 w0[SK][2], w1[SK][2], w2[SK][2], w3[SK][2];
     auto issue = [&](uint4 (&w)[SK][2]) {
       if (lu >= sc.cnt) return;
       if (lj == 0) {
         const Unit un = sched_unit(g, sc, lu);
         pr = prod(g, xr, un.t, un.tb, tl, hh);
         rec = pr.rec;
-        const uint32_t sh2 = (uint32_t)(lu & 3) * 2;
+        const uint32_t sh2 = (uint32_t)(lu & 7) * 2;
         info = (info & ~(3u << sh2)) | ((uint32_t)((pr.live ? 1 : 0) | (pr.add ? 2 : 0)) << sh2);
       }
 #pragma unroll
       for (int kk = 0; kk < SK; ++kk) {
         if (pr.live && lj * SK + kk < g.CS) {
           const uint8_t* r = rec + (size_t)kk * g.cbs;
-          w[kk][0] = __ldg(reinterpret_cast<const uint4*>(r + pr.ox));
-          w[kk][1] = __ldg(reinterpret_cast<const uint4*>(r + pr.oy));
+          w[kk][0] = WINO_RES_LOAD(reinterpret_cast<const uint4*>(r + pr.ox));
+          w[kk][1] = WINO_RES_LOAD(reinterpret_cast<const uint4*>(r + pr.oy));
         }
       }
       rec += step_bytes;
@@ -1331,7 +1399,7 @@ __global__ void __launch_bounds__(trs::NTHREAD, 1) twostage_res_kernel(KernelPar
       if (it >= NSTAGE &&
           !mbar_wait_warp(&sh.empty[st], (it / NSTAGE - 1) & 1, abort_flag, err, ERR_WAIT_EMPTY, SLEEP_NS))
         return false;
-      const uint32_t inf = (info >> ((uint32_t)(cu & 3) * 2)) & 3u;
+      const uint32_t inf = (info >> ((uint32_t)(cu & 7) * 2)) & 3u;
       uint8_t* adst = smem + U_BYTES + st * STAGE_A + (tl >> 3) * 256 + hh * 128 + (tl & 7) * 16;
 #pragma unroll
       for (int kk = 0; kk < SK; ++kk) {
@@ -1349,7 +1417,21 @@ __global__ void __launch_bounds__(trs::NTHREAD, 1) twostage_res_kernel(KernelPar
       return cu < sc.cnt && !*abort_flag;
     };
     if (sc.cnt > 0) {
-      if constexpr (RING == 3) {
+      if constexpr (RING == 4) {
+        issue(w0);
+        issue(w1);
+        issue(w2);
+        while (true) {
+          issue(w3);
+          if (!consume(w0)) break;
+          issue(w0);
+          if (!consume(w1)) break;
+          issue(w1);
+          if (!consume(w2)) break;
+          issue(w2);
+          if (!consume(w3)) break;
+        }
+      } else if constexpr (RING == 3) {
         issue(w0);
         issue(w1);
         while (true) {
@@ -1376,6 +1458,41 @@ __global__ void __launch_bounds__(trs::NTHREAD, 1) twostage_res_kernel(KernelPar
   if (warp == WARP_MMA) {
     tc_fence_after();
     tmem_dealloc(tmem, 512);
+  }
+}
+
+// =============================================================================
+// Transformed input tiles V2 (pre-pass of the bulk-copy-fed GEMM)
+// =============================================================================
+// V2 holds V[t][tile][c] in tile blocks of 128 tiles, without padding beyond
+// the tile count rounded up to 8 (NT8): block tb of tap t starts at element
+// (t * NT8 + 128 tb) * C, its K-step cs at + cs * rows * 16 (rows =
+// min(128, NT8 - 128 tb)); inside a K-step the MN-major core-matrix
+// interleave puts tile i, channel c at byte (i >> 3) * 256 + (c >> 3) * 128
+// + (c & 7) * 16 + (i & 7) * 2.  16 * NT8 * C fp16 in all: the reference's
+// transform_pin holds exactly V for even H = W and tiles a multiple of 8.
+// Values as the unfused comparator's input transform (produce_v8: B^T rows
+// on column pairs, then columns; every +- sum rounded once in fp16), which
+// the reference computes at src/preprocessing.cuh:273-424.  Item = (tile
+// block, K-step); thread = (8-tile group, channel); grid-stride over items.
+__global__ void __launch_bounds__(256) v2_layout_kernel(KernelParam p) {
+  const Geometry g = make_geometry(p, TB2);
+  const int NT8 = ((int)g.NT + 7) & ~7;
+  const int items = g.nTB * g.CS;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int grp = 2 * warp + (lane >> 4), cl = lane & 15;
+  uint8_t* v2 = static_cast<uint8_t*>(p.transform_pin);
+  const size_t inner = (size_t)grp * 256 + (cl >> 3) * 128 + (cl & 7) * 16;
+  for (int item = blockIdx.x; item < items; item += gridDim.x) {
+    const int tb = item / g.CS, cs = item - tb * g.CS;
+    const int rows = min(128, NT8 - tb * 128);
+    if (grp * 8 >= rows) continue;
+    uint8_t* base = v2 + (((size_t)tb * 128) * g.C + (size_t)cs * rows * 16) * 2 + inner;
+    const size_t tap_bytes = (size_t)NT8 * g.C * 2;
+    produce_v8(static_cast<const __half*>(p.pin), g, (long long)tb * 128 + grp * 8, cs * 16 + cl, -1,
+               [&](int t, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+                 *reinterpret_cast<uint4*>(base + (size_t)t * tap_bytes) = make_uint4(a, b, c, d);
+               });
   }
 }
 
@@ -1523,36 +1640,43 @@ extern "C" {
 // for up to 256 channels, the streamed-U kernel takes any C.
 static_assert(WINO_PAIR_MAX_C <= 16 * tp::CS_MAX, "the tap-pair kernel keeps U for at most 256 channels");
 static_assert(WINO_RES_MAX_C <= 16 * trs::CS_MAX, "the resident-U kernel keeps U for at most 256 channels");
-enum GemmKind { GEMM_STREAM = 0, GEMM_RES = 1, GEMM_PAIR = 2 };
+enum GemmKind { GEMM_STREAM = 0, GEMM_RES = 1, GEMM_PAIR = 2, GEMM_RESV = 3 };
 static GemmKind gemm_kind(int c) {
   if (c <= WINO_PAIR_MAX_C) return GEMM_PAIR;
-  if (c <= WINO_RES_MAX_C) return GEMM_RES;
+  if (c <= WINO_RES_XR_MAX_C) return GEMM_RES;
+  if (c <= WINO_RES_MAX_C) return GEMM_RESV;
   return GEMM_STREAM;
 }
-static bool use_xr(int c) { return gemm_kind(c) != GEMM_STREAM; }
+static bool use_xr(int c) { return gemm_kind(c) == GEMM_RES || gemm_kind(c) == GEMM_PAIR; }
+static bool use_v2(int c) { return gemm_kind(c) == GEMM_RESV; }
+static long long tiles8(int n, int h, int w) { return ((long long)n * ((h + 1) / 2) * ((w + 1) / 2) + 7) / 8 * 8; }
 
 void* wino_twostage_gemm_kernel_ptr_for(int c) {
   switch (gemm_kind(c)) {
     case GEMM_PAIR: return (void*)twostage_pair_kernel;
-    case GEMM_RES: return (void*)twostage_res_kernel;
+    case GEMM_RES: return (void*)twostage_res_kernel_t<false>;
+    case GEMM_RESV: return (void*)twostage_res_kernel_t<true>;
     default: return (void*)twostage_stream_kernel;
   }
 }
 void* wino_twostage_pair_kernel_ptr() { return (void*)twostage_pair_kernel; }
-void* wino_twostage_res_kernel_ptr() { return (void*)twostage_res_kernel; }
+void* wino_twostage_res_kernel_ptr() { return (void*)twostage_res_kernel_t<false>; }
+void* wino_twostage_resv_kernel_ptr() { return (void*)twostage_res_kernel_t<true>; }
 void* wino_twostage_stream_kernel_ptr() { return (void*)twostage_stream_kernel; }
 void* wino_twostage_output_kernel_ptr() { return (void*)twostage_output_kernel; }
 int wino_twostage_threads_for(int c) {
   switch (gemm_kind(c)) {
     case GEMM_PAIR: return tp::NTHREAD;
     case GEMM_RES: return trs::NTHREAD;
+    case GEMM_RESV: return trs::NTHREAD_V;
     default: return tsk::NTHREAD;
   }
 }
 int wino_twostage_smem_bytes_for(int c) {
   switch (gemm_kind(c)) {
     case GEMM_PAIR: return tp::SMEM_BYTES;
-    case GEMM_RES: return trs::SMEM_BYTES;
+    case GEMM_RES:
+    case GEMM_RESV: return trs::SMEM_BYTES;
     default: return tsk::SMEM_BYTES;
   }
 }
@@ -1566,8 +1690,15 @@ int wino_twostage_prepare() {
   if (cudaFuncSetAttribute(twostage_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            tsk::SMEM_BYTES) != cudaSuccess)
     return 1;
-  if (cudaFuncSetAttribute(twostage_res_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  if (cudaFuncSetAttribute(twostage_res_kernel_t<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           trs::SMEM_BYTES) != cudaSuccess ||
+      cudaFuncSetAttribute(twostage_res_kernel_t<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            trs::SMEM_BYTES) != cudaSuccess)
+    return 1;
+  // the resident-U kernel's warpgroups split exactly the registers it is
+  // launched with; any other launch count would leave an increase waiting
+  cudaFuncAttributes fa{};
+  if (cudaFuncGetAttributes(&fa, twostage_res_kernel_t<false>) != cudaSuccess || fa.numRegs != trs::REGS_LAUNCH)
     return 1;
   return (int)cudaFuncSetAttribute(twostage_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    tp::SMEM_BYTES);
@@ -1581,16 +1712,24 @@ unsigned wino_xb_layout_grid(int n, int c, int h, int w);
 void* wino_xb_layout_kernel_ptr();
 
 size_t wino_twostage_prepass_bytes(int n, int c, int h, int w) {
+  if (use_v2(c)) return (size_t)16 * (size_t)tiles8(n, h, w) * (size_t)c * 2;
   return use_xr(c) ? xr::bytes(n, c, h, w) : wino_xb_bytes(n, c, h, w);
 }
 long long wino_twostage_prepass_items(int n, int c, int h, int w) {
+  if (use_v2(c)) return (tiles8(n, h, w) + 127) / 128 * (c >> 4);
   const long long rows = use_xr(c) ? xr::rows(h) : xb_rows(h);
   return (long long)n * (c >> 4) * rows * xb_entries(w);
 }
 void* wino_twostage_prepass_kernel_ptr_for(int c) {
+  if (use_v2(c)) return (void*)v2_layout_kernel;
   return use_xr(c) ? (void*)xr_layout_kernel : wino_xb_layout_kernel_ptr();
 }
 unsigned wino_twostage_prepass_grid(int n, int c, int h, int w) {
+  if (use_v2(c)) {
+    const long long items = wino_twostage_prepass_items(n, c, h, w);
+    const long long cap = 148LL * 16;
+    return (unsigned)(items < cap ? (items > 0 ? items : 1) : cap);
+  }
   if (!use_xr(c)) return wino_xb_layout_grid(n, c, h, w);
   const long long blocks = (wino_twostage_prepass_items(n, c, h, w) / 4 + 255) / 256;
   const long long cap = 148LL * 64;

@@ -255,11 +255,15 @@ def _xr_bytes(n, c, h, w):
 
 
 def _pre_bytes(L, n, c, h, w):
-    """Pre-pass records of the kernel the build routes C to: row-transformed
-    for the resident-U and tap-pair kernels, channel-blocked for the
-    streamed-U kernel."""
-    if L.wino_twostage_gemm_kernel_ptr_for(c) in (L.wino_twostage_pair_kernel_ptr(),
-                                                  L.wino_twostage_res_kernel_ptr()):
+    """Pre-pass output of the kernel the build routes C to: transformed tiles
+    V2 for the bulk-copy-fed resident-U kernel, row-transformed records for
+    the producer-fed resident-U and tap-pair kernels, channel-blocked records
+    for the streamed-U kernel."""
+    kp = L.wino_twostage_gemm_kernel_ptr_for(c)
+    if kp == L.wino_twostage_resv_kernel_ptr():
+        tiles8 = (n * ((h + 1) // 2) * ((w + 1) // 2) + 7) // 8 * 8
+        return 16 * tiles8 * c * 2
+    if kp in (L.wino_twostage_pair_kernel_ptr(), L.wino_twostage_res_kernel_ptr()):
         return _xr_bytes(n, c, h, w)
     return L.wino_xb_bytes(n, c, h, w)
 
@@ -277,7 +281,8 @@ def test_twostage_entry_points_validate_and_size(wino):
     m = 16 * 256 * 25088 * 2
     assert m == 4 * 256 * 28 * 28 * 128 * 2
     assert L.wino_twostage_workspace_bytes(128, 256, 28, 28, 256) == r256(_pre_bytes(L, 128, 256, 28, 28)) + m
-    # either kind of record fits the reference harness's transform_pin (4*h*h*n*c fp16)
+    # every kind of pre-pass output fits the reference harness's transform_pin (4*h*h*n*c fp16)
+    assert 16 * 25088 * 256 * 2 == 4 * 28 * 28 * 128 * 256 * 2
     assert _xr_bytes(128, 256, 28, 28) <= 4 * 28 * 28 * 128 * 256 * 2
     assert L.wino_xb_bytes(128, 256, 28, 28) <= 4 * 28 * 28 * 128 * 256 * 2
     # odd sizes: tiles = n * ceil(h/2) * ceil(w/2)

@@ -136,7 +136,10 @@ def test_dropin_two_stage_route(wino, cuda, oracle_mod, shape):
     """Even H and W: getkernelInfo fills the four slots with the U2 filter
     transform, the pre-pass, the two-stage GEMM and the output transform
     (M in the caller's mid_result), and the result equals the extension
-    entry point's."""
+    entry point's.  The 2x2 image has one tile: its transformed tiles (V2,
+    tiles rounded up to 8) do not fit the harness's transform_pin when the
+    build reads V2, and getkernelInfo takes the fused route after the
+    pre-pass instead."""
     import ctypes
     import torch
     n, c, h, w, k = shape
@@ -149,6 +152,14 @@ def test_dropin_two_stage_route(wino, cuda, oracle_mod, shape):
     rc, ki = wino.get_kernel_info(pr, param)
     assert rc == 0
     L = wino.lib()
+    fits = L.wino_twostage_prepass_bytes(n, c, h, w) <= 4 * h * h * n * c * 2
+    if not fits:
+        assert L.wino_dropin_route(ctypes.byref(pr)) == 2
+        y2 = wino.dropin_conv2d(xt, wtt, ws=ws)
+        torch.cuda.synchronize()
+        assert wino.error_read_clear() == 0
+        _check(oracle_mod, y2.cpu().numpy(), oracle_mod.conv2d_f64(x, wt), str(shape))
+        return
     assert ki.slot(3)["kernel"] == L.wino_twostage_gemm_kernel_ptr_for(c)
     assert ki.slot(4)["kernel"] == L.wino_twostage_output_kernel_ptr()
     y2 = wino.dropin_conv2d(xt, wtt, ws=ws)
@@ -205,3 +216,59 @@ def test_twostage_row_prepass_bit_exact(wino, cuda, oracle_mod, shape):
     torch.cuda.synchronize()
     got = ws[:ref.nbytes].cpu().numpy().view(np.uint16)
     assert np.array_equal(got, ref.view(np.uint16).reshape(-1))
+
+
+def _v2_layout_np(x16):
+    """NumPy statement of the transformed tiles V2 that the bulk-copy-fed
+    resident-U kernel reads: V = B^T d B of each tile's 4x4 window (rows
+    first: R = fp16(s0 d_i0 + s1 d_i1), then columns: V = fp16(s0 R_j0 + s1
+    R_j1)), stored per tap in 128-tile blocks (tiles rounded up to 8), per
+    16-channel step in the MN-major core-matrix interleave: tile i, channel c
+    at byte (i >> 3) * 256 + (c >> 3) * 128 + (c & 7) * 16 + (i & 7) * 2."""
+    from oracle import winograd as W
+    n, c, h, w = x16.shape
+    tp, tq = (h + 1) // 2, (w + 1) // 2
+    pad = np.zeros((n, c, 2 * tp + 2, 2 * tq + 2), np.float64)
+    pad[:, :, 1:h + 1, 1:w + 1] = x16.astype(np.float64)
+    win = np.stack([np.stack([pad[:, :, 2 * a:2 * a + 4, 2 * b:2 * b + 4] for b in range(tq)], axis=2)
+                    for a in range(tp)], axis=2)                               # n c ty tx i j
+    r = np.einsum("ai,ncyxij->ncyxaj", W.BT, win).astype(np.float16).astype(np.float64)
+    v = np.einsum("bj,ncyxaj->ncyxab", W.BT, r).astype(np.float16)            # n c ty tx a b
+    nt = n * tp * tq
+    nt8 = (nt + 7) // 8 * 8
+    vt = v.transpose(4, 5, 0, 2, 3, 1).reshape(16, nt, c)                      # tap, tile, channel
+    vt = np.concatenate([vt, np.zeros((16, nt8 - nt, c), np.float16)], axis=1)
+    out = []
+    for t in range(16):
+        for tb in range((nt8 + 127) // 128):
+            rows = min(128, nt8 - 128 * tb)
+            blk = vt[t, 128 * tb:128 * tb + rows]                              # rows x c
+            for cs in range(c // 16):
+                piece = blk[:, 16 * cs:16 * cs + 16].reshape(rows // 8, 8, 2, 8)    # grp, i&7, hh, c&7
+                out.append(piece.transpose(0, 2, 3, 1).reshape(-1))            # grp, hh, c&7, i&7
+    return np.concatenate(out)
+
+
+@pytest.mark.parametrize("shape", [(2, 32, 12, 10), (1, 16, 9, 7), (3, 48, 1, 1), (1, 16, 28, 28)])
+def test_twostage_tile_prepass_bit_exact(wino, cuda, oracle_mod, shape):
+    """The transformed-tile pre-pass (stage 0 of conv2d_twostage when the
+    build routes C to the bulk-copy-fed resident-U kernel) writes exactly the
+    NumPy statement of V2, partial last tile blocks included."""
+    import torch
+    n, c, h, w = shape
+    L = wino.lib()
+    if L.wino_twostage_gemm_kernel_ptr_for(c) != L.wino_twostage_resv_kernel_ptr():
+        pytest.skip("this build does not route C to the bulk-copy-fed resident-U kernel")
+    k = 16
+    x16, _ = oracle_mod.make_inputs(n, c, h, w, k, seed=6, x_dist="normal")
+    ref = _v2_layout_np(x16)
+    nb = wino.twostage_workspace_bytes(n, c, h, w, k)
+    ws = wino._aligned_ws(nb, cuda)
+    ws.fill_(0xA5)                                                 # poison
+    x = _t(x16, cuda)
+    u2 = torch.zeros(16 * k * c, dtype=torch.float16, device=cuda)
+    y = torch.empty((n, k, h, w), dtype=torch.float16, device=cuda)
+    wino.twostage_stage(0, x, u2, k, y, ws)
+    torch.cuda.synchronize()
+    got = ws[:ref.nbytes].cpu().numpy().view(np.uint16)
+    assert np.array_equal(got, ref.view(np.uint16))
