@@ -1265,8 +1265,8 @@ __global__ void __launch_bounds__(TMAV ? trs::NTHREAD_V : trs::NTHREAD, 1) twost
           ++nload;
         }
         // one MMA per K-step: M = 128 tiles, N = the k pair's rows (<= 256);
-        // V2 is tile-major (MN-major A), the producers' V channel-major
-        const uint32_t idesc = instr_desc(128, (uint32_t)(kbs[0] + kbs[1]), 0, 0, TMAV ? 1 : 0, 0);
+        // V2 and the producers' V share the K-major tile-operand layout
+        const uint32_t idesc = instr_desc(128, (uint32_t)(kbs[0] + kbs[1]), 0, 0, 0, 0);
         const int ab = i & 1;
         if (i >= 2 && !mbar_wait(&sh.accempty[ab], ((i >> 1) - 1) & 1, abort_flag, err, ERR_WAIT_DRAIN)) break;
         tc_fence_after();
@@ -1467,32 +1467,111 @@ __global__ void __launch_bounds__(TMAV ? trs::NTHREAD_V : trs::NTHREAD, 1) twost
 // V2 holds V[t][tile][c] in tile blocks of 128 tiles, without padding beyond
 // the tile count rounded up to 8 (NT8): block tb of tap t starts at element
 // (t * NT8 + 128 tb) * C, its K-step cs at + cs * rows * 16 (rows =
-// min(128, NT8 - 128 tb)); inside a K-step the MN-major core-matrix
-// interleave puts tile i, channel c at byte (i >> 3) * 256 + (c >> 3) * 128
-// + (c & 7) * 16 + (i & 7) * 2.  16 * NT8 * C fp16 in all: the reference's
-// transform_pin holds exactly V for even H = W and tiles a multiple of 8.
-// Values as the unfused comparator's input transform (produce_v8: B^T rows
-// on column pairs, then columns; every +- sum rounded once in fp16), which
-// the reference computes at src/preprocessing.cuh:273-424.  Item = (tile
-// block, K-step); thread = (8-tile group, channel); grid-stride over items.
-__global__ void __launch_bounds__(256) v2_layout_kernel(KernelParam p) {
-  const Geometry g = make_geometry(p, TB2);
-  const int NT8 = ((int)g.NT + 7) & ~7;
-  const int items = g.nTB * g.CS;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int grp = 2 * warp + (lane >> 4), cl = lane & 15;
+// min(128, NT8 - 128 tb)); inside a K-step the K-major core-matrix
+// interleave of the GEMM's tile operand puts tile i, channel c at byte
+// (i >> 3) * 256 + (c >> 3) * 128 + (i & 7) * 16 + (c & 7) * 2.  16 * NT8 *
+// C fp16 in all: the reference's transform_pin holds exactly V for even
+// H = W and tiles a multiple of 8.  Values as the fused kernel's producers
+// and the unfused comparator's input transform (B^T rows first, then
+// columns; every +- sum of two fp16 values rounded once), which the
+// reference computes at src/preprocessing.cuh:273-424.
+//
+// Thread = (tile, channel half): lanes are consecutive tiles, so each
+// window-row load of a warp (4 bytes: columns 2x, 2x + 1) is one contiguous
+// run per tile row; two channels go through the transform together as the
+// halves of fp16x2 values, which is also how they sit in a V2 word, and each
+// tap's 8 channels leave as one 16-byte store.  Item = (tile block, K-step),
+// 256 threads, grid-stride over items.  W odd (4-byte words would be
+// misaligned) reads single elements instead.
+namespace v2t {
+constexpr int SMEM_BYTES = 0;
+}  // namespace v2t
+
+__global__ void __launch_bounds__(256, 2) v2_layout_kernel(KernelParam p) {
+  const int C = p.c, H = p.h, W = p.w;
+  const int TP = (p.Oh + 1) >> 1, TQ = (p.Ow + 1) >> 1;
+  const int NT = p.n * TP * TQ;                  // < 2^30 (host bound)
+  const int NT8 = (NT + 7) & ~7;
+  const int CS = C >> 4, nTB = (NT8 + 127) >> 7;
+  const int items = nTB * CS;
+  const int il = threadIdx.x & 127, hh = threadIdx.x >> 7;
+  const unsigned short* X = static_cast<const unsigned short*>(p.pin);
   uint8_t* v2 = static_cast<uint8_t*>(p.transform_pin);
-  const size_t inner = (size_t)grp * 256 + (cl >> 3) * 128 + (cl & 7) * 16;
+  const size_t plane = (size_t)H * W;
+  const size_t tap_bytes = (size_t)NT8 * C * 2;
+  const bool w_even = (W & 1) == 0;
   for (int item = blockIdx.x; item < items; item += gridDim.x) {
-    const int tb = item / g.CS, cs = item - tb * g.CS;
+    const int tb = item / CS, cs = item - tb * CS;
     const int rows = min(128, NT8 - tb * 128);
-    if (grp * 8 >= rows) continue;
-    uint8_t* base = v2 + (((size_t)tb * 128) * g.C + (size_t)cs * rows * 16) * 2 + inner;
-    const size_t tap_bytes = (size_t)NT8 * g.C * 2;
-    produce_v8(static_cast<const __half*>(p.pin), g, (long long)tb * 128 + grp * 8, cs * 16 + cl, -1,
-               [&](int t, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
-                 *reinterpret_cast<uint4*>(base + (size_t)t * tap_bytes) = make_uint4(a, b, c, d);
-               });
+    if (il >= rows) continue;
+    const int tile = tb * 128 + il;
+    const bool live = tile < NT;
+    int n = 0, ty = 0, tx = 0;
+    if (live) {
+      const int per = TP * TQ;
+      n = tile / per;
+      const int r = tile - n * per;
+      ty = r / TQ;
+      tx = r - ty * TQ;
+    }
+    const int y0 = 2 * ty - 1, x0 = 2 * tx;      // window rows y0 .., columns x0 - 1 .. x0 + 2
+    const unsigned short* base = X + ((size_t)n * C + cs * 16 + hh * 8) * plane;
+    uint32_t vt[16][4];                          // [tap][channel pair]
+#pragma unroll
+    for (int cp = 0; cp < 4; ++cp) {
+      // col[r][j] = (channel 2cp, channel 2cp + 1) at row y0 + r, column x0 - 1 + j
+      uint32_t col[4][4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int y = y0 + r;
+        const bool rok = live && y >= 0 && y < H;
+        uint32_t a[2][3];                        // channel, word (columns x0-2.., x0.., x0+2..)
+#pragma unroll
+        for (int ch = 0; ch < 2; ++ch) {
+          const unsigned short* row = base + (size_t)(2 * cp + ch) * plane + (size_t)(rok ? y : 0) * W;
+          if (w_even) {
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+              const int x = x0 - 2 + 2 * q;
+              a[ch][q] = (rok && x >= 0 && x < W) ? *reinterpret_cast<const uint32_t*>(row + x) : 0u;
+            }
+          } else {
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+              const int x = x0 - 2 + 2 * q;
+              const uint32_t lo = (rok && x >= 0 && x < W) ? row[x] : 0u;
+              const uint32_t hi = (rok && x + 1 >= 0 && x + 1 < W) ? row[x + 1] : 0u;
+              a[ch][q] = lo | (hi << 16);
+            }
+          }
+        }
+        col[r][0] = __byte_perm(a[0][0], a[1][0], 0x7632);   // column x0 - 1
+        col[r][1] = __byte_perm(a[0][1], a[1][1], 0x5410);   // x0
+        col[r][2] = __byte_perm(a[0][1], a[1][1], 0x7632);   // x0 + 1
+        col[r][3] = __byte_perm(a[0][2], a[1][2], 0x5410);   // x0 + 2
+      }
+      // rows of B^T d (d0 - d2, d1 + d2, d2 - d1, d1 - d3), then the same on columns
+      uint32_t e[4][4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        e[0][j] = hsub2(col[0][j], col[2][j]);
+        e[1][j] = hadd2(col[1][j], col[2][j]);
+        e[2][j] = hsub2(col[2][j], col[1][j]);
+        e[3][j] = hsub2(col[1][j], col[3][j]);
+      }
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        vt[4 * a + 0][cp] = hsub2(e[a][0], e[a][2]);
+        vt[4 * a + 1][cp] = hadd2(e[a][1], e[a][2]);
+        vt[4 * a + 2][cp] = hsub2(e[a][2], e[a][1]);
+        vt[4 * a + 3][cp] = hsub2(e[a][1], e[a][3]);
+      }
+    }
+    uint8_t* out = v2 + ((size_t)tb * 128 * C + (size_t)cs * rows * 16) * 2 + (il >> 3) * 256 + hh * 128 +
+                   (il & 7) * 16;
+#pragma unroll
+    for (int t = 0; t < 16; ++t)
+      *reinterpret_cast<uint4*>(out + (size_t)t * tap_bytes) = make_uint4(vt[t][0], vt[t][1], vt[t][2], vt[t][3]);
   }
 }
 
@@ -1726,8 +1805,9 @@ void* wino_twostage_prepass_kernel_ptr_for(int c) {
 }
 unsigned wino_twostage_prepass_grid(int n, int c, int h, int w) {
   if (use_v2(c)) {
+    // two resident CTAs per SM (128 registers a thread), grid-stride over the items
     const long long items = wino_twostage_prepass_items(n, c, h, w);
-    const long long cap = 148LL * 16;
+    const long long cap = 148LL * 2;
     return (unsigned)(items < cap ? (items > 0 ? items : 1) : cap);
   }
   if (!use_xr(c)) return wino_xb_layout_grid(n, c, h, w);
@@ -1735,11 +1815,12 @@ unsigned wino_twostage_prepass_grid(int n, int c, int h, int w) {
   const long long cap = 148LL * 64;
   return (unsigned)(blocks < cap ? (blocks > 0 ? blocks : 1) : cap);
 }
+int wino_twostage_prepass_smem_bytes(int c) { return use_v2(c) ? v2t::SMEM_BYTES : 0; }
 int wino_launch_twostage_prepass(const KernelParam* p, cudaStream_t stream) {
   void* args[] = {const_cast<KernelParam*>(p)};
   return (int)cudaLaunchKernel(wino_twostage_prepass_kernel_ptr_for(p->c),
-                               dim3(wino_twostage_prepass_grid(p->n, p->c, p->h, p->w)), dim3(256), args, 0,
-                               stream);
+                               dim3(wino_twostage_prepass_grid(p->n, p->c, p->h, p->w)), dim3(256), args,
+                               (size_t)wino_twostage_prepass_smem_bytes(p->c), stream);
 }
 
 // Tiles and the M16 bytes of a shape (no padding).

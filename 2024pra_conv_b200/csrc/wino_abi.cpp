@@ -92,6 +92,7 @@ long long wino_twostage_prepass_items(int n, int c, int h, int w);
 void* wino_twostage_prepass_kernel_ptr_for(int c);
 unsigned wino_twostage_prepass_grid(int n, int c, int h, int w);
 int wino_launch_twostage_prepass(const wino::KernelParam* p, cudaStream_t stream);
+int wino_twostage_prepass_smem_bytes(int c);
 void wino_twostage_output_grid(int n, int h, int w, int k, int sms, unsigned* gx, unsigned* gy);
 int wino_twostage_output_smem_bytes();
 uint32_t wino_twostage_error_read_clear();
@@ -282,8 +283,8 @@ int getkernelInfo(problem_t* problem, kernelInfo_t* kernelInfo, void* param) {
     set_slot(kernelInfo, 1, (unsigned)((kc + 255) / 256), 1, 1, 256, 1, 1, 0,
              wino_dropin_filter_u2_kernel_ptr());
     const int c = (int)pr.c;
-    set_slot(kernelInfo, 2, wino_twostage_prepass_grid((int)pr.n, c, (int)pr.h, (int)pr.w), 1, 1, 256, 1, 1, 0,
-             wino_twostage_prepass_kernel_ptr_for(c));
+    set_slot(kernelInfo, 2, wino_twostage_prepass_grid((int)pr.n, c, (int)pr.h, (int)pr.w), 1, 1, 256, 1, 1,
+             wino_twostage_prepass_smem_bytes(c), wino_twostage_prepass_kernel_ptr_for(c));
     set_slot(kernelInfo, 3, wino_twostage_gemm_grid((int)pr.n, c, (int)pr.h, (int)pr.w, (int)pr.k, sm_count()), 1,
              1, (unsigned)wino_twostage_threads_for(c), 1, 1, (unsigned)wino_twostage_smem_bytes_for(c),
              wino_twostage_gemm_kernel_ptr_for(c));

@@ -223,8 +223,8 @@ def _v2_layout_np(x16):
     resident-U kernel reads: V = B^T d B of each tile's 4x4 window (rows
     first: R = fp16(s0 d_i0 + s1 d_i1), then columns: V = fp16(s0 R_j0 + s1
     R_j1)), stored per tap in 128-tile blocks (tiles rounded up to 8), per
-    16-channel step in the MN-major core-matrix interleave: tile i, channel c
-    at byte (i >> 3) * 256 + (c >> 3) * 128 + (c & 7) * 16 + (i & 7) * 2."""
+    16-channel step in the K-major core-matrix interleave: tile i, channel c
+    at byte (i >> 3) * 256 + (c >> 3) * 128 + (i & 7) * 16 + (c & 7) * 2."""
     from oracle import winograd as W
     n, c, h, w = x16.shape
     tp, tq = (h + 1) // 2, (w + 1) // 2
@@ -245,7 +245,7 @@ def _v2_layout_np(x16):
             blk = vt[t, 128 * tb:128 * tb + rows]                              # rows x c
             for cs in range(c // 16):
                 piece = blk[:, 16 * cs:16 * cs + 16].reshape(rows // 8, 8, 2, 8)    # grp, i&7, hh, c&7
-                out.append(piece.transpose(0, 2, 3, 1).reshape(-1))            # grp, hh, c&7, i&7
+                out.append(piece.transpose(0, 2, 1, 3).reshape(-1))            # grp, hh, i&7, c&7
     return np.concatenate(out)
 
 
