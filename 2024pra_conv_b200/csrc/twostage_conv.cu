@@ -1094,17 +1094,21 @@ struct Unit {
   int combo, t, kp, tb;
 };
 
+// Tile blocks are taken in decreasing order: the pre-pass writes them in
+// increasing order, so the most recently written, still in L2, come first.
 __device__ __forceinline__ Unit sched_unit(const Geo& g, const Sched& sc, int i) {
   Unit x;
   const int ncombo = 16 * g.nKP;
+  int r;
   if (sc.G < ncombo) {
     const int m = i / g.nTB;
     x.combo = sc.combo + m * sc.G;
-    x.tb = i - m * g.nTB;
+    r = i - m * g.nTB;
   } else {
     x.combo = sc.combo;
-    x.tb = sc.j + i * sc.s;
+    r = sc.j + i * sc.s;
   }
+  x.tb = g.nTB - 1 - r;
   x.t = x.combo / g.nKP;
   x.kp = x.combo - x.t * g.nKP;
   return x;
@@ -1487,7 +1491,10 @@ namespace v2t {
 constexpr int SMEM_BYTES = 0;
 }  // namespace v2t
 
-__global__ void __launch_bounds__(256, 2) v2_layout_kernel(KernelParam p) {
+#ifndef WINO_V2_MINB
+#define WINO_V2_MINB 2
+#endif
+__global__ void __launch_bounds__(256, WINO_V2_MINB) v2_layout_kernel(KernelParam p) {
   const int C = p.c, H = p.h, W = p.w;
   const int TP = (p.Oh + 1) >> 1, TQ = (p.Ow + 1) >> 1;
   const int NT = p.n * TP * TQ;                  // < 2^30 (host bound)
@@ -1579,7 +1586,8 @@ __global__ void __launch_bounds__(256, 2) v2_layout_kernel(KernelParam p) {
 // Output transform
 // =============================================================================
 // Persistent: work item = (tile block tb, 8 output channels kg), item i =
-// kg * tile blocks + tb, CTA b takes items b, b + grid, ...  An item's 16
+// tb * (K / 8) + kg, CTA b takes items b, b + grid, ...: the tile blocks in
+// increasing order, the GEMM's last-written (still in L2) first.  An item's 16
 // taps x 8 channels of the blocked M (16 contiguous runs of 8 * ntb fp16)
 // come in by bulk copy into one of three shared-memory buffers, issued as
 // soon as a buffer is free, so two items per CTA are in flight while the
@@ -1607,7 +1615,8 @@ __global__ void __launch_bounds__(256, 2) twostage_output_kernel(KernelParam p) 
   const int TP = (P + 1) >> 1, TQ = (Q + 1) >> 1;
   const long long NT = (long long)p.n * TP * TQ;
   const int nTB = (int)((NT + 127) / 128);
-  const int nitems = nTB * (K / ot::KG);
+  const int nKG = K / ot::KG;
+  const int nitems = nTB * nKG;
   const __half* m16 = static_cast<const __half*>(p.mid_result);
   if (threadIdx.x == 0) {
     for (int b = 0; b < ot::NBUF; ++b) mbar_init(&full[b], 1);
@@ -1616,7 +1625,7 @@ __global__ void __launch_bounds__(256, 2) twostage_output_kernel(KernelParam p) 
   __syncthreads();
   // issue the copies of `item` into buffer `buf` (warp 0)
   auto fetch = [&](int item, int buf) {
-    const int tb = item % nTB, k0 = (item / nTB) * ot::KG;
+    const int tb = item / nKG, k0 = (item - tb * nKG) * ot::KG;
     const long long rem = NT - (long long)tb * 128;
     const int ntb = rem < 128 ? (int)rem : 128;
     const uint32_t run = (uint32_t)(ot::KG * ntb * 2);
@@ -1636,7 +1645,7 @@ __global__ void __launch_bounds__(256, 2) twostage_output_kernel(KernelParam p) 
   int j = 0;
   for (int item = blockIdx.x; item < nitems; item += gridDim.x, ++j) {
     const int buf = j % ot::NBUF;
-    const int tb = item % nTB, k = (item / nTB) * ot::KG + kl;
+    const int tb = item / nKG, k = (item - tb * nKG) * ot::KG + kl;
     const long long rem = NT - (long long)tb * 128;
     const int ntb = rem < 128 ? (int)rem : 128;
     const uint32_t run = (uint32_t)(ot::KG * ntb * 2);
@@ -1805,9 +1814,9 @@ void* wino_twostage_prepass_kernel_ptr_for(int c) {
 }
 unsigned wino_twostage_prepass_grid(int n, int c, int h, int w) {
   if (use_v2(c)) {
-    // two resident CTAs per SM (128 registers a thread), grid-stride over the items
+    // the resident CTAs (WINO_V2_MINB per SM), grid-stride over the items
     const long long items = wino_twostage_prepass_items(n, c, h, w);
-    const long long cap = 148LL * 2;
+    const long long cap = 148LL * WINO_V2_MINB;
     return (unsigned)(items < cap ? (items > 0 ? items : 1) : cap);
   }
   if (!use_xr(c)) return wino_xb_layout_grid(n, c, h, w);
