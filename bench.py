@@ -13,10 +13,11 @@ Printed (rank 0, one JSON line):
              inputs resident in HBM, L2 flushed between steps
   e2e        the same metric through the C-ABI with host buffers: each step
              copies x host->device, runs the four slots, copies y back
-  roofline   the step's GEMM kernel (two-stage tap GEMM, or the fused kernel
-             on the other route) against the tensor-pipe roofline: Winograd
-             GEMM FLOPs (2*16*K*C*N*ceil(P/2)*ceil(Q/2)) per launch over its
-             CUDA-event time, peak from MEASURED_PEAKS.json
+  roofline   the step's slowest kernel against its own roofline (the slower
+             of Winograd GEMM FLOPs 2*16*K*C*N*ceil(P/2)*ceil(Q/2) over the
+             measured bf16 GEMM peak and its compulsory DRAM bytes over the
+             measured copy bandwidth, MEASURED_PEAKS.json), each kernel timed
+             alone by CUDA events; roofline.kernels lists all three
   cpu_baseline  the reference's own conv2dcpu (oracle/_ref) on this host's
              cores over a bounded sample of images
 plus the fused-vs-unfused comparison and the error against FP64.
@@ -81,13 +82,35 @@ def measured_peaks():
 
 def committed_traffic(kernel):
     """DRAM bytes per launch of `kernel` from the committed ncu summaries, if any."""
-    name = {"fused_wino_f16_kernel": "fused_conv_n128_c256_h28.json",
-            "twostage_gemm_kernel": "twostage_conv_n128_c256_h28.json"}[kernel]
+    if kernel == "fused_wino_f16_kernel":
+        name = "fused_conv_n128_c256_h28.json"
+    else:
+        name = "twostage_conv_n128_c256_h28.json"
     try:
         with open(os.path.join(ROOT, "profiles", name)) as f:
-            return json.load(f).get("dram_bytes_per_launch")
+            d = json.load(f)
+        if "kernels" in d:
+            return d["kernels"].get(kernel, {}).get("dram_bytes_per_launch")
+        return d.get("dram_bytes_per_launch")
     except (OSError, ValueError):
         return None
+
+
+def kernel_roofline(name, us, flops, nbytes, peaks):
+    """One kernel against its roofline: the slower of its tensor time
+    (flops / measured bf16 GEMM peak) and its HBM time (compulsory bytes /
+    measured copy bandwidth) decides the bound; achieved and peak are in
+    that bound's unit."""
+    t_tensor = flops / (peaks["tflops"] * 1e12) if flops else 0.0
+    t_hbm = nbytes / (peaks["hbm_gbs"] * 1e9)
+    if t_tensor >= t_hbm:
+        achieved, peak, unit, bound = flops / (us * 1e-6) / 1e12, peaks["tflops"], "TFLOP/s", "tensor"
+    else:
+        achieved, peak, unit, bound = nbytes / (us * 1e-6) / 1e9, peaks["hbm_gbs"], "GB/s", "hbm"
+    return {"kernel": name, "bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
+            "frac": achieved / peak, "us": us, "flops": flops, "bytes": nbytes,
+            "floor_us": max(t_tensor, t_hbm) * 1e6, "traffic": committed_traffic(name),
+            "peak_source": peaks["source"]}
 
 
 # ------------------------------------------------------------------ clocks --
@@ -439,10 +462,30 @@ def run_ours(args, rank, world, local_rank):
         return 0
     peaks = measured_peaks()
     wflops = wino_flops(n, c, h, w, k)
-    roof_kernel = "twostage_gemm_kernel" if two_stage else "fused_wino_f16_kernel"
-    roof_us = ts_gemm_us if two_stage else kernel_us
-    achieved = wflops / (roof_us * 1e-6) / 1e12
-    traffic = committed_traffic(roof_kernel)
+    L = wino.lib()
+    tiles = n * ((h + 1) // 2) * ((w + 1) // 2)
+    x_bytes, y_bytes = n * c * h * w * 2, n * k * h * w * 2
+    m_bytes, u_bytes = 16 * k * tiles * 2, 16 * k * c * 2
+    if two_stage:
+        pre_bytes = L.wino_twostage_prepass_bytes(n, c, h, w)
+        gk = L.wino_twostage_gemm_kernel_ptr_for(c)
+        gname = ("twostage_res_kernel_t<1>" if gk == L.wino_twostage_resv_kernel_ptr() else
+                 "twostage_res_kernel_t<0>" if gk == L.wino_twostage_res_kernel_ptr() else
+                 "twostage_pair_kernel" if gk == L.wino_twostage_pair_kernel_ptr() else "twostage_stream_kernel")
+        pname = "v2_layout_kernel" if gk == L.wino_twostage_resv_kernel_ptr() else "prepass"
+        kern = [kernel_roofline(pname, ts_pre_us, 0, x_bytes + pre_bytes, peaks),
+                kernel_roofline(gname, ts_gemm_us, wflops, pre_bytes + u_bytes + m_bytes, peaks),
+                kernel_roofline("twostage_output_kernel", ts_out_us, 0, m_bytes + y_bytes, peaks)]
+    else:
+        kern = [kernel_roofline("fused_wino_f16_kernel", kernel_us, wflops, x_bytes + y_bytes + u_bytes, peaks)]
+    dom = max(kern, key=lambda r: r["us"])
+    roofline = {k2: dom[k2] for k2 in ("bound", "achieved", "peak", "unit", "frac", "traffic", "peak_source",
+                                       "kernel")}
+    roofline["algorithmic"] = (f"{dom['bytes'] / 1e6:.1f} MB compulsory DRAM bytes and {dom['flops'] / 1e9:.2f} "
+                               "Winograd GEMM GFLOP per launch; the bound is the slower of the two")
+    roofline["kernels"] = kern
+    roofline["step_floor_us"] = sum(r["floor_us"] for r in kern)
+    roofline["step_frac_of_kernel_floors"] = roofline["step_floor_us"] / (max_ms / args.steps * 1e3)
     cpu = None
     if world == 1 and not args.no_cpu:
         try:
@@ -479,11 +522,7 @@ def run_ours(args, rank, world, local_rank):
         "unfused_us": unfused_us,
         "speedup_vs_unfused": unfused_us / (ts_us if two_stage else fused_us),
         "rel_l2": rel_l2, "max_norm": max_norm, "unfused_rel_diff": unf_rel,
-        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peaks["tflops"],
-                     "unit": "TFLOP/s", "frac": achieved / peaks["tflops"],
-                     "traffic": traffic, "peak_source": peaks["source"],
-                     "kernel": roof_kernel,
-                     "algorithmic": "Winograd GEMM FLOPs 2*16*K*C*N*ceil(H/2)*ceil(W/2) per launch"},
+        "roofline": roofline,
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": "TFLOP/s", "h2d_bytes_per_step": x.numel() * 2,
                 "d2h_bytes_per_step": y.numel() * 2, "rel_l2_of_downloaded_output": e2e_err,
