@@ -27,9 +27,12 @@
  *
  *     two-stage route: r = s = 3, u = v = 1, p = q = 1, c % 16 == k % 16
  *       == 0, even h and w, all three workspaces present, transform_pin
- *       16-byte aligned:
+ *       16-byte aligned and large enough for the pre-pass output:
  *         slot 1  filter transform   weight -> transform_filter (U)
- *         slot 2  input re-layout    in -> transform_pin (channel-blocked)
+ *         slot 2  input pre-pass     in -> transform_pin (c <= 256: the
+ *                                    transformed tiles V, 16*c*tiles rounded
+ *                                    up to 8 tiles; c > 256: the
+ *                                    channel-blocked input)
  *         slot 3  tap GEMMs          transform_pin, transform_filter ->
  *                                    mid_result (M, 16*k*n*(h/2)*(w/2) fp16,
  *                                    all of the caller's 4*k*h*w*n)

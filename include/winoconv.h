@@ -146,18 +146,21 @@ size_t wino_variant_workspace_bytes(int variant, int n, int c, int h, int w, int
 int wino_conv2d_variant(int variant, const void* x, const void* weight, void* y, void* workspace,
                         int n, int c, int h, int w, int k, void* stream);
 
-/* Two-stage F(2x2,3x3): the input transform runs inside full-width tcgen05
- * tap GEMMs (one tap x 128 tiles x 256 output channels per work unit, V formed
- * in shared memory from the channel-blocked input), M is written as fp16
- * (16 * k * tiles elements, tiles = n * ceil(h/2) * ceil(w/2)) and a second
- * kernel applies the output transform.  ucache2: U in the unfused GEMM
- * layout (wino_filter_transform_unfused).  workspace: 256-byte aligned,
- * wino_twostage_workspace_bytes() bytes (channel-blocked input, then M).
+/* Two-stage F(2x2,3x3): an input pre-pass, full-width tcgen05 tap GEMMs
+ * (one tap x 128 tiles x 256 output channels per work unit), M is
+ * written as fp16 (16 * k * tiles elements, tiles = n * ceil(h/2) *
+ * ceil(w/2)) and a third kernel applies the output transform.  For c <= 256
+ * the pre-pass writes the transformed tiles V (16 * tiles8 * c fp16, tiles8
+ * = tiles rounded up to 8) and the GEMM keeps each CTA's U resident and reads
+ * V by bulk copy; for c > 256 the pre-pass writes the channel-blocked input
+ * and the GEMM forms V in shared memory and streams U.  ucache2: U in the
+ * unfused GEMM layout (wino_filter_transform_unfused).  workspace: 256-byte
+ * aligned, wino_twostage_workspace_bytes() bytes (pre-pass output, then M).
  * The output equals the unfused comparator's (same operands and rounding
- * points) without V's HBM round trip; the reference's pipeline writes V and M
- * to its workspaces (src/preprocessing.cuh:273-424, src/matrixmul.cuh:139-556).
+ * points); the reference's pipeline writes V and M to its workspaces the same
+ * way (src/preprocessing.cuh:273-424, src/matrixmul.cuh:139-556).
  * getkernelInfo takes this route when M fits the caller's mid_result
- * (4*k*h*w*n fp16: even h and w) and the blocked input fits transform_pin.
+ * (4*k*h*w*n fp16: even h and w) and the pre-pass output fits transform_pin.
  * Shapes whose blocked-input record block (one image, 16 channels) reaches
  * 2^31 bytes return WINO_EUNSUPPORTED (workspace size 0). */
 size_t wino_twostage_workspace_bytes(int n, int c, int h, int w, int k);
