@@ -1,24 +1,27 @@
-// Two-stage Winograd F(2x2,3x3): input transform fused into the tap GEMMs,
-// output transform as a second kernel.
+// Two-stage Winograd F(2x2,3x3): an input pre-pass, full-width tcgen05 tap
+// GEMMs writing M, and the output transform as a third kernel.
 //
 // The single fused kernel (fused_conv.cu) keeps all 16 taps of a tile block
 // in TMEM until the output transform, which caps its MMAs at N = 32 tiles.
 // This path gives that up for full-width MMAs: the GEMM writes M once, in
 // fp16 (16 * K * tiles elements, the size of the reference's mid_result for
-// even H, W), and a second kernel applies A^T m A.  V never reaches HBM: it
-// is formed in shared memory by producer warps straight from the
-// channel-blocked input (XB, written by the input pre-pass).  Against the
+// even H, W), and a third kernel applies A^T m A, the stages of the
 // reference's pipeline (src/preprocessing.cuh:273-424 writing V to
 // transform_pin, src/matrixmul.cuh:139-556 reading it back,
-// src/conv2d.cpp:17-250 reading M from mid_result) it drops the V round trip.
+// src/conv2d.cpp:17-250 reading M from mid_result).
 //
-//   slot 1  dropin_filter_u2_kernel   W -> U2 (unfused GEMM layout), transform_filter
-//   slot 2  xb_layout_kernel          X -> XB, transform_pin
-//   slot 3  twostage_stream_kernel    XB, U2 -> M (blocked, below), mid_result
-//           (twostage_pair_kernel on XR when C <= WINO_PAIR_MAX_C)
-//   slot 4  twostage_output_kernel    M -> Y
-// (the drop-in ABI's route when M fits mid_result, i.e. even H and W; the
-// extension entry point wino_conv2d_twostage runs slots 2-4 on any shape).
+//   slot 1  dropin_filter_u2_kernel     W -> U2 (unfused GEMM layout), transform_filter
+//   slot 2  v2_layout_kernel            X -> V2 (transformed tiles), transform_pin
+//   slot 3  twostage_res_kernel_t<1>    V2, U2 -> M (blocked, below), mid_result
+//   slot 4  twostage_output_kernel      M -> Y
+// for C <= 256; for larger C slot 2 is xb_layout_kernel (X -> XB, the
+// channel-blocked input) and slot 3 twostage_stream_kernel (V formed in
+// shared memory from XB, U streamed).  The drop-in ABI takes this route
+// when M fits mid_result (even H and W) and the pre-pass output fits
+// transform_pin; the extension entry point wino_conv2d_twostage runs slots
+// 2-4 on any shape.  Build options route C to the producer-fed kernels on
+// row-transformed input (XR): twostage_res_kernel_t<0> (WINO_RES_XR_MAX_C)
+// and twostage_pair_kernel (WINO_PAIR_MAX_C); both are slower on B200.
 //
 // M layout (blocked by 128-tile blocks): block tb holds M[t][k][i] for the
 // block's ntb = min(128, tiles - 128 tb) tiles, element
@@ -33,7 +36,10 @@
 // comparator's; with M rounded once to fp16 the output equals the unfused
 // comparator's.
 //
-// twostage_pair_kernel (C <= 256): a cluster of two CTAs issues
+// twostage_res_kernel_t (C <= 256, the drop-in's GEMM) is described at its
+// definition below.
+//
+// twostage_pair_kernel (build option): a cluster of two CTAs issues
 // tcgen05.mma.cta_group::2 of M = 256 output channels x N = 128 tiles x 16
 // channels.  A work unit is a PAIR of taps x 256 output channels x 128
 // tiles, all C.  The taps of a pair are chosen so that they read common
