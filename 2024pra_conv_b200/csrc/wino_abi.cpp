@@ -94,6 +94,7 @@ unsigned wino_twostage_prepass_grid(int n, int c, int h, int w);
 int wino_launch_twostage_prepass(const wino::KernelParam* p, cudaStream_t stream);
 int wino_twostage_prepass_smem_bytes(int c);
 void wino_twostage_output_grid(int n, int h, int w, int k, int sms, unsigned* gx, unsigned* gy);
+int wino_twostage_output_threads();
 int wino_twostage_output_smem_bytes();
 uint32_t wino_twostage_error_read_clear();
 }
@@ -290,7 +291,8 @@ int getkernelInfo(problem_t* problem, kernelInfo_t* kernelInfo, void* param) {
              wino_twostage_gemm_kernel_ptr_for(c));
     unsigned ox, oy;
     wino_twostage_output_grid((int)pr.n, (int)pr.h, (int)pr.w, (int)pr.k, sm_count(), &ox, &oy);
-    set_slot(kernelInfo, 4, ox, oy, 1, 256, 1, 1, (unsigned)wino_twostage_output_smem_bytes(),
+    set_slot(kernelInfo, 4, ox, oy, 1, (unsigned)wino_twostage_output_threads(), 1, 1,
+             (unsigned)wino_twostage_output_smem_bytes(),
              wino_twostage_output_kernel_ptr());
     return WINO_OK;
   }
@@ -416,7 +418,7 @@ extern "C" int wino_twostage_stage(int stage, const void* x, const void* ucache2
                : WINO_ECUDA;
   unsigned ox, oy;
   wino_twostage_output_grid(n, h, w, k, sm_count(), &ox, &oy);
-  return cudaLaunchKernel(wino_twostage_output_kernel_ptr(), dim3(ox, oy), dim3(256), args,
+  return cudaLaunchKernel(wino_twostage_output_kernel_ptr(), dim3(ox, oy), dim3(wino_twostage_output_threads()), args,
                           (size_t)wino_twostage_output_smem_bytes(), s) ==
                  cudaSuccess
              ? WINO_OK
