@@ -1167,8 +1167,16 @@ __device__ __forceinline__ Prod prod(const Geo& g, const uint8_t* xr, int t, int
 // TMAV true: V read by bulk copy from the transformed tiles V2 in
 // transform_pin (v2_layout_kernel); warp 5 lane 0 issues the copies and no
 // producer warps run.
-template <bool TMAV>
+// F8 (with TMAV): the fp8 hi+lo variant.  V2 and U hold e4m3 hi and lo
+// terms (x = hi + lo to about 8 bits), 32 channels per K-step, the two terms
+// of a K-step back to back (so a K-step's two pieces take the place of two
+// fp16 K-steps' pieces: loader and stages are unchanged); per K-step three
+// kind::f8f6f4 MMAs accumulate hi.hi + lo.hi + hi.lo; the per-input-channel
+// V scale is folded into U, and the epilogue multiplies by the per-(tap,
+// output channel) U scale su (p.pweight, fp32 [16][K]) before rounding M.
+template <bool TMAV, bool F8 = false>
 __global__ void __launch_bounds__(TMAV ? trs::NTHREAD_V : trs::NTHREAD, 1) twostage_res_kernel_t(KernelParam p) {
+  static_assert(!F8 || TMAV, "the fp8 variant reads V2 by bulk copy");
   using namespace trs;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   __shared__ Shared sh;
@@ -1216,6 +1224,7 @@ __global__ void __launch_bounds__(TMAV ? trs::NTHREAD_V : trs::NTHREAD, 1) twost
       for (int i = 0; i < sc.cnt && !*abort_flag; ++i) {
         const Unit un = sched_unit(g, sc, i);
         const int rows = min(128, NT8 - un.tb * 128);
+        // two bytes per tile and channel: fp16, or the fp8 hi and lo terms
         const uint8_t* src = v2 + ((size_t)un.t * NT8 + (size_t)un.tb * 128) * g.C * 2;
         bool ok = true;
         for (int j = 0; j < nst; ++j, ++it) {
@@ -1265,12 +1274,17 @@ __global__ void __launch_bounds__(TMAV ? trs::NTHREAD_V : trs::NTHREAD, 1) twost
 #pragma unroll
           for (int q = 0; q < KPU; ++q) bytes += (uint32_t)(kbs[q] * g.C * 2);
           mbar_arrive_expect_tx(&sh.ufull, bytes);
-          for (int cs = 0; cs < g.CS; ++cs)
+          if constexpr (F8) {
+            // the combo's [K-step][term][rows x 32 B] block is contiguous
+            bulk_g2s(smem, u2 + ((size_t)un.t * g.K + (size_t)un.kp * 2 * KB2) * g.C * 2, bytes, &sh.ufull);
+          } else {
+            for (int cs = 0; cs < g.CS; ++cs)
 #pragma unroll
-            for (int q = 0; q < KPU; ++q)
-              if (kbs[q])
-                bulk_g2s(smem + cs * U_CS + q * (KB2 * 32), u2 + u2_piece(un.t, kb + q, cs, g.K, g.C) * 2,
-                         (uint32_t)(kbs[q] * 32), &sh.ufull);
+              for (int q = 0; q < KPU; ++q)
+                if (kbs[q])
+                  bulk_g2s(smem + cs * U_CS + q * (KB2 * 32), u2 + u2_piece(un.t, kb + q, cs, g.K, g.C) * 2,
+                           (uint32_t)(kbs[q] * 32), &sh.ufull);
+          }
           if (!mbar_wait(&sh.ufull, nload & 1, abort_flag, err, ERR_WAIT_FULL)) break;
           ++nload;
         }
@@ -1292,6 +1306,21 @@ __global__ void __launch_bounds__(TMAV ? trs::NTHREAD_V : trs::NTHREAD, 1) twost
           tc_fence_after();
           const int nk = min(SK, g.CS - j * SK);
           const uint64_t adesc = smem_desc(sbase + U_BYTES + st * STAGE_A, 128, 256);
+          if constexpr (F8) {
+            // nk pieces = nk / 2 K-steps of 32 channels, each hi then lo
+            const uint32_t rk = (uint32_t)(kbs[0] + kbs[1]);
+            const uint32_t term = rk * 32 >> 4;        // descriptor step between the terms of U
+            for (int kk = 0; kk < nk / 2; ++kk) {
+              const int cs32 = j * (SK / 2) + kk;
+              const uint64_t ah = adesc + (uint64_t)(2 * kk * (A_STEP >> 4)), al = ah + (uint64_t)(A_STEP >> 4);
+              const uint64_t bh = bdesc0 + (uint64_t)(2 * cs32) * term, bl = bh + term;
+              mma_f8(d, ah, bh, idesc, (j > 0 || kk > 0) ? 1u : 0u);
+              mma_f8(d, al, bh, idesc, 1u);
+              mma_f8(d, ah, bl, idesc, 1u);
+            }
+            mma_commit(&sh.empty[st]);
+            continue;
+          }
           const uint64_t bdesc = bdesc0 + (uint64_t)(j * SK * (U_CS >> 4));
           if (nk == SK) {
 #pragma unroll
@@ -1339,14 +1368,18 @@ __global__ void __launch_bounds__(TMAV ? trs::NTHREAD_V : trs::NTHREAD, 1) twost
         tmem_ld16(taddr + cc, v);
         if (cc + 16 < nrows) tmem_ld16(taddr + cc + 16, v + 16);
       };
+      // fp8: M = su[t][k] * D (one fp32 product, then the fp16 rounding)
+      const float* sur = F8 ? static_cast<const float*>(p.pweight) + (size_t)un.t * g.K + kb * KB2 : nullptr;
       auto st = [&](int cc, const float* v) {
         if (!live) return;
         __half* dst = mrow + (size_t)cc * ntb;
 #pragma unroll
-        for (int jj = 0; jj < 16; ++jj) dst[(size_t)jj * ntb] = __float2half_rn(v[jj]);
+        for (int jj = 0; jj < 16; ++jj)
+          dst[(size_t)jj * ntb] = __float2half_rn(F8 ? v[jj] * __ldg(sur + cc + jj) : v[jj]);
         if (cc + 16 < nrows) {
 #pragma unroll
-          for (int jj = 16; jj < 32; ++jj) dst[(size_t)jj * ntb] = __float2half_rn(v[jj]);
+          for (int jj = 16; jj < 32; ++jj)
+            dst[(size_t)jj * ntb] = __float2half_rn(F8 ? v[jj] * __ldg(sur + cc + jj) : v[jj]);
         }
       };
       float va[32], vb[32];
@@ -1589,6 +1622,190 @@ __global__ void __launch_bounds__(256, WINO_V2_MINB) v2_layout_kernel(KernelPara
 }
 
 // =============================================================================
+// fp8 hi+lo two-stage variant: channel scales, U and V2 in e4m3 hi + lo
+// =============================================================================
+// x = hi + lo with hi = e4m3(x) and lo = e4m3(x - hi) keeps about 8 bits of
+// x; the tap GEMM accumulates U_hi V_hi + U_lo V_hi + U_hi V_lo (the dropped
+// U_lo V_lo is ~2^-8 of a product), so the fp8 tensor path reaches the
+// accuracy of fp16 operands.  Scales as the fused fp8 variant's: per input
+// channel inv_c = fp16(min(448 / (4 max|x_c|), 65504)) (|V| <= 4 max|x_c|),
+// V' = fp16(V) * inv_c; U'[t][k][c] = U * (1 / inv_c), su[t][k] = max_c |U'|
+// / 448, U'' = U' / su; M = su * sum_c U'' V'.  The reference has no fp8
+// path (src/matrixmul.cuh:28-35 is fp16).
+
+// per-channel max |x| as fp16 magnitude bits (monotonic as unsigned);
+// amax must be zero on entry.  Grid (C, chunks of images).
+__global__ void __launch_bounds__(256) f8_amax_kernel(const unsigned short* __restrict__ x, unsigned* amax, int n,
+                                                      int c, int hw) {
+  const int ch = blockIdx.x;
+  unsigned m = 0;
+  for (int img = blockIdx.y; img < n; img += gridDim.y) {
+    const unsigned short* pl = x + ((size_t)img * c + ch) * hw;
+    for (int i = threadIdx.x; i < hw; i += blockDim.x) m = max(m, (unsigned)(pl[i] & 0x7fffu));
+  }
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0 && m) atomicMax(amax + ch, m);
+}
+
+__device__ __forceinline__ float f8_inv_scale(unsigned amax_bits) {
+  const float a = __half2float(__ushort_as_half((unsigned short)amax_bits));
+  return a > 0.f ? __half2float(__float2half_rn(fminf(448.f / (4.f * a), 65504.f))) : 1.f;
+}
+
+// e4m3 hi and lo of an fp32 value
+__device__ __forceinline__ void f8_split(float v, uint8_t& hi, uint8_t& lo) {
+  const __nv_fp8_e4m3 h(v);
+  const float hf = static_cast<float>(h);
+  const __nv_fp8_e4m3 l(v - hf);
+  hi = h.__x;
+  lo = l.__x;
+}
+
+// U (fp16, unfused GEMM layout) -> U8 [t][k pair][K-step of 32][term][rows x
+// 32 bytes in the K-major core-matrix interleave] and su[t][k].  Thread per
+// (tap, output channel); inv_c is recomputed from amax.
+__global__ void __launch_bounds__(256) f8_u_kernel(const __half* __restrict__ u2, const unsigned* __restrict__ amax,
+                                                   uint8_t* u8, float* su, int K, int C) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= 16 * K) return;
+  const int t = row / K, k = row - t * K;
+  auto uval = [&](int c) { return __half2float(u2[u2_offset(t, k, c, K, C)]) / f8_inv_scale(amax[c]); };
+  float m = 0.f;
+  for (int c = 0; c < C; ++c) m = fmaxf(m, fabsf(uval(c)));
+  const float s = m > 0.f ? m / 448.f : 1.f;
+  su[row] = s;
+  const int kp = k / (2 * KB2), r = k - kp * 2 * KB2;          // row within the k pair
+  const int rk = min(2 * KB2, K - kp * 2 * KB2);                // rows of the k pair
+  uint8_t* blk = u8 + ((size_t)t * K + (size_t)kp * 2 * KB2) * C * 2;
+  for (int c = 0; c < C; ++c) {
+    uint8_t hi, lo;
+    f8_split(uval(c) / s, hi, lo);
+    const int c32 = c >> 5, cc = c & 31;
+    const size_t off = (size_t)(r >> 3) * 256 + (cc >> 4) * 128 + (r & 7) * 16 + (cc & 15);
+    blk[((size_t)c32 * 2 + 0) * rk * 32 + off] = hi;
+    blk[((size_t)c32 * 2 + 1) * rk * 32 + off] = lo;
+  }
+}
+
+// V2 in e4m3 hi + lo: as v2_layout_kernel, then V' = fp16(V) * inv_c (fp16
+// product, as the fused fp8 variant) split into e4m3 hi and lo.  Per tap the
+// tile block's K-steps of 32 channels hold [hi | lo] pieces of rows x 32
+// bytes; inside a piece tile i, channel c (of 32) at byte (i >> 3) * 256 +
+// (c >> 4) * 128 + (i & 7) * 16 + (c & 15).  Item = (tile block, 16-channel
+// half of a K-step); thread = (tile, 8 channels).
+__global__ void __launch_bounds__(256, 2) v2f8_layout_kernel(KernelParam p) {
+  const int C = p.c, H = p.h, W = p.w;
+  const int TP = (p.Oh + 1) >> 1, TQ = (p.Ow + 1) >> 1;
+  const int NT = p.n * TP * TQ;
+  const int NT8 = (NT + 7) & ~7;
+  const int CS = C >> 4, nTB = (NT8 + 127) >> 7;
+  const int items = nTB * CS;
+  const int il = threadIdx.x & 127, hh = threadIdx.x >> 7;
+  const unsigned short* X = static_cast<const unsigned short*>(p.pin);
+  const unsigned* amax = static_cast<const unsigned*>(p.mid_result);
+  uint8_t* v2 = static_cast<uint8_t*>(p.transform_pin);
+  const size_t plane = (size_t)H * W;
+  const size_t tap_bytes = (size_t)NT8 * C * 2;   // hi and lo: two bytes per tile and channel
+  const bool w_even = (W & 1) == 0;
+  for (int item = blockIdx.x; item < items; item += gridDim.x) {
+    const int tb = item / CS, cs = item - tb * CS;
+    const int rows = min(128, NT8 - tb * 128);
+    if (il >= rows) continue;
+    const int tile = tb * 128 + il;
+    const bool live = tile < NT;
+    int n = 0, ty = 0, tx = 0;
+    if (live) {
+      const int per = TP * TQ;
+      n = tile / per;
+      const int r = tile - n * per;
+      ty = r / TQ;
+      tx = r - ty * TQ;
+    }
+    const int y0 = 2 * ty - 1, x0 = 2 * tx;
+    const int c0 = cs * 16 + hh * 8;
+    const unsigned short* base = X + ((size_t)n * C + c0) * plane;
+    uint32_t inv2[4];                            // (inv_c, inv_c+1) as fp16x2
+#pragma unroll
+    for (int cp = 0; cp < 4; ++cp) {
+      const __half2 iv = __floats2half2_rn(f8_inv_scale(amax[c0 + 2 * cp]), f8_inv_scale(amax[c0 + 2 * cp + 1]));
+      inv2[cp] = *reinterpret_cast<const uint32_t*>(&iv);
+    }
+    uint32_t vt[16][4];
+#pragma unroll
+    for (int cp = 0; cp < 4; ++cp) {
+      uint32_t col[4][4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int y = y0 + r;
+        const bool rok = live && y >= 0 && y < H;
+        uint32_t a[2][3];
+#pragma unroll
+        for (int ch = 0; ch < 2; ++ch) {
+          const unsigned short* row = base + (size_t)(2 * cp + ch) * plane + (size_t)(rok ? y : 0) * W;
+          if (w_even) {
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+              const int x = x0 - 2 + 2 * q;
+              a[ch][q] = (rok && x >= 0 && x < W) ? *reinterpret_cast<const uint32_t*>(row + x) : 0u;
+            }
+          } else {
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+              const int x = x0 - 2 + 2 * q;
+              const uint32_t lo = (rok && x >= 0 && x < W) ? row[x] : 0u;
+              const uint32_t hi = (rok && x + 1 >= 0 && x + 1 < W) ? row[x + 1] : 0u;
+              a[ch][q] = lo | (hi << 16);
+            }
+          }
+        }
+        col[r][0] = __byte_perm(a[0][0], a[1][0], 0x7632);
+        col[r][1] = __byte_perm(a[0][1], a[1][1], 0x5410);
+        col[r][2] = __byte_perm(a[0][1], a[1][1], 0x7632);
+        col[r][3] = __byte_perm(a[0][2], a[1][2], 0x5410);
+      }
+      uint32_t e[4][4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        e[0][j] = hsub2(col[0][j], col[2][j]);
+        e[1][j] = hadd2(col[1][j], col[2][j]);
+        e[2][j] = hsub2(col[2][j], col[1][j]);
+        e[3][j] = hsub2(col[1][j], col[3][j]);
+      }
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        vt[4 * a + 0][cp] = hsub2(e[a][0], e[a][2]);
+        vt[4 * a + 1][cp] = hadd2(e[a][1], e[a][2]);
+        vt[4 * a + 2][cp] = hsub2(e[a][2], e[a][1]);
+        vt[4 * a + 3][cp] = hsub2(e[a][1], e[a][3]);
+      }
+    }
+    // K-step cs >> 1 of 32 channels, this thread's 8 channels at (cs & 1) * 16 + hh * 8
+    const int rws = rows * 32;                   // bytes of one piece
+    uint8_t* out = v2 + (size_t)tb * 128 * C * 2 + (size_t)(cs >> 1) * 2 * rws + (il >> 3) * 256 + (cs & 1) * 128 +
+                   (il & 7) * 16 + hh * 8;
+#pragma unroll
+    for (int t = 0; t < 16; ++t) {
+      uint32_t hw[2], lw[2];
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        uint8_t hb[4], lb[4];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const uint32_t w = hmul2_u32(vt[t][2 * q + u], inv2[2 * q + u]);
+          const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&w));
+          f8_split(f.x, hb[2 * u], lb[2 * u]);
+          f8_split(f.y, hb[2 * u + 1], lb[2 * u + 1]);
+        }
+        hw[q] = (uint32_t)hb[0] | ((uint32_t)hb[1] << 8) | ((uint32_t)hb[2] << 16) | ((uint32_t)hb[3] << 24);
+        lw[q] = (uint32_t)lb[0] | ((uint32_t)lb[1] << 8) | ((uint32_t)lb[2] << 16) | ((uint32_t)lb[3] << 24);
+      }
+      *reinterpret_cast<uint2*>(out + (size_t)t * tap_bytes) = make_uint2(hw[0], hw[1]);
+      *reinterpret_cast<uint2*>(out + (size_t)t * tap_bytes + rws) = make_uint2(lw[0], lw[1]);
+    }
+  }
+}
+
+// =============================================================================
 // Output transform
 // =============================================================================
 // Persistent: work item = (tile block tb, 8 output channels kg), item i =
@@ -1795,6 +2012,7 @@ void* wino_twostage_gemm_kernel_ptr_for(int c) {
 void* wino_twostage_pair_kernel_ptr() { return (void*)twostage_pair_kernel; }
 void* wino_twostage_res_kernel_ptr() { return (void*)twostage_res_kernel_t<false>; }
 void* wino_twostage_resv_kernel_ptr() { return (void*)twostage_res_kernel_t<true>; }
+void* wino_twostage_f8_kernel_ptr() { return (void*)twostage_res_kernel_t<true, true>; }
 void* wino_twostage_stream_kernel_ptr() { return (void*)twostage_stream_kernel; }
 void* wino_twostage_output_kernel_ptr() { return (void*)twostage_output_kernel; }
 int wino_twostage_threads_for(int c) {
@@ -1827,6 +2045,8 @@ int wino_twostage_prepare() {
   if (cudaFuncSetAttribute(twostage_res_kernel_t<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            trs::SMEM_BYTES) != cudaSuccess ||
       cudaFuncSetAttribute(twostage_res_kernel_t<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           trs::SMEM_BYTES) != cudaSuccess ||
+      cudaFuncSetAttribute(twostage_res_kernel_t<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            trs::SMEM_BYTES) != cudaSuccess)
     return 1;
   // the resident-U kernel's warpgroups split exactly the registers it is
@@ -1913,6 +2133,72 @@ void wino_twostage_output_grid(int n, int h, int w, int k, int sms, unsigned* gx
   const long long cap = (long long)WINO_OT_MINB * sms;
   *gx = (unsigned)(items < cap ? items : cap);
   *gy = 1;
+}
+
+// fp8 hi+lo two-stage path (extension API).  Workspace, each part 256-byte
+// aligned: channel maxima (C u32), su (16 K fp32), U8 (16 K C x 2 bytes),
+// V2 hi/lo (16 x tiles rounded up to 8 x C x 2 bytes), M16 (16 K tiles fp16).
+static size_t al256(size_t b) { return (b + 255) / 256 * 256; }
+static bool f8_ok(int n, int c, int h, int w, int k) {
+  return n >= 1 && h >= 1 && w >= 1 && k >= 16 && k % 16 == 0 && c >= 32 && c % 32 == 0 && c <= 256 &&
+         k <= 32767 && n <= 32767 && h <= 32767 && w <= 32767 && wino_twostage_tiles(n, h, w) < (1LL << 30) &&
+         (long long)n * (c >> 4) * ((tiles8(n, h, w) + 127) / 128) < (1LL << 31);
+}
+size_t wino_twostage_f8_workspace_bytes(int n, int c, int h, int w, int k) {
+  if (!f8_ok(n, c, h, w, k)) return 0;
+  return al256((size_t)c * 4) + al256((size_t)16 * k * 4) + al256((size_t)16 * k * c * 2) +
+         al256((size_t)16 * tiles8(n, h, w) * c * 2) + wino_twostage_m_bytes(n, h, w, k);
+}
+int wino_conv2d_twostage_f8(const void* x, const void* ucache2, void* workspace, void* y, int n, int c, int h,
+                            int w, int k, void* stream) {
+  if (!x || !ucache2 || !workspace || !y) return 1;                  // WINO_EINVAL
+  if ((reinterpret_cast<uintptr_t>(workspace) & 255) != 0) return 1;
+  if (!f8_ok(n, c, h, w, k)) return 2;                               // WINO_EUNSUPPORTED
+  if (wino_twostage_prepare() != 0) return 3;                         // WINO_ECUDA
+  uint8_t* ws = static_cast<uint8_t*>(workspace);
+  unsigned* amax = reinterpret_cast<unsigned*>(ws);
+  float* su = reinterpret_cast<float*>(ws + al256((size_t)c * 4));
+  uint8_t* u8 = reinterpret_cast<uint8_t*>(su) + al256((size_t)16 * k * 4);
+  uint8_t* v2 = u8 + al256((size_t)16 * k * c * 2);
+  uint8_t* m16 = v2 + al256((size_t)16 * tiles8(n, h, w) * c * 2);
+  const cudaStream_t s = (cudaStream_t)stream;
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return 3;
+  KernelParam p{};
+  p.pin = const_cast<void*>(x);
+  p.pout = y;
+  p.n = (short)n; p.c = (short)c; p.h = (short)h; p.w = (short)w; p.k = (short)k;
+  p.r = 3; p.s = 3; p.u = 1; p.v = 1; p.p = 1; p.q = 1; p.Oh = (short)h; p.Ow = (short)w;
+  if (cudaMemsetAsync(amax, 0, (size_t)c * 4, s) != cudaSuccess) return 3;
+  f8_amax_kernel<<<dim3(c, n < 16 ? n : 16), 256, 0, s>>>(static_cast<const unsigned short*>(x), amax, n, c, h * w);
+  f8_u_kernel<<<(16 * k + 255) / 256, 256, 0, s>>>(static_cast<const __half*>(ucache2), amax, u8, su, k, c);
+  // V2 hi/lo: the channel maxima come in through mid_result
+  p.transform_pin = v2;
+  p.mid_result = amax;
+  {
+    const long long items = (tiles8(n, h, w) + 127) / 128 * (c >> 4);
+    const long long cap = 2LL * sms;
+    v2f8_layout_kernel<<<(unsigned)(items < cap ? items : cap), 256, 0, s>>>(p);
+  }
+  // tap GEMM: U8 resident, su through pweight, M into the workspace
+  p.transform_filter = u8;
+  p.pweight = su;
+  p.mid_result = m16;
+  {
+    void* args[] = {&p};
+    if (cudaLaunchKernel((void*)twostage_res_kernel_t<true, true>,
+                         dim3(wino_twostage_gemm_grid(n, c, h, w, k, sms)), dim3(trs::NTHREAD_V), args,
+                         (size_t)trs::SMEM_BYTES, s) != cudaSuccess)
+      return 3;
+    unsigned ox, oy;
+    wino_twostage_output_grid(n, h, w, k, sms, &ox, &oy);
+    if (cudaLaunchKernel((void*)twostage_output_kernel, dim3(ox, oy), dim3(ot::NTHREAD), args,
+                         (size_t)ot::SMEM_BYTES, s) != cudaSuccess)
+      return 3;
+  }
+  return cudaGetLastError() == cudaSuccess ? 0 : 3;
 }
 
 uint32_t wino_twostage_error_read_clear() {

@@ -135,6 +135,31 @@ def conv2d_winograd_f8_emulated(x, w):
     return output_transform(m, n, k, h, wd)
 
 
+def conv2d_winograd_f8hilo_emulated(x, w):
+    """The two-stage fp8 hi+lo path's rounding points (a model of that path;
+    the reference has no fp8 path): inv_c as in the fp8 variant above;
+    V' = fp16(fp16(V) * inv_c), V_hi = e4m3(V'), V_lo = e4m3(V' - V_hi);
+    U' = fp16(U) / inv_c, su[t][k] = max_c |U'| / 448, U_hi / U_lo the same
+    split of U' / su; M = fp16(su * (U_hi V_hi + U_lo V_hi + U_hi V_lo)) with
+    wide accumulation; output transform in wide precision."""
+    n, c, h, wd = x.shape
+    k = w.shape[0]
+    amax = np.abs(np.asarray(x, np.float64)).max(axis=(0, 2, 3))
+    inv = np.where(amax > 0, 448.0 / (4.0 * np.where(amax > 0, amax, 1.0)), 1.0)
+    inv = _f16(np.minimum(inv, 65504.0))
+    vp = _f16(input_transform_f16(x) * inv[None, None, :])
+    vh = _e4m3(vp)
+    vl = _e4m3(vp - vh)
+    u1 = _f16(filter_transform(w)) / inv[None, None, :]
+    su = np.abs(u1).max(axis=2) / 448.0
+    su = np.where(su > 0, su, 1.0)
+    a = u1 / su[:, :, None]
+    uh = _e4m3(a)
+    ul = _e4m3(a - uh)
+    m = _f16((gemm(uh, vh) + gemm(ul, vh) + gemm(uh, vl)) * su[:, None, :])
+    return output_transform(m, n, k, h, wd)
+
+
 def conv2d_winograd_emulated(x, w, operand="f16"):
     """Winograd with the rounding points of the fused fp16/bf16 kernels.
 
