@@ -1373,13 +1373,22 @@ __global__ void __launch_bounds__(TMAV ? trs::NTHREAD_V : trs::NTHREAD, 1) twost
       auto st = [&](int cc, const float* v) {
         if (!live) return;
         __half* dst = mrow + (size_t)cc * ntb;
+        float sc[32];
+        if constexpr (F8) {
+          // the chunk's 32 scales (the same for every lane), 16-byte loads
+          const float4* s4 = reinterpret_cast<const float4*>(sur + cc);
 #pragma unroll
-        for (int jj = 0; jj < 16; ++jj)
-          dst[(size_t)jj * ntb] = __float2half_rn(F8 ? v[jj] * __ldg(sur + cc + jj) : v[jj]);
+          for (int q = 0; q < 8; ++q) {
+            if (q >= 4 && cc + 16 >= nrows) break;
+            const float4 f = __ldg(s4 + q);
+            sc[4 * q] = f.x; sc[4 * q + 1] = f.y; sc[4 * q + 2] = f.z; sc[4 * q + 3] = f.w;
+          }
+        }
+#pragma unroll
+        for (int jj = 0; jj < 16; ++jj) dst[(size_t)jj * ntb] = __float2half_rn(F8 ? v[jj] * sc[jj] : v[jj]);
         if (cc + 16 < nrows) {
 #pragma unroll
-          for (int jj = 16; jj < 32; ++jj)
-            dst[(size_t)jj * ntb] = __float2half_rn(F8 ? v[jj] * __ldg(sur + cc + jj) : v[jj]);
+          for (int jj = 16; jj < 32; ++jj) dst[(size_t)jj * ntb] = __float2half_rn(F8 ? v[jj] * sc[jj] : v[jj]);
         }
       };
       float va[32], vb[32];
@@ -1634,22 +1643,53 @@ __global__ void __launch_bounds__(256, WINO_V2_MINB) v2_layout_kernel(KernelPara
 // path (src/matrixmul.cuh:28-35 is fp16).
 
 // per-channel max |x| as fp16 magnitude bits (monotonic as unsigned);
-// amax must be zero on entry.  Grid (C, chunks of images).
-__global__ void __launch_bounds__(256) f8_amax_kernel(const unsigned short* __restrict__ x, unsigned* amax, int n,
+// amax must be zero on entry.  Grid (C, image groups): a CTA reduces its
+// channel over images g, g + gridDim.y, ... (16-byte loads when the planes
+// are 16-byte aligned, hw % 8 == 0) and issues one atomicMax.
+__global__ void __launch_bounds__(128) f8_amax_kernel(const unsigned short* __restrict__ x, unsigned* amax, int n,
                                                       int c, int hw) {
+  __shared__ unsigned wmax[4];
   const int ch = blockIdx.x;
+  const bool vec = (hw & 7) == 0 && (reinterpret_cast<uintptr_t>(x) & 15) == 0;
   unsigned m = 0;
   for (int img = blockIdx.y; img < n; img += gridDim.y) {
-    const unsigned short* pl = x + ((size_t)img * c + ch) * hw;
-    for (int i = threadIdx.x; i < hw; i += blockDim.x) m = max(m, (unsigned)(pl[i] & 0x7fffu));
+    const unsigned short* src = x + ((size_t)img * c + ch) * hw;
+    if (vec) {
+      const uint4* s4 = reinterpret_cast<const uint4*>(src);
+      for (int i = threadIdx.x; i < hw / 8; i += blockDim.x) {
+        const uint4 v = __ldg(s4 + i);
+        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) m = max(m, max(w[j] & 0x7fffu, (w[j] >> 16) & 0x7fffu));
+      }
+    } else {
+      for (int i = threadIdx.x; i < hw; i += blockDim.x) m = max(m, (unsigned)(src[i] & 0x7fffu));
+    }
   }
   for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
-  if ((threadIdx.x & 31) == 0 && m) atomicMax(amax + ch, m);
+  if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    m = max(max(wmax[0], wmax[1]), max(wmax[2], wmax[3]));
+    if (m) atomicMax(amax + ch, m);
+  }
 }
 
 __device__ __forceinline__ float f8_inv_scale(unsigned amax_bits) {
   const float a = __half2float(__ushort_as_half((unsigned short)amax_bits));
   return a > 0.f ? __half2float(__float2half_rn(fminf(448.f / (4.f * a), 65504.f))) : 1.f;
+}
+
+// two fp16 -> two e4m3 (round to nearest, saturating) and back
+__device__ __forceinline__ uint32_t e4m3x2_of_h2(uint32_t h2) {
+  unsigned short r;
+  asm("cvt.rn.satfinite.e4m3x2.f16x2 %0, %1;" : "=h"(r) : "r"(h2));
+  return r;
+}
+__device__ __forceinline__ uint32_t h2_of_e4m3x2(uint32_t e2) {
+  uint32_t r;
+  asm("cvt.rn.f16x2.e4m3x2 %0, %1;" : "=r"(r) : "h"((unsigned short)e2));
+  return r;
 }
 
 // e4m3 hi and lo of an fp32 value
@@ -1662,22 +1702,24 @@ __device__ __forceinline__ void f8_split(float v, uint8_t& hi, uint8_t& lo) {
 }
 
 // U (fp16, unfused GEMM layout) -> U8 [t][k pair][K-step of 32][term][rows x
-// 32 bytes in the K-major core-matrix interleave] and su[t][k].  Thread per
-// (tap, output channel); inv_c is recomputed from amax.
+// 32 bytes in the K-major core-matrix interleave] and su[t][k].  Warp per
+// (tap, output channel): lanes stride over the channels, the row maximum by
+// shuffles; inv_c is recomputed from amax.
 __global__ void __launch_bounds__(256) f8_u_kernel(const __half* __restrict__ u2, const unsigned* __restrict__ amax,
                                                    uint8_t* u8, float* su, int K, int C) {
-  const int row = blockIdx.x * blockDim.x + threadIdx.x;
-  if (row >= 16 * K) return;
+  const int row = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (row >= 16 * K) return;                     // whole warps leave together
   const int t = row / K, k = row - t * K;
   auto uval = [&](int c) { return __half2float(u2[u2_offset(t, k, c, K, C)]) / f8_inv_scale(amax[c]); };
   float m = 0.f;
-  for (int c = 0; c < C; ++c) m = fmaxf(m, fabsf(uval(c)));
+  for (int c = lane; c < C; c += 32) m = fmaxf(m, fabsf(uval(c)));
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
   const float s = m > 0.f ? m / 448.f : 1.f;
-  su[row] = s;
+  if (lane == 0) su[row] = s;
   const int kp = k / (2 * KB2), r = k - kp * 2 * KB2;          // row within the k pair
   const int rk = min(2 * KB2, K - kp * 2 * KB2);                // rows of the k pair
   uint8_t* blk = u8 + ((size_t)t * K + (size_t)kp * 2 * KB2) * C * 2;
-  for (int c = 0; c < C; ++c) {
+  for (int c = lane; c < C; c += 32) {
     uint8_t hi, lo;
     f8_split(uval(c) / s, hi, lo);
     const int c32 = c >> 5, cc = c & 31;
@@ -1785,19 +1827,20 @@ __global__ void __launch_bounds__(256, 2) v2f8_layout_kernel(KernelParam p) {
                    (il & 7) * 16 + hh * 8;
 #pragma unroll
     for (int t = 0; t < 16; ++t) {
+      // V' = fp16(V * inv); hi = e4m3(V'); lo = e4m3(V' - hi), the fp16
+      // difference exact (hi is V' rounded to 4 significant bits)
       uint32_t hw[2], lw[2];
 #pragma unroll
       for (int q = 0; q < 2; ++q) {
-        uint8_t hb[4], lb[4];
+        uint32_t hp[2], lp[2];
 #pragma unroll
         for (int u = 0; u < 2; ++u) {
           const uint32_t w = hmul2_u32(vt[t][2 * q + u], inv2[2 * q + u]);
-          const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&w));
-          f8_split(f.x, hb[2 * u], lb[2 * u]);
-          f8_split(f.y, hb[2 * u + 1], lb[2 * u + 1]);
+          hp[u] = e4m3x2_of_h2(w);
+          lp[u] = e4m3x2_of_h2(hsub2(w, h2_of_e4m3x2(hp[u])));
         }
-        hw[q] = (uint32_t)hb[0] | ((uint32_t)hb[1] << 8) | ((uint32_t)hb[2] << 16) | ((uint32_t)hb[3] << 24);
-        lw[q] = (uint32_t)lb[0] | ((uint32_t)lb[1] << 8) | ((uint32_t)lb[2] << 16) | ((uint32_t)lb[3] << 24);
+        hw[q] = hp[0] | (hp[1] << 16);
+        lw[q] = lp[0] | (lp[1] << 16);
       }
       *reinterpret_cast<uint2*>(out + (size_t)t * tap_bytes) = make_uint2(hw[0], hw[1]);
       *reinterpret_cast<uint2*>(out + (size_t)t * tap_bytes + rws) = make_uint2(lw[0], lw[1]);
@@ -2172,8 +2215,13 @@ int wino_conv2d_twostage_f8(const void* x, const void* ucache2, void* workspace,
   p.n = (short)n; p.c = (short)c; p.h = (short)h; p.w = (short)w; p.k = (short)k;
   p.r = 3; p.s = 3; p.u = 1; p.v = 1; p.p = 1; p.q = 1; p.Oh = (short)h; p.Ow = (short)w;
   if (cudaMemsetAsync(amax, 0, (size_t)c * 4, s) != cudaSuccess) return 3;
-  f8_amax_kernel<<<dim3(c, n < 16 ? n : 16), 256, 0, s>>>(static_cast<const unsigned short*>(x), amax, n, c, h * w);
-  f8_u_kernel<<<(16 * k + 255) / 256, 256, 0, s>>>(static_cast<const __half*>(ucache2), amax, u8, su, k, c);
+  {
+    // enough CTAs to cover the GPU several times, at most one per image
+    int groups = (32 * sms + c - 1) / c;
+    if (groups > n) groups = n;
+    f8_amax_kernel<<<dim3(c, groups), 128, 0, s>>>(static_cast<const unsigned short*>(x), amax, n, c, h * w);
+  }
+  f8_u_kernel<<<(16 * k * 32 + 255) / 256, 256, 0, s>>>(static_cast<const __half*>(ucache2), amax, u8, su, k, c);
   // V2 hi/lo: the channel maxima come in through mid_result
   p.transform_pin = v2;
   p.mid_result = amax;
