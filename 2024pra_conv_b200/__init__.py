@@ -121,9 +121,9 @@ def lib():
             "wino_twostage_res_kernel_ptr": ([], vp),
             "wino_twostage_resv_kernel_ptr": ([], vp),
             "wino_twostage_prepass_bytes": ([i, i, i, i], sz),
-            "wino_twostage_f8_workspace_bytes": ([i, i, i, i, i], sz),
-            "wino_conv2d_twostage_f8": ([vp, vp, vp, vp, i, i, i, i, i, vp], i),
-            "wino_twostage_f8_kernel_ptr": ([], vp),
+            "wino_twostage_f8_workspace_bytes": ([i, i, i, i, i, i], sz),
+            "wino_conv2d_twostage_f8": ([vp, vp, vp, vp, i, i, i, i, i, i, vp], i),
+            "wino_twostage_f8_kernel_ptr": ([i], vp),
             "wino_twostage_stream_kernel_ptr": ([], vp),
             "wino_dropin_filter_u2_kernel_ptr": ([], vp),
             "wino_twostage_output_kernel_ptr": ([], vp),
@@ -390,21 +390,23 @@ def conv2d_twostage(x, ucache2, k, out=None, workspace=None, stream=None):
     return y
 
 
-def conv2d_twostage_f8(x, ucache2, k, out=None, workspace=None, stream=None):
-    """Two-stage conv with the fp8 hi+lo tensor-core GEMM (U and V each as
-    e4m3 hi + lo, three kind::f8f6f4 MMAs per 32-channel step) on a U cache
-    from filter_transform_unfused.  C a multiple of 32, at most 256."""
+def conv2d_twostage_f8(x, ucache2, k, hilo=True, out=None, workspace=None, stream=None):
+    """Two-stage conv with an fp8 e4m3 tensor-core GEMM on a U cache from
+    filter_transform_unfused: hilo=True splits U and V into hi + lo terms
+    (three kind::f8f6f4 MMAs per 32-channel step, fp16-level accuracy),
+    hilo=False uses single terms (one MMA, faster, single-term fp8
+    accuracy).  C a multiple of 32, at most 256."""
     import torch
     n, c, h, wd = x.shape
     y = out if out is not None else torch.empty((n, k, h, wd), dtype=torch.float16, device=x.device)
-    nb = int(lib().wino_twostage_f8_workspace_bytes(n, c, h, wd, k))
+    nb = int(lib().wino_twostage_f8_workspace_bytes(n, c, h, wd, k, int(hilo)))
     if nb == 0:
         raise WinoError(WINO_EUNSUPPORTED, "wino_twostage_f8_workspace_bytes")
     if workspace is None:
         workspace = _aligned_ws(nb, x.device)
     _check(lib().wino_conv2d_twostage_f8(ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(ucache2.data_ptr()),
                                          ctypes.c_void_p(workspace.data_ptr()), ctypes.c_void_p(y.data_ptr()),
-                                         n, c, h, wd, k, _stream(stream)), "conv2d_twostage_f8")
+                                         n, c, h, wd, k, int(hilo), _stream(stream)), "conv2d_twostage_f8")
     return y
 
 

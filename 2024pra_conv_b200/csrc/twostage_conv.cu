@@ -1174,9 +1174,12 @@ __device__ __forceinline__ Prod prod(const Geo& g, const uint8_t* xr, int t, int
 // kind::f8f6f4 MMAs accumulate hi.hi + lo.hi + hi.lo; the per-input-channel
 // V scale is folded into U, and the epilogue multiplies by the per-(tap,
 // output channel) U scale su (p.pweight, fp32 [16][K]) before rounding M.
-template <bool TMAV, bool F8 = false>
+// F8 = 1: single e4m3 terms (one MMA per K-step, one byte per tile and
+// channel, a K-step of 32 channels per piece).
+template <bool TMAV, int F8 = 0>
 __global__ void __launch_bounds__(TMAV ? trs::NTHREAD_V : trs::NTHREAD, 1) twostage_res_kernel_t(KernelParam p) {
-  static_assert(!F8 || TMAV, "the fp8 variant reads V2 by bulk copy");
+  static_assert(F8 == 0 || TMAV, "the fp8 variants read V2 by bulk copy");
+  constexpr int TERMS = F8 == 1 ? 1 : 2;        // bytes per tile and channel in V2 and U
   using namespace trs;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   __shared__ Shared sh;
@@ -1186,7 +1189,10 @@ __global__ void __launch_bounds__(TMAV ? trs::NTHREAD_V : trs::NTHREAD, 1) twost
   const int warp = warp_id(), lane = lane_id();
   uint32_t* err = &g_twostage_err;
   const Sched sc = make_sched(16 * g.nKP, g.nTB, (int)blockIdx.x, (int)gridDim.x);
-  const int nst = (g.CS + SK - 1) / SK;
+  // pieces of rows x 32 bytes per unit: 16-channel steps (fp16), K-step
+  // terms (fp8 hi+lo: two per 32 channels), K-steps (single fp8)
+  const int npc = F8 == 1 ? g.C / 32 : g.CS;
+  const int nst = (npc + SK - 1) / SK;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < NSTAGE; ++s) {
@@ -1224,8 +1230,8 @@ __global__ void __launch_bounds__(TMAV ? trs::NTHREAD_V : trs::NTHREAD, 1) twost
       for (int i = 0; i < sc.cnt && !*abort_flag; ++i) {
         const Unit un = sched_unit(g, sc, i);
         const int rows = min(128, NT8 - un.tb * 128);
-        // two bytes per tile and channel: fp16, or the fp8 hi and lo terms
-        const uint8_t* src = v2 + ((size_t)un.t * NT8 + (size_t)un.tb * 128) * g.C * 2;
+        // TERMS bytes per tile and channel: fp16 or the fp8 hi and lo terms (2), single fp8 (1)
+        const uint8_t* src = v2 + ((size_t)un.t * NT8 + (size_t)un.tb * 128) * g.C * TERMS;
         bool ok = true;
         for (int j = 0; j < nst; ++j, ++it) {
           const int st = it % NSTAGE;
@@ -1234,7 +1240,7 @@ __global__ void __launch_bounds__(TMAV ? trs::NTHREAD_V : trs::NTHREAD, 1) twost
             ok = false;
             break;
           }
-          const int nk = min(SK, g.CS - j * SK);
+          const int nk = min(SK, npc - j * SK);
           const uint32_t piece = (uint32_t)(rows * 32);
           mbar_arrive_expect_tx(&sh.full[st], (uint32_t)nk * piece);
           uint8_t* dst = smem + U_BYTES + st * STAGE_A;
@@ -1272,11 +1278,11 @@ __global__ void __launch_bounds__(TMAV ? trs::NTHREAD_V : trs::NTHREAD, 1) twost
           cur = un.combo;
           uint32_t bytes = 0;
 #pragma unroll
-          for (int q = 0; q < KPU; ++q) bytes += (uint32_t)(kbs[q] * g.C * 2);
+          for (int q = 0; q < KPU; ++q) bytes += (uint32_t)(kbs[q] * g.C * TERMS);
           mbar_arrive_expect_tx(&sh.ufull, bytes);
-          if constexpr (F8) {
+          if constexpr (F8 != 0) {
             // the combo's [K-step][term][rows x 32 B] block is contiguous
-            bulk_g2s(smem, u2 + ((size_t)un.t * g.K + (size_t)un.kp * 2 * KB2) * g.C * 2, bytes, &sh.ufull);
+            bulk_g2s(smem, u2 + ((size_t)un.t * g.K + (size_t)un.kp * 2 * KB2) * g.C * TERMS, bytes, &sh.ufull);
           } else {
             for (int cs = 0; cs < g.CS; ++cs)
 #pragma unroll
@@ -1304,9 +1310,17 @@ __global__ void __launch_bounds__(TMAV ? trs::NTHREAD_V : trs::NTHREAD, 1) twost
             break;
           }
           tc_fence_after();
-          const int nk = min(SK, g.CS - j * SK);
+          const int nk = min(SK, npc - j * SK);
           const uint64_t adesc = smem_desc(sbase + U_BYTES + st * STAGE_A, 128, 256);
-          if constexpr (F8) {
+          if constexpr (F8 == 1) {
+            const uint32_t step = (uint32_t)(kbs[0] + kbs[1]) * 32 >> 4;   // one K-step of U
+            for (int kk = 0; kk < nk; ++kk)
+              mma_f8(d, adesc + (uint64_t)(kk * (A_STEP >> 4)), bdesc0 + (uint64_t)(j * SK + kk) * step, idesc,
+                     (j > 0 || kk > 0) ? 1u : 0u);
+            mma_commit(&sh.empty[st]);
+            continue;
+          }
+          if constexpr (F8 == 2) {
             // nk pieces = nk / 2 K-steps of 32 channels, each hi then lo
             const uint32_t rk = (uint32_t)(kbs[0] + kbs[1]);
             const uint32_t term = rk * 32 >> 4;        // descriptor step between the terms of U
@@ -1369,12 +1383,12 @@ __global__ void __launch_bounds__(TMAV ? trs::NTHREAD_V : trs::NTHREAD, 1) twost
         if (cc + 16 < nrows) tmem_ld16(taddr + cc + 16, v + 16);
       };
       // fp8: M = su[t][k] * D (one fp32 product, then the fp16 rounding)
-      const float* sur = F8 ? static_cast<const float*>(p.pweight) + (size_t)un.t * g.K + kb * KB2 : nullptr;
+      const float* sur = F8 != 0 ? static_cast<const float*>(p.pweight) + (size_t)un.t * g.K + kb * KB2 : nullptr;
       auto st = [&](int cc, const float* v) {
         if (!live) return;
         __half* dst = mrow + (size_t)cc * ntb;
         float sc[32];
-        if constexpr (F8) {
+        if constexpr (F8 != 0) {
           // the chunk's 32 scales (the same for every lane), 16-byte loads
           const float4* s4 = reinterpret_cast<const float4*>(sur + cc);
 #pragma unroll
@@ -1385,10 +1399,10 @@ __global__ void __launch_bounds__(TMAV ? trs::NTHREAD_V : trs::NTHREAD, 1) twost
           }
         }
 #pragma unroll
-        for (int jj = 0; jj < 16; ++jj) dst[(size_t)jj * ntb] = __float2half_rn(F8 ? v[jj] * sc[jj] : v[jj]);
+        for (int jj = 0; jj < 16; ++jj) dst[(size_t)jj * ntb] = __float2half_rn(F8 != 0 ? v[jj] * sc[jj] : v[jj]);
         if (cc + 16 < nrows) {
 #pragma unroll
-          for (int jj = 16; jj < 32; ++jj) dst[(size_t)jj * ntb] = __float2half_rn(F8 ? v[jj] * sc[jj] : v[jj]);
+          for (int jj = 16; jj < 32; ++jj) dst[(size_t)jj * ntb] = __float2half_rn(F8 != 0 ? v[jj] * sc[jj] : v[jj]);
         }
       };
       float va[32], vb[32];
@@ -1706,7 +1720,7 @@ __device__ __forceinline__ void f8_split(float v, uint8_t& hi, uint8_t& lo) {
 // (tap, output channel): lanes stride over the channels, the row maximum by
 // shuffles; inv_c is recomputed from amax.
 __global__ void __launch_bounds__(256) f8_u_kernel(const __half* __restrict__ u2, const unsigned* __restrict__ amax,
-                                                   uint8_t* u8, float* su, int K, int C) {
+                                                   uint8_t* u8, float* su, int K, int C, int terms) {
   const int row = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
   if (row >= 16 * K) return;                     // whole warps leave together
   const int t = row / K, k = row - t * K;
@@ -1718,14 +1732,14 @@ __global__ void __launch_bounds__(256) f8_u_kernel(const __half* __restrict__ u2
   if (lane == 0) su[row] = s;
   const int kp = k / (2 * KB2), r = k - kp * 2 * KB2;          // row within the k pair
   const int rk = min(2 * KB2, K - kp * 2 * KB2);                // rows of the k pair
-  uint8_t* blk = u8 + ((size_t)t * K + (size_t)kp * 2 * KB2) * C * 2;
+  uint8_t* blk = u8 + ((size_t)t * K + (size_t)kp * 2 * KB2) * C * terms;
   for (int c = lane; c < C; c += 32) {
     uint8_t hi, lo;
     f8_split(uval(c) / s, hi, lo);
     const int c32 = c >> 5, cc = c & 31;
     const size_t off = (size_t)(r >> 3) * 256 + (cc >> 4) * 128 + (r & 7) * 16 + (cc & 15);
-    blk[((size_t)c32 * 2 + 0) * rk * 32 + off] = hi;
-    blk[((size_t)c32 * 2 + 1) * rk * 32 + off] = lo;
+    blk[((size_t)c32 * terms + 0) * rk * 32 + off] = hi;
+    if (terms == 2) blk[((size_t)c32 * 2 + 1) * rk * 32 + off] = lo;
   }
 }
 
@@ -1735,6 +1749,7 @@ __global__ void __launch_bounds__(256) f8_u_kernel(const __half* __restrict__ u2
 // bytes; inside a piece tile i, channel c (of 32) at byte (i >> 3) * 256 +
 // (c >> 4) * 128 + (i & 7) * 16 + (c & 15).  Item = (tile block, 16-channel
 // half of a K-step); thread = (tile, 8 channels).
+template <int TERMS>
 __global__ void __launch_bounds__(256, 2) v2f8_layout_kernel(KernelParam p) {
   const int C = p.c, H = p.h, W = p.w;
   const int TP = (p.Oh + 1) >> 1, TQ = (p.Ow + 1) >> 1;
@@ -1747,7 +1762,7 @@ __global__ void __launch_bounds__(256, 2) v2f8_layout_kernel(KernelParam p) {
   const unsigned* amax = static_cast<const unsigned*>(p.mid_result);
   uint8_t* v2 = static_cast<uint8_t*>(p.transform_pin);
   const size_t plane = (size_t)H * W;
-  const size_t tap_bytes = (size_t)NT8 * C * 2;   // hi and lo: two bytes per tile and channel
+  const size_t tap_bytes = (size_t)NT8 * C * TERMS;   // bytes per tile and channel: the terms
   const bool w_even = (W & 1) == 0;
   for (int item = blockIdx.x; item < items; item += gridDim.x) {
     const int tb = item / CS, cs = item - tb * CS;
@@ -1823,7 +1838,7 @@ __global__ void __launch_bounds__(256, 2) v2f8_layout_kernel(KernelParam p) {
     }
     // K-step cs >> 1 of 32 channels, this thread's 8 channels at (cs & 1) * 16 + hh * 8
     const int rws = rows * 32;                   // bytes of one piece
-    uint8_t* out = v2 + (size_t)tb * 128 * C * 2 + (size_t)(cs >> 1) * 2 * rws + (il >> 3) * 256 + (cs & 1) * 128 +
+    uint8_t* out = v2 + (size_t)tb * 128 * C * TERMS + (size_t)(cs >> 1) * TERMS * rws + (il >> 3) * 256 + (cs & 1) * 128 +
                    (il & 7) * 16 + hh * 8;
 #pragma unroll
     for (int t = 0; t < 16; ++t) {
@@ -1837,13 +1852,13 @@ __global__ void __launch_bounds__(256, 2) v2f8_layout_kernel(KernelParam p) {
         for (int u = 0; u < 2; ++u) {
           const uint32_t w = hmul2_u32(vt[t][2 * q + u], inv2[2 * q + u]);
           hp[u] = e4m3x2_of_h2(w);
-          lp[u] = e4m3x2_of_h2(hsub2(w, h2_of_e4m3x2(hp[u])));
+          lp[u] = TERMS == 2 ? e4m3x2_of_h2(hsub2(w, h2_of_e4m3x2(hp[u]))) : 0u;
         }
         hw[q] = hp[0] | (hp[1] << 16);
         lw[q] = lp[0] | (lp[1] << 16);
       }
       *reinterpret_cast<uint2*>(out + (size_t)t * tap_bytes) = make_uint2(hw[0], hw[1]);
-      *reinterpret_cast<uint2*>(out + (size_t)t * tap_bytes + rws) = make_uint2(lw[0], lw[1]);
+      if (TERMS == 2) *reinterpret_cast<uint2*>(out + (size_t)t * tap_bytes + rws) = make_uint2(lw[0], lw[1]);
     }
   }
 }
@@ -2055,7 +2070,6 @@ void* wino_twostage_gemm_kernel_ptr_for(int c) {
 void* wino_twostage_pair_kernel_ptr() { return (void*)twostage_pair_kernel; }
 void* wino_twostage_res_kernel_ptr() { return (void*)twostage_res_kernel_t<false>; }
 void* wino_twostage_resv_kernel_ptr() { return (void*)twostage_res_kernel_t<true>; }
-void* wino_twostage_f8_kernel_ptr() { return (void*)twostage_res_kernel_t<true, true>; }
 void* wino_twostage_stream_kernel_ptr() { return (void*)twostage_stream_kernel; }
 void* wino_twostage_output_kernel_ptr() { return (void*)twostage_output_kernel; }
 int wino_twostage_threads_for(int c) {
@@ -2089,7 +2103,9 @@ int wino_twostage_prepare() {
                            trs::SMEM_BYTES) != cudaSuccess ||
       cudaFuncSetAttribute(twostage_res_kernel_t<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            trs::SMEM_BYTES) != cudaSuccess ||
-      cudaFuncSetAttribute(twostage_res_kernel_t<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      cudaFuncSetAttribute(twostage_res_kernel_t<true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           trs::SMEM_BYTES) != cudaSuccess ||
+      cudaFuncSetAttribute(twostage_res_kernel_t<true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            trs::SMEM_BYTES) != cudaSuccess)
     return 1;
   // the resident-U kernel's warpgroups split exactly the registers it is
@@ -2178,32 +2194,39 @@ void wino_twostage_output_grid(int n, int h, int w, int k, int sms, unsigned* gx
   *gy = 1;
 }
 
-// fp8 hi+lo two-stage path (extension API).  Workspace, each part 256-byte
-// aligned: channel maxima (C u32), su (16 K fp32), U8 (16 K C x 2 bytes),
-// V2 hi/lo (16 x tiles rounded up to 8 x C x 2 bytes), M16 (16 K tiles fp16).
+// fp8 two-stage path (extension API); hilo 1: e4m3 hi + lo terms, 0: single
+// e4m3 terms.  Workspace, each part 256-byte aligned: channel maxima (C
+// u32), su (16 K fp32), U8 (16 K C x terms bytes), V2 (16 x tiles rounded up
+// to 8 x C x terms bytes), M16 (16 K tiles fp16).
 static size_t al256(size_t b) { return (b + 255) / 256 * 256; }
-static bool f8_ok(int n, int c, int h, int w, int k) {
-  return n >= 1 && h >= 1 && w >= 1 && k >= 16 && k % 16 == 0 && c >= 32 && c % 32 == 0 && c <= 256 &&
-         k <= 32767 && n <= 32767 && h <= 32767 && w <= 32767 && wino_twostage_tiles(n, h, w) < (1LL << 30) &&
+static bool f8_ok(int n, int c, int h, int w, int k, int hilo) {
+  return (hilo == 0 || hilo == 1) && n >= 1 && h >= 1 && w >= 1 && k >= 16 && k % 16 == 0 && c >= 32 &&
+         c % 32 == 0 && c <= 256 && k <= 32767 && n <= 32767 && h <= 32767 && w <= 32767 &&
+         wino_twostage_tiles(n, h, w) < (1LL << 30) &&
          (long long)n * (c >> 4) * ((tiles8(n, h, w) + 127) / 128) < (1LL << 31);
 }
-size_t wino_twostage_f8_workspace_bytes(int n, int c, int h, int w, int k) {
-  if (!f8_ok(n, c, h, w, k)) return 0;
-  return al256((size_t)c * 4) + al256((size_t)16 * k * 4) + al256((size_t)16 * k * c * 2) +
-         al256((size_t)16 * tiles8(n, h, w) * c * 2) + wino_twostage_m_bytes(n, h, w, k);
+size_t wino_twostage_f8_workspace_bytes(int n, int c, int h, int w, int k, int hilo) {
+  if (!f8_ok(n, c, h, w, k, hilo)) return 0;
+  const size_t terms = hilo ? 2 : 1;
+  return al256((size_t)c * 4) + al256((size_t)16 * k * 4) + al256((size_t)16 * k * c * terms) +
+         al256((size_t)16 * tiles8(n, h, w) * c * terms) + wino_twostage_m_bytes(n, h, w, k);
+}
+void* wino_twostage_f8_kernel_ptr(int hilo) {
+  return hilo ? (void*)twostage_res_kernel_t<true, 2> : (void*)twostage_res_kernel_t<true, 1>;
 }
 int wino_conv2d_twostage_f8(const void* x, const void* ucache2, void* workspace, void* y, int n, int c, int h,
-                            int w, int k, void* stream) {
+                            int w, int k, int hilo, void* stream) {
   if (!x || !ucache2 || !workspace || !y) return 1;                  // WINO_EINVAL
   if ((reinterpret_cast<uintptr_t>(workspace) & 255) != 0) return 1;
-  if (!f8_ok(n, c, h, w, k)) return 2;                               // WINO_EUNSUPPORTED
+  if (!f8_ok(n, c, h, w, k, hilo)) return 2;                         // WINO_EUNSUPPORTED
   if (wino_twostage_prepare() != 0) return 3;                         // WINO_ECUDA
+  const int terms = hilo ? 2 : 1;
   uint8_t* ws = static_cast<uint8_t*>(workspace);
   unsigned* amax = reinterpret_cast<unsigned*>(ws);
   float* su = reinterpret_cast<float*>(ws + al256((size_t)c * 4));
   uint8_t* u8 = reinterpret_cast<uint8_t*>(su) + al256((size_t)16 * k * 4);
-  uint8_t* v2 = u8 + al256((size_t)16 * k * c * 2);
-  uint8_t* m16 = v2 + al256((size_t)16 * tiles8(n, h, w) * c * 2);
+  uint8_t* v2 = u8 + al256((size_t)16 * k * c * terms);
+  uint8_t* m16 = v2 + al256((size_t)16 * tiles8(n, h, w) * c * terms);
   const cudaStream_t s = (cudaStream_t)stream;
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) != cudaSuccess ||
@@ -2221,14 +2244,17 @@ int wino_conv2d_twostage_f8(const void* x, const void* ucache2, void* workspace,
     if (groups > n) groups = n;
     f8_amax_kernel<<<dim3(c, groups), 128, 0, s>>>(static_cast<const unsigned short*>(x), amax, n, c, h * w);
   }
-  f8_u_kernel<<<(16 * k * 32 + 255) / 256, 256, 0, s>>>(static_cast<const __half*>(ucache2), amax, u8, su, k, c);
-  // V2 hi/lo: the channel maxima come in through mid_result
+  f8_u_kernel<<<(16 * k * 32 + 255) / 256, 256, 0, s>>>(static_cast<const __half*>(ucache2), amax, u8, su, k, c,
+                                                         terms);
+  // V2: the channel maxima come in through mid_result
   p.transform_pin = v2;
   p.mid_result = amax;
   {
     const long long items = (tiles8(n, h, w) + 127) / 128 * (c >> 4);
     const long long cap = 2LL * sms;
-    v2f8_layout_kernel<<<(unsigned)(items < cap ? items : cap), 256, 0, s>>>(p);
+    const unsigned grid = (unsigned)(items < cap ? items : cap);
+    if (hilo) v2f8_layout_kernel<2><<<grid, 256, 0, s>>>(p);
+    else v2f8_layout_kernel<1><<<grid, 256, 0, s>>>(p);
   }
   // tap GEMM: U8 resident, su through pweight, M into the workspace
   p.transform_filter = u8;
@@ -2236,9 +2262,8 @@ int wino_conv2d_twostage_f8(const void* x, const void* ucache2, void* workspace,
   p.mid_result = m16;
   {
     void* args[] = {&p};
-    if (cudaLaunchKernel((void*)twostage_res_kernel_t<true, true>,
-                         dim3(wino_twostage_gemm_grid(n, c, h, w, k, sms)), dim3(trs::NTHREAD_V), args,
-                         (size_t)trs::SMEM_BYTES, s) != cudaSuccess)
+    if (cudaLaunchKernel(wino_twostage_f8_kernel_ptr(hilo), dim3(wino_twostage_gemm_grid(n, c, h, w, k, sms)),
+                         dim3(trs::NTHREAD_V), args, (size_t)trs::SMEM_BYTES, s) != cudaSuccess)
       return 3;
     unsigned ox, oy;
     wino_twostage_output_grid(n, h, w, k, sms, &ox, &oy);

@@ -170,10 +170,12 @@ int wino_conv2d_twostage(const void* x, const void* ucache2, void* workspace, vo
 int wino_twostage_stage(int stage, const void* x, const void* ucache2, void* workspace, void* y,
                         int n, int c, int h, int w, int k, void* stream);
 
-/* The same two-stage F(2x2,3x3) with an fp8 e4m3 tensor-core GEMM that keeps
- * fp16-level accuracy: U and V are each split into e4m3 hi + lo terms (hi =
- * e4m3(v), lo = e4m3(v - hi)) and the GEMM accumulates hi.hi + lo.hi +
- * hi.lo with kind::f8f6f4 MMAs, 32 channels per step.  Scales: per input
+/* The same two-stage F(2x2,3x3) with an fp8 e4m3 tensor-core GEMM.  hilo
+ * 1: U and V are each split into e4m3 hi + lo terms (hi = e4m3(v), lo =
+ * e4m3(v - hi)) and the GEMM accumulates hi.hi + lo.hi + hi.lo with
+ * kind::f8f6f4 MMAs, 32 channels per step -- fp16-level accuracy; hilo 0:
+ * single e4m3 terms, one MMA per step and half the transformed-tile bytes
+ * -- faster, at single-term fp8 accuracy.  Scales: per input
  * channel from its max |x| (|V| <= 4 max|x_c|, folded into U) and per (tap,
  * output channel) on U, applied before M is rounded to fp16.  Launches a
  * channel-max pass, the U split, the V split (transformed tiles), the GEMM
@@ -182,9 +184,9 @@ int wino_twostage_stage(int stage, const void* x, const void* ucache2, void* wor
  * workspace 256-byte aligned, wino_twostage_f8_workspace_bytes() bytes (0:
  * shape not supported).  The reference computes in fp16 only
  * (src/matrixmul.cuh:28-35); this variant has no counterpart there. */
-size_t wino_twostage_f8_workspace_bytes(int n, int c, int h, int w, int k);
+size_t wino_twostage_f8_workspace_bytes(int n, int c, int h, int w, int k, int hilo);
 int wino_conv2d_twostage_f8(const void* x, const void* ucache2, void* workspace, void* y, int n, int c,
-                            int h, int w, int k, void* stream);
+                            int h, int w, int k, int hilo, void* stream);
 
 /* Winograd F(4x4,3x3) (36 taps, 4x4 output tiles; no counterpart in the
  * reference, which has F(2x2,3x3) only: src/preprocessing.cuh:75-424,

@@ -135,13 +135,14 @@ def conv2d_winograd_f8_emulated(x, w):
     return output_transform(m, n, k, h, wd)
 
 
-def conv2d_winograd_f8hilo_emulated(x, w):
-    """The two-stage fp8 hi+lo path's rounding points (a model of that path;
-    the reference has no fp8 path): inv_c as in the fp8 variant above;
+def conv2d_winograd_f8_twostage_emulated(x, w, hilo=True):
+    """The two-stage fp8 path's rounding points (a model of that path; the
+    reference has no fp8 path): inv_c as in the fp8 variant above;
     V' = fp16(fp16(V) * inv_c), V_hi = e4m3(V'), V_lo = e4m3(V' - V_hi);
     U' = fp16(U) / inv_c, su[t][k] = max_c |U'| / 448, U_hi / U_lo the same
-    split of U' / su; M = fp16(su * (U_hi V_hi + U_lo V_hi + U_hi V_lo)) with
-    wide accumulation; output transform in wide precision."""
+    split of U' / su; M = fp16(su * (U_hi V_hi + U_lo V_hi + U_hi V_lo))
+    (hilo) or fp16(su * U_hi V_hi) (single terms), wide accumulation; output
+    transform in wide precision."""
     n, c, h, wd = x.shape
     k = w.shape[0]
     amax = np.abs(np.asarray(x, np.float64)).max(axis=(0, 2, 3))
@@ -156,7 +157,10 @@ def conv2d_winograd_f8hilo_emulated(x, w):
     a = u1 / su[:, :, None]
     uh = _e4m3(a)
     ul = _e4m3(a - uh)
-    m = _f16((gemm(uh, vh) + gemm(ul, vh) + gemm(uh, vl)) * su[:, None, :])
+    if hilo:
+        m = _f16((gemm(uh, vh) + gemm(ul, vh) + gemm(uh, vl)) * su[:, None, :])
+    else:
+        m = _f16(gemm(uh, vh) * su[:, None, :])
     return output_transform(m, n, k, h, wd)
 
 

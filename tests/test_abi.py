@@ -327,3 +327,25 @@ def test_dropin_route_rejects_invalid(wino):
     pr = _problem(wino, n=0)
     assert wino.lib().wino_dropin_route(ctypes.byref(pr)) == -1
     assert wino.lib().wino_dropin_route(None) == -1
+
+
+def test_twostage_f8_entry_points_validate_and_size(wino):
+    """fp8 two-stage path: C a multiple of 32 up to 256, K a multiple of 16;
+    workspace = channel maxima + su + U terms + V2 terms + M (each 256-byte
+    aligned); argument checks return before any CUDA call."""
+    L = wino.lib()
+    d = ctypes.c_void_p(0x10000)
+    odd = ctypes.c_void_p(0x10010)
+    r256 = lambda b: (b + 255) // 256 * 256
+    assert L.wino_twostage_f8_workspace_bytes(2, 48, 8, 8, 32, 1) == 0     # C % 32
+    assert L.wino_twostage_f8_workspace_bytes(2, 288, 8, 8, 32, 1) == 0    # C > 256
+    assert L.wino_twostage_f8_workspace_bytes(2, 64, 8, 8, 24, 1) == 0     # K % 16
+    assert L.wino_twostage_f8_workspace_bytes(2, 64, 8, 8, 32, 2) == 0     # hilo 0 or 1
+    tiles8 = (2 * 4 * 4 + 7) // 8 * 8
+    for hilo, terms in ((1, 2), (0, 1)):
+        assert (L.wino_twostage_f8_workspace_bytes(2, 64, 8, 8, 32, hilo)
+                == r256(64 * 4) + r256(16 * 32 * 4) + r256(16 * 32 * 64 * terms) + r256(16 * tiles8 * 64 * terms)
+                + 16 * 32 * 32 * 2)
+    assert L.wino_conv2d_twostage_f8(None, d, d, d, 2, 64, 8, 8, 32, 1, None) == 1
+    assert L.wino_conv2d_twostage_f8(d, d, odd, d, 2, 64, 8, 8, 32, 1, None) == 1   # workspace alignment
+    assert L.wino_conv2d_twostage_f8(d, d, d, d, 2, 48, 8, 8, 32, 1, None) == 2     # C % 32
