@@ -647,8 +647,23 @@ def extension_legs(wino, dev, flush, ev, peaks, steps):
         var[name] = {"us_per_call": us, "rel_l2": float(torch.linalg.vector_norm(d) / torch.linalg.vector_norm(y64)),
                      "max_norm": float(d.abs().max() / y64.abs().max()),
                      "direct_equiv_tflops": direct_flops(64, 256, 14, 14, 256) / (us * 1e-6) / 1e12}
+    # the two-stage route's fp16 and fp8 GEMMs on a cached fp16 U (per call:
+    # for fp8 the channel maxima, the U and V splits, GEMM, output transform)
+    u2 = wino.filter_transform_unfused(wt)
+    for name, run in [("two_stage_f16", lambda y: wino.conv2d_twostage(x, u2, 256, out=y)),
+                      ("two_stage_f8_hilo", lambda y: wino.conv2d_twostage_f8(x, u2, 256, hilo=True, out=y)),
+                      ("two_stage_f8", lambda y: wino.conv2d_twostage_f8(x, u2, 256, hilo=False, out=y))]:
+        y = torch.empty((64, 256, 14, 14), dtype=torch.float16, device=dev)
+        run(y)
+        torch.cuda.synchronize()
+        d = y.double() - y64
+        us = timed(lambda: run(y), steps)
+        var[name] = {"us_per_call": us, "rel_l2": float(torch.linalg.vector_norm(d) / torch.linalg.vector_norm(y64)),
+                     "max_norm": float(d.abs().max() / y64.abs().max()),
+                     "direct_equiv_tflops": direct_flops(64, 256, 14, 14, 256) / (us * 1e-6) / 1e12}
     out["variants"] = {"workload": "N64 C256 H14 W14 K256, x ~ U[-1,1]; per call: filter transform "
-                                   "+ input pre-pass + fused kernel", **var}
+                                   "+ input pre-pass + fused kernel (f16 .. f16_hilo); pre-pass + tap GEMM "
+                                   "+ output transform on a cached fp16 U (two_stage_*)", **var}
 
     # --- Winograd F(4x4,3x3), hi+lo and plain, on N128 C256 H28 K256 against F(2x2) fused
     n, c, h, k = 128, 256, 28, 256
