@@ -6,7 +6,7 @@ One step = one forward conv of the single-large-layer workload
 w ~ N(0, 2/(9C)), seed 0), run through the drop-in ABI exactly as the
 reference harness runs it: getkernelInfo once, then per step the four launch
 slots (for this even-sized layer: filter transform, input re-layout,
-input-fused tap GEMM writing M to mid_result, output transform).
+tap GEMM writing M to mid_result, output transform).
 
 Printed (rank 0, one JSON line):
   value      direct-conv-equivalent TFLOP/s (2*N*K*C*P*Q*9 / time), whole job,
@@ -367,7 +367,7 @@ def run_ours(args, rank, world, local_rank):
         lambda: wino.conv2d_fused(x, ucache, k, out=yf, stream=stream, workspace=xbws), iters)
     layout_ms, _ = timed(lambda: wino.input_layout(x, xbws, stream), iters)
     u2 = wino.filter_transform_unfused(wt)
-    # two-stage path on cached U: pre-pass + input-fused tap GEMM + output transform
+    # two-stage path on cached U: pre-pass + tap GEMM + output transform
     ts_ws = wino._aligned_ws(wino.twostage_workspace_bytes(n, c, h, w, k), dev)
     yt = torch.empty_like(y)
     ts_ms, _ = timed(lambda: wino.conv2d_twostage(x, u2, k, out=yt, workspace=ts_ws, stream=stream), iters)
@@ -505,7 +505,7 @@ def run_ours(args, rank, world, local_rank):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f16",
         "data": "synthetic (seeded ReLU(N(0,1)) input, N(0,2/(9C)) weights)",
         "config": {"workload": WORKLOAD_NAME, **W, "parallelism": f"replicas x{world}",
-                   "step": ("drop-in ABI: filter transform + input re-layout + input-fused tap GEMM + "
+                   "step": ("drop-in ABI: filter transform + input pre-pass (transformed tiles) + tap GEMM + "
                             "output transform" if two_stage else
                             "drop-in ABI: filter transform + input re-layout + fused conv + 1 empty slot"),
                    "l2": "flushed between steps (256 MB write)"},
@@ -707,7 +707,7 @@ def extension_legs(wino, dev, flush, ev, peaks, steps):
     del u2, ws2
     out["winograd_f4"] = {"workload": "N128 C256 H28 K256, x = relu(N(0,1)); transformed filter cached; "
                                       "per call: input transform + 36-tap GEMM + output transform (F4), "
-                                      "pre-pass + fused kernel (F2), pre-pass + input-fused tap GEMM + "
+                                      "pre-pass + fused kernel (F2), pre-pass + tap GEMM + "
                                       "output transform (F2 two-stage)", **f4}
     del x, wt, y64, y, u, ws
 
