@@ -5,8 +5,9 @@ One step = one forward conv of the single-large-layer workload
 (N=128, C=K=256, H=W=28, 3x3, stride 1, pad 1; x = ReLU(N(0,1)),
 w ~ N(0, 2/(9C)), seed 0), run through the drop-in ABI exactly as the
 reference harness runs it: getkernelInfo once, then per step the four launch
-slots (for this even-sized layer: filter transform, input re-layout,
-tap GEMM writing M to mid_result, output transform).
+slots (for this even-sized layer: filter transform, input pre-pass writing
+the transformed tiles to transform_pin, tap GEMM writing M to mid_result,
+output transform).
 
 Printed (rank 0, one JSON line):
   value      direct-conv-equivalent TFLOP/s (2*N*K*C*P*Q*9 / time), whole job,
