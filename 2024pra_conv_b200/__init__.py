@@ -98,6 +98,9 @@ def lib():
             "wino_batch_num_layers": ([vp], i),
             "wino_batch_set_config": ([vp, i, i], i),
             "wino_batch_get_config": ([vp, i, ctypes.POINTER(i)], i),
+            "wino_batch_set_route": ([vp, i, i], i),
+            "wino_batch_get_route": ([vp, i, ctypes.POINTER(i), ctypes.POINTER(ctypes.c_float),
+                                      ctypes.POINTER(ctypes.c_float)], i),
             "wino_batch_set_order": ([vp, ctypes.POINTER(i), i], i),
             "wino_batch_get_order": ([vp, ctypes.POINTER(i), i], i),
             "wino_batch_commit": ([vp], i),
@@ -579,6 +582,18 @@ class Batch:
         _check(lib().wino_batch_get_config(self._h, layer, ctypes.byref(v)), "batch_get_config")
         return v.value
 
+    def set_route(self, layer, route):
+        """0: the layer runs inside the persistent fused launch; 1: the
+        two-stage route (128 x 256 tap-GEMM units) launched before it."""
+        _check(lib().wino_batch_set_route(self._h, layer, route), "batch_set_route")
+
+    def route(self, layer):
+        """(route, fastest fused us, two-stage us) -- the timings from tune()."""
+        r, f, t = ctypes.c_int(0), ctypes.c_float(0), ctypes.c_float(0)
+        _check(lib().wino_batch_get_route(self._h, layer, ctypes.byref(r), ctypes.byref(f), ctypes.byref(t)),
+               "batch_get_route")
+        return r.value, f.value, t.value
+
     def set_order(self, order):
         arr = (ctypes.c_int * len(order))(*order)
         _check(lib().wino_batch_set_order(self._h, arr, len(order)), "batch_set_order")
@@ -601,14 +616,18 @@ class Batch:
 
     def tuning_state(self):
         """The autotuner's choices, to be saved (JSON-able) and restored later."""
-        return {"version": 1, "configs": [self.config(i) for i in range(len(self))], "order": self.order()}
+        return {"version": 2, "configs": [self.config(i) for i in range(len(self))],
+                "routes": [self.route(i)[0] for i in range(len(self))], "order": self.order()}
 
     def restore(self, state):
-        """Re-applies tuning_state() output (the same layer list) without re-tuning."""
-        if state.get("version") != 1 or len(state["configs"]) != len(self):
+        """Re-applies tuning_state() output (the same layer list) without re-tuning
+        (version 1 states carry no routes: every layer fused)."""
+        if state.get("version") not in (1, 2) or len(state["configs"]) != len(self):
             raise ValueError("tuning state of another version or layer list")
         for i, c in enumerate(state["configs"]):
             self.set_config(i, c)
+        for i, r in enumerate(state.get("routes", [0] * len(self))):
+            self.set_route(i, r)
         self.set_order(state["order"])
 
     def capture(self, stream=None):

@@ -136,6 +136,19 @@ __global__ void __launch_bounds__(256) filter_transform_f8_kernel(
   }
 }
 
+// fp16 U cache (fused layout, u_offset) -> the same values in the unfused
+// GEMM layout (u2_offset): a batch layer routed to the two-stage path
+// reuses the caller's fused U cache this way.  One thread per (t, k, c).
+__global__ void __launch_bounds__(256) u_to_u2_kernel(const __half* __restrict__ u, __half* __restrict__ u2, int K,
+                                                      int C) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (size_t)16 * K * C) return;
+  const int c = (int)(idx % C);
+  const size_t r = idx / C;
+  const int k = (int)(r % K), t = (int)(r / K);
+  u2[u2_offset(t, k, c, K, C)] = u[u_offset(t, k, c, K, C)];
+}
+
 }  // namespace wino
 
 using namespace wino;
@@ -144,6 +157,13 @@ extern "C" {
 
 void* wino_dropin_filter_kernel_ptr() { return (void*)dropin_filter_kernel; }
 void* wino_dropin_filter_u2_kernel_ptr() { return (void*)dropin_filter_u2_kernel; }
+
+int wino_launch_u_to_u2(const void* u, void* u2, int K, int C, cudaStream_t stream) {
+  const size_t n = (size_t)16 * K * C;
+  u_to_u2_kernel<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(static_cast<const __half*>(u),
+                                                                   static_cast<__half*>(u2), K, C);
+  return (int)cudaGetLastError();
+}
 
 int wino_launch_filter_transform(const void* weight, void* ucache, void* ucache_lo, int K, int C,
                                  int bf16, int layout, cudaStream_t stream) {

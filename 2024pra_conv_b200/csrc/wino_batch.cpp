@@ -39,6 +39,10 @@ long long wino_fused_nblocks(int n, int h, int w, int k);
 long long wino_fused_nblocks_cfg(int n, int c, int h, int w, int k, int cfg);
 int wino_fused_cfg_splits(int c, int cfg);
 int wino_launch_y32_to_f16(const float* y32, void* y, long long count, cudaStream_t stream);
+int wino_launch_u_to_u2(const void* u, void* u2, int K, int C, cudaStream_t stream);
+size_t wino_twostage_workspace_bytes(int n, int c, int h, int w, int k);
+int wino_twostage_stage(int stage, const void* x, const void* ucache2, void* workspace, void* y, int n, int c,
+                        int h, int w, int k, void* stream);
 }
 
 namespace {
@@ -134,11 +138,44 @@ int time_us(F&& fn, int reps, cudaStream_t s, float* us) {
   return rc;
 }
 
+// Route of a batch layer: inside the persistent fused launch (its tile
+// blocks of 128 output channels x 32 tiles), or the two-stage path (tap GEMM
+// units of 128 tiles x 256 output channels with full-width MMAs, M through
+// a batch-owned workspace) launched before it.
+constexpr int ROUTE_FUSED = 0, ROUTE_TWOSTAGE = 1;
+
 struct Layer {
   KernelParam p;
   int cfg = 0;
+  int route = ROUTE_FUSED;
   long long blocks = 0;
-  float tuned_us = 0.f;
+  float tuned_us = 0.f;     // fastest fused configuration alone
+  float twostage_us = -1.f; // the two-stage route alone (-1: not timed or not applicable)
+  void* u2 = nullptr;       // U in the two-stage GEMM's layout (batch-owned)
+  void* ws2 = nullptr;      // two-stage workspace (batch-owned)
+  // U2 and the workspace for the two-stage route, made on first use from the
+  // layer's fused U cache (synchronous: not inside a stream capture)
+  int ensure_twostage() {
+    if (u2 && ws2) return WINO_OK;
+    const size_t wsb = wino_twostage_workspace_bytes(p.n, p.c, p.h, p.w, p.k);
+    if (wsb == 0) return WINO_EUNSUPPORTED;
+    if (!u2 && cudaMalloc(&u2, (size_t)16 * p.k * p.c * 2) != cudaSuccess) return WINO_ECUDA;
+    if (!ws2 && cudaMalloc(&ws2, wsb) != cudaSuccess) return WINO_ECUDA;
+    if (wino_launch_u_to_u2(p.transform_filter, u2, p.k, p.c, nullptr) != 0) return WINO_ECUDA;
+    return cudaDeviceSynchronize() == cudaSuccess ? WINO_OK : WINO_ECUDA;
+  }
+  int run_twostage(cudaStream_t s) const {
+    for (int stage = 0; stage < 3; ++stage) {
+      const int rc = wino_twostage_stage(stage, p.pin, u2, ws2, p.pout, p.n, p.c, p.h, p.w, p.k, s);
+      if (rc != WINO_OK) return rc;
+    }
+    return WINO_OK;
+  }
+  void release() {
+    if (u2) cudaFree(u2);
+    if (ws2) cudaFree(ws2);
+    u2 = ws2 = nullptr;
+  }
 };
 
 struct Batch {
@@ -187,11 +224,12 @@ struct Batch {
     if (!table_dev && cudaMalloc(&table_dev, sizeof(BatchTable)) != cudaSuccess) return WINO_ECUDA;
     BatchTable t;
     std::memset(&t, 0, sizeof(t));
-    t.nlayers = (int)order.size();
     long long begin = 0;
+    int nt = 0;
     for (size_t i = 0; i < order.size(); ++i) {
       const Layer& L = layers[order[i]];
-      LayerDesc& d = t.layer[i];
+      if (L.route != ROUTE_FUSED) continue;     // launched on its own before the table
+      LayerDesc& d = t.layer[nt++];
       d.p = L.p;
       int cfg = L.cfg;
       if (!d.p.transform_pin) cfg |= wino::CFG_DIRECT;
@@ -200,6 +238,7 @@ struct Batch {
       d.block_begin = begin;
       begin += L.blocks;
     }
+    t.nlayers = nt;
     t.total = begin;
     total = begin;
     if (settle() != WINO_OK) return WINO_ECUDA;  // no launch still reads the old table
@@ -213,9 +252,15 @@ struct Batch {
     if (dirty) return WINO_EINVAL;  // commit first (outside any capture)
     for (int li : order) {
       const Layer& L = layers[li];
+      if (L.route == ROUTE_TWOSTAGE) {
+        const int rc = L.run_twostage(s);
+        if (rc != WINO_OK) return rc;
+        continue;
+      }
       if (L.p.transform_pin && !(L.cfg & wino::CFG_DIRECT) && wino_launch_xb_layout(&L.p, s) != 0)
         return WINO_ECUDA;
     }
+    if (total == 0) return WINO_OK;           // every layer on the two-stage route
     return wino_fused_launch_batch(table_dev, total, grid_for(total), s) == 0 ? WINO_OK : WINO_ECUDA;
   }
 };
@@ -294,6 +339,7 @@ int wino_batch_destroy(void* h) {
   if (!b) return WINO_EINVAL;
   b->settle();
   b->drop_graph();
+  for (Layer& L : b->layers) L.release();
   if (b->table_dev) cudaFree(b->table_dev);
   if (b->done) cudaEventDestroy(b->done);
   delete b;
@@ -341,6 +387,31 @@ int wino_batch_get_config(void* h, int layer, int* cfg) {
   return WINO_OK;
 }
 
+int wino_batch_set_route(void* h, int layer, int route) {
+  Batch* b = as_batch(h);
+  if (!b || layer < 0 || layer >= (int)b->layers.size() || (route != ROUTE_FUSED && route != ROUTE_TWOSTAGE))
+    return WINO_EINVAL;
+  Layer& L = b->layers[layer];
+  if (route == ROUTE_TWOSTAGE) {
+    if (b->settle() != WINO_OK) return WINO_ECUDA;
+    const int rc = L.ensure_twostage();
+    if (rc != WINO_OK) return rc;
+  }
+  L.route = route;
+  b->dirty = true;
+  return WINO_OK;
+}
+
+int wino_batch_get_route(void* h, int layer, int* route, float* fused_us, float* twostage_us) {
+  Batch* b = as_batch(h);
+  if (!b || !route || layer < 0 || layer >= (int)b->layers.size()) return WINO_EINVAL;
+  const Layer& L = b->layers[layer];
+  *route = L.route;
+  if (fused_us) *fused_us = L.tuned_us;
+  if (twostage_us) *twostage_us = L.twostage_us;
+  return WINO_OK;
+}
+
 int wino_batch_set_order(void* h, const int* order, int n) {
   Batch* b = as_batch(h);
   if (!b || !order || n != (int)b->layers.size()) return WINO_EINVAL;
@@ -374,10 +445,14 @@ int wino_batch_run(void* h, void* stream) {
   return rc != WINO_OK ? rc : b->mark((cudaStream_t)stream);
 }
 
-// Autotune: per-layer configurations (exhaustive over CFG_*), then the layer
-// order of the table among {as added, longest first, longest/shortest
-// interleaved}.  layer_us: nlayers x NCFG timings (-1 = not applicable);
-// order_us: the three whole-batch timings.  Leaves the best choice set.
+// Autotune: per-layer configurations (exhaustive over CFG_*) and routes
+// (the fused launch's 128 x 32 tile blocks or the two-stage path's 128 x 256
+// tap-GEMM units, the faster alone), then the layer order of the table among
+// {as added, longest first, longest/shortest interleaved}; the routes picked
+// stay only if the whole batch beats the all-fused batch in the best order.
+// layer_us: nlayers x NCFG timings (-1 = not applicable); order_us: the
+// three whole-batch timings with the picked routes.  Leaves the best choice
+// set; wino_batch_get_route reports each layer's route and both timings.
 int wino_batch_tune(void* h, int reps, float* layer_us, float* order_us, void* stream) {
   Batch* b = as_batch(h);
   if (!b || b->layers.empty()) return WINO_EINVAL;
@@ -403,6 +478,28 @@ int wino_batch_tune(void* h, int reps, float* layer_us, float* order_us, void* s
     L.tuned_us = us[best];
     if (layer_us)
       for (int c = 0; c < wino::NCFG; ++c) layer_us[i * wino::NCFG + c] = us[c];
+    // the two-stage route's tile shape (128 tiles x 256 output channels per
+    // tap-GEMM unit), where the shape has one
+    L.twostage_us = -1.f;
+    if (wino_twostage_workspace_bytes(L.p.n, L.p.c, L.p.h, L.p.w, L.p.k) > 0) {
+      const int rc = L.ensure_twostage();
+      if (rc == WINO_OK) {
+        float t = 0.f;
+        const int rt = time_us([&] { return L.run_twostage(s); }, reps, s, &t);
+        if (rt != WINO_OK) return rt;
+        L.twostage_us = t;
+      } else if (rc != WINO_EUNSUPPORTED) {
+        return rc;
+      }
+    }
+  }
+  // routes: each layer the faster of its best fused configuration and the
+  // two-stage route, measured alone
+  std::vector<int> picked(nl, ROUTE_FUSED);
+  for (int i = 0; i < nl; ++i) {
+    const Layer& L = b->layers[i];
+    if (L.twostage_us >= 0.f && L.twostage_us < L.tuned_us) picked[i] = ROUTE_TWOSTAGE;
+    b->layers[i].route = picked[i];
   }
   std::vector<int> natural(nl), longest(nl), inter;
   std::iota(natural.begin(), natural.end(), 0);
@@ -431,6 +528,19 @@ int wino_batch_tune(void* h, int reps, float* layer_us, float* order_us, void* s
     }
   }
   b->order = *orders[best_o];
+  // the fused launch overlaps its layers, so the picked routes are kept only
+  // if the whole batch is faster with them than with every layer fused
+  if (std::count(picked.begin(), picked.end(), ROUTE_TWOSTAGE) > 0) {
+    for (Layer& L : b->layers) L.route = ROUTE_FUSED;
+    b->dirty = true;
+    int rc = b->commit();
+    if (rc != WINO_OK) return rc;
+    float all_fused = 0.f;
+    rc = time_us([&] { return b->run(s); }, reps, s, &all_fused);
+    if (rc != WINO_OK) return rc;
+    if (best_us < all_fused)
+      for (int i = 0; i < nl; ++i) b->layers[i].route = picked[i];
+  }
   b->dirty = true;
   return b->commit();
 }

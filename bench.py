@@ -620,6 +620,10 @@ def extension_legs(wino, dev, flush, ev, peaks, steps):
         "us_graph_tuned": graph_us, "us_persistent_untuned": untuned_us, "us_sequential_launches": seq_us,
         "direct_equiv_tflops": dfl / (graph_us * 1e-6) / 1e12,
         "configs": [b.config(i) for i in range(len(layers))], "order": b.order(),
+        # the tuner's route per layer (0 fused tile blocks of 128 k x 32 tiles, 1 two-stage
+        # tap-GEMM units of 128 tiles x 256 k) with each layer's time alone on both routes
+        "routes": [b.route(i)[0] for i in range(len(layers))],
+        "alone_us_fused_twostage": [[round(b.route(i)[1], 1), round(b.route(i)[2], 1)] for i in range(len(layers))],
         "order_us": order_us, "worst_rel_l2": worst, "per_layer_alone": per_layer,
         "roofline": {"per_layer_bound": f"{n_tc} of 12 layers tensor-bound, the rest HBM-bound",
                      "target_us": t_roof * 1e6, "frac": t_roof * 1e6 / graph_us,

@@ -247,7 +247,9 @@ int wino_tune_layer(const void* x, const void* ucache, void* workspace, void* y,
  * ONE persistent fused-kernel launch over all layers' work blocks (a device
  * layer table); wino_batch_graph_capture records that sequence in a CUDA
  * graph, wino_batch_graph_launch replays it.  Batch layers run unsplit.
- * wino_batch_tune runs the autotuner: per layer the fastest unsplit
+ * wino_batch_tune runs the autotuner: per layer the route (fused or
+ * two-stage, kept only if the whole batch is faster with the picks than
+ * all-fused) and the fastest unsplit
  * configuration (exhaustive), then the
  * fastest table order among {as added, longest first, longest/shortest
  * interleaved}; layer_us receives nlayers x WINO_NCFG timings, order_us the
@@ -267,6 +269,15 @@ int wino_batch_add_layer(void* batch, const void* x, const void* ucache, void* w
 int wino_batch_num_layers(void* batch);
 int wino_batch_set_config(void* batch, int layer, int cfg);
 int wino_batch_get_config(void* batch, int layer, int* cfg);
+/* Route of a batch layer (a tile-shape choice): 0 inside the persistent
+ * fused launch (128 output channels x 32 tiles per block), 1 the two-stage
+ * path (tap-GEMM units of 128 tiles x 256 output channels, M in a
+ * batch-owned workspace, U relaid from the layer's fused U cache) launched
+ * before it.  Setting route 1 allocates those buffers (outside any stream
+ * capture).  get_route also reports the tuner's timings of the layer alone
+ * (fastest fused configuration, two-stage; -1 when not timed). */
+int wino_batch_set_route(void* batch, int layer, int route);
+int wino_batch_get_route(void* batch, int layer, int* route, float* fused_us, float* twostage_us);
 int wino_batch_set_order(void* batch, const int* order, int n);
 int wino_batch_get_order(void* batch, int* order, int n);
 int wino_batch_commit(void* batch);

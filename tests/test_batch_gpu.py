@@ -76,26 +76,43 @@ def _layer_set(wino, oracle_mod, cuda, n):
     return layers
 
 
+def _refs(wino, layers):
+    """Each layer's single-layer outputs on both routes: the fused kernel and
+    the two-stage path (U relaid to its layout)."""
+    fused = [wino.conv2d_fused(x, u, k) for (x, wt, u, ws, y, k) in layers]
+    two = [wino.conv2d_twostage(x, wino.filter_transform_unfused(wt), k) for (x, wt, u, ws, y, k) in layers]
+    return fused, two
+
+
+def _check_routes(wino, b, layers, refs, tag):
+    import torch
+    torch.cuda.synchronize()
+    for i, (x, wt, u, ws, y, k) in enumerate(layers):
+        r = refs[b.route(i)[0]][i]
+        assert torch.equal(y.view(torch.int16), r.view(torch.int16)), (tag, i, b.route(i))
+        y.fill_(float("nan"))
+
+
 def test_batched_layer_set_one_launch_graph_and_tuner(wino, cuda, oracle_mod):
-    """The 12-layer ResNet-style set at N=32 in one persistent launch."""
+    """The 12-layer ResNet-style set at N=32 in one persistent launch; after
+    tuning, layers the tuner routes to the two-stage path equal that path's
+    single-layer output bit for bit."""
     import torch
     layers = _layer_set(wino, oracle_mod, cuda, 32)
-    refs = [wino.conv2d_fused(x, u, k) for (x, wt, u, ws, y, k) in layers]
+    refs = _refs(wino, layers)
     b = wino.Batch()
     for (x, wt, u, ws, y, k) in layers:
         b.add(x, u, k, y, workspace=ws)
     assert len(b) == 12
 
     def check(tag):
-        torch.cuda.synchronize()
-        for i, ((x, wt, u, ws, y, k), r) in enumerate(zip(layers, refs)):
-            assert torch.equal(y.view(torch.int16), r.view(torch.int16)), (tag, i)
-            y.fill_(float("nan"))
+        _check_routes(wino, b, layers, refs, tag)
 
     b.run()
     check("run")
-    for (x, wt, u, ws, y, k), r in zip(layers, refs):
+    for (x, wt, u, ws, y, k), r, r2 in zip(layers, refs[0], refs[1]):
         _fp64_check(x, wt, r)
+        _fp64_check(x, wt, r2)
     # mixed configurations and a reversed table order
     for i in range(12):
         b.set_config(i, i % 4)      # unsplit configurations: batch layers run unsplit
@@ -109,6 +126,9 @@ def test_batched_layer_set_one_launch_graph_and_tuner(wino, cuda, oracle_mod):
     for i in range(12):
         row = layer_us[i]
         assert row[b.config(i)] == min(t for t in row if t > 0)
+        route, fused_us, two_us = b.route(i)
+        assert fused_us > 0 and two_us > 0          # every layer of the set has both routes
+        assert route in (0, 1)
     assert sorted(b.order()) == list(range(12))
     b.run()
     check("tuned")
@@ -127,7 +147,7 @@ def test_tuning_state_save_and_restore(wino, cuda, oracle_mod, tmp_path):
     import json
     import torch
     layers = _layer_set(wino, oracle_mod, cuda, 4)
-    refs = [wino.conv2d_fused(x, u, k) for (x, wt, u, ws, y, k) in layers]
+    refs = _refs(wino, layers)
     b = wino.Batch()
     for (x, wt, u, ws, y, k) in layers:
         b.add(x, u, k, y, workspace=ws)
@@ -142,8 +162,32 @@ def test_tuning_state_save_and_restore(wino, cuda, oracle_mod, tmp_path):
     b2.restore(state)
     assert b2.tuning_state() == state
     b2.run()
-    torch.cuda.synchronize()
-    for (x, wt, u, ws, y, k), r in zip(layers, refs):
-        assert torch.equal(y.view(torch.int16), r.view(torch.int16))
+    _check_routes(wino, b2, layers, refs, "restored")
     b2.close()
+    assert wino.error_read_clear() == 0
+
+
+def test_batch_routes_mixed(wino, cuda, oracle_mod):
+    """Layers set explicitly to the two-stage route run before the persistent
+    launch of the rest (also inside the CUDA graph) and equal the two-stage
+    path's single-layer outputs; every layer two-stage skips the persistent
+    launch altogether."""
+    layers = _layer_set(wino, oracle_mod, cuda, 2)
+    refs = _refs(wino, layers)
+    b = wino.Batch()
+    for (x, wt, u, ws, y, k) in layers:
+        b.add(x, u, k, y, workspace=ws)
+    for i in range(0, 12, 3):
+        b.set_route(i, 1)
+    b.run()
+    _check_routes(wino, b, layers, refs, "mixed")
+    assert [b.route(i)[0] for i in range(12)] == [1 if i % 3 == 0 else 0 for i in range(12)]
+    b.capture()
+    b.launch()
+    _check_routes(wino, b, layers, refs, "mixed graph")
+    for i in range(12):
+        b.set_route(i, 1)
+    b.run()
+    _check_routes(wino, b, layers, refs, "all two-stage")
+    b.close()
     assert wino.error_read_clear() == 0
