@@ -1569,6 +1569,9 @@ __global__ void __launch_bounds__(256, WINO_V2_MINB) v2_layout_kernel(KernelPara
   const size_t plane = (size_t)H * W;
   const size_t tap_bytes = (size_t)NT8 * C * 2;
   const bool w_even = (W & 1) == 0;
+  // W % 4 == 0 and an 8-byte aligned input: the window row's words at
+  // columns 2tx - 2 and 2tx (or 2tx and 2tx + 2) form one aligned 8-byte word
+  const bool w4 = (W & 3) == 0 && (reinterpret_cast<uintptr_t>(X) & 7) == 0;
   for (int item = blockIdx.x; item < items; item += gridDim.x) {
     const int tb = item / CS, cs = item - tb * CS;
     const int rows = min(128, NT8 - tb * 128);
@@ -1598,7 +1601,18 @@ __global__ void __launch_bounds__(256, WINO_V2_MINB) v2_layout_kernel(KernelPara
 #pragma unroll
         for (int ch = 0; ch < 2; ++ch) {
           const unsigned short* row = base + (size_t)(2 * cp + ch) * plane + (size_t)(rok ? y : 0) * W;
-          if (w_even) {
+          if (w4) {
+            // odd tx: [2tx-2, 2tx+1] aligned + [2tx+2, 2tx+3]; even tx: [2tx, 2tx+3]
+            // aligned + [2tx-2, 2tx-1] -- two loads, the 8-byte one shared by
+            // a pair of lanes; the aligned word never crosses the row end
+            const bool odd = (tx & 1) != 0;
+            const int xa = odd ? x0 - 2 : x0, xb = odd ? x0 + 2 : x0 - 2;
+            const uint2 wa = rok ? *reinterpret_cast<const uint2*>(row + xa) : make_uint2(0u, 0u);
+            const uint32_t wb = (rok && xb >= 0 && xb < W) ? *reinterpret_cast<const uint32_t*>(row + xb) : 0u;
+            a[ch][0] = odd ? wa.x : wb;
+            a[ch][1] = odd ? wa.y : wa.x;
+            a[ch][2] = odd ? wb : wa.y;
+          } else if (w_even) {
 #pragma unroll
             for (int q = 0; q < 3; ++q) {
               const int x = x0 - 2 + 2 * q;
