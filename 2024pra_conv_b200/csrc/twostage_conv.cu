@@ -1575,9 +1575,10 @@ __global__ void __launch_bounds__(256, WINO_V2_MINB) v2_layout_kernel(KernelPara
   for (int item = blockIdx.x; item < items; item += gridDim.x) {
     const int tb = item / CS, cs = item - tb * CS;
     const int rows = min(128, NT8 - tb * 128);
-    if (il >= rows) continue;
+    // threads past the block's rows compute zeros and store nothing
+    const bool inblk = il < rows;
     const int tile = tb * 128 + il;
-    const bool live = tile < NT;
+    const bool live = inblk && tile < NT;
     int n = 0, ty = 0, tx = 0;
     if (live) {
       const int per = TP * TQ;
@@ -1650,6 +1651,7 @@ __global__ void __launch_bounds__(256, WINO_V2_MINB) v2_layout_kernel(KernelPara
         vt[4 * a + 3][cp] = hsub2(e[a][1], e[a][3]);
       }
     }
+    if (!inblk) continue;
     uint8_t* out = v2 + ((size_t)tb * 128 * C + (size_t)cs * rows * 16) * 2 + (il >> 3) * 256 + hh * 128 +
                    (il & 7) * 16;
 #pragma unroll
