@@ -83,6 +83,9 @@ def lib():
             "wino_input_layout": ([vp, vp, i, i, i, i, vp], i),
             "wino_conv2d_fused_epilogue": ([vp, vp, vp, vp, vp, vp, i, i, i, i, i, i, vp], i),
             "wino_conv2d_direct": ([vp, vp, vp] + [i] * 11 + [vp], i),
+            "wino_igemm_weight_bytes": ([i, i, i, i], sz),
+            "wino_igemm_weight_transform": ([vp, vp, i, i, i, i, vp], i),
+            "wino_conv2d_igemm": ([vp, vp, vp] + [i] * 11 + [vp], i),
             "wino_weight_tag": ([vp, i, i, ctypes.POINTER(ctypes.c_ulonglong), vp], i),
             "wino_ucache_save": ([ctypes.c_char_p, vp, i, i, ctypes.c_ulonglong], i),
             "wino_ucache_load": ([ctypes.c_char_p, vp, i, i, ctypes.c_ulonglong], i),
@@ -297,6 +300,38 @@ def conv2d_direct(x, w, stride=1, pad=1, out=None, stream=None):
     _check(lib().wino_conv2d_direct(ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(w.data_ptr()),
                                     ctypes.c_void_p(y.data_ptr()), n, c, h, wd, k, r, s, stride, stride,
                                     pad, pad, _stream(stream)), "conv2d_direct")
+    return y
+
+
+def igemm_weight_bytes(c, k, r, s) -> int:
+    return int(lib().wino_igemm_weight_bytes(c, k, r, s))
+
+
+def igemm_weight_transform(w, stream=None):
+    """fp16 KCRS weights -> the implicit-GEMM weight operand (flat uint8
+    tensor of igemm_weight_bytes bytes)."""
+    import torch
+    k, c, r, s = w.shape
+    wp = torch.empty(igemm_weight_bytes(c, k, r, s), dtype=torch.uint8, device=w.device)
+    _check(lib().wino_igemm_weight_transform(ctypes.c_void_p(w.data_ptr()), ctypes.c_void_p(wp.data_ptr()),
+                                             k, c, r, s, _stream(stream)), "igemm_weight_transform")
+    return wp
+
+
+def conv2d_igemm(x, w, stride=1, pad=1, wprep=None, out=None, stream=None):
+    """Tensor-core implicit-GEMM convolution of any filter size / stride /
+    padding (fp16 in and out, fp32 accumulation).  wprep: the weights from
+    igemm_weight_transform (made here when None)."""
+    import torch
+    n, c, h, wd = x.shape
+    k, _, r, s = w.shape
+    oh, ow = (h - r + 2 * pad) // stride + 1, (wd - s + 2 * pad) // stride + 1
+    if wprep is None:
+        wprep = igemm_weight_transform(w, stream)
+    y = out if out is not None else torch.empty((n, k, oh, ow), dtype=torch.float16, device=x.device)
+    _check(lib().wino_conv2d_igemm(ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(wprep.data_ptr()),
+                                   ctypes.c_void_p(y.data_ptr()), n, c, h, wd, k, r, s, stride, stride,
+                                   pad, pad, _stream(stream)), "conv2d_igemm")
     return y
 
 

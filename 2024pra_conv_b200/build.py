@@ -41,7 +41,7 @@ CXX_FLAGS = ["-O2", "-fPIC", "-std=c++17", "-I", INCLUDE, "-I", CSRC,
 
 CU_SOURCES = ["filter_transform.cu", "fused_conv.cu", "input_layout.cu", "unfused_conv.cu", "misc.cu", "noalloc.cu",
               "mlp.cu", "direct_conv.cu", "ucache_store.cu", "winograd_f4.cu",
-              "twostage_conv.cu"]
+              "twostage_conv.cu", "igemm_conv.cu"]
 CPP_SOURCES = ["wino_abi.cpp", "wino_batch.cpp"]
 HEADERS = ["tc_sm100.cuh", "wino_common.cuh", "wino_param.h", "vgen.cuh", "wino_batch.h"]
 

@@ -97,6 +97,16 @@ void wino_twostage_output_grid(int n, int h, int w, int k, int sms, unsigned* gx
 int wino_twostage_output_threads();
 int wino_twostage_output_smem_bytes();
 uint32_t wino_twostage_error_read_clear();
+size_t wino_igemm_weight_bytes(int c, int k, int r, int s);
+unsigned wino_igemm_weight_grid(int c, int k, int r, int s);
+void* wino_igemm_weight_kernel_ptr();
+void* wino_igemm_kernel_ptr(int k);
+int wino_igemm_threads();
+int wino_igemm_smem_bytes();
+unsigned wino_igemm_grid(int n, int k, int oh, int ow, int sms);
+int wino_igemm_shape_ok(int n, int c, int h, int w, int k, int oh, int ow);
+int wino_igemm_prepare();
+uint32_t wino_igemm_error_read_clear();
 }
 
 namespace {
@@ -214,7 +224,17 @@ static int plan_route(const problem_t& pr) {
   const bool wino = pr.r == 3 && pr.s == 3 && pr.u == 1 && pr.v == 1 && pr.p == 1 && pr.q == 1 &&
                     wino_check_shape((int)pr.n, (int)pr.c, (int)pr.h, (int)pr.w, (int)pr.k) == WINO_OK &&
                     pr.transform_filter != nullptr;
-  if (!wino) return WINO_ROUTE_DIRECT;
+  if (!wino) {
+    // Tensor-core implicit GEMM when its re-laid-out weights fit the
+    // caller's transform_filter (16*k*c fp16, reference src/main.cpp:38).
+    const int oh = (int)((pr.h - pr.r + 2 * pr.p) / pr.u + 1), ow = (int)((pr.w - pr.s + 2 * pr.q) / pr.v + 1);
+    const bool igemm = pr.transform_filter != nullptr &&
+                       (reinterpret_cast<uintptr_t>(pr.transform_filter) & 15) == 0 &&
+                       wino_igemm_weight_bytes((int)pr.c, (int)pr.k, (int)pr.r, (int)pr.s) <=
+                           (size_t)16 * pr.k * pr.c * 2 &&
+                       wino_igemm_shape_ok((int)pr.n, (int)pr.c, (int)pr.h, (int)pr.w, (int)pr.k, oh, ow);
+    return igemm ? WINO_ROUTE_IGEMM : WINO_ROUTE_DIRECT;
+  }
   // The caller's transform_pin workspace holds 4*h*h*n*c fp16 elements
   // (reference src/main.cpp:36-38); when the channel-blocked input fits
   // there (and is 16-byte aligned) slot 2 writes it, otherwise the fused
@@ -249,7 +269,8 @@ int getkernelInfo(problem_t* problem, kernelInfo_t* kernelInfo, void* param) {
   if (st != WINO_OK) return st;
   if (!pr.in || !pr.weight || !pr.out) return WINO_EINVAL;
   int route = plan_route(pr);
-  const bool wino = route != WINO_ROUTE_DIRECT;
+  if (route == WINO_ROUTE_IGEMM && wino_igemm_prepare() != 0) route = WINO_ROUTE_DIRECT;
+  const bool wino = route != WINO_ROUTE_DIRECT && route != WINO_ROUTE_IGEMM;
 
   mykernelParamType* a = static_cast<mykernelParamType*>(param);
   a->pin = pr.in;
@@ -263,6 +284,17 @@ int getkernelInfo(problem_t* problem, kernelInfo_t* kernelInfo, void* param) {
   a->Oh = (short)oh; a->Ow = (short)ow;
   std::memset(kernelInfo, 0, sizeof(*kernelInfo));
 
+  if (route == WINO_ROUTE_IGEMM) {
+    a->transform_pin = nullptr;
+    set_slot(kernelInfo, 1, wino_igemm_weight_grid((int)pr.c, (int)pr.k, (int)pr.r, (int)pr.s), 1, 1, 256, 1,
+             1, 0, wino_igemm_weight_kernel_ptr());
+    set_slot(kernelInfo, 2, 1, 1, 1, 32, 1, 1, 0, wino_noop_kernel_ptr());
+    set_slot(kernelInfo, 3, wino_igemm_grid((int)pr.n, (int)pr.k, oh, ow, sm_count()), 1, 1,
+             (unsigned)wino_igemm_threads(), 1, 1, (unsigned)wino_igemm_smem_bytes(),
+             wino_igemm_kernel_ptr((int)pr.k));
+    set_slot(kernelInfo, 4, 1, 1, 1, 32, 1, 1, 0, wino_noop_kernel_ptr());
+    return WINO_OK;
+  }
   if (!wino) {
     unsigned gx, gy;
     wino_direct_grid((int)pr.n, (int)pr.k, oh, ow, &gx, &gy);
@@ -592,6 +624,42 @@ extern "C" int wino_conv2d_direct(const void* x, const void* weight, void* y, in
   return wino_launch_direct(&pk, (cudaStream_t)stream) == 0 ? WINO_OK : WINO_ECUDA;
 }
 
+extern "C" int wino_igemm_weight_transform(const void* weight, void* wprep, int k, int c, int r, int s,
+                                           void* stream) {
+  if (!weight || !wprep) return WINO_EINVAL;
+  if ((reinterpret_cast<uintptr_t>(wprep) & 15) != 0) return WINO_EINVAL;
+  int oh = 0, ow = 0;
+  const int st = check_general(1, c, r, s, k, r, s, 1, 1, 0, 0, &oh, &ow);
+  if (st != WINO_OK) return st;
+  wino::KernelParam pk = make_param(nullptr, weight, nullptr, nullptr, wprep, nullptr, 1, c, r, s, k);
+  pk.r = (short)r; pk.s = (short)s;
+  void* args[] = {&pk};
+  return cudaLaunchKernel(wino_igemm_weight_kernel_ptr(), dim3(wino_igemm_weight_grid(c, k, r, s)), dim3(256),
+                          args, 0, (cudaStream_t)stream) == cudaSuccess
+             ? WINO_OK
+             : WINO_ECUDA;
+}
+
+extern "C" int wino_conv2d_igemm(const void* x, const void* wprep, void* y, int n, int c, int h, int w, int k,
+                                 int r, int s, int u, int v, int p, int q, void* stream) {
+  if (!x || !wprep || !y) return WINO_EINVAL;
+  if ((reinterpret_cast<uintptr_t>(wprep) & 15) != 0) return WINO_EINVAL;
+  int oh = 0, ow = 0;
+  const int st = check_general(n, c, h, w, k, r, s, u, v, p, q, &oh, &ow);
+  if (st != WINO_OK) return st;
+  if (!wino_igemm_shape_ok(n, c, h, w, k, oh, ow)) return WINO_EUNSUPPORTED;
+  if (wino_igemm_prepare() != 0) return WINO_ECUDA;
+  wino::KernelParam pk = make_param(x, nullptr, y, nullptr, const_cast<void*>(wprep), nullptr, n, c, h, w, k);
+  pk.r = (short)r; pk.s = (short)s; pk.u = (short)u; pk.v = (short)v; pk.p = (short)p; pk.q = (short)q;
+  pk.Oh = (short)oh; pk.Ow = (short)ow;
+  void* args[] = {&pk};
+  return cudaLaunchKernel(wino_igemm_kernel_ptr(k), dim3(wino_igemm_grid(n, k, oh, ow, sm_count())),
+                          dim3(wino_igemm_threads()), args, (size_t)wino_igemm_smem_bytes(),
+                          (cudaStream_t)stream) == cudaSuccess
+             ? WINO_OK
+             : WINO_ECUDA;
+}
+
 // Launch the four slots of a filled kernelInfo_t in order on one stream, each
 // with args[0] = param, exactly as the reference harness does
 // (reference src/main.cpp:105-108, 121-124, hipExtLaunchKernel).
@@ -614,6 +682,7 @@ extern "C" int wino_error_read_clear(uint32_t* code) {
   const uint32_t a = wino_fused_error_read_clear();
   const uint32_t b = wino_unfused_error_read_clear();
   const uint32_t c = wino_twostage_error_read_clear();
-  *code = a ? a : (b ? b : c);
+  const uint32_t d = wino_igemm_error_read_clear();
+  *code = a ? a : (b ? b : (c ? c : d));
   return WINO_OK;
 }

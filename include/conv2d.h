@@ -49,10 +49,17 @@
  *       16-byte aligned or too small): slot 2 is an empty kernel and the
  *       fused kernel reads `in` directly; transform_pin and mid_result are
  *       left untouched.
- *     direct route: any other shape (filter size, stride, padding, channel
- *       counts not multiples of 16) or a null transform_filter: slot 3 is a
- *       direct convolution (fp32 accumulation), slots 1, 2, 4 empty kernels;
- *       no workspace is touched.
+ *     implicit-GEMM route: any other shape (filter size, stride, padding,
+ *       channel counts not multiples of 16) whose re-laid-out weights,
+ *       r*s*ceil(c/16)*round16(k) rows of 32 bytes, fit transform_filter
+ *       (non-null, 16-byte aligned): slot 1 weight -> transform_filter in the
+ *       tensor-core operand layout; slot 3 tcgen05 implicit GEMM reading `in`
+ *       directly -> out (fp32 accumulation); slots 2, 4 empty kernels;
+ *       transform_pin and mid_result are left untouched.
+ *     direct route: the remaining shapes (e.g. c = 3 with a 7x7 filter) or a
+ *       null transform_filter: slot 3 is a direct convolution on CUDA cores
+ *       (fp32 accumulation), slots 1, 2, 4 empty kernels; no workspace is
+ *       touched.
  *   - return value 0 on success, non-zero (a WINO_E* code from winoconv.h)
  *     for unsupported shapes, null pointers or a CUDA attribute failure.
  */
@@ -68,8 +75,8 @@ typedef struct
     _Float16*       in;                 /* input,  NCHW, device memory            */
     _Float16*       weight;             /* weights, KCRS, device memory           */
     _Float16*       out;                /* output, N K Oh Ow, device memory       */
-    _Float16*       transform_pin;      /* workspace: channel-blocked input       */
-    _Float16*       transform_filter;   /* workspace: transformed filter U        */
+    _Float16*       transform_pin;      /* workspace: pre-pass output (V, input) */
+    _Float16*       transform_filter;   /* workspace: U, or the igemm weights     */
     _Float16*       mid_result;         /* workspace: tap GEMM output M           */
     unsigned int    n;                  /* batch size                             */
     unsigned int    c;                  /* input channels                         */

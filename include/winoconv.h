@@ -48,14 +48,23 @@ enum {
 int wino_check_shape(int n, int c, int h, int w, int k);
 
 /* The route getkernelInfo takes for a problem_t (conv2d.h), without CUDA
- * calls: the direct kernel (shapes outside the Winograd contract, or no
- * transform_filter), the fused kernel reading the NCHW input (no usable
- * transform_pin), the fused kernel after the input pre-pass, or the
- * two-stage route (pre-pass, input-fused tap GEMM with M in mid_result,
- * output transform: needs mid_result of 4*k*h*w*n fp16 to hold 16*k*tiles,
- * i.e. even h and w).  Returns a WINO_ROUTE_* value, or minus a WINO_E* code
- * for an invalid problem. */
-enum { WINO_ROUTE_DIRECT = 0, WINO_ROUTE_FUSED = 1, WINO_ROUTE_FUSED_XB = 2, WINO_ROUTE_TWOSTAGE = 3 };
+ * calls: the direct kernel (no transform_filter, or a shape outside the
+ * Winograd contract whose re-laid-out weights do not fit it), the fused
+ * kernel reading the NCHW input (no usable transform_pin), the fused kernel
+ * after the input pre-pass, the two-stage route (pre-pass, input-fused tap
+ * GEMM with M in mid_result, output transform: needs mid_result of
+ * 4*k*h*w*n fp16 to hold 16*k*tiles, i.e. even h and w), or the tensor-core
+ * implicit GEMM for shapes outside the Winograd contract (weights re-laid
+ * out into transform_filter, which must hold wino_igemm_weight_bytes).
+ * Returns a WINO_ROUTE_* value, or minus a WINO_E* code for an invalid
+ * problem. */
+enum {
+  WINO_ROUTE_DIRECT = 0,
+  WINO_ROUTE_FUSED = 1,
+  WINO_ROUTE_FUSED_XB = 2,
+  WINO_ROUTE_TWOSTAGE = 3,
+  WINO_ROUTE_IGEMM = 4
+};
 int wino_dropin_route(const void* problem);
 
 /* Bytes of the U cache for a variant (fp16: 16*k*c*2). */
@@ -120,6 +129,22 @@ int wino_conv2d_fused_epilogue(const void* x, const void* ucache, void* workspac
  * (the reference ignores r, s, u, v, p, q, src/conv2d.cpp:254-271). */
 int wino_conv2d_direct(const void* x, const void* weight, void* y, int n, int c, int h, int w, int k,
                        int r, int s, int u, int v, int p, int q, void* stream);
+
+/* Implicit-GEMM convolution on the tcgen05 tensor cores for the same general
+ * shapes (any r x s, stride, padding; channel counts padded to 16 with
+ * zeros): D[pixel][k] over K-steps of (tap, 16 channels), fp16 operands,
+ * fp32 accumulation, one fp16 rounding of y.  wino_igemm_weight_transform
+ * re-lays the KCRS weights into wprep (wino_igemm_weight_bytes bytes,
+ * 16-byte aligned), which stays valid for as long as the weights do;
+ * wino_conv2d_igemm then gathers the pixel operand straight from the NCHW
+ * input.  getkernelInfo takes this route for shapes outside the Winograd
+ * contract when wprep fits the caller's transform_filter (16*k*c fp16,
+ * reference src/main.cpp:38), i.e. r*s*ceil(c/16)*round16(k) <= k*c. */
+size_t wino_igemm_weight_bytes(int c, int k, int r, int s);
+int wino_igemm_weight_transform(const void* weight, void* wprep, int k, int c, int r, int s,
+                                void* stream);
+int wino_conv2d_igemm(const void* x, const void* wprep, void* y, int n, int c, int h, int w, int k,
+                      int r, int s, int u, int v, int p, int q, void* stream);
 
 /* The plain unfused path, the comparator of the fused kernel: input
  * transform to V in global memory, the 16 tap GEMMs as one batched tcgen05

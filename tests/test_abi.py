@@ -78,12 +78,13 @@ def test_getkernelinfo_rejects_invalid(wino, field, value, code):
 
 
 @pytest.mark.parametrize("field,value", [
-    ("r", 5), ("s", 1), ("u", 2), ("v", 2), ("p", 0), ("q", 2), ("c", 8), ("k", 27), ("c", 3),
-    ("transform_filter", 0),
+    ("r", 5), ("c", 8), ("c", 3), ("transform_filter", 0),
 ])
 def test_getkernelinfo_sends_other_shapes_to_the_direct_kernel(wino, field, value):
-    """Shapes outside the Winograd contract get the direct kernel in slot 3
-    and empty kernels elsewhere (needs no GPU: no attribute is set)."""
+    """Shapes outside the Winograd contract whose implicit-GEMM weights do not
+    fit transform_filter (or with no usable transform_filter) get the direct
+    kernel in slot 3 and empty kernels elsewhere (needs no GPU: no attribute
+    is set)."""
     pr = _problem(wino, **{field: value})
     param = (ctypes.c_char * 80)()
     rc, ki = wino.get_kernel_info(pr, param)
@@ -95,6 +96,36 @@ def test_getkernelinfo_sends_other_shapes_to_the_direct_kernel(wino, field, valu
     dims = np.frombuffer(bytes(param)[48:74], dtype=np.int16)
     n, c, h, w, k, r, s, u, v, p, q, oh, ow = dims
     assert oh == (h - r + 2 * p) // u + 1 and ow == (w - s + 2 * q) // v + 1
+
+
+def test_igemm_weight_bytes_and_entry_points(wino):
+    L = wino.lib()
+    # round16(k) rows x r*s*ceil(c/16) K-steps x 32 bytes
+    assert L.wino_igemm_weight_bytes(64, 128, 3, 3) == 128 * 9 * 4 * 32
+    assert L.wino_igemm_weight_bytes(24, 40, 3, 3) == 48 * 9 * 2 * 32
+    assert L.wino_igemm_weight_bytes(3, 64, 7, 7) == 64 * 49 * 32
+    d = ctypes.c_void_p(0x10000)
+    odd = ctypes.c_void_p(0x10008)
+    assert L.wino_igemm_weight_transform(None, d, 16, 16, 3, 3, None) == 1
+    assert L.wino_igemm_weight_transform(d, odd, 16, 16, 3, 3, None) == 1   # wprep alignment
+    assert L.wino_igemm_weight_transform(d, d, 0, 16, 3, 3, None) == 1
+    assert L.wino_conv2d_igemm(None, d, d, 1, 16, 8, 8, 16, 3, 3, 2, 2, 1, 1, None) == 1
+    assert L.wino_conv2d_igemm(d, odd, d, 1, 16, 8, 8, 16, 3, 3, 2, 2, 1, 1, None) == 1
+    assert L.wino_conv2d_igemm(d, d, d, 1, 16, 8, 8, 16, 9, 9, 1, 1, 0, 0, None) == 1  # filter > input
+    # one image of 2^31 input elements: offsets would leave 32 bits
+    assert L.wino_conv2d_igemm(d, d, d, 1, 2048, 1024, 1024, 16, 1, 1, 1, 1, 0, 0, None) == 2
+
+
+@pytest.mark.parametrize("field,value", [
+    ("s", 1), ("u", 2), ("v", 2), ("p", 0), ("q", 2), ("k", 27), ("c", 24),
+])
+def test_getkernelinfo_sends_other_shapes_to_the_igemm_kernel(wino, field, value):
+    """Shapes outside the Winograd contract whose re-laid-out weights fit
+    transform_filter get the weight re-layout in slot 1 and the tensor-core
+    implicit GEMM in slot 3 (the CUDA attribute call needs a GPU, so only the
+    route is checked here)."""
+    pr = _problem(wino, **{field: value})
+    assert wino.lib().wino_dropin_route(ctypes.byref(pr)) == 4
 
 
 def test_check_shape(wino):
@@ -312,13 +343,16 @@ def test_twostage_entry_points_validate_and_size(wino):
     (dict(h=12, w=10, transform_pin=0x100008, mid_result=0x200000), 1),   # misaligned transform_pin
     (dict(h=12, w=10, transform_pin=0x100000, mid_result=0x200000, transform_filter=0), 0),
     (dict(h=12, w=10, transform_pin=0x100000, mid_result=0x200000, r=5, s=5, p=2, q=2), 0),
-    (dict(h=12, w=10, transform_pin=0x100000, mid_result=0x200000, c=24), 0),
-    (dict(h=12, w=10, transform_pin=0x100000, mid_result=0x200000, u=2, v=2), 0),
+    (dict(h=12, w=10, transform_pin=0x100000, mid_result=0x200000, c=24), 4),
+    (dict(h=12, w=10, transform_pin=0x100000, mid_result=0x200000, u=2, v=2), 4),
+    (dict(h=12, w=10, r=1, s=1, p=0, q=0), 4),                           # 1x1
+    (dict(h=12, w=10, r=1, s=1, p=0, q=0, transform_filter=0x4008), 0),  # misaligned transform_filter
+    (dict(h=12, w=10, c=3, r=7, s=7, p=3, q=3, u=2, v=2), 0),            # weights do not fit
 ])
 def test_dropin_route_selection(wino, kw, route):
     """Which kernels getkernelInfo will put in the slots (decided without CUDA
     calls): 0 direct, 1 fused on the NCHW input, 2 fused after the pre-pass,
-    3 two-stage (M in the caller's mid_result)."""
+    3 two-stage (M in the caller's mid_result), 4 tensor-core implicit GEMM."""
     pr = _problem(wino, **{"n": 2, "c": 32, "k": 32, **kw})
     assert wino.lib().wino_dropin_route(ctypes.byref(pr)) == route
 
