@@ -39,6 +39,8 @@
 namespace wino {
 
 static __device__ uint32_t g_igemm_err;
+// zero words the pixel producers read in place of padding and missing channels
+static __device__ __align__(16) unsigned short g_igemm_zero[8];
 
 namespace ig {
 constexpr int NSTAGE = 4;
@@ -133,7 +135,14 @@ __global__ void __launch_bounds__(256) igemm_weight_kernel(KernelParam p) {
   *reinterpret_cast<uint4*>(dst) = make_uint4(v[0], v[1], v[2], v[3]);
 }
 
-template <int PM>
+// FLAT: 1x1 filter, stride 1, no padding, H * W a multiple of 8 and a
+// 16-byte aligned input.  The output pixels of an image are then its input
+// pixels, eight consecutive ones of a channel are one aligned 16-byte word,
+// and the pixel operand is staged MN-major (pixels contiguous): thread =
+// (pixel octet, channel), one 16-byte load and one 16-byte shared store per
+// octet, channel and K-step.  Otherwise thread = (pixel, channel half) and
+// eight 2-byte loads build each K-major 16-byte row.
+template <int PM, bool FLAT>
 __global__ void __launch_bounds__(ig::NTHREAD, 1) igemm_conv_kernel(KernelParam p) {
   using namespace ig;
   constexpr int SKS = NPIECE / PM;          // K-steps per stage
@@ -204,13 +213,17 @@ __global__ void __launch_bounds__(ig::NTHREAD, 1) igemm_conv_kernel(KernelParam 
         mbar_wait(&sh.full[s2 % NSTAGE], (s2 / NSTAGE) & 1, nullptr, err, ERR_WAIT_FULL);
     }
     if (warp == WARP_MMA && lane == 0) {
+      // pixel operand of a piece: K-major (8-channel halves 128 bytes apart,
+      // pixel octets 256) or, FLAT, MN-major (pixel octets 128 bytes apart,
+      // channel halves 2048)
+      auto a_desc = [](uint32_t a) { return FLAT ? smem_desc(a, 2048, 128) : smem_desc(a, 128, 256); };
       uint32_t it = 0;
       bool ok = true;
       for (int i = 0; ok && i < cnt && !*abort_flag; ++i) {
         int pt, kb;
         unit_of(g, g0 + i * G, pt, kb);
         const int rows = block_rows(kb, g.Kp);
-        const uint32_t idesc = instr_desc(128, (uint32_t)rows, 0, 0, 0, 0);
+        const uint32_t idesc = instr_desc(128, (uint32_t)rows, 0, 0, FLAT ? 1 : 0, 0);
         const int ab = i & 1;
         if (i >= 2 && !mbar_wait(&sh.accempty[ab], ((i >> 1) - 1) & 1, abort_flag, err, ERR_WAIT_DRAIN)) break;
         tc_fence_after();
@@ -228,7 +241,7 @@ __global__ void __launch_bounds__(ig::NTHREAD, 1) igemm_conv_kernel(KernelParam 
             const uint64_t bd = smem_desc(b0 + (uint32_t)(q * rows * 32), 128, 256);
 #pragma unroll
             for (int h = 0; h < PM; ++h)
-              mma_f16(d + h * 128, smem_desc(a0 + (uint32_t)((q * PM + h) * PIECE), 128, 256), bd, idesc,
+              mma_f16(d + h * 128, a_desc(a0 + (uint32_t)((q * PM + h) * PIECE)), bd, idesc,
                       (j > 0 || q > 0) ? 1u : 0u);
           }
           mma_commit(&sh.empty[st]);
@@ -245,6 +258,9 @@ __global__ void __launch_bounds__(ig::NTHREAD, 1) igemm_conv_kernel(KernelParam 
     // epilogue: TMEM lane 32 * quarter + lane = pixel of the half
     const int quarter = warp & 3;
     __half* Y = static_cast<__half*>(p.pout);
+    // pixel pairs share 4-byte stores when every image holds an even pixel
+    // count (then NPIX is even too, and a pair is live or dead as a whole)
+    const bool pair = (g.OHOW & 1) == 0;
     for (int ui = 0; ui < cnt; ++ui) {
       int pt, kb;
       unit_of(g, g0 + ui * G, pt, kb);
@@ -268,11 +284,28 @@ __global__ void __launch_bounds__(ig::NTHREAD, 1) igemm_conv_kernel(KernelParam 
           tmem_ld16(taddr + cc, v);
           if (cc + 16 < rows) tmem_ld16(taddr + cc + 16, v + 16);
         };
+        // With an even pixel count per image, lanes 2i and 2i + 1 hold two
+        // neighbouring pixels of one image (P even starts a pair): the even
+        // lane stores columns cc + jj (jj even) for both pixels and the odd
+        // lane columns cc + jj + 1, one 4-byte store and one two-value
+        // conversion per lane and column pair.
+        const bool odd = lane & 1;
+        __half* yp = yb - (odd ? 1 : 0);       // the pair's first pixel
         auto st = [&](int cc, const float* v) {
-          if (!live) return;
+          if (pair) {
 #pragma unroll
-          for (int jj = 0; jj < 32; ++jj)
-            if (cc + jj < kval) yb[(size_t)(cc + jj) * g.OHOW] = __float2half_rn(v[jj]);
+            for (int jj = 0; jj < 32; jj += 2) {
+              const float mine = odd ? v[jj] : v[jj + 1];
+              const float other = __shfl_xor_sync(0xffffffffu, mine, 1);
+              const int col = cc + jj + (odd ? 1 : 0);
+              const __half2 hv = odd ? __floats2half2_rn(other, v[jj + 1]) : __floats2half2_rn(v[jj], other);
+              if (live && col < kval) *reinterpret_cast<__half2*>(yp + (size_t)col * g.OHOW) = hv;
+            }
+          } else if (live) {
+#pragma unroll
+            for (int jj = 0; jj < 32; ++jj)
+              if (cc + jj < kval) yb[(size_t)(cc + jj) * g.OHOW] = __float2half_rn(v[jj]);
+          }
         };
         float va[32], vb[32];
         ld(0, va);
@@ -290,6 +323,81 @@ __global__ void __launch_bounds__(ig::NTHREAD, 1) igemm_conv_kernel(KernelParam 
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&sh.accempty[ab]);
+    }
+  } else if constexpr (FLAT) {
+    regs_inc<REGS_PROD>();
+    // octet producers: warp pw covers octets 4 (pw & 3) .. + 3 of each
+    // 128-pixel half and channels 8 (pw >> 2) .. + 7 of the K-step; lane l
+    // takes octet l >> 3 of those and channel l & 7, so the eight lanes of a
+    // shared-store phase fill one 128-byte octet row without bank conflicts
+    // and lanes 8 apart load neighbouring octets of a channel.
+    const int pw = warp - WARP_P0;
+    const int o = (lane >> 3) + 4 * (pw & 3), c16 = (lane & 7) + 8 * (pw >> 2);
+    const __half* X = static_cast<const __half*>(p.pin);
+    const uint4* zero4 = reinterpret_cast<const uint4*>(g_igemm_zero);
+    int lu = 0, lj = 0;
+    long long off[PM];
+    bool live[PM];
+#pragma unroll
+    for (int h = 0; h < PM; ++h) {
+      off[h] = 0;
+      live[h] = false;
+    }
+    uint4 w0[NPIECE], w1[NPIECE], w2[NPIECE];
+    auto issue = [&](uint4 (&w)[NPIECE]) {
+      if (lu >= cnt) return;
+      if (lj == 0) {
+        int pt, kb;
+        unit_of(g, g0 + lu * G, pt, kb);
+#pragma unroll
+        for (int h = 0; h < PM; ++h) {
+          const long long P = (long long)pt * (128 * PM) + h * 128 + 8 * o;   // octets lie in one image
+          live[h] = P < g.NPIX;
+          const long long n = live[h] ? P / g.HW : 0;
+          off[h] = n * g.C * g.HW + (P - n * g.HW);
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < SKS; ++q) {
+        const int ch = (lj * SKS + q) * 16 + c16;      // one K-step per 16 channels
+        const bool kv = lj * SKS + q < g.NKS && ch < g.C;
+#pragma unroll
+        for (int h = 0; h < PM; ++h)
+          w[q * PM + h] = __ldg(kv && live[h] ? reinterpret_cast<const uint4*>(X + off[h] + (long long)ch * g.HW)
+                                              : zero4);
+      }
+      if (++lj == nst) { lj = 0; ++lu; }
+    };
+    uint32_t it = 0;
+    int cu = 0, cj = 0;
+    auto consume = [&](const uint4 (&w)[NPIECE]) -> bool {
+      const int st = it % NSTAGE;
+      if (it >= NSTAGE &&
+          !mbar_wait_warp(&sh.empty[st], (it / NSTAGE - 1) & 1, abort_flag, err, ERR_WAIT_EMPTY, SLEEP_NS))
+        return false;
+      const int npc = min(NPIECE, (g.NKS - cj * SKS) * PM);
+      uint8_t* adst = smem + st * STAGE + (c16 >> 3) * 2048 + o * 128 + (c16 & 7) * 16;
+#pragma unroll
+      for (int pc = 0; pc < NPIECE; ++pc)
+        if (pc < npc) *reinterpret_cast<uint4*>(adst + pc * PIECE) = w[pc];
+      fence_proxy_async_shared();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&sh.full[st]);
+      ++it;
+      if (++cj == nst) { cj = 0; ++cu; }
+      return cu < cnt && !*abort_flag;
+    };
+    if (cnt > 0) {
+      issue(w0);
+      issue(w1);
+      while (true) {
+        issue(w2);
+        if (!consume(w0)) break;
+        issue(w0);
+        if (!consume(w1)) break;
+        issue(w1);
+        if (!consume(w2)) break;
+      }
     }
   } else {
     regs_inc<REGS_PROD>();
@@ -342,9 +450,17 @@ __global__ void __launch_bounds__(ig::NTHREAD, 1) igemm_conv_kernel(KernelParam 
         for (int h = 0; h < PM; ++h) {
           const int iy = iy0[h] + kr, ix = ix0[h] + kx;
           const bool ok = live[h] && nc > 0 && (unsigned)iy < (unsigned)g.H && (unsigned)ix < (unsigned)g.W;
-          const unsigned short* src = img[h] + (ok ? c0 * g.HW + iy * g.W + ix : 0);
+          // every load is unconditional (so none waits on another): what is
+          // outside the image or past C reads the zero words instead
+          const unsigned short* src = ok ? img[h] + (c0 * g.HW + iy * g.W + ix) : g_igemm_zero;
+          const int step = ok ? g.HW : 0;
+          if (nc >= 8) {
 #pragma unroll
-          for (int e = 0; e < 8; ++e) w[q * PM + h][e] = (ok && e < nc) ? __ldg(src + e * g.HW) : 0u;
+            for (int e = 0; e < 8; ++e) w[q * PM + h][e] = __ldg(src + e * step);
+          } else {
+#pragma unroll
+            for (int e = 0; e < 8; ++e) w[q * PM + h][e] = __ldg(e < nc ? src + e * step : g_igemm_zero);
+          }
         }
         if (++kc == g.CB) {
           kc = 0;
@@ -420,8 +536,16 @@ void* wino_igemm_weight_kernel_ptr() { return (void*)igemm_weight_kernel; }
 // Two pixel halves a unit when the output channels fit one 128-row block.
 static int igemm_pm(int k) { return ig::kpad(k) <= 128 ? 2 : 1; }
 
-void* wino_igemm_kernel_ptr(int k) {
-  return igemm_pm(k) == 2 ? (void*)igemm_conv_kernel<2> : (void*)igemm_conv_kernel<1>;
+// The octet-loading (FLAT) instance serves 1x1 / stride 1 / pad 0 problems
+// with H * W a multiple of 8 and a 16-byte aligned input.
+int wino_igemm_flat(const void* x, int h, int w, int r, int s, int u, int v, int p, int q) {
+  return r == 1 && s == 1 && u == 1 && v == 1 && p == 0 && q == 0 && ((long long)h * w) % 8 == 0 &&
+         (reinterpret_cast<uintptr_t>(x) & 15) == 0;
+}
+
+void* wino_igemm_kernel_ptr(int k, int flat) {
+  if (flat) return igemm_pm(k) == 2 ? (void*)igemm_conv_kernel<2, true> : (void*)igemm_conv_kernel<1, true>;
+  return igemm_pm(k) == 2 ? (void*)igemm_conv_kernel<2, false> : (void*)igemm_conv_kernel<1, false>;
 }
 
 int wino_igemm_threads() { return ig::NTHREAD; }
@@ -448,15 +572,22 @@ int wino_igemm_shape_ok(int n, int c, int h, int w, int k, int oh, int ow) {
 }
 
 int wino_igemm_prepare() {
-  if (cudaFuncSetAttribute(igemm_conv_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, ig::SMEM_BYTES) !=
-          cudaSuccess ||
-      cudaFuncSetAttribute(igemm_conv_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, ig::SMEM_BYTES) !=
-          cudaSuccess)
-    return 1;
-  // the warpgroups split exactly the registers the block launches with
-  cudaFuncAttributes fa{};
-  if (cudaFuncGetAttributes(&fa, igemm_conv_kernel<1>) != cudaSuccess || fa.numRegs != ig::REGS_LAUNCH) return 1;
-  if (cudaFuncGetAttributes(&fa, igemm_conv_kernel<2>) != cudaSuccess || fa.numRegs != ig::REGS_LAUNCH) return 1;
+  // attributes are per function and device: set them once per device (a
+  // repeated set from another thread is harmless)
+  static int done[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 1;
+  if (dev >= 0 && dev < 64 && done[dev]) return 0;
+  const void* fns[4] = {(void*)igemm_conv_kernel<1, false>, (void*)igemm_conv_kernel<2, false>,
+                        (void*)igemm_conv_kernel<1, true>, (void*)igemm_conv_kernel<2, true>};
+  for (const void* f : fns) {
+    if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, ig::SMEM_BYTES) != cudaSuccess)
+      return 1;
+    // the warpgroups split exactly the registers the block launches with
+    cudaFuncAttributes fa{};
+    if (cudaFuncGetAttributes(&fa, f) != cudaSuccess || fa.numRegs != ig::REGS_LAUNCH) return 1;
+  }
+  if (dev >= 0 && dev < 64) done[dev] = 1;
   return 0;
 }
 

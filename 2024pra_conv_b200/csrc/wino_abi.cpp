@@ -100,7 +100,8 @@ uint32_t wino_twostage_error_read_clear();
 size_t wino_igemm_weight_bytes(int c, int k, int r, int s);
 unsigned wino_igemm_weight_grid(int c, int k, int r, int s);
 void* wino_igemm_weight_kernel_ptr();
-void* wino_igemm_kernel_ptr(int k);
+void* wino_igemm_kernel_ptr(int k, int flat);
+int wino_igemm_flat(const void* x, int h, int w, int r, int s, int u, int v, int p, int q);
 int wino_igemm_threads();
 int wino_igemm_smem_bytes();
 unsigned wino_igemm_grid(int n, int k, int oh, int ow, int sms);
@@ -291,7 +292,8 @@ int getkernelInfo(problem_t* problem, kernelInfo_t* kernelInfo, void* param) {
     set_slot(kernelInfo, 2, 1, 1, 1, 32, 1, 1, 0, wino_noop_kernel_ptr());
     set_slot(kernelInfo, 3, wino_igemm_grid((int)pr.n, (int)pr.k, oh, ow, sm_count()), 1, 1,
              (unsigned)wino_igemm_threads(), 1, 1, (unsigned)wino_igemm_smem_bytes(),
-             wino_igemm_kernel_ptr((int)pr.k));
+             wino_igemm_kernel_ptr((int)pr.k, wino_igemm_flat(pr.in, (int)pr.h, (int)pr.w, (int)pr.r, (int)pr.s,
+                                                              (int)pr.u, (int)pr.v, (int)pr.p, (int)pr.q)));
     set_slot(kernelInfo, 4, 1, 1, 1, 32, 1, 1, 0, wino_noop_kernel_ptr());
     return WINO_OK;
   }
@@ -653,7 +655,8 @@ extern "C" int wino_conv2d_igemm(const void* x, const void* wprep, void* y, int 
   pk.r = (short)r; pk.s = (short)s; pk.u = (short)u; pk.v = (short)v; pk.p = (short)p; pk.q = (short)q;
   pk.Oh = (short)oh; pk.Ow = (short)ow;
   void* args[] = {&pk};
-  return cudaLaunchKernel(wino_igemm_kernel_ptr(k), dim3(wino_igemm_grid(n, k, oh, ow, sm_count())),
+  return cudaLaunchKernel(wino_igemm_kernel_ptr(k, wino_igemm_flat(x, h, w, r, s, u, v, p, q)),
+                          dim3(wino_igemm_grid(n, k, oh, ow, sm_count())),
                           dim3(wino_igemm_threads()), args, (size_t)wino_igemm_smem_bytes(),
                           (cudaStream_t)stream) == cudaSuccess
              ? WINO_OK

@@ -38,6 +38,10 @@ SHAPES = [  # n, c, h, w, k, r, s, stride, pad
     (2, 3, 32, 32, 64, 7, 7, 2, 3),       # stem 7x7 stride 2, C = 3
     (1, 16, 9, 9, 16, 3, 3, 1, 0),        # pad 0, one unit, one K-step a tap
     (3, 32, 7, 7, 48, 1, 3, 1, 0),        # 1x3 filter, 147 pixels (a partial unit)
+    # 1x1 / stride 1 / pad 0 with H * W % 8 == 0: pixel octets by 16-byte loads
+    (2, 24, 16, 16, 40, 1, 1, 1, 0),      # ragged C and K, two pixel halves
+    (3, 64, 28, 28, 320, 1, 1, 1, 0),     # two k-blocks, 2352 pixels (a partial unit)
+    (1, 512, 8, 12, 128, 1, 1, 1, 0),     # 32 K-steps, one partial unit
 ]
 
 
