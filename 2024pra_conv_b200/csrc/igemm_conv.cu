@@ -61,6 +61,12 @@ constexpr int REGS_LAUNCH = 128, REGS_EPI = 104, REGS_MMA = 56, REGS_PROD = 176;
 static_assert(128 * REGS_EPI + 128 * REGS_MMA + 256 * REGS_PROD == NTHREAD * REGS_LAUNCH,
               "the warpgroups' register limits add up to the launch allocation");
 constexpr uint32_t SLEEP_NS = 32;
+// stages of 16-byte loads each octet producer keeps in registers
+#ifndef WINO_IG_RING
+#define WINO_IG_RING 3
+#endif
+constexpr int RING_F = WINO_IG_RING;
+static_assert(RING_F >= 2 && RING_F <= 8, "ring of two to eight stages");
 
 struct Shared {
   uint64_t full[NSTAGE], empty[NSTAGE];
@@ -284,28 +290,9 @@ __global__ void __launch_bounds__(ig::NTHREAD, 1) igemm_conv_kernel(KernelParam 
           tmem_ld16(taddr + cc, v);
           if (cc + 16 < rows) tmem_ld16(taddr + cc + 16, v + 16);
         };
-        // With an even pixel count per image, lanes 2i and 2i + 1 hold two
-        // neighbouring pixels of one image (P even starts a pair): the even
-        // lane stores columns cc + jj (jj even) for both pixels and the odd
-        // lane columns cc + jj + 1, one 4-byte store and one two-value
-        // conversion per lane and column pair.
-        const bool odd = lane & 1;
-        __half* yp = yb - (odd ? 1 : 0);       // the pair's first pixel
+        // pixel pairs of one image share 4-byte stores (see `pair`)
         auto st = [&](int cc, const float* v) {
-          if (pair) {
-#pragma unroll
-            for (int jj = 0; jj < 32; jj += 2) {
-              const float mine = odd ? v[jj] : v[jj + 1];
-              const float other = __shfl_xor_sync(0xffffffffu, mine, 1);
-              const int col = cc + jj + (odd ? 1 : 0);
-              const __half2 hv = odd ? __floats2half2_rn(other, v[jj + 1]) : __floats2half2_rn(v[jj], other);
-              if (live && col < kval) *reinterpret_cast<__half2*>(yp + (size_t)col * g.OHOW) = hv;
-            }
-          } else if (live) {
-#pragma unroll
-            for (int jj = 0; jj < 32; ++jj)
-              if (cc + jj < kval) yb[(size_t)(cc + jj) * g.OHOW] = __float2half_rn(v[jj]);
-          }
+          store_cols_f16<32>(yb + (size_t)cc * g.OHOW, (size_t)g.OHOW, v, kval - cc, live, pair);
         };
         float va[32], vb[32];
         ld(0, va);
@@ -343,7 +330,7 @@ __global__ void __launch_bounds__(ig::NTHREAD, 1) igemm_conv_kernel(KernelParam 
       off[h] = 0;
       live[h] = false;
     }
-    uint4 w0[NPIECE], w1[NPIECE], w2[NPIECE];
+    uint4 w[RING_F][NPIECE];
     auto issue = [&](uint4 (&w)[NPIECE]) {
       if (lu >= cnt) return;
       if (lj == 0) {
@@ -388,15 +375,19 @@ __global__ void __launch_bounds__(ig::NTHREAD, 1) igemm_conv_kernel(KernelParam 
       return cu < cnt && !*abort_flag;
     };
     if (cnt > 0) {
-      issue(w0);
-      issue(w1);
-      while (true) {
-        issue(w2);
-        if (!consume(w0)) break;
-        issue(w0);
-        if (!consume(w1)) break;
-        issue(w1);
-        if (!consume(w2)) break;
+      // RING_F - 1 stages of loads in flight while one is stored
+#pragma unroll
+      for (int r = 0; r + 1 < RING_F; ++r) issue(w[r]);
+      bool more = true;
+      while (more) {
+#pragma unroll
+        for (int r = 0; r < RING_F; ++r) {
+          issue(w[(r + RING_F - 1) % RING_F]);
+          if (!consume(w[r])) {
+            more = false;
+            break;
+          }
+        }
       }
     }
   } else {

@@ -339,6 +339,45 @@ __device__ __forceinline__ void tmem_ld_wait() {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// Epilogue store of NC accumulator columns held one row a lane (v[c] = row
+// lane, column c, as tcgen05.ld 32x32b returns them) into fp16 memory where
+// a row's consecutive elements are neighbours and columns are `stride`
+// elements apart: element (lane, c) goes to row[c * stride], `row` being this
+// lane's element of column 0.  Columns c < lim are stored (lim uniform across
+// the warp; v may hold garbage past it).  With `pair` (stride even, the even
+// lane's row element 4-byte aligned, lanes 2i and 2i + 1 live together) the
+// two lanes of a pair swap one value per column pair, so each stores one
+// 4-byte word of both rows: half the stores and one two-value conversion per
+// word.  The loop has no early exit, so the shuffles of a chunk issue back
+// to back.  All 32 lanes call.
+template <int NC>
+__device__ __forceinline__ void store_cols_f16(__half* row, size_t stride, const float* v, int lim, bool live,
+                                               bool pair) {
+  const bool odd = (threadIdx.x & 1) != 0;
+  if (pair) {
+    __half* first = row - (odd ? 1 : 0);   // the pair's even row
+    // groups of eight column pairs: eight shuffles in flight, then their stores
+#pragma unroll
+    for (int j0 = 0; j0 < NC / 2; j0 += 8) {
+      float other[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j)
+        other[j] = __shfl_xor_sync(0xffffffffu, odd ? v[2 * (j0 + j)] : v[2 * (j0 + j) + 1], 1);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int c = 2 * (j0 + j);
+        const __half2 hv = odd ? __floats2half2_rn(other[j], v[c + 1]) : __floats2half2_rn(v[c], other[j]);
+        const int col = c + (odd ? 1 : 0);
+        if (live && col < lim) *reinterpret_cast<__half2*>(first + (size_t)col * stride) = hv;
+      }
+    }
+  } else if (live) {
+#pragma unroll
+    for (int jj = 0; jj < NC; ++jj)
+      if (jj < lim) row[(size_t)jj * stride] = __float2half_rn(v[jj]);
+  }
+}
+
 // ------------------------------------------------- CTA pairs (cta_group::2) --
 // A cluster of two CTAs on two SMs runs one MMA over both: A (M = 256) is
 // split by rows, each CTA holding 128 rows in its own shared memory; B is
