@@ -739,6 +739,9 @@ def extension_legs(wino, dev, flush, ev, peaks, steps):
                              "us_fused": fused_ep, "us_conv_then_torch_elementwise": sep}
     del x, wt, u, ws, res, y
 
+    # --- tensor-core implicit GEMM on the shapes outside the Winograd contract
+    out["implicit_gemm"] = implicit_gemm_leg(wino, dev, timed, peaks, steps)
+
     # --- learned cost model vs exhaustive tuning (committed timings)
     path = os.path.join(ROOT, "tests", "golden", "tuning_timings.json")
     if os.path.exists(path):
@@ -753,6 +756,66 @@ def extension_legs(wino, dev, flush, ev, peaks, steps):
     if err:
         raise SystemExit(f"device error word {err}")
     return out
+
+
+# ResNet-50 layers at N = 128 that the Winograd path does not take (1x1
+# projections and expansions, stride-2 3x3 downsampling): name, c, h, k, r,
+# stride, pad.
+IGEMM_LAYERS = [
+    ("1x1 64->256 h56", 64, 56, 256, 1, 1, 0),
+    ("1x1 256->64 h56", 256, 56, 64, 1, 1, 0),
+    ("1x1 256->128 h56 s2", 256, 56, 128, 1, 2, 0),
+    ("3x3 128 s2 h56", 128, 56, 128, 3, 2, 1),
+    ("1x1 512->128 h28", 512, 28, 128, 1, 1, 0),
+    ("1x1 128->512 h28", 128, 28, 512, 1, 1, 0),
+    ("3x3 256 s2 h28", 256, 28, 256, 3, 2, 1),
+    ("1x1 1024->256 h14", 1024, 14, 256, 1, 1, 0),
+    ("3x3 512 s2 h14", 512, 14, 512, 3, 2, 1),
+]
+
+
+def implicit_gemm_leg(wino, dev, timed, peaks, steps):
+    """Each IGEMM_LAYERS layer at N = 128 through the tcgen05 implicit GEMM
+    (weights re-laid out once, L2 flushed before every call) beside the
+    CUDA-core direct kernel it replaces and the library convolution
+    (torch / cuDNN, fp16), with its roofline: floor = max(input + output +
+    weight bytes / HBM peak, direct FLOPs / bf16 peak).  rel-L2 against FP64
+    on the first 4 images."""
+    import torch
+    n = 128
+    rows = []
+    t_sum = floor_sum = 0.0
+    for name, c, h, k, r, st, pd in IGEMM_LAYERS:
+        g = torch.Generator(device=dev).manual_seed(c * 131 + h * 7 + k)
+        x = torch.randn((n, c, h, h), device=dev, generator=g).half()
+        wt = (torch.randn((k, c, r, r), device=dev, generator=g) / (c * r * r) ** 0.5).half()
+        oh = (h - r + 2 * pd) // st + 1
+        y = torch.empty((n, k, oh, oh), dtype=torch.float16, device=dev)
+        wp = wino.igemm_weight_transform(wt)
+        us = timed(lambda: wino.conv2d_igemm(x, wt, stride=st, pad=pd, wprep=wp, out=y), steps)
+        us_direct = timed(lambda: wino.conv2d_direct(x, wt, stride=st, pad=pd, out=y), max(3, steps // 4))
+        us_lib = timed(lambda: torch.nn.functional.conv2d(x, wt, stride=st, padding=pd), steps)
+        xs = x[:4].contiguous()
+        ys = wino.conv2d_igemm(xs, wt, stride=st, pad=pd, wprep=wp)
+        y64 = torch.nn.functional.conv2d(xs.double(), wt.double(), stride=st, padding=pd)
+        rl2 = float(torch.linalg.vector_norm(ys.double() - y64) / torch.linalg.vector_norm(y64))
+        flops = 2.0 * n * oh * oh * k * c * r * r
+        nbytes = 2.0 * (x.numel() + y.numel() + wt.numel())
+        floor = max(nbytes / (peaks["hbm_gbs"] * 1e9), flops / (peaks["tflops"] * 1e12)) * 1e6
+        t_sum += us
+        floor_sum += floor
+        rows.append({"layer": name, "us": round(us, 1), "us_direct_cuda_cores": round(us_direct, 1),
+                     "us_library_cudnn": round(us_lib, 1), "tflops": round(flops / (us * 1e-6) / 1e12, 1),
+                     "floor_us": round(floor, 1), "frac_of_floor": round(floor / us, 3),
+                     "bound": "hbm" if nbytes / (peaks["hbm_gbs"] * 1e9) > flops / (peaks["tflops"] * 1e12)
+                     else "tensor",
+                     "flat_octet_loads": bool(r == 1 and st == 1 and pd == 0 and (h * h) % 8 == 0),
+                     "rel_l2_fp64": rl2})
+        del x, wt, y, wp, xs, ys, y64
+    return {"workload": "ResNet-50 layers outside the Winograd contract, N128, x ~ N(0,1), "
+                        "weights ~ N(0, 1/(c r s)); drop-in route 4 runs the same kernels",
+            "layers": rows, "sum_us": round(t_sum, 1), "sum_floor_us": round(floor_sum, 1),
+            "frac_of_floor": round(floor_sum / t_sum, 3)}
 
 
 def run_only(args):
@@ -788,6 +851,15 @@ def run_only(args):
         conv = wino.ConvF4(wt, n, h, w, hilo=True)
         for _ in range(args.steps):
             conv(x)
+    elif args.only == "igemm":
+        # the 1x1 512->128 layer at 28x28 (octet loads) and the stride-2
+        # 3x3 128 layer at 56x56 (2-byte gather), batch n
+        for (c2, h2, k2, r2, st2, pd2) in ((512, 28, 128, 1, 1, 0), (128, 56, 128, 3, 2, 1)):
+            x2 = torch.randn((n, c2, h2, h2), device=dev).half()
+            w2 = (torch.randn((k2, c2, r2, r2), device=dev) / (c2 * r2 * r2) ** 0.5).half()
+            wp2 = wino.igemm_weight_transform(w2)
+            for _ in range(args.steps):
+                wino.conv2d_igemm(x2, w2, stride=st2, pad=pd2, wprep=wp2)
     else:
         for _ in range(args.steps):
             wino.dropin_conv2d(x, wt)
@@ -807,7 +879,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the layer-set / variants / cost-model legs")
-    ap.add_argument("--only", choices=["fused", "unfused", "dropin", "f4", "twostage"],
+    ap.add_argument("--only", choices=["fused", "unfused", "dropin", "f4", "twostage", "igemm"],
                     help="only launch this path (profiler captures)")
     ap.add_argument("--n", type=int, default=0, help="batch size for --only")
     args = ap.parse_args()
