@@ -116,6 +116,21 @@ def test_igemm_weight_bytes_and_entry_points(wino):
     assert L.wino_conv2d_igemm(d, d, d, 1, 2048, 1024, 1024, 16, 1, 1, 1, 1, 0, 0, None) == 2
 
 
+@pytest.mark.parametrize("x,h,w,r,s,u,v,p,q,flat", [
+    (0x1000, 14, 14, 1, 1, 1, 1, 0, 0, 0),     # 1x1 but H*W % 8 != 0: 2-byte gather
+    (0x1000, 28, 28, 1, 1, 1, 1, 0, 0, 1),     # 1x1, H*W % 8 == 0: 16-byte pixel octets
+    (0x1008, 28, 28, 1, 1, 1, 1, 0, 0, 0),     # misaligned input
+    (0x1000, 28, 28, 1, 1, 2, 2, 0, 0, 0),     # stride 2
+    (0x1000, 28, 28, 3, 3, 1, 1, 1, 1, 0),     # 3x3
+])
+def test_igemm_producer_choice(wino, x, h, w, r, s, u, v, p, q, flat):
+    """Which pixel-operand producer the implicit GEMM uses: 1 = 16-byte
+    pixel octets (1x1 / stride 1 / pad 0), 0 = 2-byte gathers."""
+    L = wino.lib()
+    L.wino_igemm_flat.argtypes = [ctypes.c_void_p] + [ctypes.c_int] * 8
+    assert L.wino_igemm_flat(x, h, w, r, s, u, v, p, q) == flat
+
+
 @pytest.mark.parametrize("field,value", [
     ("s", 1), ("u", 2), ("v", 2), ("p", 0), ("q", 2), ("k", 27), ("c", 24),
 ])

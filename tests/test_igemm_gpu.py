@@ -42,6 +42,13 @@ SHAPES = [  # n, c, h, w, k, r, s, stride, pad
     (2, 24, 16, 16, 40, 1, 1, 1, 0),      # ragged C and K, two pixel halves
     (3, 64, 28, 28, 320, 1, 1, 1, 0),     # two k-blocks, 2352 pixels (a partial unit)
     (1, 512, 8, 12, 128, 1, 1, 1, 0),     # 32 K-steps, one partial unit
+    # more 2-byte-gather cases: strides, paddings and row lengths
+    (2, 64, 16, 16, 128, 3, 3, 2, 1),     # stride-2 3x3, 8-column output rows
+    (2, 32, 8, 24, 48, 1, 1, 2, 0),       # stride-2 1x1, 12-column output rows
+    (1, 24, 10, 16, 40, 3, 3, 1, 1),      # stride 1, ragged C and K
+    (3, 16, 9, 8, 16, 3, 3, 1, 0),        # pad 0, 6-column output rows, odd H
+    (2, 48, 16, 16, 24, 5, 5, 1, 2),      # 5x5 (extension API only)
+    (2, 32, 16, 40, 320, 3, 3, 2, 1),     # two k-blocks, 20-column output rows
 ]
 
 
@@ -94,6 +101,19 @@ def test_igemm_persistent_many_units(wino, cuda):
     torch.cuda.synchronize()
     assert wino.error_read_clear() == 0
     _check(y, x, wt, 1, 0)
+
+
+def test_igemm_stride2_persistent_many_units(wino, cuda):
+    """Stride-2 3x3 on 56x56 at N64 (K <= 128: two pixel halves a unit): 196
+    units of 256 pixels on at most 148 CTAs."""
+    import torch
+    n, c, h, w, k = 64, 64, 56, 56, 64
+    x16, w16 = _inputs(n, c, h, w, k, 3, 3, seed=6)
+    x, wt = torch.from_numpy(x16).to(cuda), torch.from_numpy(w16).to(cuda)
+    y = wino.conv2d_igemm(x, wt, stride=2, pad=1)
+    torch.cuda.synchronize()
+    assert wino.error_read_clear() == 0
+    _check(y, x, wt, 2, 1)
 
 
 def test_igemm_weights_reused_and_matches_direct(wino, cuda):
