@@ -418,8 +418,8 @@ extern "C" int wino_conv2d_fused(const void* x, const void* ucache, void* y, int
 }
 
 // ------------------------------------------------------ two-stage path ----
-// Workspace: the pre-pass records (row-transformed XR when C <= 256, else the
-// channel-blocked XB) then M16, each 256-byte aligned.
+// Workspace: the pre-pass output (the transformed tiles V2 when C <= 256,
+// else the channel-blocked input XB) then M16, each 256-byte aligned.
 extern "C" size_t wino_twostage_workspace_bytes(int n, int c, int h, int w, int k) {
   if (wino_check_shape(n, c, h, w, k) != WINO_OK || !twostage_ok(n, c, h, w)) return 0;
   const size_t xb = (wino_twostage_prepass_bytes(n, c, h, w) + 255) / 256 * 256;
