@@ -22,15 +22,18 @@
 //  - igemm_conv_kernel<PM> (slot 3): persistent; a unit is 128 * PM output
 //    pixels x one k-block (PM = 2 when K <= 128, so the pixel operand of a
 //    K-step feeds two MMAs of 128 pixels each and the accumulator is 256
-//    columns either way).  Warps 8-15 gather the pixel operand straight from
-//    the NCHW input (thread = pixel, 8-channel half; eight 2-byte loads per
-//    K-step, lanes on consecutive pixels, zero outside the image) into the
-//    K-major A layout; warp 5 lane 0 bulk-copies the weight pieces; warp 4
-//    lane 0 issues one M128 x N(rows) x K16 MMA per K-step and pixel half;
-//    warps 0-3 read the accumulator (TMEM lane = pixel) and store y, each
-//    column a contiguous run of pixels of one output channel.  TMEM holds two
-//    256-column accumulators, so a unit's epilogue overlaps the next unit's
-//    MMAs.
+//    columns either way).  Warps 8-15 build the pixel operand straight from
+//    the NCHW input: for 1x1 / stride 1 / pad 0 layers whose H * W is a
+//    multiple of 8 (FLAT), one 16-byte load of eight neighbouring pixels per
+//    channel into an MN-major operand; otherwise eight 2-byte loads per
+//    K-step (thread = pixel, 8-channel half, lanes on consecutive pixels,
+//    zero outside the image) into a K-major one.  Warp 5 lane 0 bulk-copies
+//    the weight pieces; warp 4 lane 0 issues one M128 x N(rows) x K16 MMA per
+//    K-step and pixel half; warps 0-3 read the accumulator (TMEM lane =
+//    pixel) and store y, each column a contiguous run of pixels of one output
+//    channel, neighbouring lanes pairing up for 4-byte stores.  TMEM holds
+//    two 256-column accumulators, so a unit's epilogue overlaps the next
+//    unit's MMAs.
 #include <cuda_runtime.h>
 #include <cuda_fp16.h>
 #include "tc_sm100.cuh"
