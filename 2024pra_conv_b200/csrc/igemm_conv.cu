@@ -64,9 +64,11 @@ constexpr int REGS_LAUNCH = 128, REGS_EPI = 104, REGS_MMA = 56, REGS_PROD = 176;
 static_assert(128 * REGS_EPI + 128 * REGS_MMA + 256 * REGS_PROD == NTHREAD * REGS_LAUNCH,
               "the warpgroups' register limits add up to the launch allocation");
 constexpr uint32_t SLEEP_NS = 32;
-// stages of 16-byte loads each octet producer keeps in registers
+// stages of 16-byte loads each octet producer keeps in registers (five
+// measured 4-7 % faster than three on the 1x1 256->64 and 512->128 ResNet
+// layers; seven slower)
 #ifndef WINO_IG_RING
-#define WINO_IG_RING 3
+#define WINO_IG_RING 5
 #endif
 constexpr int RING_F = WINO_IG_RING;
 static_assert(RING_F >= 2 && RING_F <= 8, "ring of two to eight stages");
