@@ -72,6 +72,13 @@ constexpr uint32_t SLEEP_NS = 32;
 #endif
 constexpr int RING_F = WINO_IG_RING;
 static_assert(RING_F >= 2 && RING_F <= 8, "ring of two to eight stages");
+// stages of 2-byte loads each gathering producer keeps in registers (32 a
+// stage, one value a register; four measured 5-11 % slower than three)
+#ifndef WINO_IG_RING_GATHER
+#define WINO_IG_RING_GATHER 3
+#endif
+constexpr int RING_G = WINO_IG_RING_GATHER;
+static_assert(RING_G >= 2 && RING_G <= 4, "ring of two to four stages");
 
 struct Shared {
   uint64_t full[NSTAGE], empty[NSTAGE];
@@ -415,7 +422,7 @@ __global__ void __launch_bounds__(ig::NTHREAD, 1) igemm_conv_kernel(KernelParam 
       iy0[h] = ix0[h] = 0;
       live[h] = false;
     }
-    uint32_t w0[NPIECE][8], w1[NPIECE][8], w2[NPIECE][8];
+    uint32_t wr[RING_G][NPIECE][8];
     auto issue = [&](uint32_t (&w)[NPIECE][8]) {
       if (lu >= cnt) return;
       if (lj == 0) {
@@ -490,15 +497,19 @@ __global__ void __launch_bounds__(ig::NTHREAD, 1) igemm_conv_kernel(KernelParam 
       return cu < cnt && !*abort_flag;
     };
     if (cnt > 0) {
-      issue(w0);
-      issue(w1);
-      while (true) {
-        issue(w2);
-        if (!consume(w0)) break;
-        issue(w0);
-        if (!consume(w1)) break;
-        issue(w1);
-        if (!consume(w2)) break;
+      // RING_G - 1 stages of loads in flight while one is stored
+#pragma unroll
+      for (int r = 0; r + 1 < RING_G; ++r) issue(wr[r]);
+      bool more = true;
+      while (more) {
+#pragma unroll
+        for (int r = 0; r < RING_G; ++r) {
+          issue(wr[(r + RING_G - 1) % RING_G]);
+          if (!consume(wr[r])) {
+            more = false;
+            break;
+          }
+        }
       }
     }
   }
