@@ -1,6 +1,7 @@
 """General shapes (any filter size, stride, padding, channel count) through
-the direct kernel, directly and behind the drop-in ABI, against FP64
-(rel-L2 <= 2e-3, max-normalised <= 1e-2)."""
+the CUDA-core direct kernel, and behind the drop-in ABI (which runs them on
+the tensor-core implicit GEMM when its weights fit transform_filter, else on
+the direct kernel), against FP64 (rel-L2 <= 2e-3, max-normalised <= 1e-2)."""
 import numpy as np
 import pytest
 
@@ -47,7 +48,8 @@ def test_direct_conv(wino, cuda, oracle_mod, shape):
 
 @pytest.mark.parametrize("shape", SHAPES)
 def test_dropin_general_shapes(wino, cuda, oracle_mod, shape):
-    """getkernelInfo accepts these shapes and its four slots compute them."""
+    """getkernelInfo accepts these shapes and its four slots compute them
+    (route 4 or the direct route, whichever it picks)."""
     import torch
     n, c, h, w, k, r, stride, pad = shape
     x16, w16 = _inputs(oracle_mod, n, c, h, w, k, r, seed=7 + sum(shape))
