@@ -66,6 +66,46 @@ def test_igemm_conv(wino, cuda, shape):
     _check(y, x, wt, stride, pad)
 
 
+def _weights_layout_np(w16):
+    """The implicit GEMM's weight operand as igemm_weight_kernel writes it:
+    k-blocks of 256 output channels, then K-steps (tap-major, 16 channels
+    each), each K-step rows x 32 bytes with output channel row, channel cc at
+    (row >> 3) * 256 + (cc >> 3) * 128 + (row & 7) * 16 + (cc & 7) * 2; zeros
+    past K and C."""
+    K, C, R, S = w16.shape
+    CB = (C + 15) // 16
+    NKS = R * S * CB
+    Kp = (K + 15) // 16 * 16
+    out = np.zeros(Kp * NKS * 16, np.float16)
+    k, ks, cc = np.meshgrid(np.arange(Kp), np.arange(NKS), np.arange(16), indexing="ij")
+    kb, row = k // 256, k % 256
+    rows = np.minimum(256, Kp - kb * 256)
+    tap, cb = ks // CB, ks % CB
+    r, s_ = tap // S, tap % S
+    c = cb * 16 + cc
+    byte = (kb * 256 * NKS * 32 + ks * rows * 32 + (row >> 3) * 256 + (cc >> 3) * 128
+            + (row & 7) * 16 + (cc & 7) * 2)
+    ok = (k < K) & (c < C)
+    wpad = np.zeros((Kp, max(C, CB * 16), R, S), np.float16)
+    wpad[:K, :C] = w16
+    out[byte // 2] = np.where(ok, wpad[np.minimum(k, Kp - 1), np.minimum(c, wpad.shape[1] - 1), r, s_], 0)
+    return out
+
+
+@pytest.mark.parametrize("k,c,r,s", [(40, 24, 3, 3), (320, 64, 1, 1), (48, 3, 7, 7), (16, 16, 1, 3)])
+def test_igemm_weight_layout_bit_exact(wino, cuda, k, c, r, s):
+    """igemm_weight_transform writes exactly the documented operand layout."""
+    import torch
+    rng = np.random.default_rng(k * 7 + c)
+    w16 = rng.standard_normal((k, c, r, s)).astype(np.float16)
+    wp = wino.igemm_weight_transform(torch.from_numpy(w16).to(cuda))
+    torch.cuda.synchronize()
+    got = wp.cpu().numpy().view(np.float16)
+    want = _weights_layout_np(w16)
+    assert got.shape == want.shape
+    assert np.array_equal(got.view(np.uint16), want.view(np.uint16))
+
+
 def _route(wino, x, wt, y, ws, stride, pad):
     r, s = wt.shape[2:]
     pr = wino.make_problem(x, wt, y, ws.transform_pin, ws.transform_filter, ws.mid_result,
