@@ -34,6 +34,9 @@
 //    channel, neighbouring lanes pairing up for 4-byte stores.  TMEM holds
 //    two 256-column accumulators, so a unit's epilogue overlaps the next
 //    unit's MMAs.
+#include <cstring>
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 #include <cuda_fp16.h>
 #include "tc_sm100.cuh"
@@ -87,6 +90,12 @@ struct Shared {
   uint32_t tmem_base;
   int abort_flag;
 };
+
+// Pixel-operand producers: 2-byte gathers into a K-major operand; 16-byte
+// octet loads into an MN-major one (1x1 / stride 1 / pad 0); TMA boxes of
+// 64 pixels x 16 channels into a 128-byte-swizzled MN-major one (the same
+// layers when H * W is a multiple of 64 and a tensor map is available).
+enum : int { MODE_GATHER = 0, MODE_FLAT = 1, MODE_TMA = 2 };
 
 struct Geo {
   int C, H, W, K, S, U, V, P, Q, OW;
@@ -160,9 +169,16 @@ __global__ void __launch_bounds__(256) igemm_weight_kernel(KernelParam p) {
 // (pixel octet, channel), one 16-byte load and one 16-byte shared store per
 // octet, channel and K-step.  Otherwise thread = (pixel, channel half) and
 // eight 2-byte loads build each K-major 16-byte row.
-template <int PM, bool FLAT>
+// MODE_TMA: the weight-loader thread also copies the pixel operand, two TMA
+// boxes (64 pixels x 16 channels, 128-byte swizzle) per piece, through the
+// tensor map at p.transform_pin (CUtensorMap over the input as [N][C][H*W]);
+// the producer warps stay idle.
+template <int PM, int MODE>
 __global__ void __launch_bounds__(ig::NTHREAD, 1) igemm_conv_kernel(KernelParam p) {
   using namespace ig;
+  constexpr bool FLAT = MODE == MODE_FLAT;
+  constexpr bool TMA = MODE == MODE_TMA;
+  constexpr bool MN = MODE != MODE_GATHER;  // MN-major pixel operand
   constexpr int SKS = NPIECE / PM;          // K-steps per stage
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   __shared__ Shared sh;
@@ -181,7 +197,7 @@ __global__ void __launch_bounds__(ig::NTHREAD, 1) igemm_conv_kernel(KernelParam 
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < NSTAGE; ++s) {
-      mbar_init(&sh.full[s], NWARP_P + 1);
+      mbar_init(&sh.full[s], TMA ? 1 : NWARP_P + 1);
       mbar_init(&sh.empty[s], 1);
     }
     for (int a = 0; a < 2; ++a) {
@@ -205,6 +221,8 @@ __global__ void __launch_bounds__(ig::NTHREAD, 1) igemm_conv_kernel(KernelParam 
     if (warp == WARP_LOAD && lane == 0) {
       // weight pieces: stage j of a unit = K-steps j * SKS .., contiguous
       const uint8_t* wp = static_cast<const uint8_t*>(p.transform_filter);
+      const void* tmap = p.transform_pin;
+      if constexpr (TMA) tensormap_acquire(tmap);
       uint32_t it = 0;
       for (int i = 0; i < cnt && !*abort_flag; ++i) {
         int pt, kb;
@@ -221,8 +239,21 @@ __global__ void __launch_bounds__(ig::NTHREAD, 1) igemm_conv_kernel(KernelParam 
           }
           const int nk = min(SKS, g.NKS - j * SKS);
           const uint32_t bytes = (uint32_t)(nk * rows * 32);
-          mbar_arrive_expect_tx(&sh.full[st], bytes);
+          mbar_arrive_expect_tx(&sh.full[st], bytes + (TMA ? (uint32_t)(nk * PM * PIECE) : 0u));
           bulk_g2s(smem + st * STAGE + STAGE_A, src + (size_t)j * SKS * rows * 32, bytes, &sh.full[st]);
+          if constexpr (TMA) {
+            // piece q * PM + h = channels 16 (j SKS + q) .. of pixel half h:
+            // boxes of 64 pixels at 2 KB steps (H * W % 64 == 0, so a box
+            // lies in one image; past the last image the copy reads zeros)
+            for (int q = 0; q < nk; ++q)
+#pragma unroll
+              for (int hb = 0; hb < 2 * PM; ++hb) {
+                const long long P = (long long)pt * (128 * PM) + hb * 64;
+                const int n = (int)(P / g.HW), x = (int)(P - (long long)n * g.HW);
+                tma_load_3d(smem + st * STAGE + q * PM * PIECE + hb * 2048, tmap, x, (j * SKS + q) * 16, n,
+                            &sh.full[st]);
+              }
+          }
         }
         if (!ok) break;
       }
@@ -232,16 +263,19 @@ __global__ void __launch_bounds__(ig::NTHREAD, 1) igemm_conv_kernel(KernelParam 
     }
     if (warp == WARP_MMA && lane == 0) {
       // pixel operand of a piece: K-major (8-channel halves 128 bytes apart,
-      // pixel octets 256) or, FLAT, MN-major (pixel octets 128 bytes apart,
-      // channel halves 2048)
-      auto a_desc = [](uint32_t a) { return FLAT ? smem_desc(a, 2048, 128) : smem_desc(a, 128, 256); };
+      // pixel octets 256), FLAT MN-major (pixel octets 128 bytes apart,
+      // channel halves 2048) or TMA MN-major swizzled (64-pixel atoms 2048
+      // bytes apart, 8-channel groups 1024)
+      auto a_desc = [](uint32_t a) {
+        return TMA ? smem_desc_sw128(a, 2048, 1024) : FLAT ? smem_desc(a, 2048, 128) : smem_desc(a, 128, 256);
+      };
       uint32_t it = 0;
       bool ok = true;
       for (int i = 0; ok && i < cnt && !*abort_flag; ++i) {
         int pt, kb;
         unit_of(g, g0 + i * G, pt, kb);
         const int rows = block_rows(kb, g.Kp);
-        const uint32_t idesc = instr_desc(128, (uint32_t)rows, 0, 0, FLAT ? 1 : 0, 0);
+        const uint32_t idesc = instr_desc(128, (uint32_t)rows, 0, 0, MN ? 1 : 0, 0);
         const int ab = i & 1;
         if (i >= 2 && !mbar_wait(&sh.accempty[ab], ((i >> 1) - 1) & 1, abort_flag, err, ERR_WAIT_DRAIN)) break;
         tc_fence_after();
@@ -402,7 +436,7 @@ __global__ void __launch_bounds__(ig::NTHREAD, 1) igemm_conv_kernel(KernelParam 
         }
       }
     }
-  } else {
+  } else if constexpr (MODE == MODE_GATHER) {
     regs_inc<REGS_PROD>();
     // pixel producers: thread = (pixel tl of each 128-pixel half, channel
     // half hh).  The load cursor (lu, lj) runs up to two stages ahead of
@@ -529,9 +563,16 @@ extern "C" {
 
 // Bytes of the re-laid-out weights: K rounded up to 16 rows, R * S *
 // ceil(C / 16) K-steps of 32 bytes a row.
-size_t wino_igemm_weight_bytes(int c, int k, int r, int s) {
+size_t wino_igemm_operand_bytes(int c, int k, int r, int s) {
   return (size_t)ig::kpad(k) * (size_t)ig::kstep_count(c, r, s) * 32;
 }
+
+// The extension API's weight buffer: the operand, then (at a 128-byte
+// boundary) a 128-byte slot for the input's tensor map.
+size_t wino_igemm_map_offset(int c, int k, int r, int s) {
+  return (wino_igemm_operand_bytes(c, k, r, s) + 127) / 128 * 128;
+}
+size_t wino_igemm_weight_bytes(int c, int k, int r, int s) { return wino_igemm_map_offset(c, k, r, s) + 128; }
 
 unsigned wino_igemm_weight_grid(int c, int k, int r, int s) {
   const long long nword = (long long)ig::kpad(k) * ig::kstep_count(c, r, s) * 2;
@@ -550,9 +591,65 @@ int wino_igemm_flat(const void* x, int h, int w, int r, int s, int u, int v, int
          (reinterpret_cast<uintptr_t>(x) & 15) == 0;
 }
 
-void* wino_igemm_kernel_ptr(int k, int flat) {
-  if (flat) return igemm_pm(k) == 2 ? (void*)igemm_conv_kernel<2, true> : (void*)igemm_conv_kernel<1, true>;
-  return igemm_pm(k) == 2 ? (void*)igemm_conv_kernel<2, false> : (void*)igemm_conv_kernel<1, false>;
+// TMA boxes for the pixel operand (MODE_TMA) where they measured faster
+// than the octet loads: 1x1 64->256 at 56x56, N128, 110 -> 100 us (one pixel
+// half a unit); with two pixel halves (K <= 128: 1x1 256->64) they were
+// slower, 97 -> 117 us, so those keep the octet loads.
+#ifndef WINO_IG_TMA
+#define WINO_IG_TMA 1
+#endif
+
+// The driver's tensor-map encoder (looked up once; null when unavailable).
+static PFN_cuTensorMapEncodeTiled_v12000 map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool looked = false;
+  if (!looked) {
+    looked = true;
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  }
+  return fn;
+}
+
+// Pixel-operand producer for a problem (ig::MODE_*): TMA for FLAT problems
+// with H * W a multiple of 64 and one pixel half a unit (K > 128) when the
+// build enables it and the driver encodes tensor maps.
+int wino_igemm_mode(const void* x, int k, int h, int w, int r, int s, int u, int v, int p, int q) {
+  if (!wino_igemm_flat(x, h, w, r, s, u, v, p, q)) return ig::MODE_GATHER;
+  if (WINO_IG_TMA && igemm_pm(k) == 1 && ((long long)h * w) % 64 == 0 && map_encoder() != nullptr)
+    return ig::MODE_TMA;
+  return ig::MODE_FLAT;
+}
+
+// Tensor map of the input x (N C H*W fp16) with boxes of 64 pixels x 16
+// channels and the 128-byte swizzle, written to the 128 bytes at map_host.
+int wino_igemm_encode_map(void* map_host, const void* x, int n, int c, int hw) {
+  PFN_cuTensorMapEncodeTiled_v12000 fn = map_encoder();
+  if (!fn || !map_host || !x) return 1;
+  CUtensorMap m;
+  const cuuint64_t dims[3] = {(cuuint64_t)hw, (cuuint64_t)c, (cuuint64_t)n};
+  const cuuint64_t strides[2] = {(cuuint64_t)hw * 2, (cuuint64_t)c * hw * 2};
+  const cuuint32_t box[3] = {64, 16, 1};
+  const cuuint32_t es[3] = {1, 1, 1};
+  if (fn(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3, const_cast<void*>(x), dims, strides, box, es,
+         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return 1;
+  static_assert(sizeof(CUtensorMap) == 128, "a tensor map is 128 bytes");
+  std::memcpy(map_host, &m, sizeof(m));
+  return 0;
+}
+
+void* wino_igemm_kernel_ptr(int k, int mode) {
+  const bool two = igemm_pm(k) == 2;
+  switch (mode) {
+    case ig::MODE_TMA: return two ? (void*)igemm_conv_kernel<2, ig::MODE_TMA> : (void*)igemm_conv_kernel<1, ig::MODE_TMA>;
+    case ig::MODE_FLAT: return two ? (void*)igemm_conv_kernel<2, ig::MODE_FLAT> : (void*)igemm_conv_kernel<1, ig::MODE_FLAT>;
+    default: return two ? (void*)igemm_conv_kernel<2, ig::MODE_GATHER> : (void*)igemm_conv_kernel<1, ig::MODE_GATHER>;
+  }
 }
 
 int wino_igemm_threads() { return ig::NTHREAD; }
@@ -585,8 +682,9 @@ int wino_igemm_prepare() {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return 1;
   if (dev >= 0 && dev < 64 && done[dev]) return 0;
-  const void* fns[4] = {(void*)igemm_conv_kernel<1, false>, (void*)igemm_conv_kernel<2, false>,
-                        (void*)igemm_conv_kernel<1, true>, (void*)igemm_conv_kernel<2, true>};
+  const void* fns[6] = {(void*)igemm_conv_kernel<1, ig::MODE_GATHER>, (void*)igemm_conv_kernel<2, ig::MODE_GATHER>,
+                        (void*)igemm_conv_kernel<1, ig::MODE_FLAT>,   (void*)igemm_conv_kernel<2, ig::MODE_FLAT>,
+                        (void*)igemm_conv_kernel<1, ig::MODE_TMA>,    (void*)igemm_conv_kernel<2, ig::MODE_TMA>};
   for (const void* f : fns) {
     if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, ig::SMEM_BYTES) != cudaSuccess)
       return 1;

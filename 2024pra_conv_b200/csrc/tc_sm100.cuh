@@ -182,6 +182,24 @@ __device__ __forceinline__ void bulk_g2s_hint(void* dst_smem, const void* src_gm
       : "memory");
 }
 
+// 3-D tiled TMA load of one box of the tensor map at `tmap` (a CUtensorMap in
+// global memory) at coordinates (x, y, z), completing its bytes on `bar`.
+// x times the element size must be a multiple of 16 bytes; coordinates past
+// the tensor's extent read zeros.
+__device__ __forceinline__ void tma_load_3d(void* dst_smem, const void* tmap, int x, int y, int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_u32(dst_smem)),
+      "l"(tmap), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Makes a tensor map written to global memory before the launch visible to
+// the copy engine's reads of it.
+__device__ __forceinline__ void tensormap_acquire(const void* tmap) {
+  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(tmap) : "memory");
+}
+
 // Bring [src, src + bytes) from device memory into L2 without a destination
 // (16-byte aligned, bytes % 16 == 0); completes on its own.
 __device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes) {
@@ -267,6 +285,15 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint
   d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
   d |= (uint64_t)1 << 46;
   return d;
+}
+
+// Same with the 128-byte swizzle (layout type 2 in bits [61, 64)): the
+// operand is stored in 1024-byte atoms of 8 rows x 128 bytes whose 16-byte
+// chunks are XOR-permuted by the row index, as a TMA copy with
+// CU_TENSOR_MAP_SWIZZLE_128B writes them.  For an MN-major operand lbo is the
+// byte distance between atoms along M/N and sbo between 8-row groups along K.
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return smem_desc(saddr, lbo, sbo) | ((uint64_t)2 << 61);
 }
 
 // Instruction descriptor for kind::f16 / kind::f8f6f4 with fp32 accumulate.

@@ -100,8 +100,11 @@ uint32_t wino_twostage_error_read_clear();
 size_t wino_igemm_weight_bytes(int c, int k, int r, int s);
 unsigned wino_igemm_weight_grid(int c, int k, int r, int s);
 void* wino_igemm_weight_kernel_ptr();
-void* wino_igemm_kernel_ptr(int k, int flat);
-int wino_igemm_flat(const void* x, int h, int w, int r, int s, int u, int v, int p, int q);
+void* wino_igemm_kernel_ptr(int k, int mode);
+int wino_igemm_mode(const void* x, int k, int h, int w, int r, int s, int u, int v, int p, int q);
+int wino_igemm_encode_map(void* map_host, const void* x, int n, int c, int hw);
+size_t wino_igemm_operand_bytes(int c, int k, int r, int s);
+size_t wino_igemm_map_offset(int c, int k, int r, int s);
 int wino_igemm_threads();
 int wino_igemm_smem_bytes();
 unsigned wino_igemm_grid(int n, int k, int oh, int ow, int sms);
@@ -113,6 +116,8 @@ uint32_t wino_igemm_error_read_clear();
 namespace {
 
 constexpr int kMaxDim = 32767;  // dims are `short` in mykernelParamType
+// implicit-GEMM pixel-operand producers (igemm_conv.cu)
+constexpr int kIgemmModeFlat = 1, kIgemmModeTma = 2;
 
 int sm_count() {
   int dev = 0, n = 0;
@@ -231,7 +236,7 @@ static int plan_route(const problem_t& pr) {
     const int oh = (int)((pr.h - pr.r + 2 * pr.p) / pr.u + 1), ow = (int)((pr.w - pr.s + 2 * pr.q) / pr.v + 1);
     const bool igemm = pr.transform_filter != nullptr &&
                        (reinterpret_cast<uintptr_t>(pr.transform_filter) & 15) == 0 &&
-                       wino_igemm_weight_bytes((int)pr.c, (int)pr.k, (int)pr.r, (int)pr.s) <=
+                       wino_igemm_operand_bytes((int)pr.c, (int)pr.k, (int)pr.r, (int)pr.s) <=
                            (size_t)16 * pr.k * pr.c * 2 &&
                        wino_igemm_shape_ok((int)pr.n, (int)pr.c, (int)pr.h, (int)pr.w, (int)pr.k, oh, ow);
     return igemm ? WINO_ROUTE_IGEMM : WINO_ROUTE_DIRECT;
@@ -286,14 +291,26 @@ int getkernelInfo(problem_t* problem, kernelInfo_t* kernelInfo, void* param) {
   std::memset(kernelInfo, 0, sizeof(*kernelInfo));
 
   if (route == WINO_ROUTE_IGEMM) {
+    int mode = wino_igemm_mode(pr.in, (int)pr.k, (int)pr.h, (int)pr.w, (int)pr.r, (int)pr.s, (int)pr.u,
+                               (int)pr.v, (int)pr.p, (int)pr.q);
     a->transform_pin = nullptr;
+    if (mode == kIgemmModeTma) {
+      // the input's tensor map goes to the (otherwise unused) transform_pin
+      // workspace, 4*h*h*n*c fp16 >= 128 bytes, written once here
+      alignas(64) unsigned char map[128];
+      const bool ok = pr.transform_pin != nullptr && (reinterpret_cast<uintptr_t>(pr.transform_pin) & 127) == 0 &&
+                      (size_t)4 * pr.h * pr.h * pr.n * pr.c * 2 >= sizeof(map) &&
+                      wino_igemm_encode_map(map, pr.in, (int)pr.n, (int)pr.c, (int)(pr.h * pr.w)) == 0 &&
+                      cudaMemcpy(pr.transform_pin, map, sizeof(map), cudaMemcpyHostToDevice) == cudaSuccess;
+      if (ok) a->transform_pin = pr.transform_pin;
+      else mode = kIgemmModeFlat;
+    }
     set_slot(kernelInfo, 1, wino_igemm_weight_grid((int)pr.c, (int)pr.k, (int)pr.r, (int)pr.s), 1, 1, 256, 1,
              1, 0, wino_igemm_weight_kernel_ptr());
     set_slot(kernelInfo, 2, 1, 1, 1, 32, 1, 1, 0, wino_noop_kernel_ptr());
     set_slot(kernelInfo, 3, wino_igemm_grid((int)pr.n, (int)pr.k, oh, ow, sm_count()), 1, 1,
              (unsigned)wino_igemm_threads(), 1, 1, (unsigned)wino_igemm_smem_bytes(),
-             wino_igemm_kernel_ptr((int)pr.k, wino_igemm_flat(pr.in, (int)pr.h, (int)pr.w, (int)pr.r, (int)pr.s,
-                                                              (int)pr.u, (int)pr.v, (int)pr.p, (int)pr.q)));
+             wino_igemm_kernel_ptr((int)pr.k, mode));
     set_slot(kernelInfo, 4, 1, 1, 1, 32, 1, 1, 0, wino_noop_kernel_ptr());
     return WINO_OK;
   }
@@ -654,8 +671,20 @@ extern "C" int wino_conv2d_igemm(const void* x, const void* wprep, void* y, int 
   wino::KernelParam pk = make_param(x, nullptr, y, nullptr, const_cast<void*>(wprep), nullptr, n, c, h, w, k);
   pk.r = (short)r; pk.s = (short)s; pk.u = (short)u; pk.v = (short)v; pk.p = (short)p; pk.q = (short)q;
   pk.Oh = (short)oh; pk.Ow = (short)ow;
+  int mode = wino_igemm_mode(x, k, h, w, r, s, u, v, p, q);
+  if (mode == kIgemmModeTma) {
+    // this call's tensor map goes to wprep's map slot, in stream order
+    // (a pageable-source copy returns once the 128 bytes are staged)
+    alignas(64) unsigned char map[128];
+    void* slot = static_cast<uint8_t*>(const_cast<void*>(wprep)) + wino_igemm_map_offset(c, k, r, s);
+    if ((reinterpret_cast<uintptr_t>(slot) & 63) == 0 && wino_igemm_encode_map(map, x, n, c, h * w) == 0 &&
+        cudaMemcpyAsync(slot, map, sizeof(map), cudaMemcpyHostToDevice, (cudaStream_t)stream) == cudaSuccess)
+      pk.transform_pin = slot;
+    else
+      mode = kIgemmModeFlat;
+  }
   void* args[] = {&pk};
-  return cudaLaunchKernel(wino_igemm_kernel_ptr(k, wino_igemm_flat(x, h, w, r, s, u, v, p, q)),
+  return cudaLaunchKernel(wino_igemm_kernel_ptr(k, mode),
                           dim3(wino_igemm_grid(n, k, oh, ow, sm_count())),
                           dim3(wino_igemm_threads()), args, (size_t)wino_igemm_smem_bytes(),
                           (cudaStream_t)stream) == cudaSuccess

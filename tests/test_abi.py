@@ -100,10 +100,15 @@ def test_getkernelinfo_sends_other_shapes_to_the_direct_kernel(wino, field, valu
 
 def test_igemm_weight_bytes_and_entry_points(wino):
     L = wino.lib()
-    # round16(k) rows x r*s*ceil(c/16) K-steps x 32 bytes
-    assert L.wino_igemm_weight_bytes(64, 128, 3, 3) == 128 * 9 * 4 * 32
-    assert L.wino_igemm_weight_bytes(24, 40, 3, 3) == 48 * 9 * 2 * 32
-    assert L.wino_igemm_weight_bytes(3, 64, 7, 7) == 64 * 49 * 32
+    # round16(k) rows x r*s*ceil(c/16) K-steps x 32 bytes, then a 128-byte
+    # tensor-map slot at a 128-byte boundary
+    L.wino_igemm_operand_bytes.restype = ctypes.c_size_t
+    L.wino_igemm_map_offset.restype = ctypes.c_size_t
+    for (c, k, r, s, ops) in [(64, 128, 3, 3, 128 * 9 * 4 * 32), (24, 40, 3, 3, 48 * 9 * 2 * 32),
+                              (3, 64, 7, 7, 64 * 49 * 32), (3, 16, 1, 1, 16 * 1 * 32)]:
+        assert L.wino_igemm_operand_bytes(c, k, r, s) == ops
+        assert L.wino_igemm_map_offset(c, k, r, s) == (ops + 127) // 128 * 128
+        assert L.wino_igemm_weight_bytes(c, k, r, s) == (ops + 127) // 128 * 128 + 128
     d = ctypes.c_void_p(0x10000)
     odd = ctypes.c_void_p(0x10008)
     assert L.wino_igemm_weight_transform(None, d, 16, 16, 3, 3, None) == 1
@@ -125,10 +130,13 @@ def test_igemm_weight_bytes_and_entry_points(wino):
 ])
 def test_igemm_producer_choice(wino, x, h, w, r, s, u, v, p, q, flat):
     """Which pixel-operand producer the implicit GEMM uses: 1 = 16-byte
-    pixel octets (1x1 / stride 1 / pad 0), 0 = 2-byte gathers."""
+    pixel octets or TMA boxes (1x1 / stride 1 / pad 0), 0 = 2-byte gathers;
+    with K <= 128 (two pixel halves a unit) never TMA."""
     L = wino.lib()
     L.wino_igemm_flat.argtypes = [ctypes.c_void_p] + [ctypes.c_int] * 8
     assert L.wino_igemm_flat(x, h, w, r, s, u, v, p, q) == flat
+    L.wino_igemm_mode.argtypes = [ctypes.c_void_p] + [ctypes.c_int] * 9
+    assert L.wino_igemm_mode(x, 64, h, w, r, s, u, v, p, q) == flat     # K = 64: octet loads
 
 
 @pytest.mark.parametrize("field,value", [
