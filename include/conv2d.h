@@ -55,7 +55,11 @@
  *       (non-null, 16-byte aligned): slot 1 weight -> transform_filter in the
  *       tensor-core operand layout; slot 3 tcgen05 implicit GEMM reading `in`
  *       directly -> out (fp32 accumulation); slots 2, 4 empty kernels;
- *       transform_pin and mid_result are left untouched.
+ *       mid_result is left untouched, and so is transform_pin except for
+ *       1x1 / stride 1 / pad 0 layers with h*w % 64 == 0 and k > 128, whose
+ *       first 128 bytes receive the input's TMA tensor map (written by
+ *       getkernelInfo itself; transform_pin 128-byte aligned, else those
+ *       layers read the input without TMA).
  *     direct route: the remaining shapes (e.g. c = 3 with a 7x7 filter) or a
  *       null transform_filter: slot 3 is a direct convolution on CUDA cores
  *       (fp32 accumulation), slots 1, 2, 4 empty kernels; no workspace is

@@ -135,11 +135,15 @@ int wino_conv2d_direct(const void* x, const void* weight, void* y, int n, int c,
  * zeros): D[pixel][k] over K-steps of (tap, 16 channels), fp16 operands,
  * fp32 accumulation, one fp16 rounding of y.  wino_igemm_weight_transform
  * re-lays the KCRS weights into wprep (wino_igemm_weight_bytes bytes,
- * 16-byte aligned), which stays valid for as long as the weights do;
- * wino_conv2d_igemm then gathers the pixel operand straight from the NCHW
- * input.  getkernelInfo takes this route for shapes outside the Winograd
- * contract when wprep fits the caller's transform_filter (16*k*c fp16,
- * reference src/main.cpp:38), i.e. r*s*ceil(c/16)*round16(k) <= k*c. */
+ * 128-byte aligned: the operand, then a 128-byte slot for the input's TMA
+ * tensor map), whose operand stays valid for as long as the weights do;
+ * wino_conv2d_igemm reads the pixel operand straight from the NCHW input
+ * (1x1 / stride 1 / pad 0 layers with h*w % 64 == 0 and k > 128 through a
+ * tensor map it writes to wprep's slot in stream order, so one wprep serves
+ * one stream at a time).  getkernelInfo takes this route for shapes outside
+ * the Winograd contract when the operand fits the caller's transform_filter
+ * (16*k*c fp16, reference src/main.cpp:38), i.e. r*s*ceil(c/16)*round16(k)
+ * <= k*c. */
 size_t wino_igemm_weight_bytes(int c, int k, int r, int s);
 int wino_igemm_weight_transform(const void* weight, void* wprep, int k, int c, int r, int s,
                                 void* stream);
