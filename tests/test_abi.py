@@ -121,6 +121,23 @@ def test_igemm_weight_bytes_and_entry_points(wino):
     assert L.wino_conv2d_igemm(d, d, d, 1, 2048, 1024, 1024, 16, 1, 1, 1, 1, 0, 0, None) == 2
 
 
+def test_igemm_units_and_grid(wino):
+    """Units of the persistent implicit GEMM: 128 output pixels (256 when
+    K <= 128) x one 256-row block of output channels; the grid is capped at
+    the SM count."""
+    L = wino.lib()
+    L.wino_igemm_units.restype = ctypes.c_longlong
+    L.wino_igemm_grid.restype = ctypes.c_uint
+    assert L.wino_igemm_units(128, 256, 56, 56) == 128 * 3136 // 128            # K = 256: one block
+    assert L.wino_igemm_units(128, 64, 28, 28) == (128 * 784 + 255) // 256      # two pixel halves
+    assert L.wino_igemm_units(3, 320, 28, 28) == (3 * 784 + 127) // 128 * 2     # two k-blocks
+    assert L.wino_igemm_units(1, 27, 7, 7) == 1                                 # K padded to 32
+    assert L.wino_igemm_grid(128, 256, 56, 56, 148) == 148
+    assert L.wino_igemm_grid(1, 27, 7, 7, 148) == 1
+    assert L.wino_igemm_shape_ok(1, 64, 56, 56, 64, 56, 56) == 1
+    assert L.wino_igemm_shape_ok(1, 2048, 1024, 1024, 16, 1024, 1024) == 0      # 2^31 input elements
+
+
 @pytest.mark.parametrize("x,h,w,r,s,u,v,p,q,flat", [
     (0x1000, 14, 14, 1, 1, 1, 1, 0, 0, 0),     # 1x1 but H*W % 8 != 0: 2-byte gather
     (0x1000, 28, 28, 1, 1, 1, 1, 0, 0, 1),     # 1x1, H*W % 8 == 0: 16-byte pixel octets
