@@ -135,8 +135,9 @@ int wino_conv2d_direct(const void* x, const void* weight, void* y, int n, int c,
  * zeros): D[pixel][k] over K-steps of (tap, 16 channels), fp16 operands,
  * fp32 accumulation, one fp16 rounding of y.  wino_igemm_weight_transform
  * re-lays the KCRS weights into wprep (wino_igemm_weight_bytes bytes,
- * 128-byte aligned: the operand, then a 128-byte slot for the input's TMA
- * tensor map), whose operand stays valid for as long as the weights do;
+ * 16-byte aligned: the operand, then a 128-byte slot for the input's TMA
+ * tensor map, used when wprep is 64-byte aligned), whose operand stays
+ * valid for as long as the weights do;
  * wino_conv2d_igemm reads the pixel operand straight from the NCHW input
  * (1x1 / stride 1 / pad 0 layers with h*w % 64 == 0 and k > 128 through a
  * tensor map it writes to wprep's slot in stream order, so one wprep serves
