@@ -58,8 +58,10 @@
  *       mid_result is left untouched, and so is transform_pin except for
  *       1x1 / stride 1 / pad 0 layers with h*w % 64 == 0 and k > 128, whose
  *       first 128 bytes receive the input's TMA tensor map (written by
- *       getkernelInfo itself; transform_pin 128-byte aligned, else those
- *       layers read the input without TMA).
+ *       getkernelInfo itself with a synchronous copy, so no kernel still
+ *       using transform_pin may be in flight on another stream then;
+ *       transform_pin 128-byte aligned, else those layers read the input
+ *       without TMA).
  *     direct route: the remaining shapes (e.g. c = 3 with a 7x7 filter) or a
  *       null transform_filter: slot 3 is a direct convolution on CUDA cores
  *       (fp32 accumulation), slots 1, 2, 4 empty kernels; no workspace is
