@@ -54,6 +54,24 @@ def test_reference_check_rule_detects_planted_error(oracle_mod):
     assert oracle_mod.reference_check(bad, y) == 1
 
 
+@pytest.mark.parametrize("n,c,h,w,k,r,s,u,v,p,q", [
+    (2, 16, 9, 9, 16, 3, 3, 2, 2, 1, 1),      # stride-2 3x3
+    (2, 24, 8, 10, 16, 1, 1, 2, 2, 0, 0),     # stride-2 1x1 projection
+    (1, 3, 16, 16, 8, 7, 7, 2, 2, 3, 3),      # 7x7 stem
+    (1, 16, 7, 9, 8, 5, 5, 1, 1, 2, 2),       # 5x5
+    (2, 16, 6, 8, 8, 1, 3, 1, 1, 0, 1),       # 1x3, different row / column padding
+])
+def test_oracle_matches_reference_general_shapes_bit_exact(oracle_mod, n, c, h, w, k, r, s, u, v, p, q):
+    """The implicit GEMM's and the direct kernel's checker: the oracle equals
+    the reference's own conv2dcpu (built unmodified) bit for bit on filter
+    sizes, strides and paddings outside the Winograd contract as well."""
+    x, wt = oracle_mod.make_inputs(n, c, h, w, k, seed=n + c + h + k, x_dist="normal", r=r, s=s)
+    y64 = oracle_mod.conv2d_f64(x, wt, u=u, v=v, p=p, q=q)
+    y_ref = oracle_mod.ref_conv2dcpu(x, wt, u=u, v=v, p=p, q=q, threads=1)
+    assert y64.shape == y_ref.shape
+    assert np.array_equal(y64.astype(np.float16), y_ref)
+
+
 def test_reference_cpu_multithreaded_matches_single(oracle_mod):
     x, w = oracle_mod.make_inputs(4, 16, 6, 6, 16, seed=9)
     a = oracle_mod.ref_conv2dcpu(x, w, threads=1)
