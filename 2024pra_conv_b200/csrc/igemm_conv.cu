@@ -376,7 +376,7 @@ __global__ void __launch_bounds__(ig::NTHREAD, 1) igemm_conv_kernel(KernelParam 
       off[h] = 0;
       live[h] = false;
     }
-    uint4 w[RING_F][NPIECE];
+    uint4 ring[RING_F][NPIECE];
     auto issue = [&](uint4 (&w)[NPIECE]) {
       if (lu >= cnt) return;
       if (lj == 0) {
@@ -423,13 +423,13 @@ __global__ void __launch_bounds__(ig::NTHREAD, 1) igemm_conv_kernel(KernelParam 
     if (cnt > 0) {
       // RING_F - 1 stages of loads in flight while one is stored
 #pragma unroll
-      for (int r = 0; r + 1 < RING_F; ++r) issue(w[r]);
+      for (int r = 0; r + 1 < RING_F; ++r) issue(ring[r]);
       bool more = true;
       while (more) {
 #pragma unroll
         for (int r = 0; r < RING_F; ++r) {
-          issue(w[(r + RING_F - 1) % RING_F]);
-          if (!consume(w[r])) {
+          issue(ring[(r + RING_F - 1) % RING_F]);
+          if (!consume(ring[r])) {
             more = false;
             break;
           }
